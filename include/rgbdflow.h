@@ -1,0 +1,267 @@
+/*
+ * rgbdflow.h — C ABI of the B200-native coarse-to-fine RGB-D scene-flow solver.
+ *
+ * Every entry point has C linkage, takes plain pointers and sizes, returns an
+ * int status (RGBDFLOW_OK == 0, negative on error) and never lets a C++
+ * exception cross the boundary.  The message of the last failure on a context
+ * is available from rgbdflow_last_error().
+ *
+ * Reference interfaces replaced (paths inside eherbst/rgbd-flow):
+ *   rgbdflow_camera_params           rgbd::CameraParams              include/rgbd_util/CameraParams.h:17-28
+ *   rgbdflow_params                  OpticalFlow::sceneFlowParams    include/celiu_flow/OpticalFlow.h:105-129
+ *                                    + setUpSceneFlowParams()        src/runFlowTwoFrames.cpp:66-100
+ *                                    + solver constants              src/sceneFlowSingleScaleJacobiCUDA.cu:375,461,691,749,768,905,920
+ *   rgbdflow_scene_flow_two_frames   runFlowTwoFramesSceneFlowExperiments()  include/rgbd_flow/runFlowTwoFrames.h:49-51
+ *                                    (-> ceLiuSceneFlow -> OpticalFlow::sceneFlowMultiscale, or
+ *                                        OpticalFlow::sceneFlowWithInit when est_flow != NULL;
+ *                                        src/ceLiuOpticalFlow.cpp:190-215)
+ *   rgbdflow_scene_flow_multiscale   OpticalFlow::sceneFlowMultiscale()      include/celiu_flow/OpticalFlow.h:133
+ *   rgbdflow_scene_flow_with_init    OpticalFlow::sceneFlowWithInit()        include/celiu_flow/OpticalFlow.h:145
+ *   rgbdflow_scene_flow_single_scale sceneFlowSingleScale()                  include/celiu_flow/OpticalFlow.h:17-22
+ *   rgbdflow_batch_*, rgbdflow_server_*: no counterpart in the reference (batched and
+ *                                    served forms of the same solve).
+ */
+#ifndef RGBDFLOW_H
+#define RGBDFLOW_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RGBDFLOW_ABI_VERSION 1
+
+/* status codes */
+#define RGBDFLOW_OK                0
+#define RGBDFLOW_ERR_INVALID_ARG  (-1)
+#define RGBDFLOW_ERR_UNSUPPORTED  (-2)
+#define RGBDFLOW_ERR_CUDA         (-3)
+#define RGBDFLOW_ERR_BUDGET       (-4) /* request does not fit the context's HBM budget */
+#define RGBDFLOW_ERR_TIMEOUT      (-5) /* a bounded device or host wait expired */
+#define RGBDFLOW_ERR_NO_DEVICE    (-6)
+#define RGBDFLOW_ERR_BUSY         (-7) /* no free slot; retry later */
+#define RGBDFLOW_ERR_INTERNAL     (-8)
+
+/* regularisation types (OpticalFlow::sceneFlowRegularizationType, OpticalFlow.h:99-104) */
+#define RGBDFLOW_REG_ISOTROPIC 0
+#define RGBDFLOW_REG_LETOUZEY  1
+#define RGBDFLOW_REG_HPB       2 /* heuristic probability of boundary: not built, returns RGBDFLOW_ERR_UNSUPPORTED */
+
+/* storage type of the image / depth / gradient pyramids on the device.
+ * The flow, the linear system and every Jacobi accumulation stay FP32. */
+#define RGBDFLOW_STORE_FP32 0
+#define RGBDFLOW_STORE_FP16 1
+#define RGBDFLOW_STORE_BF16 2
+
+/* arithmetic of the device solve */
+#define RGBDFLOW_COMPUTE_FP32 0
+#define RGBDFLOW_COMPUTE_FP64 1 /* FP64 device oracle of the same schedule (EPE reference only) */
+
+/* Mirrors rgbd::CameraParams (include/rgbd_util/CameraParams.h:17-28), field for field. */
+typedef struct rgbdflow_camera_params {
+    unsigned int xRes;      /* pixels */
+    unsigned int yRes;      /* pixels */
+    float centerX;          /* pixels */
+    float centerY;          /* pixels */
+    float focalLength;      /* pixels */
+    float stereoBaseline;   /* metres */
+    float fovX, fovY;       /* radians */
+} rgbdflow_camera_params;
+
+/* OpticalFlow::sceneFlowParams (OpticalFlow.h:105-129) plus every constant the
+ * reference hard-codes in its solver.  Fill with rgbdflow_params_default(). */
+typedef struct rgbdflow_params {
+    int    regularization;             /* RGBDFLOW_REG_* */
+    double color_data_weight;          /* colorDataWeight (1) */
+    double depth_vs_color_data_weight; /* depthVsColorDataWeight (CLI -v, 1) */
+    double alpha;                      /* smoothness weight (CLI -s, 0.02) */
+    double gamma;                      /* zero-flow prior (1e-5) */
+    double pyramid_ratio;              /* (0.75; values outside [0.4, 0.98] become 0.75 as in GaussianPyramid.cpp:23-24) */
+    int    min_width;                  /* (60) */
+    int    n_outer;                    /* nOuterFPIterations (50) */
+    int    n_inner;                    /* nInnerFPIterations (1) */
+    int    n_sor;                      /* nSORIterations (maxIters, 10000 from main.cpp:100) */
+    int    depth_boundary_dist;        /* depth-sigma increase radius near depth boundaries (4) */
+    int    fill_holes;                 /* 1: recursive-median fill of zero depths before the pyramid (reference behaviour) */
+    int    fixed_schedule;             /* 1: run every outer and SOR iteration (no convergence breaks) */
+    int    storage;                    /* RGBDFLOW_STORE_* */
+    int    compute;                    /* RGBDFLOW_COMPUTE_* */
+    /* solver constants (sceneFlowSingleScaleJacobiCUDA.cu) */
+    double omega;                      /* SOR relaxation (0.7, :461) */
+    double max_flow_step;              /* per-sweep step clamp (0.3, :375) */
+    double eps_d, eps_z, eps_s;        /* Charbonnier epsilons (1e-6, 1e-10, 1e-6, :749) */
+    double sor_tol;                    /* SOR convergence threshold on max |dx| (1e-5, :920) */
+    int    sor_check_period;           /* SOR convergence check period (25, :905) */
+    double outer_tol;                  /* outer early-termination threshold (4e-4, :691) */
+    double occ_margin;                 /* occlusion test margin factor (0.02, :646) */
+    double occ_penalty;                /* colour-term weight of occluded pixels (0.01, :646) */
+    double max_depth_grad;             /* clamp of depth derivatives (0.04, :768) */
+    /* kernel tuning; 0 selects the autotuned value */
+    int    sweeps_per_launch;
+} rgbdflow_params;
+
+#define RGBDFLOW_MAX_LEVELS 16
+#define RGBDFLOW_MAX_OUTER  64
+
+/* What the solve actually executed (early exits are data dependent). */
+typedef struct rgbdflow_stats {
+    int   n_levels;
+    int   level_w[RGBDFLOW_MAX_LEVELS], level_h[RGBDFLOW_MAX_LEVELS];   /* index 0 = finest */
+    int   outer_iters[RGBDFLOW_MAX_LEVELS];                           /* outer iterations executed */
+    int   sor_iters[RGBDFLOW_MAX_LEVELS][RGBDFLOW_MAX_OUTER];         /* SOR iterations executed per outer */
+    float outer_stat[RGBDFLOW_MAX_LEVELS][RGBDFLOW_MAX_OUTER];        /* early-termination statistic (-1 if not evaluated) */
+    float sor_maxdiff[RGBDFLOW_MAX_LEVELS][RGBDFLOW_MAX_OUTER];       /* last SOR convergence statistic (-1 if not evaluated) */
+    double device_ms;                                                 /* device time of the solve, CUDA events */
+} rgbdflow_stats;
+
+/* Reference defaults: sceneFlowParams() + setUpSceneFlowParams(maxIters = 10000) with the
+ * demo's CLI defaults (alpha 0.02, depthVsColorDataWeight 1, HPB regularisation). */
+void rgbdflow_params_default(rgbdflow_params* p);
+
+/* Version of this ABI (RGBDFLOW_ABI_VERSION). */
+int rgbdflow_abi_version(void);
+
+/* ---------------------------------------------------------------------------------------------
+ * Context: owns a CUDA stream, device workspaces (sized lazily, bounded by hbm_budget_bytes),
+ * cached CUDA graphs and the last-error string.  One context per host thread; contexts are
+ * independent.  hbm_budget_bytes == 0 means "no limit beyond the device's free memory".
+ * ------------------------------------------------------------------------------------------- */
+typedef struct rgbdflow_ctx rgbdflow_ctx;
+
+int rgbdflow_ctx_create(int device, size_t hbm_budget_bytes, rgbdflow_ctx** out);
+int rgbdflow_ctx_destroy(rgbdflow_ctx* ctx);
+const char* rgbdflow_last_error(const rgbdflow_ctx* ctx);
+/* bytes of device memory the context currently holds */
+size_t rgbdflow_ctx_device_bytes(const rgbdflow_ctx* ctx);
+
+/* ---------------------------------------------------------------------------------------------
+ * Drop-in for runFlowTwoFramesSceneFlowExperiments (runFlowTwoFrames.cpp:109-121).
+ *   bgr1/bgr2: W*H*3 uint8, BGR order (cv::Mat CV_8UC3), row-major
+ *   depth1_m/depth2_m: W*H float metres, 0 = invalid
+ *   cam: full-size camera; resized to W as in getResizedCamParams (runFlowTwoFrames.cpp:14-24)
+ *   est_flow: NULL (coarse-to-fine, sceneFlowMultiscale) or W*H*3 float (u px, v px, w m)
+ *             initial estimate (single full-resolution level, sceneFlowWithInit)
+ *   flow_out: W*H*3 float (u px, v px, w m), the cv::Mat_<cv::Vec3f> layout
+ * Host buffers; the call is synchronous.  stats may be NULL.
+ * ------------------------------------------------------------------------------------------- */
+int rgbdflow_scene_flow_two_frames(rgbdflow_ctx* ctx, const rgbdflow_camera_params* cam,
+                                   const uint8_t* bgr1, const float* depth1_m,
+                                   const uint8_t* bgr2, const float* depth2_m,
+                                   int W, int H, const rgbdflow_params* params,
+                                   const float* est_flow, float* flow_out, rgbdflow_stats* stats);
+
+/* ---------------------------------------------------------------------------------------------
+ * OpticalFlow::sceneFlowMultiscale / sceneFlowWithInit over Ce Liu DImage buffers:
+ *   Im1/Im2: W*H*3 double in [0,1], channel order as given (the reference keeps BGR)
+ *   dm1/dm2: W*H double metres (0 = invalid; filled here when params->fill_holes)
+ *   depth_sigma1: W*H float depth standard deviations (params.depthSigma1), must be > 0
+ *   u, v, w: W*H double outputs (and inputs for _with_init: the estimate's planes)
+ * ------------------------------------------------------------------------------------------- */
+int rgbdflow_scene_flow_multiscale(rgbdflow_ctx* ctx, const rgbdflow_camera_params* cam,
+                                   const double* Im1, const double* dm1,
+                                   const double* Im2, const double* dm2,
+                                   const float* depth_sigma1, int W, int H,
+                                   const rgbdflow_params* params,
+                                   double* u, double* v, double* w, rgbdflow_stats* stats);
+
+int rgbdflow_scene_flow_with_init(rgbdflow_ctx* ctx, const rgbdflow_camera_params* cam,
+                                  const double* Im1, const double* dm1,
+                                  const double* Im2, const double* dm2,
+                                  const float* depth_sigma1, int W, int H,
+                                  const rgbdflow_params* params,
+                                  double* u, double* v, double* w, rgbdflow_stats* stats);
+
+/* ---------------------------------------------------------------------------------------------
+ * The per-level seam sceneFlowSingleScale (OpticalFlow.h:17-22), DImage planes as raw doubles:
+ *   Im1, Im2, warpIm2: W*H*nCh interleaved; dm1, dm2, warpDm2: W*H
+ *   u, v, w: W*H in/out; warpIm2/warpDm2 in/out (re-warped with the final flow)
+ *   depthDataTermWeights, depthSmoothnessTermWeights, depthMagTermWeights: W*H
+ *   regularizationWeights: W*H*2 (right, down)
+ * params supplies the solver constants (NULL = defaults); its iteration counts are ignored in
+ * favour of the explicit arguments, as in the reference signature.
+ * ------------------------------------------------------------------------------------------- */
+int rgbdflow_scene_flow_single_scale(rgbdflow_ctx* ctx, const rgbdflow_camera_params* cam,
+                                     const double* Im1, const double* dm1,
+                                     const double* Im2, const double* dm2,
+                                     double* warpIm2, double* warpDm2,
+                                     double* u, double* v, double* w,
+                                     int W, int H, int nCh,
+                                     double colorDataTermWeight, const double* depthDataTermWeights,
+                                     double alpha, const double* depthSmoothnessTermWeights,
+                                     double gamma, const double* depthMagTermWeights,
+                                     const double* regularizationWeights,
+                                     int nOuterFPIterations, int nInnerFPIterations, int nSORIterations,
+                                     int allowEarlyTermination,
+                                     const rgbdflow_params* params, rgbdflow_stats* stats);
+
+/* ---------------------------------------------------------------------------------------------
+ * Batched form (no reference counterpart): n independent pairs of possibly different sizes
+ * solved together, one persistent launch per pyramid level over all pairs' tiles, the level
+ * sequence replayed from a cached CUDA graph.  Each pair's result equals its solo result.
+ * ------------------------------------------------------------------------------------------- */
+typedef struct rgbdflow_pair {
+    int W, H;
+    rgbdflow_camera_params cam;  /* full-size camera, resized to W like the two-frames call */
+    const uint8_t* bgr1;         /* W*H*3 */
+    const float*   depth1_m;     /* W*H */
+    const uint8_t* bgr2;
+    const float*   depth2_m;
+    const float*   est_flow;     /* NULL or W*H*3: warm start (single full-resolution level) */
+    float*         flow_out;     /* W*H*3 */
+} rgbdflow_pair;
+
+/* Host buffers, synchronous.  stats: NULL or an array of n. */
+int rgbdflow_scene_flow_batch(rgbdflow_ctx* ctx, const rgbdflow_pair* pairs, int n,
+                              const rgbdflow_params* params, rgbdflow_stats* stats);
+
+/* Same, but every pointer in pairs[] is DEVICE memory and the work is enqueued on `stream`
+ * (a cudaStream_t passed as void*; NULL = the context's own stream).  Returns after enqueue. */
+int rgbdflow_scene_flow_batch_async(rgbdflow_ctx* ctx, const rgbdflow_pair* pairs, int n,
+                                    const rgbdflow_params* params, void* stream);
+
+/* ---------------------------------------------------------------------------------------------
+ * Served form (no reference counterpart): continuous batching over camera streams.  A frame
+ * submitted on a stream forms a pair with that stream's previous frame; the stream's previous
+ * frame pyramid and previous flow stay resident on the device for warm starts.  Requests are
+ * admitted while the HBM budget and the slot count allow; newly admitted pairs join the next
+ * device step while earlier ones are still in flight.
+ * ------------------------------------------------------------------------------------------- */
+typedef struct rgbdflow_server rgbdflow_server;
+
+typedef struct rgbdflow_server_config {
+    int    max_streams;        /* distinct camera streams */
+    int    max_batch;          /* pairs solved per device step */
+    size_t hbm_budget_bytes;   /* admission budget for resident state + in-flight pairs */
+    int    warm_start;         /* 1: initialise each pair from the stream's previous flow */
+    rgbdflow_params params;
+} rgbdflow_server_config;
+
+typedef struct rgbdflow_result {
+    int      stream_id;
+    uint64_t request_id;
+    int      W, H;
+    float*   flow;             /* caller buffer given at submit, W*H*3, filled */
+    double   submit_time_s;    /* host clock (CLOCK_MONOTONIC) */
+    double   done_time_s;
+    int      status;           /* RGBDFLOW_OK or an error code */
+} rgbdflow_result;
+
+int rgbdflow_server_create(rgbdflow_ctx* ctx, const rgbdflow_server_config* cfg, rgbdflow_server** out);
+int rgbdflow_server_destroy(rgbdflow_server* srv);
+/* Queue one frame of a stream.  The first frame of a stream only primes it (no result).
+ * flow_out (W*H*3 float) receives the flow from the stream's previous frame to this one. */
+int rgbdflow_server_submit(rgbdflow_server* srv, int stream_id, uint64_t request_id,
+                           const rgbdflow_camera_params* cam, const uint8_t* bgr, const float* depth_m,
+                           int W, int H, float* flow_out);
+/* Advance the device: admit queued requests, launch a step, retire finished pairs.
+ * Non-blocking unless `wait` is set.  Completed results are appended to out (up to max). */
+int rgbdflow_server_step(rgbdflow_server* srv, int wait, rgbdflow_result* out, int max, int* n_out);
+/* Requests queued or in flight. */
+int rgbdflow_server_pending(const rgbdflow_server* srv);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RGBDFLOW_H */

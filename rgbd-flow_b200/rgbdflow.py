@@ -1,0 +1,284 @@
+"""Python binding of librgbdflow.so (the C ABI declared in include/rgbdflow.h), via ctypes.
+
+The library is the product: C++ host code plus hand-written sm_100a CUDA kernels.  This module
+only marshals numpy arrays across the C ABI; it never computes flow itself and it raises if the
+compiled library is missing (there is no CPU fallback).
+
+Mirrors the reference's C++ entry points (paths inside eherbst/rgbd-flow):
+  scene_flow_two_frames    runFlowTwoFramesSceneFlowExperiments   src/runFlowTwoFrames.cpp:109-121
+  scene_flow_multiscale    OpticalFlow::sceneFlowMultiscale        src/sceneFlowMultiscale.cpp:30-201
+  scene_flow_with_init     OpticalFlow::sceneFlowWithInit          src/sceneFlowWithInit.cpp:7-81
+  scene_flow_single_scale  sceneFlowSingleScale                    src/sceneFlowSingleScaleJacobiCUDA.cu:660-969
+Errors surface as RgbdFlowError carrying the library's status code and message (the reference
+throws std::runtime_error from ASSERT_ALWAYS, include/rgbd_util/assert.h:57,106).
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "librgbdflow.so")
+
+REG_ISOTROPIC, REG_LETOUZEY, REG_HPB = 0, 1, 2
+STORE_FP32, STORE_FP16, STORE_BF16 = 0, 1, 2
+COMPUTE_FP32, COMPUTE_FP64 = 0, 1
+MAX_LEVELS, MAX_OUTER = 16, 64
+
+OK = 0
+ERR_NAMES = {-1: "INVALID_ARG", -2: "UNSUPPORTED", -3: "CUDA", -4: "BUDGET", -5: "TIMEOUT",
+             -6: "NO_DEVICE", -7: "BUSY", -8: "INTERNAL"}
+
+
+class RgbdFlowError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("%s (%d): %s" % (ERR_NAMES.get(code, "?"), code, msg))
+        self.code = code
+
+
+class CameraParams(ctypes.Structure):
+    """rgbd::CameraParams (include/rgbd_util/CameraParams.h:17-28)."""
+    _fields_ = [("xRes", ctypes.c_uint), ("yRes", ctypes.c_uint), ("centerX", ctypes.c_float),
+                ("centerY", ctypes.c_float), ("focalLength", ctypes.c_float),
+                ("stereoBaseline", ctypes.c_float), ("fovX", ctypes.c_float), ("fovY", ctypes.c_float)]
+
+    @classmethod
+    def make(cls, W, H, f, cx, cy):
+        return cls(W, H, cx, cy, f, 0.072, 1.0472, 1.0472)
+
+
+class Params(ctypes.Structure):
+    _fields_ = [("regularization", ctypes.c_int), ("color_data_weight", ctypes.c_double),
+                ("depth_vs_color_data_weight", ctypes.c_double), ("alpha", ctypes.c_double),
+                ("gamma", ctypes.c_double), ("pyramid_ratio", ctypes.c_double), ("min_width", ctypes.c_int),
+                ("n_outer", ctypes.c_int), ("n_inner", ctypes.c_int), ("n_sor", ctypes.c_int),
+                ("depth_boundary_dist", ctypes.c_int), ("fill_holes", ctypes.c_int),
+                ("fixed_schedule", ctypes.c_int), ("storage", ctypes.c_int), ("compute", ctypes.c_int),
+                ("omega", ctypes.c_double), ("max_flow_step", ctypes.c_double), ("eps_d", ctypes.c_double),
+                ("eps_z", ctypes.c_double), ("eps_s", ctypes.c_double), ("sor_tol", ctypes.c_double),
+                ("sor_check_period", ctypes.c_int), ("outer_tol", ctypes.c_double),
+                ("occ_margin", ctypes.c_double), ("occ_penalty", ctypes.c_double),
+                ("max_depth_grad", ctypes.c_double), ("sweeps_per_launch", ctypes.c_int)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("n_levels", ctypes.c_int), ("level_w", ctypes.c_int * MAX_LEVELS),
+                ("level_h", ctypes.c_int * MAX_LEVELS), ("outer_iters", ctypes.c_int * MAX_LEVELS),
+                ("sor_iters", (ctypes.c_int * MAX_OUTER) * MAX_LEVELS),
+                ("outer_stat", (ctypes.c_float * MAX_OUTER) * MAX_LEVELS),
+                ("sor_maxdiff", (ctypes.c_float * MAX_OUTER) * MAX_LEVELS),
+                ("device_ms", ctypes.c_double)]
+
+    def summary(self):
+        """Executed schedule, finest level first: [(W, H, outer, [sor per outer])]."""
+        out = []
+        for k in range(self.n_levels):
+            n = self.outer_iters[k]
+            out.append((self.level_w[k], self.level_h[k], n, [self.sor_iters[k][o] for o in range(min(n, MAX_OUTER))]))
+        return out
+
+
+def default_params():
+    """The reference defaults (sceneFlowParams() + setUpSceneFlowParams, runFlowTwoFrames.cpp:66-100),
+    set without calling the library so it is usable on hosts without a GPU."""
+    p = Params()
+    p.regularization = REG_HPB
+    p.color_data_weight = 1.0
+    p.depth_vs_color_data_weight = 1.0
+    p.alpha = 0.02
+    p.gamma = 1e-5
+    p.pyramid_ratio = 0.75
+    p.min_width = 60
+    p.n_outer, p.n_inner, p.n_sor = 50, 1, 10000
+    p.depth_boundary_dist = 4
+    p.fill_holes = 1
+    p.fixed_schedule = 0
+    p.storage = STORE_FP32
+    p.compute = COMPUTE_FP32
+    p.omega = 0.7
+    p.max_flow_step = 0.3
+    p.eps_d, p.eps_z, p.eps_s = 1e-6, 1e-10, 1e-6
+    p.sor_tol = 1e-5
+    p.sor_check_period = 25
+    p.outer_tol = 4e-4
+    p.occ_margin = 0.02
+    p.occ_penalty = 0.01
+    p.max_depth_grad = 0.04
+    p.sweeps_per_launch = 0
+    return p
+
+
+def benchmark_params(W, **over):
+    """The benchmark schedule: ISOTROPIC, ratio 0.5 with minWidth = W/16 (5 levels), 10 outer,
+    1 inner, 30 SOR iterations, alpha 0.02, gamma 1e-5."""
+    p = default_params()
+    p.regularization = REG_ISOTROPIC
+    p.pyramid_ratio = 0.5
+    p.min_width = max(1, W // 16)
+    p.n_outer, p.n_inner, p.n_sor = 10, 1, 30
+    for k, v in over.items():
+        setattr(p, k, v)
+    return p
+
+
+class RgbdFlowPair(ctypes.Structure):
+    _fields_ = [("W", ctypes.c_int), ("H", ctypes.c_int), ("cam", CameraParams),
+                ("bgr1", ctypes.c_void_p), ("depth1_m", ctypes.c_void_p), ("bgr2", ctypes.c_void_p),
+                ("depth2_m", ctypes.c_void_p), ("est_flow", ctypes.c_void_p), ("flow_out", ctypes.c_void_p)]
+
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("max_streams", ctypes.c_int), ("max_batch", ctypes.c_int),
+                ("hbm_budget_bytes", ctypes.c_size_t), ("warm_start", ctypes.c_int), ("params", Params)]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [("stream_id", ctypes.c_int), ("request_id", ctypes.c_uint64), ("W", ctypes.c_int),
+                ("H", ctypes.c_int), ("flow", ctypes.c_void_p), ("submit_time_s", ctypes.c_double),
+                ("done_time_s", ctypes.c_double), ("status", ctypes.c_int)]
+
+
+_lib = None
+
+_P = ctypes.POINTER
+_vp = ctypes.c_void_p
+_i = ctypes.c_int
+_d = ctypes.c_double
+
+# every symbol include/rgbdflow.h declares, with its ctypes signature
+SIGNATURES = {
+    "rgbdflow_params_default": (None, [_P(Params)]),
+    "rgbdflow_abi_version": (_i, []),
+    "rgbdflow_ctx_create": (_i, [_i, ctypes.c_size_t, _P(_vp)]),
+    "rgbdflow_ctx_destroy": (_i, [_vp]),
+    "rgbdflow_last_error": (ctypes.c_char_p, [_vp]),
+    "rgbdflow_ctx_device_bytes": (ctypes.c_size_t, [_vp]),
+    "rgbdflow_scene_flow_two_frames": (_i, [_vp, _P(CameraParams), _vp, _vp, _vp, _vp, _i, _i, _P(Params),
+                                            _vp, _vp, _P(Stats)]),
+    "rgbdflow_scene_flow_multiscale": (_i, [_vp, _P(CameraParams), _vp, _vp, _vp, _vp, _vp, _i, _i, _P(Params),
+                                            _vp, _vp, _vp, _P(Stats)]),
+    "rgbdflow_scene_flow_with_init": (_i, [_vp, _P(CameraParams), _vp, _vp, _vp, _vp, _vp, _i, _i, _P(Params),
+                                           _vp, _vp, _vp, _P(Stats)]),
+    "rgbdflow_scene_flow_single_scale": (_i, [_vp, _P(CameraParams)] + [_vp] * 9 + [_i, _i, _i, _d, _vp, _d, _vp, _d,
+                                              _vp, _vp, _i, _i, _i, _i, _P(Params), _P(Stats)]),
+    "rgbdflow_scene_flow_batch": (_i, [_vp, _P(RgbdFlowPair), _i, _P(Params), _P(Stats)]),
+    "rgbdflow_scene_flow_batch_async": (_i, [_vp, _P(RgbdFlowPair), _i, _P(Params), _vp]),
+    "rgbdflow_server_create": (_i, [_vp, _P(ServerConfig), _P(_vp)]),
+    "rgbdflow_server_destroy": (_i, [_vp]),
+    "rgbdflow_server_submit": (_i, [_vp, _i, ctypes.c_uint64, _P(CameraParams), _vp, _vp, _i, _i, _vp]),
+    "rgbdflow_server_step": (_i, [_vp, _i, _P(Result), _i, _P(_i)]),
+    "rgbdflow_server_pending": (_i, [_vp]),
+}
+
+
+def load():
+    """Load librgbdflow.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RgbdFlowError(-6, "librgbdflow.so not built at %s (run __graft_entry__.build())" % LIB_PATH)
+        lib = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None else None
+
+
+def _c(a, dt):
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+class Context:
+    """One device context (stream, workspaces, cached graphs).  Not shared across threads."""
+
+    def __init__(self, device=0, hbm_budget_bytes=0):
+        self.lib = load()
+        h = ctypes.c_void_p()
+        rc = self.lib.rgbdflow_ctx_create(device, hbm_budget_bytes, ctypes.byref(h))
+        if rc != OK:
+            raise RgbdFlowError(rc, "rgbdflow_ctx_create failed")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            self.lib.rgbdflow_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, rc):
+        if rc != OK:
+            msg = self.lib.rgbdflow_last_error(self.h)
+            raise RgbdFlowError(rc, msg.decode() if msg else "")
+
+    def device_bytes(self):
+        return self.lib.rgbdflow_ctx_device_bytes(self.h)
+
+    def scene_flow_two_frames(self, cam, bgr1, depth1, bgr2, depth2, params, est_flow=None, stats=True):
+        bgr1, bgr2 = _c(bgr1, np.uint8), _c(bgr2, np.uint8)
+        depth1, depth2 = _c(depth1, np.float32), _c(depth2, np.float32)
+        H, W = depth1.shape
+        out = np.zeros((H, W, 3), np.float32)
+        est = _c(est_flow, np.float32) if est_flow is not None else None
+        st = Stats() if stats else None
+        rc = self.lib.rgbdflow_scene_flow_two_frames(self.h, ctypes.byref(cam), _ptr(bgr1), _ptr(depth1), _ptr(bgr2),
+                                                     _ptr(depth2), W, H, ctypes.byref(params), _ptr(est), _ptr(out),
+                                                     ctypes.byref(st) if st is not None else None)
+        self._check(rc)
+        return (out, st) if stats else out
+
+    def scene_flow_single_scale(self, cam, Im1, dm1, Im2, dm2, warpIm2, warpDm2, u, v, w, colorW, ddw, alpha, dsw,
+                                gamma, mag, regw, nOuter, nInner, nSOR, allowEarly, params=None):
+        Im1, Im2 = _c(Im1, np.float64), _c(Im2, np.float64)
+        dm1, dm2 = _c(dm1, np.float64), _c(dm2, np.float64)
+        warpIm2, warpDm2 = _c(warpIm2, np.float64).copy(), _c(warpDm2, np.float64).copy()
+        u, v, w = _c(u, np.float64).copy(), _c(v, np.float64).copy(), _c(w, np.float64).copy()
+        ddw, dsw, mag, regw = (_c(x, np.float64) for x in (ddw, dsw, mag, regw))
+        H, W, C = Im1.shape
+        st = Stats()
+        rc = self.lib.rgbdflow_scene_flow_single_scale(
+            self.h, ctypes.byref(cam), _ptr(Im1), _ptr(dm1), _ptr(Im2), _ptr(dm2), _ptr(warpIm2), _ptr(warpDm2),
+            _ptr(u), _ptr(v), _ptr(w), W, H, C, colorW, _ptr(ddw), alpha, _ptr(dsw), gamma, _ptr(mag), _ptr(regw),
+            nOuter, nInner, nSOR, int(allowEarly), ctypes.byref(params) if params is not None else None,
+            ctypes.byref(st))
+        self._check(rc)
+        return u, v, w, warpIm2, warpDm2, st
+
+    def scene_flow_batch(self, pairs, params, stats=True):
+        """pairs: list of dicts with W, H, cam (CameraParams), bgr1, depth1, bgr2, depth2[, est_flow].
+        Returns the list of (H,W,3) float32 flows (and Stats list)."""
+        keep = []
+        arr = (RgbdFlowPair * len(pairs))()
+        outs = []
+        for i, p in enumerate(pairs):
+            b1, b2 = _c(p["bgr1"], np.uint8), _c(p["bgr2"], np.uint8)
+            d1, d2 = _c(p["depth1"], np.float32), _c(p["depth2"], np.float32)
+            est = _c(p["est_flow"], np.float32) if p.get("est_flow") is not None else None
+            out = np.zeros((p["H"], p["W"], 3), np.float32)
+            keep += [b1, b2, d1, d2, est, out]
+            outs.append(out)
+            arr[i].W, arr[i].H, arr[i].cam = p["W"], p["H"], p["cam"]
+            arr[i].bgr1, arr[i].depth1_m = b1.ctypes.data, d1.ctypes.data
+            arr[i].bgr2, arr[i].depth2_m = b2.ctypes.data, d2.ctypes.data
+            arr[i].est_flow = est.ctypes.data if est is not None else None
+            arr[i].flow_out = out.ctypes.data
+        st = (Stats * len(pairs))() if stats else None
+        rc = self.lib.rgbdflow_scene_flow_batch(self.h, arr, len(pairs), ctypes.byref(params), st)
+        self._check(rc)
+        return (outs, list(st)) if stats else outs

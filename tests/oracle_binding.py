@@ -1,0 +1,247 @@
+"""ctypes bindings of the CPU restatement (oracle/libsforacle.so) and of the reference's own
+code compiled in place (oracle/_ref/libref_cpu.so, oracle/_ref/libref_cuda.so).
+
+Test infrastructure only: the checker side of the parity tests, the smoke check and the CPU
+baseline of the benchmark.  The product path never imports this module.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_DIR = os.path.join(ROOT, "oracle")
+ORACLE_SO = os.path.join(ORACLE_DIR, "libsforacle.so")
+REF_CPU_SO = os.path.join(ORACLE_DIR, "_ref", "libref_cpu.so")
+REF_CUDA_SO = os.path.join(ORACLE_DIR, "_ref", "libref_cuda.so")
+
+_P = ctypes.POINTER
+_d = ctypes.c_double
+_i = ctypes.c_int
+_f = ctypes.c_float
+_pd = _P(ctypes.c_double)
+_pf = _P(ctypes.c_float)
+_pi = _P(ctypes.c_int)
+_pu8 = _P(ctypes.c_uint8)
+
+
+def build_oracle():
+    """Compile the oracle (and, where the reference sources exist, oracle/_ref) with make."""
+    subprocess.run(["make", "-s", "-C", ORACLE_DIR], check=True)
+
+
+def dptr(a):
+    return a.ctypes.data_as(_pd)
+
+
+def fptr(a):
+    return a.ctypes.data_as(_pf)
+
+
+def iptr(a):
+    return a.ctypes.data_as(_pi)
+
+
+def u8ptr(a):
+    return a.ctypes.data_as(_pu8)
+
+
+def _cont(a, dt):
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+_oracle = None
+
+
+def oracle():
+    global _oracle
+    if _oracle is None:
+        if not os.path.exists(ORACLE_SO):
+            build_oracle()
+        lib = ctypes.CDLL(ORACLE_SO)
+        lib.sfo_pyramid_levels.argtypes = [_i, _d, _i]
+        lib.sfo_build_pyramid.argtypes = [_pd, _i, _i, _i, _d, _i, _pd, _pi]
+        lib.sfo_gaussian_smooth.argtypes = [_pd, _i, _i, _i, _d, _i, _pd]
+        lib.sfo_resize_dims.argtypes = [_pd, _i, _i, _i, _i, _i, _pd]
+        lib.sfo_im2feature.argtypes = [_pd, _i, _i, _pd]
+        lib.sfo_median_fill.argtypes = [_pd, _i, _i]
+        lib.sfo_depth_sigma.argtypes = [_pf, _i, _i, _i, _pf]
+        lib.sfo_warp_cpu.argtypes = [_pd, _pd, _pd, _pd, _i, _i, _i, _pd, _pd, _pd, _pd, _pd]
+        lib.sfo_depth_mag_weights.argtypes = [_pd, _i, _i, ctypes.c_void_p, _pd]
+        lib.sfo_reg_weights.argtypes = [_pd, _i, _i, _i, _pd]
+        lib.sfo_linearize.argtypes = [_i] + [_pd] * 8 + [_i, _i, _i, _d, _pd, _d, _pd, _d, _pd, _pd, ctypes.c_void_p, _pd]
+        lib.sfo_sor.argtypes = [_i, _pd, _pd, _i, _i, _i, _d, _d]
+        lib.sfo_single_scale.argtypes = ([_i, _f] + [_pd] * 9 + [_i, _i, _i, _d, _pd, _d, _pd, _d, _pd, _pd,
+                                         _i, _i, _i, _i, ctypes.c_void_p, ctypes.c_void_p])
+        lib.sfo_scene_flow_two_frames.argtypes = [_i, ctypes.c_void_p, _pu8, _pf, _pu8, _pf, _i, _i,
+                                                  ctypes.c_void_p, _pf, _pf, ctypes.c_void_p]
+        lib.sfo_last_error.restype = ctypes.c_char_p
+        lib.sfo_set_threads.argtypes = [_i]
+        _oracle = lib
+    return _oracle
+
+
+_ref_cpu = None
+
+
+def ref_cpu_available():
+    return os.path.exists(REF_CPU_SO)
+
+
+def ref_cpu():
+    global _ref_cpu
+    if _ref_cpu is None:
+        lib = ctypes.CDLL(REF_CPU_SO)
+        lib.ref_build_pyramid.argtypes = [_pd, _i, _i, _i, _d, _i, _pd, _pi]
+        lib.ref_gaussian_smooth.argtypes = [_pd, _i, _i, _i, _d, _i, _pd]
+        lib.ref_resize_dims.argtypes = [_pd, _i, _i, _i, _i, _i, _pd]
+        lib.ref_im2feature.argtypes = [_pd, _i, _i, _pd]
+        lib.ref_warp.argtypes = [_pd, _pd, _pd, _pd, _i, _i, _i, _pd, _pd, _pd, _pd, _pd]
+        _ref_cpu = lib
+    return _ref_cpu
+
+
+_ref_cuda = None
+
+
+def ref_cuda_available():
+    return os.path.exists(REF_CUDA_SO)
+
+
+def ref_cuda():
+    global _ref_cuda
+    if _ref_cuda is None:
+        lib = ctypes.CDLL(REF_CUDA_SO)
+        lib.ref_single_scale.argtypes = ([_f] + [_pd] * 9 + [_i, _i, _i, _d, _pd, _d, _pd, _d, _pd, _pd, _i, _i, _i, _i])
+        _ref_cuda = lib
+    return _ref_cuda
+
+
+# ---------------------------------------------------------------------------------------------
+# numpy-level helpers over either implementation ("oracle" or "ref")
+
+def build_pyramid(img, ratio, min_width, impl="oracle"):
+    img = _cont(img, np.float64)
+    H, W = img.shape[:2]
+    C = 1 if img.ndim == 2 else img.shape[2]
+    lib = oracle() if impl == "oracle" else ref_cpu()
+    fn = lib.sfo_build_pyramid if impl == "oracle" else lib.ref_build_pyramid
+    dims = np.zeros(64, np.int32)
+    n = fn(dptr(img), W, H, C, ratio, min_width, None, iptr(dims))
+    total = sum(int(dims[2 * i]) * int(dims[2 * i + 1]) * C for i in range(n))
+    out = np.zeros(total, np.float64)
+    fn(dptr(img), W, H, C, ratio, min_width, dptr(out), iptr(dims))
+    levels, off = [], 0
+    for i in range(n):
+        w, h = int(dims[2 * i]), int(dims[2 * i + 1])
+        shape = (h, w) if C == 1 else (h, w, C)
+        levels.append(out[off:off + w * h * C].reshape(shape).copy())
+        off += w * h * C
+    return levels
+
+
+def gaussian_smooth(img, sigma, fsize, impl="oracle"):
+    img = _cont(img, np.float64)
+    H, W = img.shape[:2]
+    C = 1 if img.ndim == 2 else img.shape[2]
+    out = np.zeros_like(img)
+    if impl == "oracle":
+        oracle().sfo_gaussian_smooth(dptr(img), W, H, C, sigma, fsize, dptr(out))
+    else:
+        ref_cpu().ref_gaussian_smooth(dptr(img), W, H, C, sigma, fsize, dptr(out))
+    return out
+
+
+def resize_dims(img, DW, DH, impl="oracle"):
+    img = _cont(img, np.float64)
+    H, W = img.shape[:2]
+    C = 1 if img.ndim == 2 else img.shape[2]
+    out = np.zeros((DH, DW) if C == 1 else (DH, DW, C), np.float64)
+    fn = oracle().sfo_resize_dims if impl == "oracle" else ref_cpu().ref_resize_dims
+    fn(dptr(img), W, H, C, DW, DH, dptr(out))
+    return out
+
+
+def im2feature(bgr01, impl="oracle"):
+    bgr01 = _cont(bgr01, np.float64)
+    H, W = bgr01.shape[:2]
+    out = np.zeros((H, W, 5), np.float64)
+    fn = oracle().sfo_im2feature if impl == "oracle" else ref_cpu().ref_im2feature
+    fn(dptr(bgr01), W, H, dptr(out))
+    return out
+
+
+def warp(feat1, d1, feat2, d2, u, v, w, impl="oracle"):
+    feat1, feat2 = _cont(feat1, np.float64), _cont(feat2, np.float64)
+    d1, d2 = _cont(d1, np.float64), _cont(d2, np.float64)
+    u, v, w = _cont(u, np.float64), _cont(v, np.float64), _cont(w, np.float64)
+    H, W, C = feat1.shape
+    wI = np.zeros_like(feat1)
+    wD = np.zeros_like(d1)
+    fn = oracle().sfo_warp_cpu if impl == "oracle" else ref_cpu().ref_warp
+    fn(dptr(feat1), dptr(d1), dptr(feat2), dptr(d2), W, H, C, dptr(u), dptr(v), dptr(w), dptr(wI), dptr(wD))
+    return wI, wD
+
+
+def median_fill(depth):
+    d = _cont(depth, np.float64).copy()
+    H, W = d.shape
+    rc = oracle().sfo_median_fill(dptr(d), W, H)
+    if rc != 0:
+        raise RuntimeError(oracle().sfo_last_error().decode())
+    return d
+
+
+def depth_sigma(depth_m, max_dist=4):
+    d = _cont(depth_m, np.float32)
+    H, W = d.shape
+    out = np.zeros_like(d)
+    oracle().sfo_depth_sigma(fptr(d), W, H, max_dist, fptr(out))
+    return out
+
+
+def two_frames(cam, bgr1, depth1, bgr2, depth2, params, fp64=False, est_flow=None):
+    """sfo_scene_flow_two_frames: returns ((H,W,3) float32 flow, Stats).  cam and params are the
+    ctypes structs of the product binding (rgbdflow.CameraParams / rgbdflow.Params)."""
+    import rgbdflow as rf
+    bgr1, bgr2 = _cont(bgr1, np.uint8), _cont(bgr2, np.uint8)
+    depth1, depth2 = _cont(depth1, np.float32), _cont(depth2, np.float32)
+    H, W = depth1.shape
+    out = np.zeros((H, W, 3), np.float32)
+    st = rf.Stats()
+    est = _cont(est_flow, np.float32) if est_flow is not None else None
+    rc = oracle().sfo_scene_flow_two_frames(int(fp64), ctypes.byref(cam), u8ptr(bgr1), fptr(depth1), u8ptr(bgr2),
+                                            fptr(depth2), W, H, ctypes.byref(params),
+                                            fptr(est) if est is not None else None, fptr(out), ctypes.byref(st))
+    if rc != 0:
+        raise RuntimeError("oracle: %s" % oracle().sfo_last_error().decode())
+    return out, st
+
+
+def single_scale(f_level, Im1, dm1, Im2, dm2, wI2, wD2, u, v, w, colorW, ddw, alpha, dsw, gamma, mag, regw,
+                 nOuter, nInner, nSOR, allowEarly, params=None, fp64=False, impl="oracle"):
+    """The per-level seam on the oracle (impl="oracle") or on the reference's own CUDA solver
+    (impl="ref", needs a GPU).  Returns (u, v, w, warpIm2, warpDm2, stats-or-None)."""
+    import rgbdflow as rf
+    Im1, Im2 = _cont(Im1, np.float64), _cont(Im2, np.float64)
+    dm1, dm2 = _cont(dm1, np.float64), _cont(dm2, np.float64)
+    wI2, wD2 = _cont(wI2, np.float64).copy(), _cont(wD2, np.float64).copy()
+    u, v, w = _cont(u, np.float64).copy(), _cont(v, np.float64).copy(), _cont(w, np.float64).copy()
+    ddw, dsw, mag, regw = (_cont(x, np.float64) for x in (ddw, dsw, mag, regw))
+    H, W, C = Im1.shape
+    if impl == "ref":
+        rc = ref_cuda().ref_single_scale(f_level, dptr(Im1), dptr(dm1), dptr(Im2), dptr(dm2), dptr(wI2), dptr(wD2),
+                                         dptr(u), dptr(v), dptr(w), W, H, C, colorW, dptr(ddw), alpha, dptr(dsw),
+                                         gamma, dptr(mag), dptr(regw), nOuter, nInner, nSOR, int(allowEarly))
+        if rc != 0:
+            raise RuntimeError("reference CUDA solver failed: cuda error %d" % rc)
+        return u, v, w, wI2, wD2, None
+    st = rf.Stats()
+    rc = oracle().sfo_single_scale(int(fp64), f_level, dptr(Im1), dptr(dm1), dptr(Im2), dptr(dm2), dptr(wI2),
+                                   dptr(wD2), dptr(u), dptr(v), dptr(w), W, H, C, colorW, dptr(ddw), alpha,
+                                   dptr(dsw), gamma, dptr(mag), dptr(regw), nOuter, nInner, nSOR, int(allowEarly),
+                                   ctypes.byref(params) if params is not None else None, ctypes.byref(st))
+    if rc != 0:
+        raise RuntimeError("oracle: %s" % oracle().sfo_last_error().decode())
+    return u, v, w, wI2, wD2, st
