@@ -1,0 +1,938 @@
+// kernels.cuh — sm_100a device code of the RGB-D scene-flow solve.
+//
+// Every kernel walks a device-resident work list (LevelItem descriptors + tile lists), so one
+// launch serves one pair or a ragged batch of pairs of different sizes alike.  T is the
+// arithmetic type (float for the product, double for the FP64 device oracle); S is the storage
+// type of the feature / depth planes the linearisation reads (float, __half or __nv_bfloat16).
+// All steps are bandwidth- or latency-bound stencils: no step is a dense contraction, so no
+// tensor-core path exists here.
+#pragma once
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+namespace rgbdflow {
+
+constexpr int kMaxChecks = 512;  // SOR convergence checks per inner iteration (nSOR / period)
+
+// Linearisation / elementwise tiling.
+constexpr int LTW = 32, LTH = 8;  // 256 threads, one interior pixel each
+// SOR tiling (interior); the loaded region adds a halo of 2 * sweeps.
+constexpr int STW = 32, STH = 16;
+
+// ------------------------------------------------------------------------------------------
+// descriptors
+
+// Per (pair) control block, device resident; written only by the kernels named beside each field.
+struct PairCtl {
+    int level_done;               // k_control sets it when the outer early-termination test passes
+    int sor_stop;                 // k_sor (the CTA of tile 0) sets it once a convergence check breaks
+    int sor_stop_iter;            // iterations executed when the break happened
+    int pad0;
+    unsigned maxdiff[kMaxChecks]; // k_sor: max |dx| of the checked iteration (float bits), per check
+    // history (finest level = 0)
+    int outer_exec[16];
+    int sor_exec[16][64];
+    float stat[16][64];
+    float sor_maxdiff[16][64];
+};
+
+template <class T, class S>
+struct LevelItem {
+    int W, H;
+    int level;                  // 0 = finest
+    int allow_early;            // outer early termination permitted at this level
+    int est_init;               // flow initialised by the caller (warm start): no upsample
+    T f_level;                  // focal length of this level (convergence weights f / depth)
+    PairCtl* ctl;
+    // pyramid planes of this level (T): colour 1 (3), colour 2 (3), depth 1, depth 2,
+    // depth-data weight, depth-smoothness weight
+    T* pyr[10];
+    // solver inputs (S): features 1 (5), features 2 (5), depth 1, depth 2
+    S* I1[5];
+    S* I2[5];
+    S* D1;
+    S* D2;
+    T* mag;                     // depth-magnitude weight
+    T* rh;                      // regularisation weight to the right neighbour
+    T* rv;                      // regularisation weight to the lower neighbour
+    T* u[3];                    // flow (u px, v px, w m)
+    T* x[2][3];                 // SOR increment, ping-pong pair
+    T* sys[12];                 // compact linear system (see k_linearize)
+    T* stat_part;               // per SOR tile partial of the early-termination statistic
+    int lin_tiles_x, lin_tile0; // linearisation / elementwise tiles: index base in the step's list
+    int sor_tiles_x, sor_tile0;
+    int n_sor_tiles;
+    // coarser level (for the flow upsample); null at the coarsest level
+    const T* uc[3];
+    int Wc, Hc;
+    T inv_ratio;                // 1 / pyramid ratio (u, v scale on upsample)
+    // full-resolution info for the depth-magnitude quirk
+    int xres_full;
+    T f_full;
+};
+
+struct Tile {
+    int item;  // index into the step's LevelItem array
+    int tx, ty;
+    int idx;   // tile index within its item
+};
+
+// Constants of the solve (sceneFlowSingleScaleJacobiCUDA.cu:375,461,646,691,749,768,905,920).
+template <class T>
+struct SolveConst {
+    T alpha, gamma, color_w;
+    T eps_d, eps_z, eps_s;
+    T omega, step;
+    T occ_margin, occ_penalty, max_grad;
+    double sor_tol;
+    double outer_tol;
+    int fixed;
+    int n_sor;
+};
+
+// One SOR launch of the host schedule.
+struct SorLaunch {
+    int it0, nit;      // first iteration (within the inner loop) and iteration count
+    int xin;           // ping-pong buffer read (0/1); the other one is written
+    int xin_zero;      // first launch of an outer iteration: the increment starts at 0
+    int final_fold;    // last launch of the outer iteration: u += x and the statistic partials
+    int final_keep;    // last launch of a non-final inner iteration: write x
+    int check;         // the last iteration of this launch is a convergence check
+    int check_idx;     // its slot in PairCtl::maxdiff
+    int prev_check;    // the previous launch ended with a check: decide here whether to stop
+    int prev_check_idx;
+    int outer;         // outer iteration index (stats)
+};
+
+// ------------------------------------------------------------------------------------------
+// small helpers
+
+template <class S> __device__ __forceinline__ float tof(S v);
+template <> __device__ __forceinline__ float tof<float>(float v) { return v; }
+template <> __device__ __forceinline__ float tof<__half>(__half v) { return __half2float(v); }
+template <> __device__ __forceinline__ float tof<__nv_bfloat16>(__nv_bfloat16 v) { return __bfloat162float(v); }
+
+template <class T, class S> __device__ __forceinline__ T ldS(const S* p) { return (T)tof<S>(p[0]); }
+template <> __device__ __forceinline__ double ldS<double, double>(const double* p) { return p[0]; }
+
+template <class S> __device__ __forceinline__ S fromT(float v);
+template <> __device__ __forceinline__ float fromT<float>(float v) { return v; }
+template <> __device__ __forceinline__ __half fromT<__half>(float v) { return __float2half_rn(v); }
+template <> __device__ __forceinline__ __nv_bfloat16 fromT<__nv_bfloat16>(float v) { return __float2bfloat16_rn(v); }
+template <class S, class T> __device__ __forceinline__ S stS(T v) { return fromT<S>((float)v); }
+template <> __device__ __forceinline__ double stS<double, double>(double v) { return v; }
+
+template <class T> __device__ __forceinline__ T rsqrtT(T v);
+template <> __device__ __forceinline__ float rsqrtT<float>(float v) { return 1.0f / sqrtf(v); }
+template <> __device__ __forceinline__ double rsqrtT<double>(double v) { return 1.0 / sqrt(v); }
+
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// ------------------------------------------------------------------------------------------
+// Preprocessing at full resolution.
+
+// BGR8 -> [0,1] planes (cv2liuBGR keeps BGR order: ceLiuOpticalFlow.cpp:19-34); depth copies.
+template <class T>
+struct PrepItem {
+    int W, H;
+    int kind;                   // 0: BGR8 + float depth; 1: [0,1] FP64 colour + FP64 depth + given sigma
+    const uint8_t* bgr[2];
+    const float* depth[2];
+    const double* im_d[2];      // kind 1: W*H*3 interleaved
+    const double* dep_d[2];     // kind 1: W*H
+    const float* sigma_in;      // kind 1: depth sigma of frame 1 (params.depthSigma1)
+    T* col[2][3];       // level-0 colour planes
+    T* dep[2];          // level-0 depth planes (filled in place by the hole fill)
+    uint8_t* stamp[2];  // hole-fill round stamps: 0 valid, 255 unfilled, r filled in round r
+    uint8_t* bmask;     // depth-boundary mask of frame 1
+    T* ddw;             // level-0 depth-data weight
+    T* dsw;             // level-0 depth-smoothness weight
+    T f2;               // focal length squared (calculateDepthSmoothnessTermWeights)
+    T dvc;              // depthVsColorDataWeight
+    int max_dist;       // depth-sigma boundary radius
+    int* unfilled;      // per round: unfilled pixels left (both frames), for the early exit
+    int tiles_x, tile0;
+};
+
+template <class T>
+__global__ void k_prep(const PrepItem<T>* items, const Tile* tiles)
+{
+    const Tile t = tiles[blockIdx.x];
+    const PrepItem<T>& it = items[t.item];
+    const int j = t.tx * LTW + (threadIdx.x % LTW), i = t.ty * LTH + (threadIdx.x / LTW);
+    if (i >= it.H || j >= it.W) return;
+    const int l = i * it.W + j;
+    for (int f = 0; f < 2; f++) {
+        if (it.kind == 0) {
+            const uint8_t* b = it.bgr[f] + (size_t)l * 3;
+            for (int c = 0; c < 3; c++) it.col[f][c][l] = (T)b[c] / (T)255.0;
+            const float z = it.depth[f][l];
+            it.dep[f][l] = (T)z;
+            it.stamp[f][l] = (z > 0) ? 0 : 255;
+        } else {
+            const double* b = it.im_d[f] + (size_t)l * 3;
+            for (int c = 0; c < 3; c++) it.col[f][c][l] = (T)b[c];
+            const double z = it.dep_d[f][l];
+            it.dep[f][l] = (T)z;
+            it.stamp[f][l] = (z > 0) ? 0 : 255;
+        }
+    }
+    if (it.kind != 0) return;  // sigma supplied by the caller
+    // boundary mask (staticDepthNoiseModeling.cpp:92-98); stereoErrorRatio(min z) scales 0.02
+    const float* d = it.depth[0];
+    const double z = d[l];
+    bool bnd = false;
+    auto ser = [](double zz) { const double e1 = 1.0 / (1.0 / .00285 + 1.0); return (zz * zz / (1.0 / .00285 + zz)) / e1; };
+    if (i < it.H - 1 && d[l + it.W] > 0 && fabs((double)(d[l] - d[l + it.W])) > .02 * ser(fmin((double)d[l], (double)d[l + it.W])))
+        bnd = true;
+    else if (j < it.W - 1 && d[l + 1] > 0 && fabs((double)(d[l] - d[l + 1])) > .02 * ser(fmin((double)d[l], (double)d[l + 1])))
+        bnd = true;
+    (void)z;
+    it.bmask[l] = bnd;
+}
+
+// Depth sigma with the boundary increase (staticDepthNoiseModeling.cpp:232-258, 85-137): the L1
+// distance to the nearest boundary pixel is searched over the diamond of radius max_dist (the
+// exact cv::distanceTransform L1 value wherever it is <= max_dist).  Writes the level-0
+// depth-data and depth-smoothness weights (OpticalFlow.cpp:71-97).
+template <class T>
+__global__ void k_sigma(const PrepItem<T>* items, const Tile* tiles)
+{
+    const Tile t = tiles[blockIdx.x];
+    const PrepItem<T>& it = items[t.item];
+    const int j = t.tx * LTW + (threadIdx.x % LTW), i = t.ty * LTH + (threadIdx.x / LTW);
+    if (i >= it.H || j >= it.W) return;
+    const int W = it.W, H = it.H, l = i * W + j;
+    const double e1 = 1.0 / (1.0 / .00285 + 1.0);
+    if (it.kind != 0) {
+        it.ddw[l] = (T)(e1 / (double)it.sigma_in[l] * (double)it.dvc);
+        it.dsw[l] = it.f2;
+        return;
+    }
+    const float z = it.depth[0][l];
+    float s;
+    if (z > 0) {
+        const float sig1 = (float)e1;
+        const double r = ((double)z * z / (1.0 / .00285 + z)) / e1;
+        s = (float)fmax(1e-4, (double)sig1 * r);
+    } else {
+        s = 1.0f;
+    }
+    const int md = it.max_dist;
+    if (md > 0) {
+        int best = md + 1;
+        for (int di = -md; di <= md && best > 0; di++) {
+            const int ii = i + di;
+            if (ii < 0 || ii >= H) continue;
+            const int rem = md - abs(di);
+            for (int dj = -rem; dj <= rem; dj++) {
+                const int jj = j + dj;
+                if (jj < 0 || jj >= W) continue;
+                if (it.bmask[ii * W + jj]) {
+                    const int dd = abs(di) + abs(dj);
+                    if (dd < best) best = dd;
+                }
+            }
+        }
+        if (best <= md) {
+            const float a = (float)best / (float)md;
+            s = (float)exp((1 - a) * log((double)(10 * s)) + a * log((double)s));
+        }
+    }
+    it.ddw[l] = (T)(e1 / (double)s * (double)it.dvc);
+    it.dsw[l] = it.f2;
+}
+
+// One round of the parallel recursive-median hole fill.  The reference fills holes one at a
+// time, most-known-neighbours first, each from the median of its valid 3x3 neighbours
+// (recursiveMedianFiltering.cpp:35-99).  Here every unfilled pixel whose known-neighbour count is
+// >= that of every unfilled pixel in its 3x3 neighbourhood is filled in the same round, from
+// the pixels valid before the round (round stamps make the rounds deterministic).  Isolated
+// holes get exactly the reference's value; inside larger holes the order (and so the value)
+// can differ from the reference's hash-set order.
+template <class T>
+__global__ void k_fill_round(const PrepItem<T>* items, const Tile* tiles, int round)
+{
+    const Tile t = tiles[blockIdx.x];
+    const PrepItem<T>& it = items[t.item];
+    if (round > 1 && it.unfilled[round - 1] == 0) return;
+    const int j = t.tx * LTW + (threadIdx.x % LTW), i = t.ty * LTH + (threadIdx.x / LTW);
+    const int W = it.W, H = it.H;
+    const bool inside = (i < H && j < W);
+    int left = 0;
+    for (int f = 0; f < 2 && inside; f++) {
+        const int l = i * W + j;
+        uint8_t* st = it.stamp[f];
+        if (st[l] != 255) continue;  // valid or already filled
+        auto known = [&](int ii, int jj) { const int s = st[ii * W + jj]; return s < round; };
+        auto count = [&](int ci, int cj) {
+            int c = 0;
+            for (int ii = max(0, ci - 1); ii <= min(H - 1, ci + 1); ii++)
+                for (int jj = max(0, cj - 1); jj <= min(W - 1, cj + 1); jj++)
+                    if (!(ii == ci && jj == cj) && known(ii, jj)) c++;
+            return c;
+        };
+        const int c = count(i, j);
+        bool fill = c > 0;
+        for (int ii = max(0, i - 1); ii <= min(H - 1, i + 1) && fill; ii++)
+            for (int jj = max(0, j - 1); jj <= min(W - 1, j + 1); jj++) {
+                if (ii == i && jj == j) continue;
+                const int s = st[ii * W + jj];
+                if (s >= round && count(ii, jj) > c) { fill = false; break; }
+            }
+        if (!fill) { left++; continue; }
+        float v[8];
+        int n = 0;
+        for (int ii = max(0, i - 1); ii <= min(H - 1, i + 1); ii++)
+            for (int jj = max(0, j - 1); jj <= min(W - 1, j + 1); jj++)
+                if (!(ii == i && jj == j) && known(ii, jj)) {
+                    float x = (float)it.dep[f][ii * W + jj];
+                    int k = n++;
+                    while (k > 0 && v[k - 1] > x) { v[k] = v[k - 1]; k--; }
+                    v[k] = x;
+                }
+        it.dep[f][l] = (T)v[n / 2];
+        st[l] = (uint8_t)round;
+    }
+    // count pixels still unfilled after this round (warp aggregate)
+    const unsigned m = __ballot_sync(0xffffffffu, left > 0);
+    int tot = left;
+    for (int o = 16; o > 0; o >>= 1) tot += __shfl_down_sync(0xffffffffu, tot, o);
+    if ((threadIdx.x & 31) == 0 && m) atomicAdd(&it.unfilled[round], tot);
+}
+
+// ------------------------------------------------------------------------------------------
+// Gaussian pyramid (GaussianPyramid.cpp:20-63; Image::GaussianSmoothing Image.h:1179-1199,
+// ResizeImage ImageProcessing.h:203-222).  A job smooths up to 10 planes of one source level
+// and bilinearly resamples them to the destination level.
+
+template <class T>
+struct PyrJob {
+    int sW, sH, dW, dH;
+    int nplanes;
+    int fs;                // filter half-width
+    double rate;           // resize ratio
+    const T* src[10];
+    T* tmp[10];
+    T* dst[10];
+    int tiles_x_src, tile0_src;  // tiles over the source (horizontal pass)
+    int tiles_x_dst, tile0_dst;  // tiles over the destination
+};
+
+constexpr int kMaxTaps = 33;
+
+template <class T>
+__global__ void k_hfilter(const PyrJob<T>* jobs, const Tile* tiles, const T* __restrict__ gall)
+{
+    const Tile t = tiles[blockIdx.x];
+    const PyrJob<T>& jb = jobs[t.item];
+    const int j = t.tx * LTW + (threadIdx.x % LTW), i = t.ty * LTH + (threadIdx.x / LTW);
+    if (i >= jb.sH || j >= jb.sW) return;
+    const T* g = gall + t.item * kMaxTaps;
+    const int fs = jb.fs, W = jb.sW;
+    for (int p = 0; p < jb.nplanes; p++) {
+        const T* s = jb.src[p] + (size_t)i * W;
+        T acc = 0;
+        for (int l = -fs; l <= fs; l++) acc += s[clampi(j + l, 0, W - 1)] * g[l + fs];
+        jb.tmp[p][(size_t)i * W + j] = acc;
+    }
+}
+
+template <class T>
+__device__ __forceinline__ T vtap(const T* tp, int W, int H, int x, int y, const T* g, int fs)
+{
+    T acc = 0;
+    for (int l = -fs; l <= fs; l++) acc += tp[(size_t)clampi(y + l, 0, H - 1) * W + x] * g[l + fs];
+    return acc;
+}
+
+template <class T>
+__global__ void k_vresize(const PyrJob<T>* jobs, const Tile* tiles, const T* __restrict__ gall)
+{
+    const Tile t = tiles[blockIdx.x];
+    const PyrJob<T>& jb = jobs[t.item];
+    const int j = t.tx * LTW + (threadIdx.x % LTW), i = t.ty * LTH + (threadIdx.x / LTW);
+    if (i >= jb.dH || j >= jb.dW) return;
+    const T* g = gall + t.item * kMaxTaps;
+    const double x = (double)(j + 1) / jb.rate - 1, y = (double)(i + 1) / jb.rate - 1;
+    const int xx = (int)x, yy = (int)y;
+    double dx = x - xx, dy = y - yy;
+    dx = dx > 1 ? 1 : (dx < 0 ? 0 : dx);
+    dy = dy > 1 ? 1 : (dy < 0 ? 0 : dy);
+    const int u0 = clampi(xx, 0, jb.sW - 1), u1 = clampi(xx + 1, 0, jb.sW - 1);
+    const int v0 = clampi(yy, 0, jb.sH - 1), v1 = clampi(yy + 1, 0, jb.sH - 1);
+    const T s00 = (T)(fabs(1 - dx) * fabs(1 - dy)), s01 = (T)(fabs(1 - dx) * fabs(dy));
+    const T s10 = (T)(fabs(dx) * fabs(1 - dy)), s11 = (T)(fabs(dx) * fabs(dy));
+    for (int p = 0; p < jb.nplanes; p++) {
+        const T* tp = jb.tmp[p];
+        T acc = 0;
+        acc += vtap(tp, jb.sW, jb.sH, u0, v0, g, jb.fs) * s00;
+        acc += vtap(tp, jb.sW, jb.sH, u0, v1, g, jb.fs) * s01;
+        acc += vtap(tp, jb.sW, jb.sH, u1, v0, g, jb.fs) * s10;
+        acc += vtap(tp, jb.sW, jb.sH, u1, v1, g, jb.fs) * s11;
+        jb.dst[p][(size_t)i * jb.dW + j] = acc;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Level set-up: features (OpticalFlow::im2feature RGB_WITH_GRADIENT, OpticalFlow.cpp:189-214),
+// depth copies in storage type, depth-magnitude weight (OpticalFlow.cpp:104-111, including the
+// reference's full-resolution indexing), regularisation weights (OpticalFlow.cpp:113-141) and
+// the initial flow (zero at the coarsest level, else the coarser flow resized with
+// ResizeImage(dims) and u, v scaled by 1/ratio: sceneFlowMultiscale.cpp:120-134).
+
+template <class T>
+__device__ __forceinline__ T gray_at(const T* const* c, int l)
+{
+    return c[0][l] * (T).114 + c[1][l] * (T).587 + c[2][l] * (T).299;
+}
+
+template <class T, class S>
+__global__ void k_level_setup(const LevelItem<T, S>* items, const Tile* tiles, int regtype)
+{
+    const Tile t = tiles[blockIdx.x];
+    const LevelItem<T, S>& it = items[t.item];
+    const int j = t.tx * LTW + (threadIdx.x % LTW), i = t.ty * LTH + (threadIdx.x / LTW);
+    if (t.idx == 0 && threadIdx.x == 0) it.ctl->level_done = 0;
+    if (i >= it.H || j >= it.W) return;
+    const int W = it.W, H = it.H, l = i * W + j;
+    const T gf[5] = {(T)1 / 12, (T)-8 / 12, (T)0, (T)8 / 12, (T)-1 / 12};
+    for (int f = 0; f < 2; f++) {
+        const T* const* c = (const T* const*)(it.pyr + 3 * f);
+        T gx = 0, gy = 0;
+        for (int m = -2; m <= 2; m++) gx += gray_at(c, i * W + clampi(j + m, 0, W - 1)) * gf[m + 2];
+        for (int m = -2; m <= 2; m++) gy += gray_at(c, clampi(i + m, 0, H - 1) * W + j) * gf[m + 2];
+        S* const* o = f ? it.I2 : it.I1;
+        o[0][l] = stS<S>(gray_at(c, l));
+        o[1][l] = stS<S>(gx);
+        o[2][l] = stS<S>(gy);
+        o[3][l] = stS<S>(c[1][l] - c[0][l]);
+        o[4][l] = stS<S>(c[1][l] - c[2][l]);
+    }
+    const T z1 = it.pyr[6][l];
+    it.D1[l] = stS<S>(z1);
+    it.D2[l] = stS<S>(it.pyr[7][l]);
+    {
+        const int src = (l / it.xres_full) * W + (l % it.xres_full);
+        const T z = it.pyr[6][src];
+        const T q = (z > 0) ? it.f_full / z : it.f_full / 2;
+        it.mag[l] = q * q;
+    }
+    T rh = 0, rv = 0;
+    if (regtype == 1) {
+        if (j < W - 1) { const T d = (z1 - it.pyr[6][l + 1]) / (T).02; rh = exp(-(d * d)); }
+        if (i < H - 1) { const T d = (z1 - it.pyr[6][l + W]) / (T).02; rv = exp(-(d * d)); }
+    } else {
+        rh = (j < W - 1) ? (T)1 : (T)0;
+        rv = (i < H - 1) ? (T)1 : (T)0;
+    }
+    it.rh[l] = rh;
+    it.rv[l] = rv;
+    if (it.est_init) return;  // flow supplied by the caller
+    if (it.uc[0] == nullptr) {
+        it.u[0][l] = 0; it.u[1][l] = 0; it.u[2][l] = 0;
+    } else {
+        const double xr = (double)W / it.Wc, yr = (double)H / it.Hc;
+        const double x = (double)(j + 1) / xr - 1, y = (double)(i + 1) / yr - 1;
+        const int xx = (int)x, yy = (int)y;
+        double dx = x - xx, dy = y - yy;
+        dx = dx > 1 ? 1 : (dx < 0 ? 0 : dx);
+        dy = dy > 1 ? 1 : (dy < 0 ? 0 : dy);
+        const int u0 = clampi(xx, 0, it.Wc - 1), u1 = clampi(xx + 1, 0, it.Wc - 1);
+        const int v0 = clampi(yy, 0, it.Hc - 1), v1 = clampi(yy + 1, 0, it.Hc - 1);
+        const T s00 = (T)(fabs(1 - dx) * fabs(1 - dy)), s01 = (T)(fabs(1 - dx) * fabs(dy));
+        const T s10 = (T)(fabs(dx) * fabs(1 - dy)), s11 = (T)(fabs(dx) * fabs(dy));
+        for (int c = 0; c < 3; c++) {
+            const T* s = it.uc[c];
+            T acc = 0;
+            acc += s[v0 * it.Wc + u0] * s00;
+            acc += s[v1 * it.Wc + u0] * s01;
+            acc += s[v0 * it.Wc + u1] * s10;
+            acc += s[v1 * it.Wc + u1] * s11;
+            it.u[c][l] = (c < 2) ? acc * it.inv_ratio : acc;
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Linearisation: one fused kernel per inner iteration.  Per interior pixel it warps frame 2 by
+// the current flow (warpColorImgWithSceneFlowKernel / warpDepthImgWithSceneFlowKernel,
+// .cu:579-635), takes the 5-tap derivatives of 0.4*I1 + 0.6*warped I2 (.cu:84-147), the
+// occlusion weight (.cu:640-648), the robust weights phi / psi / pi (.cu:340-371), the weighted
+// products (.cu:189-230), the normalised weighted Laplacians (.cu:240-333) and writes the
+// compact form of the system of fillSystemMtxKernel (.cu:477-575):
+//   sys[0..2]  diagonal (u, v, w rows)
+//   sys[3..5]  symmetric couplings uv, uw, vw
+//   sys[6..8]  right-hand sides
+//   sys[9]     alpha * phi * (right regularisation weight)   (0 on the last column)
+//   sys[10]    alpha * phi * (down regularisation weight)    (0 on the last row)
+//   sys[11]    depth-smoothness weight s (w-row neighbour coefficients are edge * s of the
+//              edge's left / upper pixel)
+// The neighbour coefficient of the u/v rows toward the left (upper) pixel is sys[9] (sys[10])
+// of that pixel, so the 8-plane matrix of the reference is implied without being stored.
+
+constexpr int LRW = LTW + 4, LRH = LTH + 4;  // warped region (halo 2)
+template <class T> constexpr size_t lin_smem_bytes() { return sizeof(T) * 19 * LRW * LRH; }
+
+template <class T, class S>
+__global__ void __launch_bounds__(LTW * LTH)
+k_linearize(const LevelItem<T, S>* items, const Tile* tiles, SolveConst<T> k, int use_du, int xsel)
+{
+    const Tile t = tiles[blockIdx.x];
+    const LevelItem<T, S>& it = items[t.item];
+    PairCtl* ctl = it.ctl;
+    if (ctl->level_done) return;
+    if (t.idx == 0) {
+        if (threadIdx.x == 0) { ctl->sor_stop = 0; ctl->sor_stop_iter = -1; }
+        for (int c = threadIdx.x; c < kMaxChecks; c += blockDim.x) ctl->maxdiff[c] = 0;
+    }
+    const int W = it.W, H = it.H;
+    const int x0 = t.tx * LTW, y0 = t.ty * LTH;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    typedef T Plane[LRH][LRW];
+    Plane* sB = reinterpret_cast<Plane*>(smem_raw);  // [6] 0.4*I1 + 0.6*warped I2 (5 features + depth)
+    Plane* sDT = sB + 6;                              // [6] warped I2 - I1
+    Plane* sU = sDT + 6;                              // [3] flow u
+    Plane* sUD = sU + 3;                              // [3] u + du
+    Plane& sPhi = *(sUD + 3);                         // robust smoothness weight
+    const int tid = threadIdx.x;
+    for (int r = tid; r < LRW * LRH; r += blockDim.x) {
+        const int ry = r / LRW, rx = r % LRW;
+        const int gi = y0 - 2 + ry, gj = x0 - 2 + rx;
+        if (gi < 0 || gj < 0 || gi >= H || gj >= W) continue;
+        const int l = gi * W + gj;
+        T U[3], D[3];
+        for (int c = 0; c < 3; c++) {
+            U[c] = it.u[c][l];
+            D[c] = use_du ? it.x[xsel][c][l] : (T)0;
+            sU[c][ry][rx] = U[c];
+            sUD[c][ry][rx] = U[c] + D[c];
+        }
+        const T x = (T)gj + U[0], y = (T)gi + U[1];
+        T wI[6], I1v[6];
+        for (int c = 0; c < 5; c++) I1v[c] = ldS<T, S>(it.I1[c] + l);
+        I1v[5] = ldS<T, S>(it.D1 + l);
+        if (x < 0 || x > (T)(W - 1) || y < 0 || y > (T)(H - 1)) {
+            for (int c = 0; c < 5; c++) wI[c] = I1v[c];
+            wI[5] = I1v[5] - U[2];
+        } else {
+            const int xa = clampi((int)floor(x), 0, W - 1), ya = clampi((int)floor(y), 0, H - 1);
+            const int xb = min(W - 1, xa + 1), yb = min(H - 1, ya + 1);
+            const T ax = x - (T)xa, ay = y - (T)ya;
+            const T w00 = (1 - ax) * (1 - ay), w01 = (1 - ax) * ay, w10 = ax * (1 - ay), w11 = ax * ay;
+            const int p00 = ya * W + xa, p01 = yb * W + xa, p10 = ya * W + xb, p11 = yb * W + xb;
+            for (int c = 0; c < 5; c++) {
+                const S* s = it.I2[c];
+                wI[c] = w00 * ldS<T, S>(s + p00) + w01 * ldS<T, S>(s + p01) + w10 * ldS<T, S>(s + p10) +
+                        w11 * ldS<T, S>(s + p11);
+            }
+            const S* s = it.D2;
+            wI[5] = w00 * ldS<T, S>(s + p00) + w01 * ldS<T, S>(s + p01) + w10 * ldS<T, S>(s + p10) +
+                    w11 * ldS<T, S>(s + p11) - U[2];
+        }
+        for (int c = 0; c < 6; c++) {
+            sB[c][ry][rx] = (T).4 * I1v[c] + (T).6 * wI[c];
+            sDT[c][ry][rx] = wI[c] - I1v[c];
+        }
+    }
+    __syncthreads();
+    // robust smoothness weight phi on the interior plus the column to its left and the row above
+    for (int r = tid; r < (LTW + 1) * (LTH + 1); r += blockDim.x) {
+        const int ry = 1 + r / (LTW + 1), rx = 1 + r % (LTW + 1);
+        const int gi = y0 - 2 + ry, gj = x0 - 2 + rx;
+        if (gi < 0 || gj < 0 || gi >= H || gj >= W) continue;
+        T d[6];
+        for (int c = 0; c < 3; c++) {
+            d[2 * c] = (gj == W - 1) ? (T)0 : sUD[c][ry][rx + 1] - sUD[c][ry][rx];
+            d[2 * c + 1] = (gi == H - 1) ? (T)0 : sUD[c][ry + 1][rx] - sUD[c][ry][rx];
+        }
+        const T s = it.pyr[9][gi * W + gj];
+        const T q = d[0] * d[0] + d[1] * d[1] + d[2] * d[2] + d[3] * d[3] + s * (d[4] * d[4] + d[5] * d[5]);
+        sPhi[ry][rx] = (T)0.5 * rsqrtT<T>(q + k.eps_s);
+    }
+    __syncthreads();
+    const int lx = tid % LTW, ly = tid / LTW;
+    const int gi = y0 + ly, gj = x0 + lx;
+    if (gi >= H || gj >= W) return;
+    const int l = gi * W + gj;
+    const int ry = ly + 2, rx = lx + 2;
+    const T gfl[5] = {1, -8, 0, 8, -1};
+    T Ix[6], Iy[6], It[6];
+    for (int c = 0; c < 6; c++) {
+        T sx = 0, sy = 0;
+        for (int m = 0; m < 5; m++) {
+            const int cc = clampi(gj - 2 + m, 0, W - 1) - (x0 - 2);
+            const int rr = clampi(gi - 2 + m, 0, H - 1) - (y0 - 2);
+            sx += gfl[m] * sB[c][ry][cc];
+            sy += gfl[m] * sB[c][rr][rx];
+        }
+        Ix[c] = sx / (T)12;
+        Iy[c] = sy / (T)12;
+        It[c] = sDT[c][ry][rx];
+    }
+    Ix[5] = fmin(fmax(Ix[5], -k.max_grad), k.max_grad);
+    Iy[5] = fmin(fmax(Iy[5], -k.max_grad), k.max_grad);
+    It[5] = fmin(fmax(It[5], -k.max_grad), k.max_grad);
+    const T U0 = sU[0][ry][rx], U1 = sU[1][ry][rx], U2 = sU[2][ry][rx];
+    const T du0 = sUD[0][ry][rx] - U0, du1 = sUD[1][ry][rx] - U1, du2 = sUD[2][ry][rx] - U2;
+    const T z1 = ldS<T, S>(it.D1 + l);
+    const T q = (z1 + U2 < ldS<T, S>(it.D2 + l) + k.occ_margin * (z1 * z1)) ? (T)1 : k.occ_penalty;
+    T sxy = 0, sx2 = 0, sy2 = 0, stx = 0, sty = 0;
+    for (int c = 0; c < 5; c++) {
+        const T e = (It[c] + Ix[c] * du0 + Iy[c] * du1) * q;
+        const T psi = (T)0.5 * rsqrtT<T>(e * e + k.eps_d) * k.color_w;
+        sxy += psi * Ix[c] * Iy[c];
+        sx2 += psi * Ix[c] * Ix[c];
+        sy2 += psi * Iy[c] * Iy[c];
+        stx += psi * Ix[c] * It[c];
+        sty += psi * Iy[c] * It[c];
+    }
+    const T ixy = sxy / (T)5, ix2 = sx2 / (T)5, iy2 = sy2 / (T)5;
+    const T itx = stx * q * q / (T)5, ity = sty * q * q / (T)5;
+    const T e2 = It[5] + Ix[5] * du0 + Iy[5] * du1 - du2;
+    const T pi = (T)0.5 * rsqrtT<T>(e2 * e2 + k.eps_z) * it.pyr[8][l];
+    const T dxy = pi * Ix[5] * Iy[5], dx2 = pi * Ix[5] * Ix[5], dy2 = pi * Iy[5] * Iy[5];
+    const T dtx = pi * Ix[5] * It[5], dty = pi * Iy[5] * It[5];
+    // weighted Laplacians of u (not u + du) and edge weights
+    const bool hasR = gj < W - 1, hasL = gj > 0, hasD = gi < H - 1, hasU = gi > 0;
+    const T rhl = it.rh[l], rvl = it.rv[l];
+    const T rhL = hasL ? it.rh[l - 1] : (T)0, rvU = hasU ? it.rv[l - W] : (T)0;
+    const T phi = sPhi[ry][rx];
+    const T phiL = hasL ? sPhi[ry][rx - 1] : (T)0, phiU = hasU ? sPhi[ry - 1][rx] : (T)0;
+    T nrm = 0;
+    int cnt = 0;
+    if (hasR) { nrm += rhl; cnt++; }
+    if (hasL) { nrm += rhL; cnt++; }
+    if (hasD) { nrm += rvl; cnt++; }
+    if (hasU) { nrm += rvU; cnt++; }
+    T lap[3];
+    for (int c = 0; c < 3; c++) {
+        T lv = 0;
+        const T uc = sU[c][ry][rx];
+        if (hasR) lv -= (sU[c][ry][rx + 1] - uc) * phi * rhl;
+        if (hasL) lv += (uc - sU[c][ry][rx - 1]) * phiL * rhL;
+        if (hasD) lv -= (sU[c][ry + 1][rx] - uc) * phi * rvl;
+        if (hasU) lv += (uc - sU[c][ry - 1][rx]) * phiU * rvU;
+        lap[c] = (fabs(nrm) < (T)1e-5) ? (T)0 : lv / (nrm / (T)cnt);
+    }
+    const T s = it.pyr[9][l];
+    const T sL = hasL ? it.pyr[9][l - 1] : (T)0, sU_ = hasU ? it.pyr[9][l - W] : (T)0;
+    T sumXY = 0, sumZ = 0;
+    if (hasL) { const T e = phiL * rhL; sumXY += e; sumZ += e * sL; }
+    if (hasU) { const T e = phiU * rvU; sumXY += e; sumZ += e * sU_; }
+    if (hasR) { const T e = phi * rhl; sumXY += e; sumZ += e * s; }
+    if (hasD) { const T e = phi * rvl; sumXY += e; sumZ += e * s; }
+    const T al = k.alpha, ga = k.gamma, mg = it.mag[l];
+    T* const* o = it.sys;
+    o[0][l] = -(ix2 + dx2 + al * sumXY) - ga;
+    o[1][l] = -(iy2 + dy2 + al * sumXY) - ga;
+    o[2][l] = -(pi + al * sumZ) - ga * mg;
+    o[3][l] = -ixy - dxy;
+    o[4][l] = pi * Ix[5];
+    o[5][l] = pi * Iy[5];
+    o[6][l] = -(-itx - dtx + al * -lap[0]) + ga * U0;
+    o[7][l] = -(-ity - dty + al * -lap[1]) + ga * U1;
+    o[8][l] = -(pi * It[5] + al * -(s * lap[2])) + ga * mg * U2;
+    o[9][l] = hasR ? al * (phi * rhl) : (T)0;
+    o[10][l] = hasD ? al * (phi * rvl) : (T)0;
+    o[11][l] = s;
+}
+
+// ------------------------------------------------------------------------------------------
+// Red-black SOR, K iterations per launch (temporal blocking).  Each CTA loads its tile plus a
+// halo of 2K pixels into shared memory, runs the red and black half-sweeps of K iterations on the
+// whole region (errors from the region's unknown outside creep inward one pixel per half-sweep
+// and never reach the interior), and writes back the interior only; x ping-pongs between two
+// buffers so no CTA reads a neighbour's already-updated values.  Same-colour updates are
+// independent, so the result is identical to sweeping the whole image colour by colour
+// (sceneFlowSingleScaleJacobiKernel, .cu:382-470): each of the three unknowns of a pixel is
+// updated from the pre-sweep values of the other two (pointwise Jacobi inside red-black
+// Gauss-Seidel), relaxed with omega and clamped to +-max_flow_step around its old value.
+
+template <int K> struct SorGeom {
+    static constexpr int RW = STW + 4 * K, RH = STH + 4 * K;
+    static constexpr int NT = (RW / 2) * RH;  // threads: one red and one black pixel each
+};
+template <class T, int K> constexpr size_t sor_smem_bytes() { return sizeof(T) * (6 * SorGeom<K>::RW * SorGeom<K>::RH + 32); }
+
+template <class T>
+__device__ __forceinline__ void sor_point(const T* c, T aL, T aU, T aR, T aD, T sL, T sU, T s,
+                                          const T* xl, const T* xu, const T* xr, const T* xd, const T* xp,
+                                          T omega, T step, T* out)
+{
+    // u row
+    T v = 0;
+    v -= aL * xl[0]; v -= aU * xu[0]; v -= aR * xr[0]; v -= aD * xd[0];
+    v += c[6];
+    v -= c[3] * xp[1]; v -= c[4] * xp[2];
+    v /= c[0];
+    T r = omega * v + ((T)1 - omega) * xp[0];
+    out[0] = fmin(fmax(r, xp[0] - step), xp[0] + step);
+    // v row
+    v = 0;
+    v -= aL * xl[1]; v -= aU * xu[1]; v -= aR * xr[1]; v -= aD * xd[1];
+    v += c[7];
+    v -= c[3] * xp[0]; v -= c[5] * xp[2];
+    v /= c[1];
+    r = omega * v + ((T)1 - omega) * xp[1];
+    out[1] = fmin(fmax(r, xp[1] - step), xp[1] + step);
+    // w row: neighbour coefficients carry the depth-smoothness weight of the edge's source pixel
+    v = 0;
+    v -= (aL * sL) * xl[2]; v -= (aU * sU) * xu[2]; v -= (aR * s) * xr[2]; v -= (aD * s) * xd[2];
+    v += c[8];
+    v -= c[4] * xp[0]; v -= c[5] * xp[1];
+    v /= c[2];
+    r = omega * v + ((T)1 - omega) * xp[2];
+    out[2] = fmin(fmax(r, xp[2] - step), xp[2] + step);
+}
+
+template <class T, class S, int K>
+__global__ void __launch_bounds__(SorGeom<K>::NT)
+k_sor(const LevelItem<T, S>* items, const Tile* tiles, SolveConst<T> k, SorLaunch L)
+{
+    constexpr int RW = SorGeom<K>::RW, RH = SorGeom<K>::RH, HW = RW / 2;
+    const Tile t = tiles[blockIdx.x];
+    const LevelItem<T, S>& it = items[t.item];
+    PairCtl* ctl = it.ctl;
+    if (ctl->level_done) return;
+    int nit = L.nit;
+    bool stopped = ctl->sor_stop != 0;
+    if (!stopped && L.prev_check) {
+        const float md = __uint_as_float(ctl->maxdiff[L.prev_check_idx]);
+        if ((double)md < k.sor_tol || (T)md >= k.step) {
+            stopped = true;
+            if (t.idx == 0 && threadIdx.x == 0) { ctl->sor_stop = 1; ctl->sor_stop_iter = L.it0; }
+        }
+    }
+    if (stopped) nit = 0;
+    const int W = it.W, H = it.H;
+    const int x0 = t.tx * STW - 2 * K, y0 = t.ty * STH - 2 * K;  // region origin (global)
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    typedef T Plane[RH][RW];
+    Plane* sx = reinterpret_cast<Plane*>(smem_raw);  // [3] increment
+    Plane& seh = sx[3];                               // alpha * phi * right weight
+    Plane& sev = sx[4];                               // alpha * phi * down weight
+    Plane& ss = sx[5];                                // depth-smoothness weight
+    T* wsum = reinterpret_cast<T*>(sx + 6);           // [32] block-sum scratch
+    const int tx = threadIdx.x % HW, ty = threadIdx.x / HW;
+    const int gi = y0 + ty;
+    T c[2][9];
+    int gl[2];
+    bool in[2];
+    const T* const* xin = it.x[L.xin];
+    for (int b = 0; b < 2; b++) {
+        const int rx = 2 * tx + b, gj = x0 + rx;
+        in[b] = gi >= 0 && gi < H && gj >= 0 && gj < W;
+        const int l = in[b] ? gi * W + gj : 0;
+        gl[b] = l;
+        for (int v = 0; v < 3; v++) sx[v][ty][rx] = (in[b] && !L.xin_zero) ? xin[v][l] : (T)0;
+        seh[ty][rx] = in[b] ? it.sys[9][l] : (T)0;
+        sev[ty][rx] = in[b] ? it.sys[10][l] : (T)0;
+        ss[ty][rx] = in[b] ? it.sys[11][l] : (T)0;
+        for (int q = 0; q < 9; q++) c[b][q] = in[b] ? it.sys[q][l] : (T)1;
+    }
+    __syncthreads();
+    const bool interior_row = ty >= 2 * K && ty < 2 * K + STH;
+    T md = 0;
+    for (int s = 0; s < 2 * nit; s++) {
+        const int color = s & 1;
+        // the one pixel of this thread with (i + j) % 2 == color
+        const int bb = (color ^ gi ^ x0) & 1;  // x0 and 2*tx are even-offset; parity of (gi + gj)
+        T cs[9];
+#pragma unroll
+        for (int q = 0; q < 9; q++) cs[q] = bb ? c[1][q] : c[0][q];  // register select, no local memory
+        if (bb ? in[1] : in[0]) {
+            const int rx = 2 * tx + bb;
+            const int rl = rx > 0 ? rx - 1 : rx, rr = rx < RW - 1 ? rx + 1 : rx;
+            const int ru = ty > 0 ? ty - 1 : ty, rd = ty < RH - 1 ? ty + 1 : ty;
+            T xl[3], xu[3], xr[3], xd[3], xp[3], nv[3];
+            for (int v = 0; v < 3; v++) {
+                xl[v] = sx[v][ty][rl]; xr[v] = sx[v][ty][rr];
+                xu[v] = sx[v][ru][rx]; xd[v] = sx[v][rd][rx];
+                xp[v] = sx[v][ty][rx];
+            }
+            sor_point<T>(cs, seh[ty][rl], sev[ru][rx], seh[ty][rx], sev[ty][rx], ss[ty][rl], ss[ru][rx],
+                         ss[ty][rx], xl, xu, xr, xd, xp, k.omega, k.step, nv);
+            for (int v = 0; v < 3; v++) sx[v][ty][rx] = nv[v];
+            if (L.check && s >= 2 * nit - 2 && interior_row && rx >= 2 * K && rx < 2 * K + STW)
+                for (int v = 0; v < 3; v++) md = fmax(md, fabs(nv[v] - xp[v]));
+        }
+        __syncthreads();
+    }
+    // max |dx| of the checked iteration -> per-pair slot (max is order independent)
+    if (L.check && nit > 0) {
+        float m = (float)md;
+        for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if ((threadIdx.x & 31) == 0 && m > 0) atomicMax(&ctl->maxdiff[L.check_idx], __float_as_uint(m));
+    }
+    // write the interior
+    T part = 0;
+    for (int b = 0; b < 2; b++) {
+        const int rx = 2 * tx + b;
+        if (!in[b] || !interior_row || rx < 2 * K || rx >= 2 * K + STW) continue;
+        const int l = gl[b];
+        if (L.final_fold) {
+            for (int v = 0; v < 3; v++) it.u[v][l] += sx[v][ty][rx];
+            const T a = sx[0][ty][rx], bq = sx[1][ty][rx], cz = sx[2][ty][rx];
+            const T wz = it.f_level / it.pyr[6][l];
+            part += a * a + bq * bq + (cz * cz) * wz;
+        } else {
+            T* const* xo = it.x[L.xin ^ 1];
+            for (int v = 0; v < 3; v++) xo[v][l] = sx[v][ty][rx];
+        }
+    }
+    if (L.final_fold) {
+        // deterministic block sum: warp trees, then warps in order
+        for (int o = 16; o > 0; o >>= 1) part += __shfl_down_sync(0xffffffffu, part, o);
+        if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = part;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            T tot = 0;
+            for (int w = 0; w < (int)((blockDim.x + 31) >> 5); w++) tot += wsum[w];
+            it.stat_part[t.idx] = tot;
+        }
+    }
+}
+
+// After each outer iteration: the early-termination statistic of the pair (mean over 3N of
+// sqr(du) * (1, 1, f / depth1), .cu:943-951), the stop decision and the executed-schedule record.
+template <class T, class S>
+__global__ void k_control(const LevelItem<T, S>* items, int n_items, SolveConst<T> k, int outer, int n_checks)
+{
+    const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (w >= n_items) return;
+    const LevelItem<T, S>& it = items[w];
+    PairCtl* ctl = it.ctl;
+    if (ctl->level_done) return;
+    T s = 0;
+    for (int i = lane; i < it.n_sor_tiles; i += 32) s += it.stat_part[i];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) {
+        const double st = (double)s / ((double)it.W * it.H * 3);
+        const int lv = it.level;
+        if (outer < 64) {
+            ctl->sor_exec[lv][outer] = ctl->sor_stop ? ctl->sor_stop_iter : k.n_sor;
+            ctl->stat[lv][outer] = (it.allow_early && !k.fixed) ? (float)st : -1.0f;
+            float md = -1.0f;  // the last convergence check evaluated in this outer iteration
+            for (int c = min(n_checks, kMaxChecks) - 1; c >= 0; c--) {
+                const unsigned b = ctl->maxdiff[c];
+                if (b) { md = __uint_as_float(b); break; }
+            }
+            ctl->sor_maxdiff[lv][outer] = md;
+        }
+        ctl->outer_exec[lv] = outer + 1;
+        if (it.allow_early && !k.fixed && st < k.outer_tol) ctl->level_done = 1;
+    }
+}
+
+// Final flow (level 0) to the caller's interleaved (u, v, w) float layout.
+template <class T, class S>
+__global__ void k_output(const LevelItem<T, S>* items, const Tile* tiles, T* const* outs)
+{
+    const Tile t = tiles[blockIdx.x];
+    const LevelItem<T, S>& it = items[t.item];
+    const int j = t.tx * LTW + (threadIdx.x % LTW), i = t.ty * LTH + (threadIdx.x / LTW);
+    if (i >= it.H || j >= it.W) return;
+    const int l = i * it.W + j;
+    T* o = outs[t.item];
+    o[(size_t)l * 3 + 0] = it.u[0][l];
+    o[(size_t)l * 3 + 1] = it.u[1][l];
+    o[(size_t)l * 3 + 2] = it.u[2][l];
+}
+
+// Device warp of the final flow (for the single-scale seam's warpIm2 / warpDm2 outputs).
+// Output block of a pair: flow (3N interleaved), then warped features (5N interleaved), then the
+// warped depth (N).
+template <class T, class S>
+__global__ void k_warp_out(const LevelItem<T, S>* items, const Tile* tiles, T* const* outs)
+{
+    const Tile t = tiles[blockIdx.x];
+    const LevelItem<T, S>& it = items[t.item];
+    const int j = t.tx * LTW + (threadIdx.x % LTW), i = t.ty * LTH + (threadIdx.x / LTW);
+    if (i >= it.H || j >= it.W) return;
+    const int W = it.W, H = it.H, l = i * W + j;
+    T* wI = outs[t.item] + (size_t)3 * W * H;
+    T* wD = outs[t.item] + (size_t)8 * W * H;
+    const T U0 = it.u[0][l], U1 = it.u[1][l], U2 = it.u[2][l];
+    const T x = (T)j + U0, y = (T)i + U1;
+    if (x < 0 || x > (T)(W - 1) || y < 0 || y > (T)(H - 1)) {
+        for (int c = 0; c < 5; c++) wI[(size_t)l * 5 + c] = ldS<T, S>(it.I1[c] + l);
+        wD[l] = ldS<T, S>(it.D1 + l) - U2;
+        return;
+    }
+    const int xa = clampi((int)floor(x), 0, W - 1), ya = clampi((int)floor(y), 0, H - 1);
+    const int xb = min(W - 1, xa + 1), yb = min(H - 1, ya + 1);
+    const T ax = x - (T)xa, ay = y - (T)ya;
+    const T w00 = (1 - ax) * (1 - ay), w01 = (1 - ax) * ay, w10 = ax * (1 - ay), w11 = ax * ay;
+    const int p00 = ya * W + xa, p01 = yb * W + xa, p10 = ya * W + xb, p11 = yb * W + xb;
+    for (int c = 0; c < 5; c++) {
+        const S* s = it.I2[c];
+        wI[(size_t)l * 5 + c] = w00 * ldS<T, S>(s + p00) + w01 * ldS<T, S>(s + p01) + w10 * ldS<T, S>(s + p10) +
+                                w11 * ldS<T, S>(s + p11);
+    }
+    const S* s = it.D2;
+    wD[l] = w00 * ldS<T, S>(s + p00) + w01 * ldS<T, S>(s + p01) + w10 * ldS<T, S>(s + p10) + w11 * ldS<T, S>(s + p11) - U2;
+}
+
+// Warm start (sceneFlowWithInit.cpp:11-20): the caller's flow estimate becomes the finest level's u.
+struct EstSrc {
+    const float* f;   // interleaved (u, v, w) floats, or null
+    const double* d;  // planar u, v, w doubles, or null
+};
+
+template <class T, class S>
+__global__ void k_load_est(const LevelItem<T, S>* items, const Tile* tiles, const EstSrc* est)
+{
+    const Tile t = tiles[blockIdx.x];
+    const LevelItem<T, S>& it = items[t.item];
+    if (!it.est_init) return;
+    const EstSrc e = est[t.item];
+    const int j = t.tx * LTW + (threadIdx.x % LTW), i = t.ty * LTH + (threadIdx.x / LTW);
+    if (i >= it.H || j >= it.W) return;
+    const int l = i * it.W + j;
+    const size_t N = (size_t)it.W * it.H;
+    for (int c = 0; c < 3; c++) it.u[c][l] = e.f ? (T)e.f[(size_t)l * 3 + c] : (T)e.d[c * N + l];
+}
+
+// Per-level seam (sceneFlowSingleScale's own inputs): features, depths, weights and flow come
+// from the caller as FP64 planes; this kernel only converts them into the level's planes.
+struct SeamSrc {
+    const double* im1; const double* im2;   // W*H*5 interleaved features
+    const double* dm1; const double* dm2;   // W*H
+    const double* uvw;                      // 3 planes
+    const double* ddw; const double* dsw; const double* mag;
+    const double* regw;                     // W*H*2 interleaved (right, down)
+};
+
+template <class T, class S>
+__global__ void k_seam_load(const LevelItem<T, S>* items, const Tile* tiles, const SeamSrc* src)
+{
+    const Tile t = tiles[blockIdx.x];
+    const LevelItem<T, S>& it = items[t.item];
+    const SeamSrc q = src[t.item];
+    if (t.idx == 0 && threadIdx.x == 0) it.ctl->level_done = 0;
+    const int j = t.tx * LTW + (threadIdx.x % LTW), i = t.ty * LTH + (threadIdx.x / LTW);
+    if (i >= it.H || j >= it.W) return;
+    const int W = it.W, H = it.H, l = i * W + j;
+    const size_t N = (size_t)W * H;
+    for (int c = 0; c < 5; c++) {
+        it.I1[c][l] = stS<S>((T)q.im1[(size_t)l * 5 + c]);
+        it.I2[c][l] = stS<S>((T)q.im2[(size_t)l * 5 + c]);
+    }
+    it.D1[l] = stS<S>((T)q.dm1[l]);
+    it.D2[l] = stS<S>((T)q.dm2[l]);
+    it.pyr[6][l] = (T)q.dm1[l];
+    it.pyr[7][l] = (T)q.dm2[l];
+    it.pyr[8][l] = (T)q.ddw[l];
+    it.pyr[9][l] = (T)q.dsw[l];
+    it.mag[l] = (T)q.mag[l];
+    // weights of edges that leave the image are never used by the reference; keep them 0
+    it.rh[l] = (j < W - 1) ? (T)q.regw[(size_t)l * 2 + 0] : (T)0;
+    it.rv[l] = (i < H - 1) ? (T)q.regw[(size_t)l * 2 + 1] : (T)0;
+    for (int c = 0; c < 3; c++) it.u[c][l] = (T)q.uvw[c * N + l];
+}
+
+}  // namespace rgbdflow

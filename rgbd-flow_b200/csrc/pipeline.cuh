@@ -1,0 +1,658 @@
+// pipeline.cuh — host-side planning and enqueueing of a (batched) coarse-to-fine solve.
+//
+// A Plan lays every pair's device state out in one arena, builds the work lists the kernels
+// walk (LevelItem / Tile / PyrJob / PrepItem) and enqueues the whole solve on one stream:
+// preprocessing, hole fill, pyramids, then per pyramid level the level set-up and the
+// outer / inner / SOR schedule.  Levels of different pairs run in the same launches: step s
+// serves level Lmax-1-s of every pair that has it, so pairs of different sizes pack together.
+// The enqueue is pure stream work with no host synchronisation, so it is captured once into a
+// CUDA graph per batch shape and replayed.
+#pragma once
+#include <cmath>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "kernels.cuh"
+
+namespace rgbdflow {
+
+struct CudaError : std::runtime_error {
+    cudaError_t code;
+    CudaError(cudaError_t c, const std::string& where)
+        : std::runtime_error(where + ": " + cudaGetErrorString(c)), code(c) {}
+};
+#define RF_CUDA(x)                                                                   \
+    do {                                                                             \
+        cudaError_t e_ = (x);                                                        \
+        if (e_ != cudaSuccess) throw CudaError(e_, std::string(#x) + " @" + __FILE__ + ":" + std::to_string(__LINE__)); \
+    } while (0)
+
+struct ArgError : std::runtime_error {
+    int code;
+    ArgError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+static inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+// GaussianPyramid::ConstructPyramid level sizes (GaussianPyramid.cpp:22-62).
+struct PyrShape {
+    double ratio;      // ratio after the reference's clamp to [0.4, 0.98]
+    int n;             // levels built from the base image (log(0.25)/log(ratio))
+    double baseSigma;
+    std::vector<int> w, h;
+    std::vector<int> src;       // source level of each level (0 for i <= n, else i - n)
+    std::vector<double> rate;   // resize ratio of each level
+    std::vector<double> sigma;
+};
+
+static inline PyrShape pyramid_shape(int W, int H, double ratio, int min_width, int max_levels)
+{
+    PyrShape s;
+    if (ratio > 0.98 || ratio < 0.4) ratio = 0.75;
+    s.ratio = ratio;
+    double w = W * ratio;
+    int L = 1;
+    while (w >= min_width) { L++; w *= ratio; }
+    if (max_levels > 0 && L > max_levels) L = max_levels;
+    s.baseSigma = 1 / ratio - 1;
+    s.n = (int)(std::log(0.25) / std::log(ratio));
+    s.w.push_back(W); s.h.push_back(H); s.src.push_back(0); s.rate.push_back(1); s.sigma.push_back(0);
+    for (int i = 1; i < L; i++) {
+        if (i <= s.n) {
+            const double r = std::pow(ratio, i);
+            s.w.push_back((int)((double)W * r)); s.h.push_back((int)((double)H * r));
+            s.src.push_back(0); s.rate.push_back(r); s.sigma.push_back(s.baseSigma * i);
+        } else {
+            const int sl = i - s.n;
+            const double r = (double)std::pow(ratio, i) * W / s.w[sl];
+            s.w.push_back((int)((double)s.w[sl] * r)); s.h.push_back((int)((double)s.h[sl] * r));
+            s.src.push_back(sl); s.rate.push_back(r); s.sigma.push_back(s.baseSigma * s.n);
+        }
+    }
+    return s;
+}
+
+// What one pair of a batch asks for.  kind selects the caller-facing entry point:
+//   0  runFlowTwoFramesSceneFlowExperiments: BGR8 colour, float depth (m), optional float est
+//   1  sceneFlowMultiscale / sceneFlowWithInit: FP64 [0,1] colour, FP64 depth, float depth sigma,
+//      optional FP64 planar (u, v, w) estimate
+//   2  sceneFlowSingleScale: FP64 5-channel features, depths, weights and flow of one level
+struct PairSpec {
+    int kind = 0;
+    int W = 0, H = 0;
+    float f_full = 0;         // camera focal length resized to W (getResizedCamParams)
+    unsigned xres_full = 0;   // camera xRes resized to W
+    const uint8_t* bgr1 = nullptr; const float* depth1 = nullptr;
+    const uint8_t* bgr2 = nullptr; const float* depth2 = nullptr;
+    const float* est = nullptr;                 // kind 0 warm start (W*H*3 interleaved)
+    const double* im1 = nullptr; const double* im2 = nullptr;
+    const double* dm1 = nullptr; const double* dm2 = nullptr;
+    const float* sigma1 = nullptr;
+    const double* est_d = nullptr;              // kind 1 warm start (3 planes)
+    // kind 2
+    const double* feat1 = nullptr; const double* feat2 = nullptr;
+    const double* uvw = nullptr;                // 3 planes
+    const double* ddw = nullptr; const double* dsw = nullptr; const double* mag = nullptr;
+    const double* regw = nullptr;               // W*H*2
+    float f_level = 0;
+    int allow_early = 0;
+    // outputs
+    float* out = nullptr;                       // kind 0: W*H*3 interleaved float
+    double* out_u = nullptr; double* out_v = nullptr; double* out_w = nullptr;  // kinds 1, 2
+    double* out_warpI = nullptr; double* out_warpD = nullptr;                     // kind 2
+
+    bool warm() const { return est || est_d; }
+    // input block: list of (host pointer, bytes) in upload order
+    std::vector<std::pair<const void*, size_t>> inputs() const
+    {
+        const size_t N = (size_t)W * H;
+        std::vector<std::pair<const void*, size_t>> v;
+        if (kind == 0) {
+            v = {{bgr1, N * 3}, {bgr2, N * 3}, {depth1, N * 4}, {depth2, N * 4}};
+            if (est) v.push_back({est, N * 12});
+        } else if (kind == 1) {
+            v = {{im1, N * 24}, {im2, N * 24}, {dm1, N * 8}, {dm2, N * 8}, {sigma1, N * 4}};
+            if (est_d) v.push_back({est_d, N * 24});
+        } else {
+            v = {{feat1, N * 40}, {feat2, N * 40}, {dm1, N * 8}, {dm2, N * 8}, {uvw, N * 24},
+                 {ddw, N * 8}, {dsw, N * 8}, {mag, N * 8}, {regw, N * 16}};
+        }
+        return v;
+    }
+};
+
+struct HostParams {
+    int regularization;
+    double color_w, dvc, alpha, gamma, ratio;
+    int min_width, n_outer, n_inner, n_sor, max_dist, fill_holes, fixed;
+    double omega, step, eps_d, eps_z, eps_s, sor_tol, outer_tol, occ_margin, occ_penalty, max_grad;
+    int period, K, fill_rounds;
+};
+
+// Bump allocator over a byte range.
+struct Bump {
+    size_t off = 0;
+    size_t take(size_t n) { const size_t o = off; off = align_up(off + n, 256); return o; }
+};
+
+template <class T, class S>
+struct Plan {
+    // ---- shape
+    int n = 0, Lmax = 0;
+    std::vector<PyrShape> shapes;
+    std::vector<int> L;           // levels per pair
+    HostParams hp;
+    // ---- device layout (offsets into the arena)
+    size_t arena_bytes = 0;
+    size_t in_off = 0, in_bytes = 0;    // inputs uploaded each call (bgr, depth, est)
+    size_t out_off = 0, out_bytes = 0;  // flows read back
+    size_t ctl_off = 0;                 // PairCtl[n]
+    size_t desc_off = 0, desc_bytes = 0;
+    int kind = 0;
+    std::vector<std::vector<size_t>> in_seg;  // per pair: arena offset of each input segment
+    std::vector<size_t> out_pair_off;   // per pair: flow (3N T interleaved) [+ warps 5N + N T for kind 2]
+    size_t est_src_off = 0, seam_src_off = 0;
+    bool any_warm = false;
+    // ---- host descriptors (uploaded as one block at desc_off)
+    std::vector<unsigned char> desc;
+    struct StepDesc {
+        size_t items_off; int n_items;
+        size_t lin_tiles_off; int n_lin;
+        size_t sor_tiles_off; int n_sor;
+    };
+    std::vector<StepDesc> steps;
+    struct PyrLevelDesc { size_t jobs_off; int n_jobs; size_t src_tiles_off; int n_src; size_t dst_tiles_off; int n_dst; size_t g_off; };
+    std::vector<PyrLevelDesc> pyr;
+    size_t prep_items_off = 0, prep_tiles_off = 0; int n_prep_tiles = 0;
+    size_t out_ptrs_off = 0;
+    size_t unfilled_off = 0;            // int[n][256]
+    std::vector<std::vector<SorLaunch>> sor_sched;  // per inner iteration index
+    std::vector<int> n_checks;                      // per inner iteration
+    std::vector<std::vector<size_t>> u_off;         // per pair per level: offset of u[0] (for warm-start upload)
+    std::vector<int> est_flag;
+
+    template <class X> size_t put(const std::vector<X>& v)
+    {
+        const size_t o = align_up(desc.size(), 256);
+        desc.resize(o + sizeof(X) * v.size());
+        if (!v.empty()) std::memcpy(desc.data() + o, v.data(), sizeof(X) * v.size());
+        return o;
+    }
+};
+
+// SOR launch schedule of one inner iteration: launches of at most K iterations, split so every
+// convergence check (it % period == period - 1, .cu:905-921) ends a launch.
+static inline std::vector<SorLaunch> sor_schedule(int nSOR, int K, int period, int fixed, int first_inner,
+                                                  int last_inner, int& cur, int& n_checks)
+{
+    std::vector<SorLaunch> v;
+    int start = 0;
+    int prev_check = 0, prev_idx = 0;
+    n_checks = 0;
+    while (start < nSOR) {
+        int end = std::min(start + K, nSOR);
+        if (!fixed)
+            for (int it = start; it < end - 1; it++)
+                if (it % period == period - 1) { end = it + 1; break; }
+        SorLaunch L{};
+        L.it0 = start; L.nit = end - start;
+        L.xin = cur;
+        L.xin_zero = (start == 0 && first_inner);
+        L.check = (!fixed && ((end - 1) % period == period - 1));
+        L.check_idx = L.check ? std::min((end - 1) / period, kMaxChecks - 1) : 0;
+        if (L.check) n_checks = L.check_idx + 1;
+        L.prev_check = prev_check; L.prev_check_idx = prev_idx;
+        prev_check = L.check; prev_idx = L.check_idx;
+        v.push_back(L);
+        cur ^= 1;
+        start = end;
+    }
+    if (v.empty()) {
+        SorLaunch L{};
+        L.xin = cur; L.xin_zero = first_inner;
+        v.push_back(L);
+        cur ^= 1;
+    }
+    // the last launch folds (last inner) or keeps x (earlier inner iterations)
+    SorLaunch& last = v.back();
+    if (last_inner) { last.final_fold = 1; cur ^= 1; }
+    else last.final_keep = 1;
+    return v;
+}
+
+template <class T, class S>
+static Plan<T, S> make_plan(const std::vector<PairSpec>& pairs, const HostParams& hp)
+{
+    Plan<T, S> P;
+    P.hp = hp;
+    P.n = (int)pairs.size();
+    P.kind = pairs.empty() ? 0 : pairs[0].kind;
+    for (const auto& p : pairs) {
+        if (p.kind != P.kind) throw ArgError(-1, "mixed entry-point kinds in one batch");
+        const bool one = p.warm() || p.kind == 2;
+        P.shapes.push_back(pyramid_shape(p.W, p.H, hp.ratio, hp.min_width, one ? 1 : 0));
+        P.L.push_back((int)P.shapes.back().w.size());
+        P.est_flag.push_back(one);
+        P.any_warm = P.any_warm || p.warm();
+        P.Lmax = std::max(P.Lmax, P.L.back());
+    }
+    if (P.Lmax > 16) throw ArgError(-2, "more than 16 pyramid levels");
+    for (auto& s : P.shapes)
+        for (size_t i = 1; i < s.w.size(); i++) {
+            if (s.w[i] < 1 || s.h[i] < 1) throw ArgError(-1, "pyramid level collapses to zero size; raise min_width");
+            if ((int)(s.sigma[i] * 3) > (kMaxTaps - 1) / 2) throw ArgError(-2, "pyramid filter too wide");
+        }
+    Bump A;
+    P.ctl_off = A.take(sizeof(PairCtl) * P.n);
+    P.unfilled_off = A.take(sizeof(int) * 256 * P.n);
+    const size_t in0 = A.off;
+    for (int p = 0; p < P.n; p++) {
+        std::vector<size_t> seg;
+        for (const auto& x : pairs[p].inputs()) seg.push_back(A.take(x.second));
+        P.in_seg.push_back(seg);
+    }
+    P.in_off = in0; P.in_bytes = A.off - in0;
+    const size_t out0 = A.off;
+    for (int p = 0; p < P.n; p++) {
+        const size_t N = (size_t)pairs[p].W * pairs[p].H;
+        P.out_pair_off.push_back(A.take(sizeof(T) * N * (P.kind == 2 ? 9 : 3)));
+    }
+    P.out_off = out0; P.out_bytes = A.off - out0;
+
+    // per pair per level planes
+    struct LevelMem { size_t pyr[10], I1[5], I2[5], D1, D2, mag, rh, rv, u[3], x[2][3], sys[12], stat; int nsor; };
+    std::vector<std::vector<LevelMem>> mem(P.n);
+    struct L0Mem { size_t stamp[2], bmask, tmp; };
+    std::vector<L0Mem> l0(P.n);
+    for (int p = 0; p < P.n; p++) {
+        const auto& s = P.shapes[p];
+        const size_t N0 = (size_t)s.w[0] * s.h[0];
+        l0[p].stamp[0] = A.take(N0); l0[p].stamp[1] = A.take(N0); l0[p].bmask = A.take(N0);
+        l0[p].tmp = A.take(sizeof(T) * N0 * 10);
+        mem[p].resize(P.L[p]);
+        for (int k = 0; k < P.L[p]; k++) {
+            const size_t N = (size_t)s.w[k] * s.h[k];
+            LevelMem& m = mem[p][k];
+            for (int c = 0; c < 10; c++) m.pyr[c] = A.take(sizeof(T) * N);
+            for (int c = 0; c < 5; c++) { m.I1[c] = A.take(sizeof(S) * N); m.I2[c] = A.take(sizeof(S) * N); }
+            m.D1 = A.take(sizeof(S) * N); m.D2 = A.take(sizeof(S) * N);
+            m.mag = A.take(sizeof(T) * N); m.rh = A.take(sizeof(T) * N); m.rv = A.take(sizeof(T) * N);
+            for (int c = 0; c < 3; c++) m.u[c] = A.take(sizeof(T) * N);
+            for (int b = 0; b < 2; b++) for (int c = 0; c < 3; c++) m.x[b][c] = A.take(sizeof(T) * N);
+            for (int c = 0; c < 12; c++) m.sys[c] = A.take(sizeof(T) * N);
+            const int stx = (s.w[k] + STW - 1) / STW, sty = (s.h[k] + STH - 1) / STH;
+            m.nsor = stx * sty;
+            m.stat = A.take(sizeof(T) * m.nsor);
+        }
+    }
+    P.arena_bytes = A.off;  // descriptors are appended after planning (desc_off)
+    P.u_off.resize(P.n);
+    for (int p = 0; p < P.n; p++)
+        for (int k = 0; k < P.L[p]; k++) P.u_off[p].push_back(mem[p][k].u[0]);
+
+    // Descriptor pointer fields hold arena OFFSETS here; bind_plan() rebases them to device
+    // addresses once the arena exists.
+
+    // prep items
+    std::vector<PrepItem<T>> prep(P.n);
+    std::vector<Tile> prep_tiles;
+    for (int p = 0; p < P.n; p++) {
+        const auto& s = P.shapes[p];
+        const size_t N0 = (size_t)s.w[0] * s.h[0];
+        PrepItem<T>& it = prep[p];
+        std::memset(&it, 0, sizeof(it));
+        it.W = s.w[0]; it.H = s.h[0];
+        const std::vector<size_t>& sg = P.in_seg[p];
+        it.kind = pairs[p].kind;
+        if (it.kind == 0) {
+            it.bgr[0] = (const uint8_t*)sg[0]; it.bgr[1] = (const uint8_t*)sg[1];
+            it.depth[0] = (const float*)sg[2]; it.depth[1] = (const float*)sg[3];
+        } else if (it.kind == 1) {
+            it.im_d[0] = (const double*)sg[0]; it.im_d[1] = (const double*)sg[1];
+            it.dep_d[0] = (const double*)sg[2]; it.dep_d[1] = (const double*)sg[3];
+            it.sigma_in = (const float*)sg[4];
+        }
+        for (int c = 0; c < 3; c++) { it.col[0][c] = (T*)mem[p][0].pyr[c]; it.col[1][c] = (T*)mem[p][0].pyr[3 + c]; }
+        it.dep[0] = (T*)mem[p][0].pyr[6]; it.dep[1] = (T*)mem[p][0].pyr[7];
+        it.stamp[0] = (uint8_t*)l0[p].stamp[0]; it.stamp[1] = (uint8_t*)l0[p].stamp[1];
+        it.bmask = (uint8_t*)l0[p].bmask;
+        it.ddw = (T*)mem[p][0].pyr[8]; it.dsw = (T*)mem[p][0].pyr[9];
+        it.f2 = (T)((double)pairs[p].f_full * (double)pairs[p].f_full);
+        it.dvc = (T)hp.dvc;
+        it.max_dist = hp.max_dist;
+        it.unfilled = (int*)(P.unfilled_off + sizeof(int) * 256 * p);
+        it.tiles_x = (s.w[0] + LTW - 1) / LTW;
+        it.tile0 = (int)prep_tiles.size();
+        const int ty = (s.h[0] + LTH - 1) / LTH;
+        for (int y = 0; y < ty; y++)
+            for (int x = 0; x < it.tiles_x; x++) prep_tiles.push_back(Tile{p, x, y, y * it.tiles_x + x});
+    }
+    if (P.kind == 2) prep_tiles.clear();  // the seam takes ready-made level inputs
+    P.prep_items_off = P.put(prep);
+    P.prep_tiles_off = P.put(prep_tiles);
+    P.n_prep_tiles = (int)prep_tiles.size();
+
+    // pyramid jobs per level index i >= 1
+    for (int i = 1; i < P.Lmax; i++) {
+        std::vector<PyrJob<T>> jobs;
+        std::vector<Tile> st, dt;
+        std::vector<T> g;
+        for (int p = 0; p < P.n; p++) {
+            if (i >= P.L[p]) continue;
+            const auto& s = P.shapes[p];
+            PyrJob<T> jb;
+            std::memset(&jb, 0, sizeof(jb));
+            const int sl = s.src[i];
+            jb.sW = s.w[sl]; jb.sH = s.h[sl]; jb.dW = s.w[i]; jb.dH = s.h[i];
+            jb.nplanes = 10;
+            jb.fs = (int)(s.sigma[i] * 3);
+            jb.rate = s.rate[i];
+            for (int c = 0; c < 10; c++) {
+                jb.src[c] = (const T*)mem[p][sl].pyr[c];
+                jb.tmp[c] = (T*)(l0[p].tmp + sizeof(T) * (size_t)s.w[0] * s.h[0] * c);
+                jb.dst[c] = (T*)mem[p][i].pyr[c];
+            }
+            const int jid = (int)jobs.size();
+            jb.tiles_x_src = (jb.sW + LTW - 1) / LTW;
+            jb.tile0_src = (int)st.size();
+            for (int y = 0; y < (jb.sH + LTH - 1) / LTH; y++)
+                for (int x = 0; x < jb.tiles_x_src; x++) st.push_back(Tile{jid, x, y, 0});
+            jb.tiles_x_dst = (jb.dW + LTW - 1) / LTW;
+            jb.tile0_dst = (int)dt.size();
+            for (int y = 0; y < (jb.dH + LTH - 1) / LTH; y++)
+                for (int x = 0; x < jb.tiles_x_dst; x++) dt.push_back(Tile{jid, x, y, 0});
+            jobs.push_back(jb);
+            // Image::GaussianSmoothing filter (Image.h:1184-1193), computed in FP64
+            std::vector<double> gd(2 * jb.fs + 1);
+            double sum = 0;
+            const double s2 = s.sigma[i] * s.sigma[i] * 2;
+            for (int l = -jb.fs; l <= jb.fs; l++) { gd[l + jb.fs] = std::exp(-(double)(l * l) / s2); sum += gd[l + jb.fs]; }
+            for (int l = 0; l < kMaxTaps; l++) g.push_back(l < 2 * jb.fs + 1 ? (T)(gd[l] / sum) : (T)0);
+        }
+        typename Plan<T, S>::PyrLevelDesc d;
+        d.jobs_off = P.put(jobs); d.n_jobs = (int)jobs.size();
+        d.src_tiles_off = P.put(st); d.n_src = (int)st.size();
+        d.dst_tiles_off = P.put(dt); d.n_dst = (int)dt.size();
+        d.g_off = P.put(g);
+        P.pyr.push_back(d);
+    }
+
+    // level steps
+    for (int sidx = 0; sidx < P.Lmax; sidx++) {
+        const int k = P.Lmax - 1 - sidx;
+        std::vector<LevelItem<T, S>> items;
+        std::vector<Tile> lt, stt;
+        for (int p = 0; p < P.n; p++) {
+            if (k >= P.L[p]) continue;
+            const auto& s = P.shapes[p];
+            const LevelMem& m = mem[p][k];
+            LevelItem<T, S> it;
+            std::memset(&it, 0, sizeof(it));
+            it.W = s.w[k]; it.H = s.h[k];
+            it.level = k;
+            it.allow_early = (k < P.L[p] - 1) ? 1 : 0;
+            it.est_init = P.est_flag[p];
+            // getDownsizedCamParams (sceneFlowMultiscale.cpp:16-27): f *= W_k / xRes, in float
+            const double sf = (double)s.w[k] / pairs[p].xres_full;
+            it.f_level = (T)(float)(pairs[p].f_full * sf);
+            if (P.kind == 2) { it.allow_early = pairs[p].allow_early; it.f_level = (T)pairs[p].f_level; }
+            it.ctl = (PairCtl*)(P.ctl_off + sizeof(PairCtl) * p);
+            for (int c = 0; c < 10; c++) it.pyr[c] = (T*)m.pyr[c];
+            for (int c = 0; c < 5; c++) { it.I1[c] = (S*)m.I1[c]; it.I2[c] = (S*)m.I2[c]; }
+            it.D1 = (S*)m.D1; it.D2 = (S*)m.D2;
+            it.mag = (T*)m.mag; it.rh = (T*)m.rh; it.rv = (T*)m.rv;
+            for (int c = 0; c < 3; c++) it.u[c] = (T*)m.u[c];
+            for (int b = 0; b < 2; b++) for (int c = 0; c < 3; c++) it.x[b][c] = (T*)m.x[b][c];
+            for (int c = 0; c < 12; c++) it.sys[c] = (T*)m.sys[c];
+            it.stat_part = (T*)m.stat;
+            it.n_sor_tiles = m.nsor;
+            if (k + 1 < P.L[p] && !P.est_flag[p]) {
+                for (int c = 0; c < 3; c++) it.uc[c] = (const T*)mem[p][k + 1].u[c];
+                it.Wc = s.w[k + 1]; it.Hc = s.h[k + 1];
+            }
+            it.inv_ratio = (T)(1 / hp.ratio);
+            it.xres_full = (int)pairs[p].xres_full;
+            it.f_full = (T)pairs[p].f_full;
+            const int iid = (int)items.size();
+            it.lin_tiles_x = (it.W + LTW - 1) / LTW;
+            it.lin_tile0 = (int)lt.size();
+            const int lty = (it.H + LTH - 1) / LTH;
+            for (int y = 0; y < lty; y++)
+                for (int x = 0; x < it.lin_tiles_x; x++) lt.push_back(Tile{iid, x, y, y * it.lin_tiles_x + x});
+            it.sor_tiles_x = (it.W + STW - 1) / STW;
+            it.sor_tile0 = (int)stt.size();
+            const int sty = (it.H + STH - 1) / STH;
+            for (int y = 0; y < sty; y++)
+                for (int x = 0; x < it.sor_tiles_x; x++) stt.push_back(Tile{iid, x, y, y * it.sor_tiles_x + x});
+            items.push_back(it);
+        }
+        typename Plan<T, S>::StepDesc d;
+        d.items_off = P.put(items); d.n_items = (int)items.size();
+        d.lin_tiles_off = P.put(lt); d.n_lin = (int)lt.size();
+        d.sor_tiles_off = P.put(stt); d.n_sor = (int)stt.size();
+        P.steps.push_back(d);
+    }
+    // output pointers (one per pair, in the order of the finest step's items = pair order)
+    std::vector<T*> outs;
+    for (int p = 0; p < P.n; p++) outs.push_back((T*)P.out_pair_off[p]);
+    P.out_ptrs_off = P.put(outs);
+    std::vector<EstSrc> est(P.n);
+    std::vector<SeamSrc> seam(P.n);
+    for (int p = 0; p < P.n; p++) {
+        const std::vector<size_t>& sg = P.in_seg[p];
+        est[p].f = nullptr; est[p].d = nullptr;
+        if (P.kind == 0 && pairs[p].est) est[p].f = (const float*)sg[4];
+        if (P.kind == 1 && pairs[p].est_d) est[p].d = (const double*)sg[5];
+        std::memset(&seam[p], 0, sizeof(SeamSrc));
+        if (P.kind == 2) {
+            seam[p].im1 = (const double*)sg[0]; seam[p].im2 = (const double*)sg[1];
+            seam[p].dm1 = (const double*)sg[2]; seam[p].dm2 = (const double*)sg[3];
+            seam[p].uvw = (const double*)sg[4];
+            seam[p].ddw = (const double*)sg[5]; seam[p].dsw = (const double*)sg[6]; seam[p].mag = (const double*)sg[7];
+            seam[p].regw = (const double*)sg[8];
+        }
+    }
+    P.est_src_off = P.put(est);
+    P.seam_src_off = P.put(seam);
+
+    // SOR schedule per inner iteration
+    int cur = 0;
+    for (int hh = 0; hh < hp.n_inner; hh++) {
+        int nc = 0;
+        P.sor_sched.push_back(sor_schedule(hp.n_sor, hp.K, hp.period, hp.fixed, hh == 0, hh == hp.n_inner - 1, cur, nc));
+        P.n_checks.push_back(nc);
+    }
+    P.desc_off = align_up(P.arena_bytes, 256);
+    P.desc_bytes = P.desc.size();
+    P.arena_bytes = P.desc_off + P.desc_bytes;
+    return P;
+}
+
+// Rebase every pointer field of the descriptors from an arena offset to base + offset.
+template <class X> static inline void rebase(X*& p, char* base) { p = (X*)(base + (size_t)p); }
+template <class X> static inline void rebase_nz(X*& p, char* base) { if (p) p = (X*)(base + (size_t)p); }
+
+template <class T, class S>
+static void bind_plan(Plan<T, S>& P, char* base)
+{
+    unsigned char* d = P.desc.data();
+    {
+        PrepItem<T>* it = (PrepItem<T>*)(d + P.prep_items_off);
+        for (int p = 0; p < P.n; p++) {
+            for (int f = 0; f < 2; f++) {
+                rebase_nz(it[p].bgr[f], base); rebase_nz(it[p].depth[f], base);
+                rebase_nz(it[p].im_d[f], base); rebase_nz(it[p].dep_d[f], base);
+                for (int c = 0; c < 3; c++) rebase(it[p].col[f][c], base);
+                rebase(it[p].dep[f], base); rebase(it[p].stamp[f], base);
+            }
+            rebase_nz(it[p].sigma_in, base);
+            rebase(it[p].bmask, base); rebase(it[p].ddw, base); rebase(it[p].dsw, base); rebase(it[p].unfilled, base);
+        }
+    }
+    for (auto& lv : P.pyr) {
+        PyrJob<T>* jb = (PyrJob<T>*)(d + lv.jobs_off);
+        for (int j = 0; j < lv.n_jobs; j++)
+            for (int c = 0; c < 10; c++) { rebase(jb[j].src[c], base); rebase(jb[j].tmp[c], base); rebase(jb[j].dst[c], base); }
+    }
+    for (auto& st : P.steps) {
+        LevelItem<T, S>* it = (LevelItem<T, S>*)(d + st.items_off);
+        for (int i = 0; i < st.n_items; i++) {
+            LevelItem<T, S>& x = it[i];
+            rebase(x.ctl, base);
+            for (int c = 0; c < 10; c++) rebase(x.pyr[c], base);
+            for (int c = 0; c < 5; c++) { rebase(x.I1[c], base); rebase(x.I2[c], base); }
+            rebase(x.D1, base); rebase(x.D2, base);
+            rebase(x.mag, base); rebase(x.rh, base); rebase(x.rv, base);
+            for (int c = 0; c < 3; c++) rebase(x.u[c], base);
+            for (int b = 0; b < 2; b++) for (int c = 0; c < 3; c++) rebase(x.x[b][c], base);
+            for (int c = 0; c < 12; c++) rebase(x.sys[c], base);
+            rebase(x.stat_part, base);
+            for (int c = 0; c < 3; c++) rebase_nz(x.uc[c], base);
+        }
+    }
+    T** outs = (T**)(d + P.out_ptrs_off);
+    for (int p = 0; p < P.n; p++) rebase(outs[p], base);
+    EstSrc* est = (EstSrc*)(d + P.est_src_off);
+    SeamSrc* seam = (SeamSrc*)(d + P.seam_src_off);
+    for (int p = 0; p < P.n; p++) {
+        rebase_nz(est[p].f, base); rebase_nz(est[p].d, base);
+        rebase_nz(seam[p].im1, base); rebase_nz(seam[p].im2, base); rebase_nz(seam[p].dm1, base);
+        rebase_nz(seam[p].dm2, base); rebase_nz(seam[p].uvw, base); rebase_nz(seam[p].ddw, base);
+        rebase_nz(seam[p].dsw, base); rebase_nz(seam[p].mag, base); rebase_nz(seam[p].regw, base);
+    }
+}
+
+template <class T>
+static SolveConst<T> solve_const(const HostParams& hp)
+{
+    SolveConst<T> k;
+    k.alpha = (T)hp.alpha; k.gamma = (T)hp.gamma; k.color_w = (T)hp.color_w;
+    k.eps_d = (T)hp.eps_d; k.eps_z = (T)hp.eps_z; k.eps_s = (T)hp.eps_s;
+    k.omega = (T)hp.omega; k.step = (T)hp.step;
+    k.occ_margin = (T)hp.occ_margin; k.occ_penalty = (T)hp.occ_penalty; k.max_grad = (T)hp.max_grad;
+    k.sor_tol = hp.sor_tol; k.outer_tol = hp.outer_tol;
+    k.fixed = hp.fixed; k.n_sor = hp.n_sor;
+    return k;
+}
+
+// ------------------------------------------------------------------------------------------
+// kernel launch helpers
+
+template <class T, class S, int K>
+static void launch_sor_k(const LevelItem<T, S>* items, const Tile* tiles, int n, const SolveConst<T>& k,
+                         const SorLaunch& L, cudaStream_t st)
+{
+    constexpr size_t sm = sor_smem_bytes<T, K>();
+    k_sor<T, S, K><<<n, SorGeom<K>::NT, sm, st>>>(items, tiles, k, L);
+}
+
+template <class T, class S>
+static void launch_sor(int K, const LevelItem<T, S>* items, const Tile* tiles, int n, const SolveConst<T>& k,
+                       const SorLaunch& L, cudaStream_t st)
+{
+    switch (K) {
+    case 1: launch_sor_k<T, S, 1>(items, tiles, n, k, L, st); break;
+    case 2: launch_sor_k<T, S, 2>(items, tiles, n, k, L, st); break;
+    case 3: launch_sor_k<T, S, 3>(items, tiles, n, k, L, st); break;
+    case 4: launch_sor_k<T, S, 4>(items, tiles, n, k, L, st); break;
+    default: launch_sor_k<T, S, 5>(items, tiles, n, k, L, st); break;
+    }
+}
+
+template <class T, class S>
+static void set_kernel_attrs()
+{
+    RF_CUDA(cudaFuncSetAttribute(k_linearize<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lin_smem_bytes<T>()));
+    RF_CUDA(cudaFuncSetAttribute(k_sor<T, S, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sor_smem_bytes<T, 1>()));
+    RF_CUDA(cudaFuncSetAttribute(k_sor<T, S, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sor_smem_bytes<T, 2>()));
+    RF_CUDA(cudaFuncSetAttribute(k_sor<T, S, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sor_smem_bytes<T, 3>()));
+    RF_CUDA(cudaFuncSetAttribute(k_sor<T, S, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sor_smem_bytes<T, 4>()));
+    RF_CUDA(cudaFuncSetAttribute(k_sor<T, S, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sor_smem_bytes<T, 5>()));
+}
+
+// The level loop of one step (sceneFlowSingleScale's outer / inner / SOR structure, .cu:755-954).
+template <class T, class S>
+static int enqueue_level(const Plan<T, S>& P, char* base, int sidx, cudaStream_t st, int setup)
+{
+    const auto& d = P.steps[sidx];
+    if (d.n_items == 0) return 0;
+    int launches = 0;
+    const LevelItem<T, S>* items = (const LevelItem<T, S>*)(base + P.desc_off + d.items_off);
+    const Tile* lt = (const Tile*)(base + P.desc_off + d.lin_tiles_off);
+    const Tile* stt = (const Tile*)(base + P.desc_off + d.sor_tiles_off);
+    const SolveConst<T> k = solve_const<T>(P.hp);
+    if (setup) {
+        k_level_setup<T, S><<<d.n_lin, LTW * LTH, 0, st>>>(items, lt, P.hp.regularization);
+        launches++;
+    }
+    for (int outer = 0; outer < P.hp.n_outer; outer++) {
+        for (int hh = 0; hh < P.hp.n_inner; hh++) {
+            const auto& sched = P.sor_sched[hh];
+            // inner iterations after the first read the running increment (x of the previous SOR)
+            const int xsel = sched.front().xin;
+            k_linearize<T, S><<<d.n_lin, LTW * LTH, lin_smem_bytes<T>(), st>>>(items, lt, k, hh > 0, xsel);
+            launches++;
+            for (SorLaunch L : sched) {
+                L.outer = outer;
+                launch_sor<T, S>(P.hp.K, items, stt, d.n_sor, k, L, st);
+                launches++;
+            }
+        }
+        const int wpb = 4;
+        k_control<T, S><<<(d.n_items + wpb - 1) / wpb, 32 * wpb, 0, st>>>(items, d.n_items, k, outer,
+                                                                          P.n_checks.empty() ? 0 : P.n_checks.back());
+        launches++;
+    }
+    return launches;
+}
+
+// Whole solve after the inputs are resident: preprocessing, hole fill, pyramids, levels, output.
+template <class T, class S>
+static int enqueue_solve(const Plan<T, S>& P, char* base, cudaStream_t st)
+{
+    int launches = 0;
+    char* db = base + P.desc_off;
+    RF_CUDA(cudaMemsetAsync(base + P.ctl_off, 0, sizeof(PairCtl) * P.n, st));
+    const auto& fin = P.steps.back();
+    const LevelItem<T, S>* fin_items = (const LevelItem<T, S>*)(db + fin.items_off);
+    const Tile* fin_tiles = (const Tile*)(db + fin.lin_tiles_off);
+    if (P.kind == 2) {
+        k_seam_load<T, S><<<fin.n_lin, LTW * LTH, 0, st>>>(fin_items, fin_tiles, (const SeamSrc*)(db + P.seam_src_off));
+        launches++;
+        launches += enqueue_level(P, base, P.Lmax - 1, st, 0);
+        k_warp_out<T, S><<<fin.n_lin, LTW * LTH, 0, st>>>(fin_items, fin_tiles, (T* const*)(db + P.out_ptrs_off));
+        launches++;
+    } else {
+        RF_CUDA(cudaMemsetAsync(base + P.unfilled_off, 0, sizeof(int) * 256 * P.n, st));
+        const PrepItem<T>* prep = (const PrepItem<T>*)(db + P.prep_items_off);
+        const Tile* pt = (const Tile*)(db + P.prep_tiles_off);
+        k_prep<T><<<P.n_prep_tiles, LTW * LTH, 0, st>>>(prep, pt);
+        k_sigma<T><<<P.n_prep_tiles, LTW * LTH, 0, st>>>(prep, pt);
+        launches += 2;
+        if (P.hp.fill_holes)
+            for (int r = 1; r <= P.hp.fill_rounds; r++) {
+                k_fill_round<T><<<P.n_prep_tiles, LTW * LTH, 0, st>>>(prep, pt, r);
+                launches++;
+            }
+        for (const auto& lv : P.pyr) {
+            const PyrJob<T>* jobs = (const PyrJob<T>*)(db + lv.jobs_off);
+            const T* g = (const T*)(db + lv.g_off);
+            k_hfilter<T><<<lv.n_src, LTW * LTH, 0, st>>>(jobs, (const Tile*)(db + lv.src_tiles_off), g);
+            k_vresize<T><<<lv.n_dst, LTW * LTH, 0, st>>>(jobs, (const Tile*)(db + lv.dst_tiles_off), g);
+            launches += 2;
+        }
+        if (P.any_warm) {
+            k_load_est<T, S><<<fin.n_lin, LTW * LTH, 0, st>>>(fin_items, fin_tiles, (const EstSrc*)(db + P.est_src_off));
+            launches++;
+        }
+        for (int s = 0; s < P.Lmax; s++) launches += enqueue_level(P, base, s, st, 1);
+    }
+    k_output<T, S><<<fin.n_lin, LTW * LTH, 0, st>>>(fin_items, fin_tiles, (T* const*)(db + P.out_ptrs_off));
+    launches++;
+    RF_CUDA(cudaGetLastError());
+    return launches;
+}
+
+}  // namespace rgbdflow

@@ -1,0 +1,507 @@
+// rgbdflow.cu — C ABI (include/rgbdflow.h) over the sm_100a scene-flow pipeline.
+//
+// Host orchestration is C++; every arithmetic step of the solve runs in the kernels of
+// kernels.cuh.  There is no CPU fallback: without a CUDA device every entry point that computes
+// returns RGBDFLOW_ERR_NO_DEVICE.
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/rgbdflow.h"
+#include "pipeline.cuh"
+
+using namespace rgbdflow;
+
+struct GraphEntry {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int launches = 0;
+};
+
+struct rgbdflow_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    size_t budget = 0;
+    std::string err;
+    char* arena = nullptr;
+    size_t arena_cap = 0;
+    char* pin = nullptr;
+    size_t pin_cap = 0;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    std::map<std::string, GraphEntry> graphs;
+    bool attrs[4] = {false, false, false, false};
+    int last_launches = 0;
+    bool use_graphs = true;
+};
+
+namespace {
+
+void drop_graphs(rgbdflow_ctx* c)
+{
+    for (auto& kv : c->graphs) {
+        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+        if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
+    }
+    c->graphs.clear();
+}
+
+void ensure_arena(rgbdflow_ctx* c, size_t need)
+{
+    if (c->arena_cap >= need) return;
+    if (c->budget && need > c->budget)
+        throw ArgError(RGBDFLOW_ERR_BUDGET, "request needs " + std::to_string(need) + " device bytes, budget is " +
+                                                std::to_string(c->budget));
+    RF_CUDA(cudaStreamSynchronize(c->stream));
+    drop_graphs(c);  // graphs hold arena addresses
+    if (c->arena) RF_CUDA(cudaFree(c->arena));
+    c->arena = nullptr;
+    c->arena_cap = 0;
+    const size_t cap = align_up(need + need / 8, 1 << 20);
+    const size_t want = (c->budget && cap > c->budget) ? need : cap;
+    RF_CUDA(cudaMalloc(&c->arena, want));
+    c->arena_cap = want;
+}
+
+void ensure_pin(rgbdflow_ctx* c, size_t need)
+{
+    if (c->pin_cap >= need) return;
+    RF_CUDA(cudaStreamSynchronize(c->stream));
+    if (c->pin) RF_CUDA(cudaFreeHost(c->pin));
+    c->pin = nullptr;
+    const size_t cap = align_up(need + need / 8, 1 << 20);
+    RF_CUDA(cudaMallocHost(&c->pin, cap));
+    c->pin_cap = cap;
+}
+
+HostParams host_params(const rgbdflow_params& p)
+{
+    HostParams h;
+    h.regularization = p.regularization;
+    h.color_w = p.color_data_weight; h.dvc = p.depth_vs_color_data_weight;
+    h.alpha = p.alpha; h.gamma = p.gamma; h.ratio = p.pyramid_ratio;
+    h.min_width = p.min_width; h.n_outer = p.n_outer; h.n_inner = p.n_inner; h.n_sor = p.n_sor;
+    h.max_dist = p.depth_boundary_dist; h.fill_holes = p.fill_holes; h.fixed = p.fixed_schedule;
+    h.omega = p.omega; h.step = p.max_flow_step; h.eps_d = p.eps_d; h.eps_z = p.eps_z; h.eps_s = p.eps_s;
+    h.sor_tol = p.sor_tol; h.outer_tol = p.outer_tol; h.occ_margin = p.occ_margin; h.occ_penalty = p.occ_penalty;
+    h.max_grad = p.max_depth_grad;
+    h.period = p.sor_check_period > 0 ? p.sor_check_period : 25;
+    int K = p.sweeps_per_launch;
+    if (K <= 0) K = (p.compute == RGBDFLOW_COMPUTE_FP64) ? 2 : 5;
+    if (K > 5) K = 5;
+    if (p.compute == RGBDFLOW_COMPUTE_FP64 && K > 2) K = 2;
+    h.K = K;
+    h.fill_rounds = 64;
+    return h;
+}
+
+void validate(const rgbdflow_params* p)
+{
+    if (!p) throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "params is NULL");
+    if (p->regularization == RGBDFLOW_REG_HPB)
+        throw ArgError(RGBDFLOW_ERR_UNSUPPORTED,
+                       "HPB regularisation (heuristic probability of boundary) is not built; use ISOTROPIC or LETOUZEY");
+    if (p->regularization != RGBDFLOW_REG_ISOTROPIC && p->regularization != RGBDFLOW_REG_LETOUZEY)
+        throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "unknown regularisation type");
+    if (p->n_outer < 0 || p->n_inner < 1 || p->n_sor < 0) throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "bad iteration counts");
+    if (p->n_outer > 64) throw ArgError(RGBDFLOW_ERR_UNSUPPORTED, "n_outer > 64");
+    const int period = p->sor_check_period > 0 ? p->sor_check_period : 25;
+    if (!p->fixed_schedule && p->n_sor / period > kMaxChecks)
+        throw ArgError(RGBDFLOW_ERR_UNSUPPORTED, "more than 512 SOR convergence checks per inner iteration");
+    if (p->storage < 0 || p->storage > 2) throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "bad storage type");
+    if (p->compute == RGBDFLOW_COMPUTE_FP64 && p->storage != RGBDFLOW_STORE_FP32)
+        throw ArgError(RGBDFLOW_ERR_UNSUPPORTED, "the FP64 device solve stores its pyramids in FP64");
+    if (p->min_width < 1) throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "min_width < 1");
+}
+
+// getResizedCamParams (runFlowTwoFrames.cpp:14-24)
+void resized_cam(const rgbdflow_camera_params& c, int W, float& f, unsigned& xres)
+{
+    const double sf = (double)W / c.xRes;
+    xres = (unsigned)std::rint(c.xRes * sf);
+    f = (float)(c.focalLength * sf);
+}
+
+std::string plan_key(const std::vector<PairSpec>& ps, const HostParams& hp, int tag)
+{
+    std::string k = std::to_string(tag) + ":";
+    for (const auto& p : ps)
+        k += std::to_string(p.kind) + "k" + std::to_string(p.W) + "x" + std::to_string(p.H) + (p.warm() ? "e" : "") +
+             (p.kind == 2 ? "a" + std::to_string(p.allow_early) + "g" + std::to_string(p.f_level) : std::string()) + "f" + std::to_string(p.f_full) +
+             "r" + std::to_string(p.xres_full) + ",";
+    char buf[512];
+    std::snprintf(buf, sizeof buf, "|%d %.17g %.17g %.17g %.17g %.17g %d %d %d %d %d %d %d %.17g %.17g %.17g %.17g %.17g %.17g %.17g %.17g %.17g %.17g %d %d %d",
+                  hp.regularization, hp.color_w, hp.dvc, hp.alpha, hp.gamma, hp.ratio, hp.min_width, hp.n_outer, hp.n_inner,
+                  hp.n_sor, hp.max_dist, hp.fill_holes, hp.fixed, hp.omega, hp.step, hp.eps_d, hp.eps_z, hp.eps_s,
+                  hp.sor_tol, hp.outer_tol, hp.occ_margin, hp.occ_penalty, hp.max_grad, hp.period, hp.K, hp.fill_rounds);
+    return k + buf;
+}
+
+void fill_stats(const PairCtl& c, int L, const PyrShape& s, double ms, rgbdflow_stats* st)
+{
+    std::memset(st, 0, sizeof(*st));
+    st->n_levels = L;
+    for (int k = 0; k < L && k < RGBDFLOW_MAX_LEVELS; k++) {
+        st->level_w[k] = s.w[k];
+        st->level_h[k] = s.h[k];
+        st->outer_iters[k] = c.outer_exec[k];
+        for (int o = 0; o < RGBDFLOW_MAX_OUTER; o++) {
+            const bool ran = o < c.outer_exec[k];
+            st->sor_iters[k][o] = ran ? c.sor_exec[k][o] : 0;
+            st->outer_stat[k][o] = ran ? c.stat[k][o] : -1.0f;
+            st->sor_maxdiff[k][o] = ran ? c.sor_maxdiff[k][o] : -1.0f;
+        }
+    }
+    st->device_ms = ms;
+}
+
+template <class T, class S>
+void ensure_attrs(rgbdflow_ctx* c, int slot)
+{
+    if (c->attrs[slot]) return;
+    set_kernel_attrs<T, S>();
+    c->attrs[slot] = true;
+}
+
+// Runs a batch of host-buffer pairs through one graph launch.  stats: null or n entries.
+template <class T, class S>
+void run_batch(rgbdflow_ctx* c, const std::vector<PairSpec>& pairs, const HostParams& hp, rgbdflow_stats* stats, int slot)
+{
+    ensure_attrs<T, S>(c, slot);
+    Plan<T, S> P = make_plan<T, S>(pairs, hp);
+    ensure_arena(c, P.arena_bytes);
+    bind_plan(P, c->arena);
+    const size_t ctl_bytes = sizeof(PairCtl) * P.n;
+    const size_t pin_need = align_up(P.in_bytes, 256) + align_up(P.desc_bytes, 256) + align_up(P.out_bytes, 256) + ctl_bytes;
+    ensure_pin(c, pin_need);
+    char* pin_in = c->pin;
+    char* pin_desc = pin_in + align_up(P.in_bytes, 256);
+    char* pin_out = pin_desc + align_up(P.desc_bytes, 256);
+    char* pin_ctl = pin_out + align_up(P.out_bytes, 256);
+    for (int p = 0; p < P.n; p++) {
+        const auto segs = pairs[p].inputs();
+        for (size_t q = 0; q < segs.size(); q++) {
+            if (!segs[q].first) throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "pair " + std::to_string(p) + ": null input buffer");
+            std::memcpy(pin_in + (P.in_seg[p][q] - P.in_off), segs[q].first, segs[q].second);
+        }
+    }
+    std::memcpy(pin_desc, P.desc.data(), P.desc_bytes);
+    cudaStream_t st = c->stream;
+    RF_CUDA(cudaMemcpyAsync(c->arena + P.in_off, pin_in, P.in_bytes, cudaMemcpyHostToDevice, st));
+    RF_CUDA(cudaMemcpyAsync(c->arena + P.desc_off, pin_desc, P.desc_bytes, cudaMemcpyHostToDevice, st));
+    RF_CUDA(cudaEventRecord(c->e0, st));
+    const std::string key = plan_key(pairs, hp, slot);
+    auto it = c->graphs.find(key);
+    if (c->use_graphs && it == c->graphs.end()) {
+        GraphEntry g;
+        RF_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        int launches = 0;
+        try {
+            launches = enqueue_solve(P, c->arena, st);
+        } catch (...) {
+            cudaGraph_t tmp;
+            cudaStreamEndCapture(st, &tmp);
+            if (tmp) cudaGraphDestroy(tmp);
+            throw;
+        }
+        RF_CUDA(cudaStreamEndCapture(st, &g.graph));
+        RF_CUDA(cudaGraphInstantiate(&g.exec, g.graph, 0));
+        g.launches = launches;
+        if (c->graphs.size() > 32) drop_graphs(c);
+        it = c->graphs.emplace(key, g).first;
+    }
+    if (c->use_graphs) {
+        RF_CUDA(cudaGraphLaunch(it->second.exec, st));
+        c->last_launches = it->second.launches;
+    } else {
+        c->last_launches = enqueue_solve(P, c->arena, st);
+    }
+    RF_CUDA(cudaEventRecord(c->e1, st));
+    RF_CUDA(cudaMemcpyAsync(pin_out, c->arena + P.out_off, P.out_bytes, cudaMemcpyDeviceToHost, st));
+    if (stats) RF_CUDA(cudaMemcpyAsync(pin_ctl, c->arena + P.ctl_off, ctl_bytes, cudaMemcpyDeviceToHost, st));
+    RF_CUDA(cudaStreamSynchronize(st));
+    float ms = 0;
+    RF_CUDA(cudaEventElapsedTime(&ms, c->e0, c->e1));
+    for (int p = 0; p < P.n; p++) {
+        const size_t N = (size_t)pairs[p].W * pairs[p].H;
+        const T* o = (const T*)(pin_out + (P.out_pair_off[p] - P.out_off));
+        const PairSpec& q = pairs[p];
+        if (q.out)
+            for (size_t z = 0; z < N * 3; z++) q.out[z] = (float)o[z];
+        if (q.out_u)
+            for (size_t z = 0; z < N; z++) { q.out_u[z] = (double)o[z * 3]; q.out_v[z] = (double)o[z * 3 + 1]; q.out_w[z] = (double)o[z * 3 + 2]; }
+        if (q.out_warpI)
+            for (size_t z = 0; z < N * 5; z++) q.out_warpI[z] = (double)o[N * 3 + z];
+        if (q.out_warpD)
+            for (size_t z = 0; z < N; z++) q.out_warpD[z] = (double)o[N * 8 + z];
+    }
+    if (stats)
+        for (int p = 0; p < P.n; p++) fill_stats(((PairCtl*)pin_ctl)[p], P.L[p], P.shapes[p], ms, &stats[p]);
+}
+
+}  // namespace
+
+
+static void dispatch(rgbdflow_ctx* c, const std::vector<PairSpec>& ps, const rgbdflow_params& p, rgbdflow_stats* stats)
+{
+    const HostParams hp = host_params(p);
+    if (p.compute == RGBDFLOW_COMPUTE_FP64) run_batch<double, double>(c, ps, hp, stats, 1);
+    else if (p.storage == RGBDFLOW_STORE_FP16) run_batch<float, __half>(c, ps, hp, stats, 2);
+    else if (p.storage == RGBDFLOW_STORE_BF16) run_batch<float, __nv_bfloat16>(c, ps, hp, stats, 3);
+    else run_batch<float, float>(c, ps, hp, stats, 0);
+}
+
+static int fail(rgbdflow_ctx* c, int code, const std::string& m)
+{
+    if (c) c->err = m;
+    return code;
+}
+
+#define API_BEGIN try {
+#define API_END(ctx)                                                                        \
+    }                                                                                        \
+    catch (const ArgError& e) { return fail(ctx, e.code, e.what()); }                        \
+    catch (const CudaError& e) { return fail(ctx, RGBDFLOW_ERR_CUDA, e.what()); }            \
+    catch (const std::bad_alloc&) { return fail(ctx, RGBDFLOW_ERR_INTERNAL, "host out of memory"); } \
+    catch (const std::exception& e) { return fail(ctx, RGBDFLOW_ERR_INTERNAL, e.what()); }   \
+    catch (...) { return fail(ctx, RGBDFLOW_ERR_INTERNAL, "unknown error"); }
+
+extern "C" {
+
+void rgbdflow_params_default(rgbdflow_params* p)
+{
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->regularization = RGBDFLOW_REG_HPB;
+    p->color_data_weight = 1;
+    p->depth_vs_color_data_weight = 1;
+    p->alpha = 0.02;
+    p->gamma = 1e-5;
+    p->pyramid_ratio = 0.75;
+    p->min_width = 60;
+    p->n_outer = 50;
+    p->n_inner = 1;
+    p->n_sor = 10000;
+    p->depth_boundary_dist = 4;
+    p->fill_holes = 1;
+    p->fixed_schedule = 0;
+    p->storage = RGBDFLOW_STORE_FP32;
+    p->compute = RGBDFLOW_COMPUTE_FP32;
+    p->omega = 0.7;
+    p->max_flow_step = 0.3;
+    p->eps_d = 1e-6;
+    p->eps_z = 1e-10;
+    p->eps_s = 1e-6;
+    p->sor_tol = 1e-5;
+    p->sor_check_period = 25;
+    p->outer_tol = 4e-4;
+    p->occ_margin = 0.02;
+    p->occ_penalty = 0.01;
+    p->max_depth_grad = 0.04;
+    p->sweeps_per_launch = 0;
+}
+
+int rgbdflow_abi_version(void) { return RGBDFLOW_ABI_VERSION; }
+
+int rgbdflow_ctx_create(int device, size_t hbm_budget_bytes, rgbdflow_ctx** out)
+{
+    if (!out) return RGBDFLOW_ERR_INVALID_ARG;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) { cudaGetLastError(); return RGBDFLOW_ERR_NO_DEVICE; }
+    if (device < 0 || device >= n) return RGBDFLOW_ERR_INVALID_ARG;
+    std::unique_ptr<rgbdflow_ctx> c(new rgbdflow_ctx());
+    c->device = device;
+    c->budget = hbm_budget_bytes;
+    if (cudaSetDevice(device) != cudaSuccess) return RGBDFLOW_ERR_CUDA;
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return RGBDFLOW_ERR_CUDA;
+    if (cudaEventCreate(&c->e0) != cudaSuccess || cudaEventCreate(&c->e1) != cudaSuccess) return RGBDFLOW_ERR_CUDA;
+    const char* g = std::getenv("RGBDFLOW_NO_GRAPHS");
+    c->use_graphs = !(g && g[0] == '1');
+    *out = c.release();
+    return RGBDFLOW_OK;
+}
+
+int rgbdflow_ctx_destroy(rgbdflow_ctx* c)
+{
+    if (!c) return RGBDFLOW_ERR_INVALID_ARG;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    drop_graphs(c);
+    if (c->arena) cudaFree(c->arena);
+    if (c->pin) cudaFreeHost(c->pin);
+    if (c->e0) cudaEventDestroy(c->e0);
+    if (c->e1) cudaEventDestroy(c->e1);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return RGBDFLOW_OK;
+}
+
+const char* rgbdflow_last_error(const rgbdflow_ctx* c) { return c ? c->err.c_str() : "no context"; }
+
+size_t rgbdflow_ctx_device_bytes(const rgbdflow_ctx* c) { return c ? c->arena_cap : 0; }
+
+int rgbdflow_scene_flow_batch(rgbdflow_ctx* c, const rgbdflow_pair* pairs, int n, const rgbdflow_params* params,
+                              rgbdflow_stats* stats)
+{
+    if (!c) return RGBDFLOW_ERR_INVALID_ARG;
+    API_BEGIN
+    validate(params);
+    if (!pairs || n <= 0) throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "no pairs");
+    RF_CUDA(cudaSetDevice(c->device));
+    std::vector<PairSpec> ps;
+    for (int i = 0; i < n; i++) {
+        const rgbdflow_pair& q = pairs[i];
+        if (q.W < 2 || q.H < 2 || !q.bgr1 || !q.bgr2 || !q.depth1_m || !q.depth2_m || !q.flow_out)
+            throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "pair " + std::to_string(i) + ": bad size or null buffer");
+        if (q.cam.xRes == 0 || !(q.cam.focalLength > 0))
+            throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "pair " + std::to_string(i) + ": bad camera");
+        PairSpec s;
+        s.W = q.W; s.H = q.H;
+        resized_cam(q.cam, q.W, s.f_full, s.xres_full);
+        s.bgr1 = q.bgr1; s.depth1 = q.depth1_m; s.bgr2 = q.bgr2; s.depth2 = q.depth2_m;
+        s.est = q.est_flow; s.out = q.flow_out;
+        ps.push_back(s);
+    }
+    dispatch(c, ps, *params, stats);
+    return RGBDFLOW_OK;
+    API_END(c)
+}
+
+int rgbdflow_scene_flow_two_frames(rgbdflow_ctx* c, const rgbdflow_camera_params* cam, const uint8_t* bgr1,
+                                   const float* depth1_m, const uint8_t* bgr2, const float* depth2_m, int W, int H,
+                                   const rgbdflow_params* params, const float* est_flow, float* flow_out,
+                                   rgbdflow_stats* stats)
+{
+    if (!c) return RGBDFLOW_ERR_INVALID_ARG;
+    if (!cam) return fail(c, RGBDFLOW_ERR_INVALID_ARG, "cam is NULL");
+    rgbdflow_pair p;
+    p.W = W; p.H = H; p.cam = *cam;
+    p.bgr1 = bgr1; p.depth1_m = depth1_m; p.bgr2 = bgr2; p.depth2_m = depth2_m;
+    p.est_flow = est_flow; p.flow_out = flow_out;
+    return rgbdflow_scene_flow_batch(c, &p, 1, params, stats);
+}
+
+int rgbdflow_scene_flow_multiscale(rgbdflow_ctx* c, const rgbdflow_camera_params* cam, const double* Im1,
+                                   const double* dm1, const double* Im2, const double* dm2, const float* depth_sigma1,
+                                   int W, int H, const rgbdflow_params* params, double* u, double* v, double* w,
+                                   rgbdflow_stats* stats)
+{
+    if (!c) return RGBDFLOW_ERR_INVALID_ARG;
+    API_BEGIN
+    validate(params);
+    if (!cam || !Im1 || !dm1 || !Im2 || !dm2 || !depth_sigma1 || !u || !v || !w || W < 2 || H < 2)
+        throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "null buffer or bad size");
+    RF_CUDA(cudaSetDevice(c->device));
+    PairSpec s;
+    s.kind = 1; s.W = W; s.H = H;
+    resized_cam(*cam, W, s.f_full, s.xres_full);
+    s.im1 = Im1; s.im2 = Im2; s.dm1 = dm1; s.dm2 = dm2; s.sigma1 = depth_sigma1;
+    s.out_u = u; s.out_v = v; s.out_w = w;
+    dispatch(c, {s}, *params, stats);
+    return RGBDFLOW_OK;
+    API_END(c)
+}
+
+int rgbdflow_scene_flow_with_init(rgbdflow_ctx* c, const rgbdflow_camera_params* cam, const double* Im1,
+                                  const double* dm1, const double* Im2, const double* dm2, const float* depth_sigma1,
+                                  int W, int H, const rgbdflow_params* params, double* u, double* v, double* w,
+                                  rgbdflow_stats* stats)
+{
+    if (!c) return RGBDFLOW_ERR_INVALID_ARG;
+    API_BEGIN
+    validate(params);
+    if (!cam || !Im1 || !dm1 || !Im2 || !dm2 || !depth_sigma1 || !u || !v || !w || W < 2 || H < 2)
+        throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "null buffer or bad size");
+    RF_CUDA(cudaSetDevice(c->device));
+    const size_t N = (size_t)W * H;
+    std::vector<double> est(N * 3);
+    std::memcpy(est.data(), u, N * 8);
+    std::memcpy(est.data() + N, v, N * 8);
+    std::memcpy(est.data() + 2 * N, w, N * 8);
+    PairSpec s;
+    s.kind = 1; s.W = W; s.H = H;
+    resized_cam(*cam, W, s.f_full, s.xres_full);
+    s.im1 = Im1; s.im2 = Im2; s.dm1 = dm1; s.dm2 = dm2; s.sigma1 = depth_sigma1;
+    s.est_d = est.data();
+    s.out_u = u; s.out_v = v; s.out_w = w;
+    dispatch(c, {s}, *params, stats);
+    return RGBDFLOW_OK;
+    API_END(c)
+}
+
+int rgbdflow_scene_flow_single_scale(rgbdflow_ctx* c, const rgbdflow_camera_params* cam, const double* Im1,
+                                     const double* dm1, const double* Im2, const double* dm2, double* warpIm2,
+                                     double* warpDm2, double* u, double* v, double* w, int W, int H, int nCh,
+                                     double colorDataTermWeight, const double* depthDataTermWeights, double alpha,
+                                     const double* depthSmoothnessTermWeights, double gamma,
+                                     const double* depthMagTermWeights, const double* regularizationWeights,
+                                     int nOuterFPIterations, int nInnerFPIterations, int nSORIterations,
+                                     int allowEarlyTermination, const rgbdflow_params* params, rgbdflow_stats* stats)
+{
+    if (!c) return RGBDFLOW_ERR_INVALID_ARG;
+    API_BEGIN
+    if (nCh != 5) throw ArgError(RGBDFLOW_ERR_UNSUPPORTED, "the device solve takes the 5-channel RGB_WITH_GRADIENT features");
+    if (!cam || !Im1 || !dm1 || !Im2 || !dm2 || !u || !v || !w || !depthDataTermWeights || !depthSmoothnessTermWeights ||
+        !depthMagTermWeights || !regularizationWeights || W < 2 || H < 2)
+        throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "null buffer or bad size");
+    rgbdflow_params p;
+    if (params) p = *params; else rgbdflow_params_default(&p);
+    p.regularization = RGBDFLOW_REG_ISOTROPIC;  // weights are given explicitly
+    p.color_data_weight = colorDataTermWeight;
+    p.alpha = alpha;
+    p.gamma = gamma;
+    p.n_outer = nOuterFPIterations;
+    p.n_inner = nInnerFPIterations;
+    p.n_sor = nSORIterations;
+    validate(&p);
+    RF_CUDA(cudaSetDevice(c->device));
+    const size_t N = (size_t)W * H;
+    std::vector<double> uvw(N * 3);
+    std::memcpy(uvw.data(), u, N * 8);
+    std::memcpy(uvw.data() + N, v, N * 8);
+    std::memcpy(uvw.data() + 2 * N, w, N * 8);
+    PairSpec s;
+    s.kind = 2; s.W = W; s.H = H;
+    s.f_full = cam->focalLength; s.xres_full = (unsigned)W;
+    s.f_level = cam->focalLength;
+    s.allow_early = allowEarlyTermination ? 1 : 0;
+    s.feat1 = Im1; s.feat2 = Im2; s.dm1 = dm1; s.dm2 = dm2; s.uvw = uvw.data();
+    s.ddw = depthDataTermWeights; s.dsw = depthSmoothnessTermWeights; s.mag = depthMagTermWeights;
+    s.regw = regularizationWeights;
+    s.out_u = u; s.out_v = v; s.out_w = w;
+    s.out_warpI = warpIm2; s.out_warpD = warpDm2;
+    dispatch(c, {s}, p, stats);
+    return RGBDFLOW_OK;
+    API_END(c)
+}
+
+int rgbdflow_scene_flow_batch_async(rgbdflow_ctx* c, const rgbdflow_pair*, int, const rgbdflow_params*, void*)
+{
+    return fail(c, RGBDFLOW_ERR_UNSUPPORTED, "device-pointer batches are not built yet");
+}
+
+int rgbdflow_server_create(rgbdflow_ctx* c, const rgbdflow_server_config*, rgbdflow_server** out)
+{
+    if (out) *out = nullptr;
+    return fail(c, RGBDFLOW_ERR_UNSUPPORTED, "serving is not built yet");
+}
+int rgbdflow_server_destroy(rgbdflow_server*) { return RGBDFLOW_ERR_UNSUPPORTED; }
+int rgbdflow_server_submit(rgbdflow_server*, int, uint64_t, const rgbdflow_camera_params*, const uint8_t*, const float*,
+                           int, int, float*)
+{
+    return RGBDFLOW_ERR_UNSUPPORTED;
+}
+int rgbdflow_server_step(rgbdflow_server*, int, rgbdflow_result*, int, int* n)
+{
+    if (n) *n = 0;
+    return RGBDFLOW_ERR_UNSUPPORTED;
+}
+int rgbdflow_server_pending(const rgbdflow_server*) { return 0; }
+
+}  // extern "C"
