@@ -1,0 +1,309 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 scene-flow solve: 640x480 pairs/s.
+
+A step is one batched solve of B synthetic 640x480 RGB-D pairs (B = 16 by default) with the
+reference's schedule restated for the benchmark: ISOTROPIC regularisation, pyramid ratio 0.5 with
+minWidth = W/16 (5 levels), 10 outer warps, 1 inner, 30 red-black SOR iterations, the reference's
+convergence breaks and outer early termination on.  Every pair is an independent unit, so N GPUs
+run N replicas (weak scaling, no collective on the data path).
+
+  value      pairs/s with inputs resident in HBM (device-pointer API, CUDA events on the launching
+             stream, max over ranks); the batch's working set (~1.5 GB) is far above L2
+  e2e        pairs/s through the host-buffer C ABI call, host->device inputs and device->host
+             flows inside the timed region
+  plain      one pair per call (the drop-in solve): pairs/s and p50 / p99 latency
+  roofline   the dominant kernel (red-black SOR) from a profiled pass of the same workload
+  cpu_baseline  the CPU restatement of the reference (oracle, all host threads) on one pair
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B] [--impl ours|reference]
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "rgbd-flow_b200"))
+
+import synthetic as syn  # noqa: E402
+
+METRIC = "640×480 pairs/s & p99 latency, served+batched vs plain GPU at matched 3-D EPE"
+W, H = 640, 480
+
+
+def peaks():
+    try:
+        m = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(m["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """DRAM bytes per SOR launch from the committed ncu summary (profiles/), if present."""
+    try:
+        d = json.load(open(os.path.join(ROOT, "profiles", "sor_traffic.json")))
+        return d
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index):
+        self.p = None
+        self.path = os.path.join(ROOT, "gpurun_out", "clocks_rank%d.csv" % index)
+        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        try:
+            self.f = open(self.path, "w")
+            self.p = subprocess.Popen(
+                ["nvidia-smi", "-i", str(index), "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,"
+                 "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        self.p.wait()
+        self.f.close()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_pairs(n, seed0):
+    out = []
+    for i in range(n):
+        p = syn.make_config_pair("640x480", seed=seed0 + i)
+        out.append(p)
+    return out
+
+
+def cam_of(rf, p):
+    c = p["cam"]
+    return rf.CameraParams.make(p["W"], p["H"], c.f, c.cx, c.cy)
+
+
+def oracle_pairs_per_s(pairs, steps):
+    """The CPU restatement on the host cores: one 640x480 pair per step."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_binding as ob
+    import rgbdflow as rf
+    ob.build_oracle()
+    threads = ob.oracle().sfo_set_threads(0)
+    prm = rf.benchmark_params(W)
+    outs, ts = [], []
+    for s in range(steps):
+        p = pairs[s % len(pairs)]
+        t = time.perf_counter()
+        f, _ = ob.two_frames(cam_of(rf, p), p["bgr1"], p["depth1"], p["bgr2"], p["depth2"], prm)
+        ts.append(time.perf_counter() - t)
+        outs.append(f)
+    return steps / sum(ts), threads, outs, ts
+
+
+def run_reference(args, rank, world):
+    """The reference arm: the reference has no CPU implementation of its 3-D solver, so its
+    restatement (oracle/, the same arithmetic and schedule) runs on the host cores."""
+    if rank != 0:
+        return
+    pairs = make_pairs(2, 1000)
+    if args.warmup:
+        oracle_pairs_per_s(pairs, min(args.warmup, 1))
+    v, threads, _, ts = oracle_pairs_per_s(pairs, args.steps)
+    line = {"metric": METRIC, "value": v, "unit": "pairs/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(ts)),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64 (mixed, as the reference)",
+            "data": "synthetic (seeded RGB-D patch scenes, 640x480)",
+            "config": {"workload": "one 640x480 RGB-D pair per step, 5 levels x 10 outer x 30 SOR, CPU restatement",
+                       "threads": threads},
+            "cpu_baseline": {"value": v, "unit": "pairs/s", "cores": threads, "kind": "port",
+                             "sample": "%d pairs of 640x480, one per step" % args.steps},
+            "e2e": {"value": v, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--batch", type=int, default=16)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    import torch.distributed as dist
+    import rgbdflow as rf
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    B = args.batch
+    host = make_pairs(B, 1000 * rank)
+    prm = rf.benchmark_params(W)
+    ctx = rf.Context(local)
+    dev = []
+    for p in host:
+        dev.append(dict(W=W, H=H, cam=cam_of(rf, p),
+                        bgr1=torch.from_numpy(p["bgr1"]).cuda(), bgr2=torch.from_numpy(p["bgr2"]).cuda(),
+                        depth1=torch.from_numpy(p["depth1"]).cuda(), depth2=torch.from_numpy(p["depth2"]).cuda(),
+                        out=torch.empty((H, W, 3), dtype=torch.float32, device="cuda")))
+    stream = torch.cuda.Stream()  # the stream every solve below is enqueued on and timed on
+    torch.cuda.set_stream(stream)
+
+    # ---- value: device-resident batched solve
+    for _ in range(args.warmup):
+        ctx.scene_flow_batch_device(dev, prm)
+    torch.cuda.synchronize()
+    launches_per_step = ctx.last_launch_count()
+    clocks = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    step_ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    e0.record(stream)
+    step_ev[0].record(stream)
+    for s in range(args.steps):
+        ctx.scene_flow_batch_device(dev, prm)
+        step_ev[s + 1].record(stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    step_ms = [step_ev[i].elapsed_time(step_ev[i + 1]) for i in range(args.steps)]
+    value = B * args.steps * world / (ms / 1e3)
+
+    # ---- batched result check: pair 0 of the batch equals the same pair solved alone
+    solo = torch.empty((H, W, 3), dtype=torch.float32, device="cuda")
+    d0 = dict(dev[0])
+    d0["out"] = solo
+    ctx.scene_flow_batch_device([d0], prm)
+    torch.cuda.synchronize()
+    same = bool(torch.equal(solo, dev[0]["out"]))
+
+    # ---- plain: one pair per call (the drop-in form), per-call latency
+    lat = []
+    for s in range(max(args.warmup, 2) + 20):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        ctx.scene_flow_batch_device([dev[s % B]], prm)
+        b.record(stream)
+        torch.cuda.synchronize()
+        if s >= max(args.warmup, 2):
+            lat.append(a.elapsed_time(b))
+    plain = {"pairs_per_s": 1e3 / float(np.mean(lat)), "p50_ms": float(np.percentile(lat, 50)),
+             "p99_ms": float(np.percentile(lat, 99)), "calls": len(lat)}
+
+    # ---- e2e: host buffers through the synchronous C ABI call
+    hp = [dict(W=W, H=H, cam=cam_of(rf, p), bgr1=p["bgr1"], depth1=p["depth1"], bgr2=p["bgr2"], depth2=p["depth2"])
+          for p in host]
+    for _ in range(args.warmup):
+        flows = ctx.scene_flow_batch(hp, prm, stats=False)
+    barrier()
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        flows = ctx.scene_flow_batch(hp, prm, stats=False)
+    e2e_s = max_over_ranks(time.perf_counter() - t)
+    e2e = {"value": B * args.steps * world / e2e_s, "unit": "pairs/s",
+           "h2d_bytes_per_step": B * W * H * (3 + 3 + 4 + 4), "d2h_bytes_per_step": B * W * H * 12}
+
+    # ---- roofline of the dominant kernel from a profiled pass of the same workload
+    ctx.profile(1)
+    for _ in range(2):
+        ctx.scene_flow_batch_device(dev, prm)
+    torch.cuda.synchronize()
+    kst = ctx.profile_read()
+    ctx.profile(0)
+    peak, peak_kind = peaks()
+    n_sor, sor_ms, sor_bytes = kst.get("sor", (0, 0.0, 0.0))
+    tot_ms = sum(v[1] for v in kst.values())
+    achieved = sor_bytes / (sor_ms / 1e3) / 1e9 if sor_ms > 0 else 0.0
+    tr = ncu_traffic()
+    roofline = {"kernel": "k_sor (red-black SOR, 5 iterations per launch)", "bound": "hbm", "achieved": achieved,
+                "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                "traffic": (tr["dram_bytes_per_launch"] if tr else None),
+                "algorithmic_bytes_per_launch": sor_bytes / max(n_sor, 1),
+                "avg_launch_us": 1e3 * sor_ms / max(n_sor, 1), "launches": n_sor,
+                "share_of_device_time": sor_ms / tot_ms if tot_ms else None,
+                "kernel_ms": {k: round(v[1], 3) for k, v in kst.items()}}
+    if tr:
+        roofline["traffic_note"] = tr.get("note", "")
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, threads, outs, ts = oracle_pairs_per_s(host[:1], 2)
+        mask = host[0]["depth1"] > 0
+        mean, mx = syn.epe3d(dev[0]["out"].cpu().numpy(), outs[0], host[0]["z1_true"], host[0]["cam"], mask)
+        cpu = {"value": v, "unit": "pairs/s", "cores": threads, "kind": "port",
+               "sample": "2 solves of one 640x480 pair (the oracle, OpenMP over rows)",
+               "epe_vs_gpu_mm": {"mean": mean * 1e3, "max": mx * 1e3}}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded RGB-D patch scenes, 640x480)",
+                "config": {"workload": "batched solve of %d independent 640x480 pairs per step per GPU "
+                                       "(5 levels x 10 outer x 30 SOR, reference convergence breaks)" % B,
+                           "global_batch": B * world, "parallelism": "replicas x%d" % world,
+                           "l2": "inputs larger than L2 (working set %.2f GB per GPU)" % (ctx.device_bytes() / 1e9)},
+                "p50_ms": float(np.percentile(step_ms, 50)), "p99_ms": float(np.percentile(step_ms, 99)),
+                "plain": plain, "batch_equals_solo": same,
+                "gpu_launches": launches_per_step * args.steps,
+                "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -79,7 +79,7 @@ typedef struct rgbdflow_params {
     double alpha;                      /* smoothness weight (CLI -s, 0.02) */
     double gamma;                      /* zero-flow prior (1e-5) */
     double pyramid_ratio;              /* (0.75; values outside [0.4, 0.98] become 0.75 as in GaussianPyramid.cpp:23-24) */
-    int    min_width;                  /* (60) */
+    int    min_width;                  /* (60); a negative value -d means W / d for each pair (W/16 for -16) */
     int    n_outer;                    /* nOuterFPIterations (50) */
     int    n_inner;                    /* nInnerFPIterations (1) */
     int    n_sor;                      /* nSORIterations (maxIters, 10000 from main.cpp:100) */
@@ -122,6 +122,17 @@ void rgbdflow_params_default(rgbdflow_params* p);
 
 /* Version of this ABI (RGBDFLOW_ABI_VERSION). */
 int rgbdflow_abi_version(void);
+
+/* Pyramid level sizes a W x H pair is solved at, finest first (GaussianPyramid::ConstructPyramid,
+ * src/GaussianPyramid.cpp:22-62).  Host-only: needs no device.  w, h: arrays of at least
+ * RGBDFLOW_MAX_LEVELS ints (either may be NULL).  Returns the level count or a negative status. */
+int rgbdflow_pyramid_levels(int W, int H, double ratio, int min_width, int* w, int* h);
+
+/* Device bytes a batch of the given pair sizes needs (the context's HBM budget is checked
+ * against this).  Host-only.  Ws/Hs: n sizes; warm: NULL or n flags (warm-started pairs are
+ * solved at one level).  Returns 0 on success. */
+int rgbdflow_batch_device_bytes(const int* Ws, const int* Hs, const int* warm, int n,
+                                const rgbdflow_params* params, size_t* bytes);
 
 /* ---------------------------------------------------------------------------------------------
  * Context: owns a CUDA stream, device workspaces (sized lazily, bounded by hbm_budget_bytes),
@@ -220,6 +231,29 @@ int rgbdflow_scene_flow_batch(rgbdflow_ctx* ctx, const rgbdflow_pair* pairs, int
  * (a cudaStream_t passed as void*; NULL = the context's own stream).  Returns after enqueue. */
 int rgbdflow_scene_flow_batch_async(rgbdflow_ctx* ctx, const rgbdflow_pair* pairs, int n,
                                     const rgbdflow_params* params, void* stream);
+
+/* Wait for every solve this context enqueued (on any stream). */
+int rgbdflow_ctx_synchronize(rgbdflow_ctx* ctx);
+
+/* Kernel launches of the last solve enqueued on this context. */
+int rgbdflow_ctx_last_launch_count(const rgbdflow_ctx* ctx);
+
+/* ---------------------------------------------------------------------------------------------
+ * Kernel timing (no reference counterpart; the reference prints wall-clock phase timers,
+ * include/rgbd_util/timer.h:29-56).  While enabled, solves launch their kernels directly (no
+ * graph) with CUDA events around every launch; times, launch counts and the algorithmic bytes of
+ * the executed work accumulate per kernel class until profiling is disabled.
+ * ------------------------------------------------------------------------------------------- */
+typedef struct rgbdflow_kernel_stat {
+    char   name[32];
+    int    launches;
+    double ms;      /* summed device time */
+    double bytes;   /* algorithmic bytes of the executed work (0 where not counted) */
+} rgbdflow_kernel_stat;
+
+int rgbdflow_profile(rgbdflow_ctx* ctx, int enable);
+/* Fills up to max entries; returns the number of kernel classes with launches. */
+int rgbdflow_profile_read(rgbdflow_ctx* ctx, rgbdflow_kernel_stat* out, int max);
 
 /* ---------------------------------------------------------------------------------------------
  * Served form (no reference counterpart): continuous batching over camera streams.  A frame

@@ -150,6 +150,7 @@ void resize_dims(const Img& in, Img& out, int DW, int DH)
 /* GaussianPyramid::ConstructPyramid level count (GaussianPyramid.cpp:22-32). */
 int pyramid_levels(int width, double ratio, int min_width)
 {
+    if (min_width < 0) min_width = std::max(1, width / -min_width);  // API convention: W / d per pair
     if (ratio > 0.98 || ratio < 0.4) ratio = 0.75;
     double w = width * ratio;
     int n = 1;
@@ -160,6 +161,7 @@ int pyramid_levels(int width, double ratio, int min_width)
 /* GaussianPyramid::ConstructPyramid (GaussianPyramid.cpp:20-63). */
 void build_pyramid(const Img& image, double ratio, int min_width, std::vector<Img>& lev)
 {
+    if (min_width < 0) min_width = std::max(1, image.w / -min_width);
     if (ratio > 0.98 || ratio < 0.4) ratio = 0.75;
     const int nLevels = pyramid_levels(image.w, ratio, min_width);
     lev.assign(nLevels, Img());

@@ -18,8 +18,6 @@ constexpr int kMaxChecks = 512;  // SOR convergence checks per inner iteration (
 
 // Linearisation / elementwise tiling.
 constexpr int LTW = 32, LTH = 8;  // 256 threads, one interior pixel each
-// SOR tiling (interior); the loaded region adds a halo of 2 * sweeps.
-constexpr int STW = 32, STH = 16;
 
 // ------------------------------------------------------------------------------------------
 // descriptors
@@ -57,16 +55,17 @@ struct LevelItem {
     T* mag;                     // depth-magnitude weight
     T* rh;                      // regularisation weight to the right neighbour
     T* rv;                      // regularisation weight to the lower neighbour
+    int pitch;                  // row pitch (elements) of the u planes: W rounded up to 4
+    int hwp;                    // checkerboard half-row length of the x and sys planes (see cs_idx)
     T* u[3];                    // flow (u px, v px, w m)
     T* x[2][3];                 // SOR increment, ping-pong pair
     T* sys[12];                 // compact linear system (see k_linearize)
     T* stat_part;               // per SOR tile partial of the early-termination statistic
     int lin_tiles_x, lin_tile0; // linearisation / elementwise tiles: index base in the step's list
-    int sor_tiles_x, sor_tile0;
-    int n_sor_tiles;
+    int n_sor_tiles;            // SOR tiles (32 x 32 interior) of this item
     // coarser level (for the flow upsample); null at the coarsest level
     const T* uc[3];
-    int Wc, Hc;
+    int Wc, Hc, pitch_c;
     T inv_ratio;                // 1 / pyramid ratio (u, v scale on upsample)
     // full-resolution info for the depth-magnitude quirk
     int xres_full;
@@ -129,6 +128,11 @@ template <> __device__ __forceinline__ float rsqrtT<float>(float v) { return 1.0
 template <> __device__ __forceinline__ double rsqrtT<double>(double v) { return 1.0 / sqrt(v); }
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// Checkerboard ("colour-split") layout of the SOR's planes (system and increment): every row
+// holds its (i + j) even pixels first, then its odd ones, each half hwp long, so one colour's
+// pixels -- and their other-colour neighbours -- are contiguous.
+__host__ __device__ __forceinline__ int cs_idx(int i, int j, int hwp) { return i * 2 * hwp + ((i + j) & 1) * hwp + (j >> 1); }
 
 // ------------------------------------------------------------------------------------------
 // Preprocessing at full resolution.
@@ -431,8 +435,9 @@ __global__ void k_level_setup(const LevelItem<T, S>* items, const Tile* tiles, i
     it.rh[l] = rh;
     it.rv[l] = rv;
     if (it.est_init) return;  // flow supplied by the caller
+    const int lp = i * it.pitch + j;
     if (it.uc[0] == nullptr) {
-        it.u[0][l] = 0; it.u[1][l] = 0; it.u[2][l] = 0;
+        it.u[0][lp] = 0; it.u[1][lp] = 0; it.u[2][lp] = 0;
     } else {
         const double xr = (double)W / it.Wc, yr = (double)H / it.Hc;
         const double x = (double)(j + 1) / xr - 1, y = (double)(i + 1) / yr - 1;
@@ -446,12 +451,13 @@ __global__ void k_level_setup(const LevelItem<T, S>* items, const Tile* tiles, i
         const T s10 = (T)(fabs(dx) * fabs(1 - dy)), s11 = (T)(fabs(dx) * fabs(dy));
         for (int c = 0; c < 3; c++) {
             const T* s = it.uc[c];
+            const int pc = it.pitch_c;
             T acc = 0;
-            acc += s[v0 * it.Wc + u0] * s00;
-            acc += s[v1 * it.Wc + u0] * s01;
-            acc += s[v0 * it.Wc + u1] * s10;
-            acc += s[v1 * it.Wc + u1] * s11;
-            it.u[c][l] = (c < 2) ? acc * it.inv_ratio : acc;
+            acc += s[v0 * pc + u0] * s00;
+            acc += s[v1 * pc + u0] * s01;
+            acc += s[v0 * pc + u1] * s10;
+            acc += s[v1 * pc + u1] * s11;
+            it.u[c][lp] = (c < 2) ? acc * it.inv_ratio : acc;
         }
     }
 }
@@ -463,7 +469,7 @@ __global__ void k_level_setup(const LevelItem<T, S>* items, const Tile* tiles, i
 // occlusion weight (.cu:640-648), the robust weights phi / psi / pi (.cu:340-371), the weighted
 // products (.cu:189-230), the normalised weighted Laplacians (.cu:240-333) and writes the
 // compact form of the system of fillSystemMtxKernel (.cu:477-575):
-//   sys[0..2]  diagonal (u, v, w rows)
+//   sys[0..2]  reciprocal of the diagonal (u, v, w rows)
 //   sys[3..5]  symmetric couplings uv, uw, vw
 //   sys[6..8]  right-hand sides
 //   sys[9]     alpha * phi * (right regularisation weight)   (0 on the last column)
@@ -502,11 +508,11 @@ k_linearize(const LevelItem<T, S>* items, const Tile* tiles, SolveConst<T> k, in
         const int ry = r / LRW, rx = r % LRW;
         const int gi = y0 - 2 + ry, gj = x0 - 2 + rx;
         if (gi < 0 || gj < 0 || gi >= H || gj >= W) continue;
-        const int l = gi * W + gj;
+        const int l = gi * W + gj, lp = gi * it.pitch + gj;
         T U[3], D[3];
         for (int c = 0; c < 3; c++) {
-            U[c] = it.u[c][l];
-            D[c] = use_du ? it.x[xsel][c][l] : (T)0;
+            U[c] = it.u[c][lp];
+            D[c] = use_du ? it.x[xsel][c][cs_idx(gi, gj, it.hwp)] : (T)0;
             sU[c][ry][rx] = U[c];
             sUD[c][ry][rx] = U[c] + D[c];
         }
@@ -626,36 +632,57 @@ k_linearize(const LevelItem<T, S>* items, const Tile* tiles, SolveConst<T> k, in
     if (hasD) { const T e = phi * rvl; sumXY += e; sumZ += e * s; }
     const T al = k.alpha, ga = k.gamma, mg = it.mag[l];
     T* const* o = it.sys;
-    o[0][l] = -(ix2 + dx2 + al * sumXY) - ga;
-    o[1][l] = -(iy2 + dy2 + al * sumXY) - ga;
-    o[2][l] = -(pi + al * sumZ) - ga * mg;
-    o[3][l] = -ixy - dxy;
-    o[4][l] = pi * Ix[5];
-    o[5][l] = pi * Iy[5];
-    o[6][l] = -(-itx - dtx + al * -lap[0]) + ga * U0;
-    o[7][l] = -(-ity - dty + al * -lap[1]) + ga * U1;
-    o[8][l] = -(pi * It[5] + al * -(s * lap[2])) + ga * mg * U2;
-    o[9][l] = hasR ? al * (phi * rhl) : (T)0;
-    o[10][l] = hasD ? al * (phi * rvl) : (T)0;
-    o[11][l] = s;
+    const int lp = cs_idx(gi, gj, it.hwp);
+    // reciprocals of the diagonal: the SOR multiplies instead of dividing
+    o[0][lp] = (T)1 / (-(ix2 + dx2 + al * sumXY) - ga);
+    o[1][lp] = (T)1 / (-(iy2 + dy2 + al * sumXY) - ga);
+    o[2][lp] = (T)1 / (-(pi + al * sumZ) - ga * mg);
+    o[3][lp] = -ixy - dxy;
+    o[4][lp] = pi * Ix[5];
+    o[5][lp] = pi * Iy[5];
+    o[6][lp] = -(-itx - dtx + al * -lap[0]) + ga * U0;
+    o[7][lp] = -(-ity - dty + al * -lap[1]) + ga * U1;
+    o[8][lp] = -(pi * It[5] + al * -(s * lap[2])) + ga * mg * U2;
+    o[9][lp] = hasR ? al * (phi * rhl) : (T)0;
+    o[10][lp] = hasD ? al * (phi * rvl) : (T)0;
+    o[11][lp] = s;
 }
 
 // ------------------------------------------------------------------------------------------
-// Red-black SOR, K iterations per launch (temporal blocking).  Each CTA loads its tile plus a
-// halo of 2K pixels into shared memory, runs the red and black half-sweeps of K iterations on the
-// whole region (errors from the region's unknown outside creep inward one pixel per half-sweep
-// and never reach the interior), and writes back the interior only; x ping-pongs between two
-// buffers so no CTA reads a neighbour's already-updated values.  Same-colour updates are
-// independent, so the result is identical to sweeping the whole image colour by colour
-// (sceneFlowSingleScaleJacobiKernel, .cu:382-470): each of the three unknowns of a pixel is
-// updated from the pre-sweep values of the other two (pointwise Jacobi inside red-black
-// Gauss-Seidel), relaxed with omega and clamped to +-max_flow_step around its old value.
+// Red-black SOR, K iterations per launch (temporal blocking), persistent CTAs.
+//
+// The work unit is a fixed 32 x 32 interior tile.  A CTA loads the tile plus a halo of 2K pixels
+// (12 system planes + 3 increment planes) into shared memory with cp.async, runs the red and
+// black half-sweeps of K iterations over the whole region (errors from the unknown outside of the
+// halo creep inward one pixel per half-sweep and never reach the interior), and writes back the
+// interior.  With NBUF = 2 the next tile's region streams in while the current one is solved.
+// x ping-pongs between two global buffers, so no CTA reads a neighbour's already-updated values.
+// Same-colour updates are independent, so the interior equals a whole-image sweep colour by
+// colour (sceneFlowSingleScaleJacobiKernel, .cu:382-470): each unknown of a pixel is updated from
+// the pre-sweep values of the other two (pointwise Jacobi inside red-black Gauss-Seidel), relaxed
+// with omega and clamped to +-max_flow_step around its old value; the result does not depend on
+// K or on the tiling.
 
-template <int K> struct SorGeom {
-    static constexpr int RW = STW + 4 * K, RH = STH + 4 * K;
-    static constexpr int NT = (RW / 2) * RH;  // threads: one red and one black pixel each
+constexpr int kSorTW = 32, kSorTH = 32;  // interior tile (fixed: per-tile reductions stay identical)
+
+template <class T, int K, int NBUF> struct SorGeom {
+    static constexpr int RW = (kSorTW + 4 * K + 8 + 7) & ~7;  // region width incl. alignment slack; HRW % 4 == 0
+    static constexpr int HRW = RW / 2;                // checkerboard half-row length
+    static constexpr int RH = kSorTH + 4 * K;
+    static constexpr int NPL = 15;                    // planes: 12 system + 3 increment
+    static constexpr int NT = 512;
+    static constexpr size_t buf_elems = (size_t)NPL * RH * RW;
+    static constexpr size_t smem = sizeof(T) * (NBUF * buf_elems + 64);
 };
-template <class T, int K> constexpr size_t sor_smem_bytes() { return sizeof(T) * (6 * SorGeom<K>::RW * SorGeom<K>::RH + 32); }
+template <class T, int K, int NBUF> constexpr size_t sor_smem_bytes() { return SorGeom<T, K, NBUF>::smem; }
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int src_bytes)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 template <class T>
 __device__ __forceinline__ void sor_point(const T* c, T aL, T aU, T aR, T aD, T sL, T sU, T s,
@@ -667,7 +694,7 @@ __device__ __forceinline__ void sor_point(const T* c, T aL, T aU, T aR, T aD, T 
     v -= aL * xl[0]; v -= aU * xu[0]; v -= aR * xr[0]; v -= aD * xd[0];
     v += c[6];
     v -= c[3] * xp[1]; v -= c[4] * xp[2];
-    v /= c[0];
+    v *= c[0];
     T r = omega * v + ((T)1 - omega) * xp[0];
     out[0] = fmin(fmax(r, xp[0] - step), xp[0] + step);
     // v row
@@ -675,7 +702,7 @@ __device__ __forceinline__ void sor_point(const T* c, T aL, T aU, T aR, T aD, T 
     v -= aL * xl[1]; v -= aU * xu[1]; v -= aR * xr[1]; v -= aD * xd[1];
     v += c[7];
     v -= c[3] * xp[0]; v -= c[5] * xp[2];
-    v /= c[1];
+    v *= c[1];
     r = omega * v + ((T)1 - omega) * xp[1];
     out[1] = fmin(fmax(r, xp[1] - step), xp[1] + step);
     // w row: neighbour coefficients carry the depth-smoothness weight of the edge's source pixel
@@ -683,117 +710,181 @@ __device__ __forceinline__ void sor_point(const T* c, T aL, T aU, T aR, T aD, T 
     v -= (aL * sL) * xl[2]; v -= (aU * sU) * xu[2]; v -= (aR * s) * xr[2]; v -= (aD * s) * xd[2];
     v += c[8];
     v -= c[4] * xp[0]; v -= c[5] * xp[1];
-    v /= c[2];
+    v *= c[2];
     r = omega * v + ((T)1 - omega) * xp[2];
     out[2] = fmin(fmax(r, xp[2] - step), xp[2] + step);
 }
 
-template <class T, class S, int K>
-__global__ void __launch_bounds__(SorGeom<K>::NT)
-k_sor(const LevelItem<T, S>* items, const Tile* tiles, SolveConst<T> k, SorLaunch L)
+// Region of a tile: global columns [ws, ws + RW), rows [y0, y0 + RH); ws a multiple of 8 so
+// each checkerboard half-row segment starts 16-byte aligned.  Shared layout per plane:
+// [RH rows][2 colours][HRW], colour = parity of (global row + column).
+template <class T, int K>
+__device__ __forceinline__ int sor_ws(int tx) { return (tx * kSorTW - 2 * K) & ~7; }
+
+template <class T, class S, int K, int NBUF>
+__device__ __forceinline__ void sor_load(const LevelItem<T, S>& it, const Tile& t, const SorLaunch& L, T* buf)
 {
-    constexpr int RW = SorGeom<K>::RW, RH = SorGeom<K>::RH, HW = RW / 2;
-    const Tile t = tiles[blockIdx.x];
-    const LevelItem<T, S>& it = items[t.item];
-    PairCtl* ctl = it.ctl;
-    if (ctl->level_done) return;
-    int nit = L.nit;
-    bool stopped = ctl->sor_stop != 0;
-    if (!stopped && L.prev_check) {
-        const float md = __uint_as_float(ctl->maxdiff[L.prev_check_idx]);
-        if ((double)md < k.sor_tol || (T)md >= k.step) {
-            stopped = true;
-            if (t.idx == 0 && threadIdx.x == 0) { ctl->sor_stop = 1; ctl->sor_stop_iter = L.it0; }
-        }
-    }
-    if (stopped) nit = 0;
-    const int W = it.W, H = it.H;
-    const int x0 = t.tx * STW - 2 * K, y0 = t.ty * STH - 2 * K;  // region origin (global)
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    typedef T Plane[RH][RW];
-    Plane* sx = reinterpret_cast<Plane*>(smem_raw);  // [3] increment
-    Plane& seh = sx[3];                               // alpha * phi * right weight
-    Plane& sev = sx[4];                               // alpha * phi * down weight
-    Plane& ss = sx[5];                                // depth-smoothness weight
-    T* wsum = reinterpret_cast<T*>(sx + 6);           // [32] block-sum scratch
-    const int tx = threadIdx.x % HW, ty = threadIdx.x / HW;
-    const int gi = y0 + ty;
-    T c[2][9];
-    int gl[2];
-    bool in[2];
+    typedef SorGeom<T, K, NBUF> G;
+    constexpr int CH = 16 / sizeof(T), NCH = G::HRW / CH;
+    const int W = it.W, H = it.H, hw = it.hwp;
+    const int m0 = sor_ws<T, K>(t.tx) / 2;
+    const int y0 = t.ty * kSorTH - 2 * K;
     const T* const* xin = it.x[L.xin];
-    for (int b = 0; b < 2; b++) {
-        const int rx = 2 * tx + b, gj = x0 + rx;
-        in[b] = gi >= 0 && gi < H && gj >= 0 && gj < W;
-        const int l = in[b] ? gi * W + gj : 0;
-        gl[b] = l;
-        for (int v = 0; v < 3; v++) sx[v][ty][rx] = (in[b] && !L.xin_zero) ? xin[v][l] : (T)0;
-        seh[ty][rx] = in[b] ? it.sys[9][l] : (T)0;
-        sev[ty][rx] = in[b] ? it.sys[10][l] : (T)0;
-        ss[ty][rx] = in[b] ? it.sys[11][l] : (T)0;
-        for (int q = 0; q < 9; q++) c[b][q] = in[b] ? it.sys[q][l] : (T)1;
-    }
-    __syncthreads();
-    const bool interior_row = ty >= 2 * K && ty < 2 * K + STH;
-    T md = 0;
-    for (int s = 0; s < 2 * nit; s++) {
-        const int color = s & 1;
-        // the one pixel of this thread with (i + j) % 2 == color
-        const int bb = (color ^ gi ^ x0) & 1;  // x0 and 2*tx are even-offset; parity of (gi + gj)
-        T cs[9];
-#pragma unroll
-        for (int q = 0; q < 9; q++) cs[q] = bb ? c[1][q] : c[0][q];  // register select, no local memory
-        if (bb ? in[1] : in[0]) {
-            const int rx = 2 * tx + bb;
-            const int rl = rx > 0 ? rx - 1 : rx, rr = rx < RW - 1 ? rx + 1 : rx;
-            const int ru = ty > 0 ? ty - 1 : ty, rd = ty < RH - 1 ? ty + 1 : ty;
-            T xl[3], xu[3], xr[3], xd[3], xp[3], nv[3];
-            for (int v = 0; v < 3; v++) {
-                xl[v] = sx[v][ty][rl]; xr[v] = sx[v][ty][rr];
-                xu[v] = sx[v][ru][rx]; xd[v] = sx[v][rd][rx];
-                xp[v] = sx[v][ty][rx];
-            }
-            sor_point<T>(cs, seh[ty][rl], sev[ru][rx], seh[ty][rx], sev[ty][rx], ss[ty][rl], ss[ru][rx],
-                         ss[ty][rx], xl, xu, xr, xd, xp, k.omega, k.step, nv);
-            for (int v = 0; v < 3; v++) sx[v][ty][rx] = nv[v];
-            if (L.check && s >= 2 * nit - 2 && interior_row && rx >= 2 * K && rx < 2 * K + STW)
-                for (int v = 0; v < 3; v++) md = fmax(md, fabs(nv[v] - xp[v]));
+    for (int q = threadIdx.x; q < G::NPL * G::RH * 2 * NCH; q += G::NT) {
+        const int ch = q % NCH, c = (q / NCH) & 1, rr = (q / (2 * NCH)) % G::RH, pl = q / (2 * NCH * G::RH);
+        const int gi = y0 + rr, m = m0 + ch * CH;
+        // pixels of colour c in row gi: columns (c ^ (gi & 1)) + 2m', m' < count
+        const int cnt = (W + 1 - (c ^ (gi & 1))) >> 1;
+        int nb = 0;
+        const T* src = it.sys[0];  // any valid address when nothing is read
+        if (gi >= 0 && gi < H && m >= 0 && m < cnt && !(pl >= 12 && L.xin_zero)) {
+            nb = min(CH, cnt - m) * (int)sizeof(T);
+            src = (pl < 12 ? it.sys[pl] : xin[pl - 12]) + (size_t)gi * 2 * hw + c * hw + m;
         }
-        __syncthreads();
+        cp_async16(buf + (((size_t)pl * G::RH + rr) * 2 + c) * G::HRW + ch * CH, src, nb);
     }
-    // max |dx| of the checked iteration -> per-pair slot (max is order independent)
-    if (L.check && nit > 0) {
-        float m = (float)md;
-        for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-        if ((threadIdx.x & 31) == 0 && m > 0) atomicMax(&ctl->maxdiff[L.check_idx], __float_as_uint(m));
-    }
-    // write the interior
-    T part = 0;
-    for (int b = 0; b < 2; b++) {
-        const int rx = 2 * tx + b;
-        if (!in[b] || !interior_row || rx < 2 * K || rx >= 2 * K + STW) continue;
-        const int l = gl[b];
-        if (L.final_fold) {
-            for (int v = 0; v < 3; v++) it.u[v][l] += sx[v][ty][rx];
-            const T a = sx[0][ty][rx], bq = sx[1][ty][rx], cz = sx[2][ty][rx];
-            const T wz = it.f_level / it.pyr[6][l];
-            part += a * a + bq * bq + (cz * cz) * wz;
+}
+
+template <class T, class S, int K, int NBUF, int ILP, int MINB>
+__global__ void __launch_bounds__(512, MINB)
+k_sor(const LevelItem<T, S>* items, const Tile* tiles, int ntiles, SolveConst<T> k, SorLaunch L)
+{
+    typedef SorGeom<T, K, NBUF> G;
+    constexpr int RW = G::RW, RH = G::RH, PL = RH * RW, HRW = G::HRW;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* bufs = reinterpret_cast<T*>(smem_raw);
+    T* red = bufs + NBUF * G::buf_elems;  // [64] reduction scratch
+    int cur = 0;
+    int tid = blockIdx.x;
+    if (tid < ntiles) sor_load<T, S, K, NBUF>(items[tiles[tid].item], tiles[tid], L, bufs);
+    cp_async_commit();
+    for (; tid < ntiles; tid += gridDim.x) {
+        const Tile t = tiles[tid];
+        const LevelItem<T, S>& it = items[t.item];
+        T* buf = bufs + cur * G::buf_elems;
+        const int nxt = tid + gridDim.x;
+        if (NBUF == 2) {
+            if (nxt < ntiles) sor_load<T, S, K, NBUF>(items[tiles[nxt].item], tiles[nxt], L, bufs + (cur ^ 1) * G::buf_elems);
+            cp_async_commit();
+            cp_async_wait<1>();
         } else {
-            T* const* xo = it.x[L.xin ^ 1];
-            for (int v = 0; v < 3; v++) xo[v][l] = sx[v][ty][rx];
+            cp_async_wait<0>();
         }
-    }
-    if (L.final_fold) {
-        // deterministic block sum: warp trees, then warps in order
-        for (int o = 16; o > 0; o >>= 1) part += __shfl_down_sync(0xffffffffu, part, o);
-        if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = part;
         __syncthreads();
-        if (threadIdx.x == 0) {
-            T tot = 0;
-            for (int w = 0; w < (int)((blockDim.x + 31) >> 5); w++) tot += wsum[w];
-            it.stat_part[t.idx] = tot;
+        PairCtl* ctl = it.ctl;
+        const bool done = ctl->level_done != 0;
+        int nit = L.nit;
+        bool stopped = ctl->sor_stop != 0;
+        if (!stopped && L.prev_check) {
+            const float md = __uint_as_float(ctl->maxdiff[L.prev_check_idx]);
+            if ((double)md < k.sor_tol || (T)md >= k.step) {
+                stopped = true;
+                if (t.idx == 0 && threadIdx.x == 0) { ctl->sor_stop = 1; ctl->sor_stop_iter = L.it0; }
+            }
         }
+        if (stopped) nit = 0;
+        const int W = it.W, H = it.H;
+        const int ws = sor_ws<T, K>(t.tx);
+        const int y0 = t.ty * kSorTH - 2 * K;
+        const int ix0 = t.tx * kSorTW, iy0 = t.ty * kSorTH;  // interior origin
+        T md = 0;
+        if (!done) {
+            for (int hs = 0; hs < 2 * nit; hs++) {
+                const int color = hs & 1;
+                const bool chk = L.check && hs >= 2 * nit - 2;
+                for (int q0 = threadIdx.x; q0 < RH * HRW; q0 += ILP * G::NT) {
+                    T c[ILP][9], xl[ILP][3], xu[ILP][3], xr[ILP][3], xd[ILP][3], xp[ILP][3], nv[ILP][3];
+                    T aL[ILP], aU[ILP], aR[ILP], aD[ILP], sL[ILP], sU[ILP], sC[ILP];
+                    int o[ILP];
+                    bool ok[ILP], in_int[ILP];
+#pragma unroll
+                    for (int u = 0; u < ILP; u++) {
+                        const int q = q0 + u * G::NT;
+                        const int rr = q / HRW, m = q % HRW;
+                        const int gi = y0 + rr;
+                        const int b = color ^ (gi & 1);           // column parity of this colour in row gi
+                        const int gj = ws + 2 * m + b;
+                        ok[u] = q < RH * HRW && gi >= 0 && gi < H && gj >= 0 && gj < W;
+                        in_int[u] = gi >= iy0 && gi < iy0 + kSorTH && gj >= ix0 && gj < ix0 + kSorTW;
+                        const int rq = ok[u] ? rr : 0, mq = ok[u] ? m : 0;
+                        // own pixel: colour `color`; neighbours: the other colour
+                        const int own = (rq * 2 + color) * HRW + mq;
+                        const int oth = (rq * 2 + (color ^ 1)) * HRW;
+                        const int ml = clampi(mq - 1 + b, 0, HRW - 1), mr = clampi(mq + b, 0, HRW - 1);
+                        const int ru = rq > 0 ? rq - 1 : rq, rd = rq < RH - 1 ? rq + 1 : rq;
+                        const int ol = oth + ml, orr = oth + mr;
+                        const int ou = (ru * 2 + (color ^ 1)) * HRW + mq, od = (rd * 2 + (color ^ 1)) * HRW + mq;
+                        o[u] = own;
+#pragma unroll
+                        for (int z = 0; z < 9; z++) c[u][z] = buf[z * PL + own];
+#pragma unroll
+                        for (int v = 0; v < 3; v++) {
+                            const T* xv = buf + (12 + v) * PL;
+                            xl[u][v] = xv[ol]; xr[u][v] = xv[orr]; xu[u][v] = xv[ou]; xd[u][v] = xv[od]; xp[u][v] = xv[own];
+                        }
+                        aL[u] = buf[9 * PL + ol]; aU[u] = buf[10 * PL + ou]; aR[u] = buf[9 * PL + own];
+                        aD[u] = buf[10 * PL + own]; sL[u] = buf[11 * PL + ol]; sU[u] = buf[11 * PL + ou];
+                        sC[u] = buf[11 * PL + own];
+                    }
+#pragma unroll
+                    for (int u = 0; u < ILP; u++)
+                        sor_point<T>(c[u], aL[u], aU[u], aR[u], aD[u], sL[u], sU[u], sC[u], xl[u], xu[u], xr[u], xd[u],
+                                     xp[u], k.omega, k.step, nv[u]);
+#pragma unroll
+                    for (int u = 0; u < ILP; u++) {
+                        if (!ok[u]) continue;
+#pragma unroll
+                        for (int v = 0; v < 3; v++) buf[(12 + v) * PL + o[u]] = nv[u][v];
+                        if (chk && in_int[u])
+                            for (int v = 0; v < 3; v++) md = fmax(md, fabs(nv[u][v] - xp[u][v]));
+                    }
+                }
+                __syncthreads();
+            }
+            // interior out: x to the other buffer, or the fold u += x with the statistic partial
+            T part = 0;
+            for (int q = threadIdx.x; q < kSorTW * kSorTH; q += G::NT) {
+                const int gi = iy0 + q / kSorTW, gj = ix0 + q % kSorTW;
+                if (gi >= H || gj >= W) continue;
+                const int cl = (gi + gj) & 1;
+                const int o = ((gi - y0) * 2 + cl) * HRW + ((gj - ws) >> 1);
+                const T a = buf[12 * PL + o], bq = buf[13 * PL + o], cz = buf[14 * PL + o];
+                if (L.final_fold) {
+                    const size_t lp = (size_t)gi * it.pitch + gj;
+                    it.u[0][lp] += a; it.u[1][lp] += bq; it.u[2][lp] += cz;
+                    const T wz = it.f_level / it.pyr[6][(size_t)gi * W + gj];
+                    part += a * a + bq * bq + (cz * cz) * wz;
+                } else {
+                    T* const* xo = it.x[L.xin ^ 1];
+                    const int lc = cs_idx(gi, gj, it.hwp);
+                    xo[0][lc] = a; xo[1][lc] = bq; xo[2][lc] = cz;
+                }
+            }
+            if (L.check && nit > 0) {
+                float mm = (float)md;
+                for (int off = 16; off > 0; off >>= 1) mm = fmaxf(mm, __shfl_xor_sync(0xffffffffu, mm, off));
+                if ((threadIdx.x & 31) == 0 && mm > 0) atomicMax(&ctl->maxdiff[L.check_idx], __float_as_uint(mm));
+            }
+            if (L.final_fold) {
+                // deterministic per-tile sum: warp trees, then warps in order
+                for (int off = 16; off > 0; off >>= 1) part += __shfl_down_sync(0xffffffffu, part, off);
+                if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = part;
+                __syncthreads();
+                if (threadIdx.x == 0) {
+                    T tot = 0;
+                    for (int w = 0; w < G::NT / 32; w++) tot += red[w];
+                    it.stat_part[t.idx] = tot;
+                }
+            }
+        }
+        __syncthreads();  // buffer `cur` is free for the load after next
+        if (NBUF == 1) {
+            if (nxt < ntiles) sor_load<T, S, K, NBUF>(items[tiles[nxt].item], tiles[nxt], L, bufs);
+            cp_async_commit();
+        }
+        cur ^= (NBUF - 1);
     }
+    cp_async_wait<0>();
 }
 
 // After each outer iteration: the early-termination statistic of the pair (mean over 3N of
@@ -838,9 +929,10 @@ __global__ void k_output(const LevelItem<T, S>* items, const Tile* tiles, T* con
     if (i >= it.H || j >= it.W) return;
     const int l = i * it.W + j;
     T* o = outs[t.item];
-    o[(size_t)l * 3 + 0] = it.u[0][l];
-    o[(size_t)l * 3 + 1] = it.u[1][l];
-    o[(size_t)l * 3 + 2] = it.u[2][l];
+    const int lp = i * it.pitch + j;
+    o[(size_t)l * 3 + 0] = it.u[0][lp];
+    o[(size_t)l * 3 + 1] = it.u[1][lp];
+    o[(size_t)l * 3 + 2] = it.u[2][lp];
 }
 
 // Device warp of the final flow (for the single-scale seam's warpIm2 / warpDm2 outputs).
@@ -856,7 +948,8 @@ __global__ void k_warp_out(const LevelItem<T, S>* items, const Tile* tiles, T* c
     const int W = it.W, H = it.H, l = i * W + j;
     T* wI = outs[t.item] + (size_t)3 * W * H;
     T* wD = outs[t.item] + (size_t)8 * W * H;
-    const T U0 = it.u[0][l], U1 = it.u[1][l], U2 = it.u[2][l];
+    const int lp = i * it.pitch + j;
+    const T U0 = it.u[0][lp], U1 = it.u[1][lp], U2 = it.u[2][lp];
     const T x = (T)j + U0, y = (T)i + U1;
     if (x < 0 || x > (T)(W - 1) || y < 0 || y > (T)(H - 1)) {
         for (int c = 0; c < 5; c++) wI[(size_t)l * 5 + c] = ldS<T, S>(it.I1[c] + l);
@@ -894,7 +987,8 @@ __global__ void k_load_est(const LevelItem<T, S>* items, const Tile* tiles, cons
     if (i >= it.H || j >= it.W) return;
     const int l = i * it.W + j;
     const size_t N = (size_t)it.W * it.H;
-    for (int c = 0; c < 3; c++) it.u[c][l] = e.f ? (T)e.f[(size_t)l * 3 + c] : (T)e.d[c * N + l];
+    const int lp = i * it.pitch + j;
+    for (int c = 0; c < 3; c++) it.u[c][lp] = e.f ? (T)e.f[(size_t)l * 3 + c] : (T)e.d[c * N + l];
 }
 
 // Per-level seam (sceneFlowSingleScale's own inputs): features, depths, weights and flow come
@@ -932,7 +1026,8 @@ __global__ void k_seam_load(const LevelItem<T, S>* items, const Tile* tiles, con
     // weights of edges that leave the image are never used by the reference; keep them 0
     it.rh[l] = (j < W - 1) ? (T)q.regw[(size_t)l * 2 + 0] : (T)0;
     it.rv[l] = (i < H - 1) ? (T)q.regw[(size_t)l * 2 + 1] : (T)0;
-    for (int c = 0; c < 3; c++) it.u[c][l] = (T)q.uvw[c * N + l];
+    const int lp = i * it.pitch + j;
+    for (int c = 0; c < 3; c++) it.u[c][lp] = (T)q.uvw[c * N + l];
 }
 
 }  // namespace rgbdflow

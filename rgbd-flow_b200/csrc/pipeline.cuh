@@ -50,6 +50,7 @@ struct PyrShape {
 static inline PyrShape pyramid_shape(int W, int H, double ratio, int min_width, int max_levels)
 {
     PyrShape s;
+    if (min_width < 0) min_width = std::max(1, W / -min_width);  // per-pair W / d
     if (ratio > 0.98 || ratio < 0.4) ratio = 0.75;
     s.ratio = ratio;
     double w = W * ratio;
@@ -129,7 +130,37 @@ struct HostParams {
     int min_width, n_outer, n_inner, n_sor, max_dist, fill_holes, fixed;
     double omega, step, eps_d, eps_z, eps_s, sor_tol, outer_tol, occ_margin, occ_penalty, max_grad;
     int period, K, fill_rounds;
+    int sor_ilp, sor_nbuf;  // 0 = automatic
 };
+
+// Row pitch of the u planes, and the checkerboard half-row length of the x / sys planes (16-byte
+// aligned half-rows for the SOR's cp.async loads).
+static inline int pitch_of(int W) { return (W + 3) & ~3; }
+static inline int hwp_of(int W) { return (((W + 1) / 2) + 3) & ~3; }
+
+// A SOR kernel configuration: K sweeps per launch, NBUF region buffers, ILP pixels gathered per
+// thread pass.
+struct SorConfig {
+    int K = 2, nbuf = 1, ilp = 1;
+};
+
+template <class T> static inline bool sor_cfg_fits(const SorConfig& c);
+
+// Configuration of the SOR launches of one level: explicit parameters win; otherwise large levels
+// (bandwidth-bound) and small ones (launch-bound) get the settings measured best for them.
+template <class T>
+static inline SorConfig choose_sor_config(const HostParams& hp, long level_px)
+{
+    SorConfig c;
+    c.K = hp.K > 0 ? hp.K : (level_px >= (1L << 20) ? 2 : 5);
+    c.nbuf = hp.sor_nbuf > 0 ? hp.sor_nbuf : 1;
+    c.ilp = hp.sor_ilp > 0 ? hp.sor_ilp : 2;
+    while (c.K > 1 && !sor_cfg_fits<T>(c)) {
+        if (c.nbuf == 2) c.nbuf = 1;
+        else c.K--;
+    }
+    return c;
+}
 
 // Bump allocator over a byte range.
 struct Bump {
@@ -141,6 +172,8 @@ template <class T, class S>
 struct Plan {
     // ---- shape
     int n = 0, Lmax = 0;
+    int sms = 148;                // multiprocessors of the device (persistent SOR grid)
+    std::vector<SorConfig> sor_cfg;  // SOR kernel configuration per step
     std::vector<PyrShape> shapes;
     std::vector<int> L;           // levels per pair
     HostParams hp;
@@ -158,6 +191,7 @@ struct Plan {
     // ---- host descriptors (uploaded as one block at desc_off)
     std::vector<unsigned char> desc;
     struct StepDesc {
+        long level_px;  // pixels of this level summed over the step's pairs
         size_t items_off; int n_items;
         size_t lin_tiles_off; int n_lin;
         size_t sor_tiles_off; int n_sor;
@@ -168,8 +202,8 @@ struct Plan {
     size_t prep_items_off = 0, prep_tiles_off = 0; int n_prep_tiles = 0;
     size_t out_ptrs_off = 0;
     size_t unfilled_off = 0;            // int[n][256]
-    std::vector<std::vector<SorLaunch>> sor_sched;  // per inner iteration index
-    std::vector<int> n_checks;                      // per inner iteration
+    std::vector<std::vector<std::vector<SorLaunch>>> sor_sched;  // [step][inner iteration]
+    std::vector<std::vector<int>> n_checks;                     // [step][inner iteration]
     std::vector<std::vector<size_t>> u_off;         // per pair per level: offset of u[0] (for warm-start upload)
     std::vector<int> est_flag;
 
@@ -279,11 +313,12 @@ static Plan<T, S> make_plan(const std::vector<PairSpec>& pairs, const HostParams
             for (int c = 0; c < 5; c++) { m.I1[c] = A.take(sizeof(S) * N); m.I2[c] = A.take(sizeof(S) * N); }
             m.D1 = A.take(sizeof(S) * N); m.D2 = A.take(sizeof(S) * N);
             m.mag = A.take(sizeof(T) * N); m.rh = A.take(sizeof(T) * N); m.rv = A.take(sizeof(T) * N);
-            for (int c = 0; c < 3; c++) m.u[c] = A.take(sizeof(T) * N);
-            for (int b = 0; b < 2; b++) for (int c = 0; c < 3; c++) m.x[b][c] = A.take(sizeof(T) * N);
-            for (int c = 0; c < 12; c++) m.sys[c] = A.take(sizeof(T) * N);
-            const int stx = (s.w[k] + STW - 1) / STW, sty = (s.h[k] + STH - 1) / STH;
-            m.nsor = stx * sty;
+            const size_t NP = (size_t)pitch_of(s.w[k]) * s.h[k];
+            const size_t NC = (size_t)2 * hwp_of(s.w[k]) * s.h[k];
+            for (int c = 0; c < 3; c++) m.u[c] = A.take(sizeof(T) * NP);
+            for (int b = 0; b < 2; b++) for (int c = 0; c < 3; c++) m.x[b][c] = A.take(sizeof(T) * NC);
+            for (int c = 0; c < 12; c++) m.sys[c] = A.take(sizeof(T) * NC);
+            m.nsor = ((s.w[k] + kSorTW - 1) / kSorTW) * ((s.h[k] + kSorTH - 1) / kSorTH);
             m.stat = A.take(sizeof(T) * m.nsor);
         }
     }
@@ -407,10 +442,11 @@ static Plan<T, S> make_plan(const std::vector<PairSpec>& pairs, const HostParams
             for (int b = 0; b < 2; b++) for (int c = 0; c < 3; c++) it.x[b][c] = (T*)m.x[b][c];
             for (int c = 0; c < 12; c++) it.sys[c] = (T*)m.sys[c];
             it.stat_part = (T*)m.stat;
-            it.n_sor_tiles = m.nsor;
+            it.pitch = pitch_of(s.w[k]);
+            it.hwp = hwp_of(s.w[k]);
             if (k + 1 < P.L[p] && !P.est_flag[p]) {
                 for (int c = 0; c < 3; c++) it.uc[c] = (const T*)mem[p][k + 1].u[c];
-                it.Wc = s.w[k + 1]; it.Hc = s.h[k + 1];
+                it.Wc = s.w[k + 1]; it.Hc = s.h[k + 1]; it.pitch_c = pitch_of(s.w[k + 1]);
             }
             it.inv_ratio = (T)(1 / hp.ratio);
             it.xres_full = (int)pairs[p].xres_full;
@@ -421,14 +457,17 @@ static Plan<T, S> make_plan(const std::vector<PairSpec>& pairs, const HostParams
             const int lty = (it.H + LTH - 1) / LTH;
             for (int y = 0; y < lty; y++)
                 for (int x = 0; x < it.lin_tiles_x; x++) lt.push_back(Tile{iid, x, y, y * it.lin_tiles_x + x});
-            it.sor_tiles_x = (it.W + STW - 1) / STW;
-            it.sor_tile0 = (int)stt.size();
-            const int sty = (it.H + STH - 1) / STH;
-            for (int y = 0; y < sty; y++)
-                for (int x = 0; x < it.sor_tiles_x; x++) stt.push_back(Tile{iid, x, y, y * it.sor_tiles_x + x});
             items.push_back(it);
         }
+        for (auto& x : items) {
+            const int sx = (x.W + kSorTW - 1) / kSorTW, sy = (x.H + kSorTH - 1) / kSorTH;
+            x.n_sor_tiles = sx * sy;
+            for (int y = 0; y < sy; y++)
+                for (int xx = 0; xx < sx; xx++) stt.push_back(Tile{(int)(&x - items.data()), xx, y, y * sx + xx});
+        }
         typename Plan<T, S>::StepDesc d;
+        d.level_px = 0;
+        for (const auto& x : items) d.level_px += (long)x.W * x.H;
         d.items_off = P.put(items); d.n_items = (int)items.size();
         d.lin_tiles_off = P.put(lt); d.n_lin = (int)lt.size();
         d.sor_tiles_off = P.put(stt); d.n_sor = (int)stt.size();
@@ -457,12 +496,20 @@ static Plan<T, S> make_plan(const std::vector<PairSpec>& pairs, const HostParams
     P.est_src_off = P.put(est);
     P.seam_src_off = P.put(seam);
 
-    // SOR schedule per inner iteration
-    int cur = 0;
-    for (int hh = 0; hh < hp.n_inner; hh++) {
-        int nc = 0;
-        P.sor_sched.push_back(sor_schedule(hp.n_sor, hp.K, hp.period, hp.fixed, hh == 0, hh == hp.n_inner - 1, cur, nc));
-        P.n_checks.push_back(nc);
+    // SOR configuration and launch schedule per step (level) and inner iteration
+    for (int sidx = 0; sidx < P.Lmax; sidx++) {
+        const SorConfig c = choose_sor_config<T>(hp, P.steps[sidx].level_px);
+        P.sor_cfg.push_back(c);
+        int cur = 0;
+        std::vector<std::vector<SorLaunch>> sch;
+        std::vector<int> ncs;
+        for (int hh = 0; hh < hp.n_inner; hh++) {
+            int nc = 0;
+            sch.push_back(sor_schedule(hp.n_sor, c.K, hp.period, hp.fixed, hh == 0, hh == hp.n_inner - 1, cur, nc));
+            ncs.push_back(nc);
+        }
+        P.sor_sched.push_back(sch);
+        P.n_checks.push_back(ncs);
     }
     P.desc_off = align_up(P.arena_bytes, 256);
     P.desc_bytes = P.desc.size();
@@ -538,43 +585,146 @@ static SolveConst<T> solve_const(const HostParams& hp)
 }
 
 // ------------------------------------------------------------------------------------------
+// Optional kernel timing: CUDA events around every launch, aggregated per kernel class.
+
+enum KClass { KC_PREP, KC_SIGMA, KC_FILL, KC_PYR_H, KC_PYR_V, KC_SETUP, KC_LIN, KC_SOR, KC_CTL, KC_OUT, KC_MISC, KC_N };
+constexpr int KC_SOR_LEVEL0 = KC_N;           // per-level SOR classes: KC_SOR_LEVEL0 + level
+constexpr int KC_TOTAL = KC_N + 16;
+static const char* const kClassNames[KC_N] = {"prep", "depth_sigma", "hole_fill", "pyr_hfilter", "pyr_vresize",
+                                              "level_setup", "linearize", "sor", "control", "output", "misc"};
+
+struct Prof {
+    std::vector<cudaEvent_t> pool;
+    std::vector<int> cls;
+    size_t used = 0;
+    void begin(int c, cudaStream_t st)
+    {
+        if (used + 2 > pool.size()) {
+            for (int i = 0; i < 256; i++) {
+                cudaEvent_t e;
+                RF_CUDA(cudaEventCreate(&e));
+                pool.push_back(e);
+            }
+        }
+        cls.push_back(c);
+        RF_CUDA(cudaEventRecord(pool[used++], st));
+    }
+    void end(cudaStream_t st) { RF_CUDA(cudaEventRecord(pool[used++], st)); }
+    // after the stream synchronised: add per-class time
+    void collect(double* ms, int* n)
+    {
+        for (size_t i = 0; i < cls.size(); i++) {
+            float t = 0;
+            RF_CUDA(cudaEventElapsedTime(&t, pool[2 * i], pool[2 * i + 1]));
+            ms[cls[i]] += t;
+            n[cls[i]]++;
+        }
+        cls.clear();
+        used = 0;
+    }
+    ~Prof() { for (auto e : pool) cudaEventDestroy(e); }
+};
+#define RF_PROF_B(pf, c, st) do { if (pf) (pf)->begin((c), (st)); } while (0)
+#define RF_PROF_E(pf, st) do { if (pf) (pf)->end(st); } while (0)
+
+// ------------------------------------------------------------------------------------------
 // kernel launch helpers
 
-template <class T, class S, int K>
-static void launch_sor_k(const LevelItem<T, S>* items, const Tile* tiles, int n, const SolveConst<T>& k,
+// SOR configurations.  A configuration is (K sweeps per launch, NBUF region buffers, ILP pixels
+// gathered per thread pass); MINB = 2 CTAs per SM where the shared memory allows it.
+static inline int sor_cfg_id(const SorConfig& c) { return (c.K - 1) * 4 + (c.nbuf - 1) * 2 + (c.ilp - 1); }
+
+template <class T, int K, int NB> constexpr bool sor_fits() { return SorGeom<T, K, NB>::smem <= 227 * 1024; }
+template <class T, int K, int NB> constexpr int sor_minb() { return SorGeom<T, K, NB>::smem * 2 + 2048 <= 228 * 1024 ? 2 : 1; }
+
+template <class T, class S, int K, int NB, int ILP>
+static void launch_sor_k(const LevelItem<T, S>* items, const Tile* tiles, int n, int sms, const SolveConst<T>& k,
                          const SorLaunch& L, cudaStream_t st)
 {
-    constexpr size_t sm = sor_smem_bytes<T, K>();
-    k_sor<T, S, K><<<n, SorGeom<K>::NT, sm, st>>>(items, tiles, k, L);
+    if constexpr (sor_fits<T, K, NB>()) {
+        constexpr int MB = sor_minb<T, K, NB>();
+        typedef SorGeom<T, K, NB> G;
+        k_sor<T, S, K, NB, ILP, MB><<<std::min(n, sms * MB), G::NT, G::smem, st>>>(items, tiles, n, k, L);
+    } else {
+        throw ArgError(-2, "SOR configuration does not fit shared memory");
+    }
+}
+
+template <class T, class S, int K>
+static void launch_sor_kk(const SorConfig& c, const LevelItem<T, S>* items, const Tile* tiles, int n, int sms,
+                          const SolveConst<T>& k, const SorLaunch& L, cudaStream_t st)
+{
+    if (c.nbuf == 2) {
+        if (c.ilp == 2) launch_sor_k<T, S, K, 2, 2>(items, tiles, n, sms, k, L, st);
+        else launch_sor_k<T, S, K, 2, 1>(items, tiles, n, sms, k, L, st);
+    } else {
+        if (c.ilp == 2) launch_sor_k<T, S, K, 1, 2>(items, tiles, n, sms, k, L, st);
+        else launch_sor_k<T, S, K, 1, 1>(items, tiles, n, sms, k, L, st);
+    }
 }
 
 template <class T, class S>
-static void launch_sor(int K, const LevelItem<T, S>* items, const Tile* tiles, int n, const SolveConst<T>& k,
-                       const SorLaunch& L, cudaStream_t st)
+static void launch_sor(const SorConfig& c, const LevelItem<T, S>* items, const Tile* tiles, int n, int sms,
+                       const SolveConst<T>& k, const SorLaunch& L, cudaStream_t st)
 {
-    switch (K) {
-    case 1: launch_sor_k<T, S, 1>(items, tiles, n, k, L, st); break;
-    case 2: launch_sor_k<T, S, 2>(items, tiles, n, k, L, st); break;
-    case 3: launch_sor_k<T, S, 3>(items, tiles, n, k, L, st); break;
-    case 4: launch_sor_k<T, S, 4>(items, tiles, n, k, L, st); break;
-    default: launch_sor_k<T, S, 5>(items, tiles, n, k, L, st); break;
+    switch (c.K) {
+    case 1: launch_sor_kk<T, S, 1>(c, items, tiles, n, sms, k, L, st); break;
+    case 2: launch_sor_kk<T, S, 2>(c, items, tiles, n, sms, k, L, st); break;
+    case 3: launch_sor_kk<T, S, 3>(c, items, tiles, n, sms, k, L, st); break;
+    case 4: launch_sor_kk<T, S, 4>(c, items, tiles, n, sms, k, L, st); break;
+    case 5: launch_sor_kk<T, S, 5>(c, items, tiles, n, sms, k, L, st); break;
+    default: launch_sor_kk<T, S, 6>(c, items, tiles, n, sms, k, L, st); break;
     }
+}
+
+template <class T, class S, int K, int NB, int ILP>
+static void sor_attr1()
+{
+    if constexpr (sor_fits<T, K, NB>()) {
+        constexpr int MB = sor_minb<T, K, NB>();
+        RF_CUDA(cudaFuncSetAttribute(k_sor<T, S, K, NB, ILP, MB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)SorGeom<T, K, NB>::smem));
+    }
+}
+template <class T, class S, int K>
+static void sor_attr()
+{
+    sor_attr1<T, S, K, 1, 1>();
+    sor_attr1<T, S, K, 1, 2>();
+    sor_attr1<T, S, K, 2, 1>();
+    sor_attr1<T, S, K, 2, 2>();
 }
 
 template <class T, class S>
 static void set_kernel_attrs()
 {
     RF_CUDA(cudaFuncSetAttribute(k_linearize<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lin_smem_bytes<T>()));
-    RF_CUDA(cudaFuncSetAttribute(k_sor<T, S, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sor_smem_bytes<T, 1>()));
-    RF_CUDA(cudaFuncSetAttribute(k_sor<T, S, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sor_smem_bytes<T, 2>()));
-    RF_CUDA(cudaFuncSetAttribute(k_sor<T, S, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sor_smem_bytes<T, 3>()));
-    RF_CUDA(cudaFuncSetAttribute(k_sor<T, S, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sor_smem_bytes<T, 4>()));
-    RF_CUDA(cudaFuncSetAttribute(k_sor<T, S, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sor_smem_bytes<T, 5>()));
+    sor_attr<T, S, 1>();
+    sor_attr<T, S, 2>();
+    sor_attr<T, S, 3>();
+    sor_attr<T, S, 4>();
+    sor_attr<T, S, 5>();
+    sor_attr<T, S, 6>();
+}
+
+// Whether configuration c fits shared memory for type T.
+template <class T> static inline bool sor_cfg_fits(const SorConfig& c)
+{
+    size_t sm = 0;
+    switch (c.K) {
+    case 1: sm = c.nbuf == 2 ? SorGeom<T, 1, 2>::smem : SorGeom<T, 1, 1>::smem; break;
+    case 2: sm = c.nbuf == 2 ? SorGeom<T, 2, 2>::smem : SorGeom<T, 2, 1>::smem; break;
+    case 3: sm = c.nbuf == 2 ? SorGeom<T, 3, 2>::smem : SorGeom<T, 3, 1>::smem; break;
+    case 4: sm = c.nbuf == 2 ? SorGeom<T, 4, 2>::smem : SorGeom<T, 4, 1>::smem; break;
+    case 5: sm = c.nbuf == 2 ? SorGeom<T, 5, 2>::smem : SorGeom<T, 5, 1>::smem; break;
+    default: sm = c.nbuf == 2 ? SorGeom<T, 6, 2>::smem : SorGeom<T, 6, 1>::smem; break;
+    }
+    return sm <= 227 * 1024;
 }
 
 // The level loop of one step (sceneFlowSingleScale's outer / inner / SOR structure, .cu:755-954).
 template <class T, class S>
-static int enqueue_level(const Plan<T, S>& P, char* base, int sidx, cudaStream_t st, int setup)
+static int enqueue_level(const Plan<T, S>& P, char* base, int sidx, cudaStream_t st, int setup, Prof* pf)
 {
     const auto& d = P.steps[sidx];
     if (d.n_items == 0) return 0;
@@ -584,33 +734,43 @@ static int enqueue_level(const Plan<T, S>& P, char* base, int sidx, cudaStream_t
     const Tile* stt = (const Tile*)(base + P.desc_off + d.sor_tiles_off);
     const SolveConst<T> k = solve_const<T>(P.hp);
     if (setup) {
+        RF_PROF_B(pf, KC_SETUP, st);
         k_level_setup<T, S><<<d.n_lin, LTW * LTH, 0, st>>>(items, lt, P.hp.regularization);
+        RF_PROF_E(pf, st);
         launches++;
     }
     for (int outer = 0; outer < P.hp.n_outer; outer++) {
         for (int hh = 0; hh < P.hp.n_inner; hh++) {
-            const auto& sched = P.sor_sched[hh];
+            const auto& sched = P.sor_sched[sidx][hh];
             // inner iterations after the first read the running increment (x of the previous SOR)
             const int xsel = sched.front().xin;
+            RF_PROF_B(pf, KC_LIN, st);
             k_linearize<T, S><<<d.n_lin, LTW * LTH, lin_smem_bytes<T>(), st>>>(items, lt, k, hh > 0, xsel);
+            RF_PROF_E(pf, st);
             launches++;
+            const int lvl = P.Lmax - 1 - sidx;
             for (SorLaunch L : sched) {
                 L.outer = outer;
-                launch_sor<T, S>(P.hp.K, items, stt, d.n_sor, k, L, st);
+                RF_PROF_B(pf, KC_SOR_LEVEL0 + lvl, st);
+                launch_sor<T, S>(P.sor_cfg[sidx], items, stt, d.n_sor, P.sms, k, L, st);
+                RF_PROF_E(pf, st);
                 launches++;
             }
         }
         const int wpb = 4;
+        RF_PROF_B(pf, KC_CTL, st);
         k_control<T, S><<<(d.n_items + wpb - 1) / wpb, 32 * wpb, 0, st>>>(items, d.n_items, k, outer,
-                                                                          P.n_checks.empty() ? 0 : P.n_checks.back());
+                                                                          P.n_checks[sidx].back());
+        RF_PROF_E(pf, st);
         launches++;
     }
     return launches;
 }
 
 // Whole solve after the inputs are resident: preprocessing, hole fill, pyramids, levels, output.
+// outs: the output-pointer array the final kernels write through (device memory).
 template <class T, class S>
-static int enqueue_solve(const Plan<T, S>& P, char* base, cudaStream_t st)
+static int enqueue_solve(const Plan<T, S>& P, char* base, cudaStream_t st, Prof* pf = nullptr)
 {
     int launches = 0;
     char* db = base + P.desc_off;
@@ -619,40 +779,82 @@ static int enqueue_solve(const Plan<T, S>& P, char* base, cudaStream_t st)
     const LevelItem<T, S>* fin_items = (const LevelItem<T, S>*)(db + fin.items_off);
     const Tile* fin_tiles = (const Tile*)(db + fin.lin_tiles_off);
     if (P.kind == 2) {
+        RF_PROF_B(pf, KC_SETUP, st);
         k_seam_load<T, S><<<fin.n_lin, LTW * LTH, 0, st>>>(fin_items, fin_tiles, (const SeamSrc*)(db + P.seam_src_off));
+        RF_PROF_E(pf, st);
         launches++;
-        launches += enqueue_level(P, base, P.Lmax - 1, st, 0);
+        launches += enqueue_level(P, base, P.Lmax - 1, st, 0, pf);
+        RF_PROF_B(pf, KC_OUT, st);
         k_warp_out<T, S><<<fin.n_lin, LTW * LTH, 0, st>>>(fin_items, fin_tiles, (T* const*)(db + P.out_ptrs_off));
+        RF_PROF_E(pf, st);
         launches++;
     } else {
         RF_CUDA(cudaMemsetAsync(base + P.unfilled_off, 0, sizeof(int) * 256 * P.n, st));
         const PrepItem<T>* prep = (const PrepItem<T>*)(db + P.prep_items_off);
         const Tile* pt = (const Tile*)(db + P.prep_tiles_off);
+        RF_PROF_B(pf, KC_PREP, st);
         k_prep<T><<<P.n_prep_tiles, LTW * LTH, 0, st>>>(prep, pt);
+        RF_PROF_E(pf, st);
+        RF_PROF_B(pf, KC_SIGMA, st);
         k_sigma<T><<<P.n_prep_tiles, LTW * LTH, 0, st>>>(prep, pt);
+        RF_PROF_E(pf, st);
         launches += 2;
         if (P.hp.fill_holes)
             for (int r = 1; r <= P.hp.fill_rounds; r++) {
+                RF_PROF_B(pf, KC_FILL, st);
                 k_fill_round<T><<<P.n_prep_tiles, LTW * LTH, 0, st>>>(prep, pt, r);
+                RF_PROF_E(pf, st);
                 launches++;
             }
         for (const auto& lv : P.pyr) {
             const PyrJob<T>* jobs = (const PyrJob<T>*)(db + lv.jobs_off);
             const T* g = (const T*)(db + lv.g_off);
+            RF_PROF_B(pf, KC_PYR_H, st);
             k_hfilter<T><<<lv.n_src, LTW * LTH, 0, st>>>(jobs, (const Tile*)(db + lv.src_tiles_off), g);
+            RF_PROF_E(pf, st);
+            RF_PROF_B(pf, KC_PYR_V, st);
             k_vresize<T><<<lv.n_dst, LTW * LTH, 0, st>>>(jobs, (const Tile*)(db + lv.dst_tiles_off), g);
+            RF_PROF_E(pf, st);
             launches += 2;
         }
         if (P.any_warm) {
+            RF_PROF_B(pf, KC_MISC, st);
             k_load_est<T, S><<<fin.n_lin, LTW * LTH, 0, st>>>(fin_items, fin_tiles, (const EstSrc*)(db + P.est_src_off));
+            RF_PROF_E(pf, st);
             launches++;
         }
-        for (int s = 0; s < P.Lmax; s++) launches += enqueue_level(P, base, s, st, 1);
+        for (int s = 0; s < P.Lmax; s++) launches += enqueue_level(P, base, s, st, 1, pf);
     }
+    RF_PROF_B(pf, KC_OUT, st);
     k_output<T, S><<<fin.n_lin, LTW * LTH, 0, st>>>(fin_items, fin_tiles, (T* const*)(db + P.out_ptrs_off));
+    RF_PROF_E(pf, st);
     launches++;
     RF_CUDA(cudaGetLastError());
     return launches;
+}
+
+// Algorithmic bytes of the work a solve actually executed (early exits included), per class:
+//   SOR: per level pixel and executed iteration, the 12-float system (48 B) read plus the
+//        3-float increment read and written (24 B) = 72 B; plus, once per outer iteration, the
+//        fold u += x (u read and written, 24 B).
+//   linearisation: per level pixel and execution, 20 input values (5 + 5 features, 2 depths,
+//        3 flow, 5 weights; the 12 feature/depth values in the storage type) plus the 12-float
+//        system written.
+template <class T, class S>
+static void executed_bytes(const Plan<T, S>& P, const PairCtl* ctl, double* sor_bytes, double* lin_bytes)
+{
+    *sor_bytes = 0;
+    *lin_bytes = 0;
+    const double lin_px = 12.0 * sizeof(S) + 8.0 * sizeof(T) + 12.0 * sizeof(T);
+    for (int p = 0; p < P.n; p++)
+        for (int k = 0; k < P.L[p]; k++) {
+            const double N = (double)P.shapes[p].w[k] * P.shapes[p].h[k];
+            const int O = std::min(ctl[p].outer_exec[k], 64);
+            for (int o = 0; o < O; o++) {
+                *sor_bytes += N * (ctl[p].sor_exec[k][o] * 72.0 * sizeof(T) / 4.0 + 24.0 * sizeof(T) / 4.0);
+                *lin_bytes += N * lin_px * P.hp.n_inner;
+            }
+        }
 }
 
 }  // namespace rgbdflow

@@ -37,7 +37,17 @@ struct rgbdflow_ctx {
     std::map<std::string, GraphEntry> graphs;
     bool attrs[4] = {false, false, false, false};
     int last_launches = 0;
+    int sms = 148;
     bool use_graphs = true;
+    // ordering of work that reuses the arena / pinned staging across calls and streams
+    cudaEvent_t done = nullptr;       // end of the last enqueued solve
+    cudaEvent_t desc_up = nullptr;    // last upload out of the pinned staging
+    bool pending = false;
+    // kernel profiling
+    std::unique_ptr<Prof> prof;
+    double prof_ms[KC_TOTAL] = {0};
+    int prof_n[KC_TOTAL] = {0};
+    double prof_bytes[KC_TOTAL] = {0};
 };
 
 namespace {
@@ -51,13 +61,20 @@ void drop_graphs(rgbdflow_ctx* c)
     c->graphs.clear();
 }
 
+void wait_idle(rgbdflow_ctx* c)
+{
+    if (c->pending) RF_CUDA(cudaEventSynchronize(c->done));
+    RF_CUDA(cudaStreamSynchronize(c->stream));
+    c->pending = false;
+}
+
 void ensure_arena(rgbdflow_ctx* c, size_t need)
 {
     if (c->arena_cap >= need) return;
     if (c->budget && need > c->budget)
         throw ArgError(RGBDFLOW_ERR_BUDGET, "request needs " + std::to_string(need) + " device bytes, budget is " +
                                                 std::to_string(c->budget));
-    RF_CUDA(cudaStreamSynchronize(c->stream));
+    wait_idle(c);
     drop_graphs(c);  // graphs hold arena addresses
     if (c->arena) RF_CUDA(cudaFree(c->arena));
     c->arena = nullptr;
@@ -71,7 +88,7 @@ void ensure_arena(rgbdflow_ctx* c, size_t need)
 void ensure_pin(rgbdflow_ctx* c, size_t need)
 {
     if (c->pin_cap >= need) return;
-    RF_CUDA(cudaStreamSynchronize(c->stream));
+    wait_idle(c);
     if (c->pin) RF_CUDA(cudaFreeHost(c->pin));
     c->pin = nullptr;
     const size_t cap = align_up(need + need / 8, 1 << 20);
@@ -91,11 +108,11 @@ HostParams host_params(const rgbdflow_params& p)
     h.sor_tol = p.sor_tol; h.outer_tol = p.outer_tol; h.occ_margin = p.occ_margin; h.occ_penalty = p.occ_penalty;
     h.max_grad = p.max_depth_grad;
     h.period = p.sor_check_period > 0 ? p.sor_check_period : 25;
-    int K = p.sweeps_per_launch;
-    if (K <= 0) K = (p.compute == RGBDFLOW_COMPUTE_FP64) ? 2 : 5;
-    if (K > 5) K = 5;
-    if (p.compute == RGBDFLOW_COMPUTE_FP64 && K > 2) K = 2;
-    h.K = K;
+    h.K = p.sweeps_per_launch > 0 ? std::min(p.sweeps_per_launch, 6) : 0;  // 0: chosen per level
+    const char* e = std::getenv("RGBDFLOW_SOR_ILP");
+    h.sor_ilp = e ? std::atoi(e) : 0;
+    e = std::getenv("RGBDFLOW_SOR_NBUF");
+    h.sor_nbuf = e ? std::atoi(e) : 0;
     h.fill_rounds = 64;
     return h;
 }
@@ -116,7 +133,7 @@ void validate(const rgbdflow_params* p)
     if (p->storage < 0 || p->storage > 2) throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "bad storage type");
     if (p->compute == RGBDFLOW_COMPUTE_FP64 && p->storage != RGBDFLOW_STORE_FP32)
         throw ArgError(RGBDFLOW_ERR_UNSUPPORTED, "the FP64 device solve stores its pyramids in FP64");
-    if (p->min_width < 1) throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "min_width < 1");
+    if (p->min_width == 0) throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "min_width == 0");
 }
 
 // getResizedCamParams (runFlowTwoFrames.cpp:14-24)
@@ -138,7 +155,7 @@ std::string plan_key(const std::vector<PairSpec>& ps, const HostParams& hp, int 
     std::snprintf(buf, sizeof buf, "|%d %.17g %.17g %.17g %.17g %.17g %d %d %d %d %d %d %d %.17g %.17g %.17g %.17g %.17g %.17g %.17g %.17g %.17g %.17g %d %d %d",
                   hp.regularization, hp.color_w, hp.dvc, hp.alpha, hp.gamma, hp.ratio, hp.min_width, hp.n_outer, hp.n_inner,
                   hp.n_sor, hp.max_dist, hp.fill_holes, hp.fixed, hp.omega, hp.step, hp.eps_d, hp.eps_z, hp.eps_s,
-                  hp.sor_tol, hp.outer_tol, hp.occ_margin, hp.occ_penalty, hp.max_grad, hp.period, hp.K, hp.fill_rounds);
+                  hp.sor_tol, hp.outer_tol, hp.occ_margin, hp.occ_penalty, hp.max_grad, hp.period, hp.K * 100 + hp.sor_ilp * 10 + hp.sor_nbuf, hp.fill_rounds);
     return k + buf;
 }
 
@@ -168,78 +185,118 @@ void ensure_attrs(rgbdflow_ctx* c, int slot)
     c->attrs[slot] = true;
 }
 
-// Runs a batch of host-buffer pairs through one graph launch.  stats: null or n entries.
+// Runs a batch through one graph launch.
+//   user_stream == nullptr: host buffers, synchronous (pinned staging, H2D, solve, D2H).
+//   user_stream != nullptr: every PairSpec pointer is device memory; the solve is enqueued on
+//                           user_stream and the call returns without waiting.
 template <class T, class S>
-void run_batch(rgbdflow_ctx* c, const std::vector<PairSpec>& pairs, const HostParams& hp, rgbdflow_stats* stats, int slot)
+void run_batch(rgbdflow_ctx* c, const std::vector<PairSpec>& pairs, const HostParams& hp, rgbdflow_stats* stats, int slot,
+               cudaStream_t user_stream = nullptr)
 {
     ensure_attrs<T, S>(c, slot);
+    const bool dev = user_stream != nullptr;
     Plan<T, S> P = make_plan<T, S>(pairs, hp);
+    P.sms = c->sms;
     ensure_arena(c, P.arena_bytes);
     bind_plan(P, c->arena);
+    if (dev) {
+        // point the work lists at the caller's device buffers
+        unsigned char* d = P.desc.data();
+        PrepItem<T>* prep = (PrepItem<T>*)(d + P.prep_items_off);
+        T** outs = (T**)(d + P.out_ptrs_off);
+        EstSrc* est = (EstSrc*)(d + P.est_src_off);
+        for (int p = 0; p < P.n; p++) {
+            prep[p].bgr[0] = pairs[p].bgr1; prep[p].bgr[1] = pairs[p].bgr2;
+            prep[p].depth[0] = pairs[p].depth1; prep[p].depth[1] = pairs[p].depth2;
+            outs[p] = (T*)pairs[p].out;
+            est[p].f = pairs[p].est;
+        }
+    }
     const size_t ctl_bytes = sizeof(PairCtl) * P.n;
-    const size_t pin_need = align_up(P.in_bytes, 256) + align_up(P.desc_bytes, 256) + align_up(P.out_bytes, 256) + ctl_bytes;
+    const size_t in_b = dev ? 0 : align_up(P.in_bytes, 256);
+    const size_t out_b = dev ? 0 : align_up(P.out_bytes, 256);
+    const size_t pin_need = in_b + align_up(P.desc_bytes, 256) + out_b + ctl_bytes;
     ensure_pin(c, pin_need);
+    // the pinned staging may still feed the previous call's uploads
+    RF_CUDA(cudaEventSynchronize(c->desc_up));
     char* pin_in = c->pin;
-    char* pin_desc = pin_in + align_up(P.in_bytes, 256);
+    char* pin_desc = pin_in + in_b;
     char* pin_out = pin_desc + align_up(P.desc_bytes, 256);
-    char* pin_ctl = pin_out + align_up(P.out_bytes, 256);
-    for (int p = 0; p < P.n; p++) {
-        const auto segs = pairs[p].inputs();
-        for (size_t q = 0; q < segs.size(); q++) {
-            if (!segs[q].first) throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "pair " + std::to_string(p) + ": null input buffer");
-            std::memcpy(pin_in + (P.in_seg[p][q] - P.in_off), segs[q].first, segs[q].second);
+    char* pin_ctl = pin_out + out_b;
+    if (!dev)
+        for (int p = 0; p < P.n; p++) {
+            const auto segs = pairs[p].inputs();
+            for (size_t q = 0; q < segs.size(); q++) {
+                if (!segs[q].first) throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "pair " + std::to_string(p) + ": null input buffer");
+                std::memcpy(pin_in + (P.in_seg[p][q] - P.in_off), segs[q].first, segs[q].second);
+            }
         }
-    }
     std::memcpy(pin_desc, P.desc.data(), P.desc_bytes);
-    cudaStream_t st = c->stream;
-    RF_CUDA(cudaMemcpyAsync(c->arena + P.in_off, pin_in, P.in_bytes, cudaMemcpyHostToDevice, st));
+    cudaStream_t st = dev ? user_stream : c->stream;
+    if (c->pending) RF_CUDA(cudaStreamWaitEvent(st, c->done, 0));  // arena reuse across streams
+    if (!dev) RF_CUDA(cudaMemcpyAsync(c->arena + P.in_off, pin_in, P.in_bytes, cudaMemcpyHostToDevice, st));
     RF_CUDA(cudaMemcpyAsync(c->arena + P.desc_off, pin_desc, P.desc_bytes, cudaMemcpyHostToDevice, st));
+    RF_CUDA(cudaEventRecord(c->desc_up, st));
     RF_CUDA(cudaEventRecord(c->e0, st));
-    const std::string key = plan_key(pairs, hp, slot);
-    auto it = c->graphs.find(key);
-    if (c->use_graphs && it == c->graphs.end()) {
-        GraphEntry g;
-        RF_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        int launches = 0;
-        try {
-            launches = enqueue_solve(P, c->arena, st);
-        } catch (...) {
-            cudaGraph_t tmp;
-            cudaStreamEndCapture(st, &tmp);
-            if (tmp) cudaGraphDestroy(tmp);
-            throw;
+    const bool graphs = c->use_graphs && !c->prof;
+    if (graphs) {
+        const std::string key = plan_key(pairs, hp, slot) + (dev ? "|dev" : "");
+        auto it = c->graphs.find(key);
+        if (it == c->graphs.end()) {
+            GraphEntry g;
+            RF_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+            int launches = 0;
+            try {
+                launches = enqueue_solve(P, c->arena, c->stream);
+            } catch (...) {
+                cudaGraph_t tmp = nullptr;
+                cudaStreamEndCapture(c->stream, &tmp);
+                if (tmp) cudaGraphDestroy(tmp);
+                throw;
+            }
+            RF_CUDA(cudaStreamEndCapture(c->stream, &g.graph));
+            RF_CUDA(cudaGraphInstantiate(&g.exec, g.graph, 0));
+            g.launches = launches;
+            if (c->graphs.size() > 32) drop_graphs(c);
+            it = c->graphs.emplace(key, g).first;
         }
-        RF_CUDA(cudaStreamEndCapture(st, &g.graph));
-        RF_CUDA(cudaGraphInstantiate(&g.exec, g.graph, 0));
-        g.launches = launches;
-        if (c->graphs.size() > 32) drop_graphs(c);
-        it = c->graphs.emplace(key, g).first;
-    }
-    if (c->use_graphs) {
         RF_CUDA(cudaGraphLaunch(it->second.exec, st));
         c->last_launches = it->second.launches;
     } else {
-        c->last_launches = enqueue_solve(P, c->arena, st);
+        c->last_launches = enqueue_solve(P, c->arena, st, c->prof.get());
     }
     RF_CUDA(cudaEventRecord(c->e1, st));
-    RF_CUDA(cudaMemcpyAsync(pin_out, c->arena + P.out_off, P.out_bytes, cudaMemcpyDeviceToHost, st));
-    if (stats) RF_CUDA(cudaMemcpyAsync(pin_ctl, c->arena + P.ctl_off, ctl_bytes, cudaMemcpyDeviceToHost, st));
-    RF_CUDA(cudaStreamSynchronize(st));
+    if (!dev) RF_CUDA(cudaMemcpyAsync(pin_out, c->arena + P.out_off, P.out_bytes, cudaMemcpyDeviceToHost, st));
+    const bool want_ctl = stats || c->prof;
+    if (want_ctl) RF_CUDA(cudaMemcpyAsync(pin_ctl, c->arena + P.ctl_off, ctl_bytes, cudaMemcpyDeviceToHost, st));
+    RF_CUDA(cudaEventRecord(c->done, st));
+    c->pending = true;
+    if (dev && !want_ctl) return;
+    RF_CUDA(cudaEventSynchronize(c->done));
+    c->pending = false;
     float ms = 0;
     RF_CUDA(cudaEventElapsedTime(&ms, c->e0, c->e1));
-    for (int p = 0; p < P.n; p++) {
-        const size_t N = (size_t)pairs[p].W * pairs[p].H;
-        const T* o = (const T*)(pin_out + (P.out_pair_off[p] - P.out_off));
-        const PairSpec& q = pairs[p];
-        if (q.out)
-            for (size_t z = 0; z < N * 3; z++) q.out[z] = (float)o[z];
-        if (q.out_u)
-            for (size_t z = 0; z < N; z++) { q.out_u[z] = (double)o[z * 3]; q.out_v[z] = (double)o[z * 3 + 1]; q.out_w[z] = (double)o[z * 3 + 2]; }
-        if (q.out_warpI)
-            for (size_t z = 0; z < N * 5; z++) q.out_warpI[z] = (double)o[N * 3 + z];
-        if (q.out_warpD)
-            for (size_t z = 0; z < N; z++) q.out_warpD[z] = (double)o[N * 8 + z];
+    if (c->prof) {
+        c->prof->collect(c->prof_ms, c->prof_n);
+        double sb, lb;
+        executed_bytes(P, (const PairCtl*)pin_ctl, &sb, &lb);
+        c->prof_bytes[KC_SOR] += sb;
+        c->prof_bytes[KC_LIN] += lb;
     }
+    if (!dev)
+        for (int p = 0; p < P.n; p++) {
+            const size_t N = (size_t)pairs[p].W * pairs[p].H;
+            const T* o = (const T*)(pin_out + (P.out_pair_off[p] - P.out_off));
+            const PairSpec& q = pairs[p];
+            if (q.out)
+                for (size_t z = 0; z < N * 3; z++) q.out[z] = (float)o[z];
+            if (q.out_u)
+                for (size_t z = 0; z < N; z++) { q.out_u[z] = (double)o[z * 3]; q.out_v[z] = (double)o[z * 3 + 1]; q.out_w[z] = (double)o[z * 3 + 2]; }
+            if (q.out_warpI)
+                for (size_t z = 0; z < N * 5; z++) q.out_warpI[z] = (double)o[N * 3 + z];
+            if (q.out_warpD)
+                for (size_t z = 0; z < N; z++) q.out_warpD[z] = (double)o[N * 8 + z];
+        }
     if (stats)
         for (int p = 0; p < P.n; p++) fill_stats(((PairCtl*)pin_ctl)[p], P.L[p], P.shapes[p], ms, &stats[p]);
 }
@@ -247,13 +304,16 @@ void run_batch(rgbdflow_ctx* c, const std::vector<PairSpec>& pairs, const HostPa
 }  // namespace
 
 
-static void dispatch(rgbdflow_ctx* c, const std::vector<PairSpec>& ps, const rgbdflow_params& p, rgbdflow_stats* stats)
+static void dispatch(rgbdflow_ctx* c, const std::vector<PairSpec>& ps, const rgbdflow_params& p, rgbdflow_stats* stats,
+                     cudaStream_t user_stream = nullptr)
 {
     const HostParams hp = host_params(p);
-    if (p.compute == RGBDFLOW_COMPUTE_FP64) run_batch<double, double>(c, ps, hp, stats, 1);
-    else if (p.storage == RGBDFLOW_STORE_FP16) run_batch<float, __half>(c, ps, hp, stats, 2);
-    else if (p.storage == RGBDFLOW_STORE_BF16) run_batch<float, __nv_bfloat16>(c, ps, hp, stats, 3);
-    else run_batch<float, float>(c, ps, hp, stats, 0);
+    if (p.compute == RGBDFLOW_COMPUTE_FP64) {
+        if (user_stream) throw ArgError(RGBDFLOW_ERR_UNSUPPORTED, "the FP64 device solve has no device-pointer form");
+        run_batch<double, double>(c, ps, hp, stats, 1);
+    } else if (p.storage == RGBDFLOW_STORE_FP16) run_batch<float, __half>(c, ps, hp, stats, 2, user_stream);
+    else if (p.storage == RGBDFLOW_STORE_BF16) run_batch<float, __nv_bfloat16>(c, ps, hp, stats, 3, user_stream);
+    else run_batch<float, float>(c, ps, hp, stats, 0, user_stream);
 }
 
 static int fail(rgbdflow_ctx* c, int code, const std::string& m)
@@ -308,6 +368,48 @@ void rgbdflow_params_default(rgbdflow_params* p)
 
 int rgbdflow_abi_version(void) { return RGBDFLOW_ABI_VERSION; }
 
+int rgbdflow_pyramid_levels(int W, int H, double ratio, int min_width, int* w, int* h)
+{
+    if (W < 1 || H < 1 || min_width == 0) return RGBDFLOW_ERR_INVALID_ARG;
+    try {
+        const PyrShape s = pyramid_shape(W, H, ratio, min_width, 0);
+        const int L = (int)s.w.size();
+        if (L > RGBDFLOW_MAX_LEVELS) return RGBDFLOW_ERR_UNSUPPORTED;
+        for (int i = 0; i < L; i++) {
+            if (w) w[i] = s.w[i];
+            if (h) h[i] = s.h[i];
+        }
+        return L;
+    } catch (...) {
+        return RGBDFLOW_ERR_INTERNAL;
+    }
+}
+
+int rgbdflow_batch_device_bytes(const int* Ws, const int* Hs, const int* warm, int n, const rgbdflow_params* params,
+                                size_t* bytes)
+{
+    if (!Ws || !Hs || n <= 0 || !params || !bytes) return RGBDFLOW_ERR_INVALID_ARG;
+    try {
+        validate(params);
+        std::vector<PairSpec> ps(n);
+        static const float dummy = 1;
+        for (int i = 0; i < n; i++) {
+            ps[i].kind = 0; ps[i].W = Ws[i]; ps[i].H = Hs[i]; ps[i].f_full = 1; ps[i].xres_full = (unsigned)Ws[i];
+            if (warm && warm[i]) ps[i].est = &dummy;
+        }
+        const HostParams hp = host_params(*params);
+        if (params->compute == RGBDFLOW_COMPUTE_FP64) *bytes = make_plan<double, double>(ps, hp).arena_bytes;
+        else if (params->storage == RGBDFLOW_STORE_FP16) *bytes = make_plan<float, __half>(ps, hp).arena_bytes;
+        else if (params->storage == RGBDFLOW_STORE_BF16) *bytes = make_plan<float, __nv_bfloat16>(ps, hp).arena_bytes;
+        else *bytes = make_plan<float, float>(ps, hp).arena_bytes;
+        return RGBDFLOW_OK;
+    } catch (const ArgError& e) {
+        return e.code;
+    } catch (...) {
+        return RGBDFLOW_ERR_INTERNAL;
+    }
+}
+
 int rgbdflow_ctx_create(int device, size_t hbm_budget_bytes, rgbdflow_ctx** out)
 {
     if (!out) return RGBDFLOW_ERR_INVALID_ARG;
@@ -319,8 +421,12 @@ int rgbdflow_ctx_create(int device, size_t hbm_budget_bytes, rgbdflow_ctx** out)
     c->device = device;
     c->budget = hbm_budget_bytes;
     if (cudaSetDevice(device) != cudaSuccess) return RGBDFLOW_ERR_CUDA;
+    if (cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return RGBDFLOW_ERR_CUDA;
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return RGBDFLOW_ERR_CUDA;
     if (cudaEventCreate(&c->e0) != cudaSuccess || cudaEventCreate(&c->e1) != cudaSuccess) return RGBDFLOW_ERR_CUDA;
+    if (cudaEventCreateWithFlags(&c->done, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->desc_up, cudaEventDisableTiming) != cudaSuccess)
+        return RGBDFLOW_ERR_CUDA;
     const char* g = std::getenv("RGBDFLOW_NO_GRAPHS");
     c->use_graphs = !(g && g[0] == '1');
     *out = c.release();
@@ -331,8 +437,12 @@ int rgbdflow_ctx_destroy(rgbdflow_ctx* c)
 {
     if (!c) return RGBDFLOW_ERR_INVALID_ARG;
     cudaSetDevice(c->device);
+    if (c->pending) cudaEventSynchronize(c->done);
     if (c->stream) cudaStreamSynchronize(c->stream);
     drop_graphs(c);
+    c->prof.reset();
+    if (c->done) cudaEventDestroy(c->done);
+    if (c->desc_up) cudaEventDestroy(c->desc_up);
     if (c->arena) cudaFree(c->arena);
     if (c->pin) cudaFreeHost(c->pin);
     if (c->e0) cudaEventDestroy(c->e0);
@@ -481,9 +591,80 @@ int rgbdflow_scene_flow_single_scale(rgbdflow_ctx* c, const rgbdflow_camera_para
     API_END(c)
 }
 
-int rgbdflow_scene_flow_batch_async(rgbdflow_ctx* c, const rgbdflow_pair*, int, const rgbdflow_params*, void*)
+int rgbdflow_scene_flow_batch_async(rgbdflow_ctx* c, const rgbdflow_pair* pairs, int n, const rgbdflow_params* params,
+                                    void* stream)
 {
-    return fail(c, RGBDFLOW_ERR_UNSUPPORTED, "device-pointer batches are not built yet");
+    if (!c) return RGBDFLOW_ERR_INVALID_ARG;
+    API_BEGIN
+    validate(params);
+    if (!pairs || n <= 0) throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "no pairs");
+    RF_CUDA(cudaSetDevice(c->device));
+    std::vector<PairSpec> ps;
+    for (int i = 0; i < n; i++) {
+        const rgbdflow_pair& q = pairs[i];
+        if (q.W < 2 || q.H < 2 || !q.bgr1 || !q.bgr2 || !q.depth1_m || !q.depth2_m || !q.flow_out)
+            throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "pair " + std::to_string(i) + ": bad size or null buffer");
+        if (q.cam.xRes == 0 || !(q.cam.focalLength > 0))
+            throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "pair " + std::to_string(i) + ": bad camera");
+        PairSpec s;
+        s.W = q.W; s.H = q.H;
+        resized_cam(q.cam, q.W, s.f_full, s.xres_full);
+        s.bgr1 = q.bgr1; s.depth1 = q.depth1_m; s.bgr2 = q.bgr2; s.depth2 = q.depth2_m;
+        s.est = q.est_flow; s.out = q.flow_out;
+        ps.push_back(s);
+    }
+    dispatch(c, ps, *params, nullptr, stream ? (cudaStream_t)stream : c->stream);
+    return RGBDFLOW_OK;
+    API_END(c)
+}
+
+int rgbdflow_ctx_synchronize(rgbdflow_ctx* c)
+{
+    if (!c) return RGBDFLOW_ERR_INVALID_ARG;
+    API_BEGIN
+    wait_idle(c);
+    return RGBDFLOW_OK;
+    API_END(c)
+}
+
+int rgbdflow_ctx_last_launch_count(const rgbdflow_ctx* c) { return c ? c->last_launches : 0; }
+
+int rgbdflow_profile(rgbdflow_ctx* c, int enable)
+{
+    if (!c) return RGBDFLOW_ERR_INVALID_ARG;
+    API_BEGIN
+    wait_idle(c);
+    if (enable) {
+        c->prof.reset(new Prof());
+        for (int i = 0; i < KC_TOTAL; i++) { c->prof_ms[i] = 0; c->prof_n[i] = 0; c->prof_bytes[i] = 0; }
+    } else {
+        c->prof.reset();
+    }
+    return RGBDFLOW_OK;
+    API_END(c)
+}
+
+int rgbdflow_profile_read(rgbdflow_ctx* c, rgbdflow_kernel_stat* out, int max)
+{
+    if (!c || (!out && max > 0)) return RGBDFLOW_ERR_INVALID_ARG;
+    // the SOR total is the sum of its per-level classes
+    c->prof_ms[KC_SOR] = 0;
+    c->prof_n[KC_SOR] = 0;
+    for (int l = 0; l < 16; l++) { c->prof_ms[KC_SOR] += c->prof_ms[KC_SOR_LEVEL0 + l]; c->prof_n[KC_SOR] += c->prof_n[KC_SOR_LEVEL0 + l]; }
+    int k = 0;
+    for (int i = 0; i < KC_TOTAL; i++) {
+        if (!c->prof_n[i]) continue;
+        if (k < max) {
+            std::memset(&out[k], 0, sizeof(out[k]));
+            if (i < KC_N) std::snprintf(out[k].name, sizeof(out[k].name), "%s", kClassNames[i]);
+            else std::snprintf(out[k].name, sizeof(out[k].name), "sor_level%d", i - KC_SOR_LEVEL0);
+            out[k].launches = c->prof_n[i];
+            out[k].ms = c->prof_ms[i];
+            out[k].bytes = c->prof_bytes[i];
+        }
+        k++;
+    }
+    return k;
 }
 
 int rgbdflow_server_create(rgbdflow_ctx* c, const rgbdflow_server_config*, rgbdflow_server** out)

@@ -109,16 +109,22 @@ def default_params():
 
 
 def benchmark_params(W, **over):
-    """The benchmark schedule: ISOTROPIC, ratio 0.5 with minWidth = W/16 (5 levels), 10 outer,
-    1 inner, 30 SOR iterations, alpha 0.02, gamma 1e-5."""
+    """The benchmark schedule: ISOTROPIC, ratio 0.5 with minWidth = W/16 for every pair (5 levels;
+    min_width = -16), 10 outer, 1 inner, 30 SOR iterations, alpha 0.02, gamma 1e-5.  W is kept for
+    call-site symmetry; the per-pair rule makes one parameter set serve a ragged batch."""
     p = default_params()
     p.regularization = REG_ISOTROPIC
     p.pyramid_ratio = 0.5
-    p.min_width = max(1, W // 16)
+    p.min_width = -16
     p.n_outer, p.n_inner, p.n_sor = 10, 1, 30
     for k, v in over.items():
         setattr(p, k, v)
     return p
+
+
+class KernelStat(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char * 32), ("launches", ctypes.c_int), ("ms", ctypes.c_double),
+                ("bytes", ctypes.c_double)]
 
 
 class RgbdFlowPair(ctypes.Structure):
@@ -149,6 +155,8 @@ _d = ctypes.c_double
 SIGNATURES = {
     "rgbdflow_params_default": (None, [_P(Params)]),
     "rgbdflow_abi_version": (_i, []),
+    "rgbdflow_pyramid_levels": (_i, [_i, _i, _d, _i, _P(_i), _P(_i)]),
+    "rgbdflow_batch_device_bytes": (_i, [_P(_i), _P(_i), _P(_i), _i, _P(Params), _P(ctypes.c_size_t)]),
     "rgbdflow_ctx_create": (_i, [_i, ctypes.c_size_t, _P(_vp)]),
     "rgbdflow_ctx_destroy": (_i, [_vp]),
     "rgbdflow_last_error": (ctypes.c_char_p, [_vp]),
@@ -163,6 +171,10 @@ SIGNATURES = {
                                               _vp, _vp, _i, _i, _i, _i, _P(Params), _P(Stats)]),
     "rgbdflow_scene_flow_batch": (_i, [_vp, _P(RgbdFlowPair), _i, _P(Params), _P(Stats)]),
     "rgbdflow_scene_flow_batch_async": (_i, [_vp, _P(RgbdFlowPair), _i, _P(Params), _vp]),
+    "rgbdflow_ctx_synchronize": (_i, [_vp]),
+    "rgbdflow_ctx_last_launch_count": (_i, [_vp]),
+    "rgbdflow_profile": (_i, [_vp, _i]),
+    "rgbdflow_profile_read": (_i, [_vp, _P(KernelStat), _i]),
     "rgbdflow_server_create": (_i, [_vp, _P(ServerConfig), _P(_vp)]),
     "rgbdflow_server_destroy": (_i, [_vp]),
     "rgbdflow_server_submit": (_i, [_vp, _i, ctypes.c_uint64, _P(CameraParams), _vp, _vp, _i, _i, _vp]),
@@ -192,6 +204,31 @@ def _ptr(a):
 
 def _c(a, dt):
     return np.ascontiguousarray(a, dtype=dt)
+
+
+def pyramid_levels(W, H, ratio, min_width):
+    """[(w, h)] of the solve's pyramid, finest first (host-only)."""
+    lib = load()
+    w = (ctypes.c_int * MAX_LEVELS)()
+    h = (ctypes.c_int * MAX_LEVELS)()
+    n = lib.rgbdflow_pyramid_levels(W, H, ratio, min_width, w, h)
+    if n < 0:
+        raise RgbdFlowError(n, "rgbdflow_pyramid_levels failed")
+    return [(w[i], h[i]) for i in range(n)]
+
+
+def batch_device_bytes(sizes, params, warm=None):
+    """Device bytes a batch of (W, H) sizes needs (host-only)."""
+    lib = load()
+    n = len(sizes)
+    Ws = (ctypes.c_int * n)(*[s[0] for s in sizes])
+    Hs = (ctypes.c_int * n)(*[s[1] for s in sizes])
+    wm = (ctypes.c_int * n)(*([int(bool(x)) for x in warm] if warm else [0] * n))
+    out = ctypes.c_size_t()
+    rc = lib.rgbdflow_batch_device_bytes(Ws, Hs, wm, n, ctypes.byref(params), ctypes.byref(out))
+    if rc != OK:
+        raise RgbdFlowError(rc, "rgbdflow_batch_device_bytes failed")
+    return out.value
 
 
 class Context:
@@ -243,6 +280,29 @@ class Context:
         self._check(rc)
         return (out, st) if stats else out
 
+    def _dimage_call(self, fn, cam, Im1, dm1, Im2, dm2, sigma1, params, u=None, v=None, w=None):
+        Im1, Im2 = _c(Im1, np.float64), _c(Im2, np.float64)
+        dm1, dm2 = _c(dm1, np.float64), _c(dm2, np.float64)
+        sigma1 = _c(sigma1, np.float32)
+        H, W = dm1.shape
+        u = np.zeros((H, W)) if u is None else _c(u, np.float64).copy()
+        v = np.zeros((H, W)) if v is None else _c(v, np.float64).copy()
+        w = np.zeros((H, W)) if w is None else _c(w, np.float64).copy()
+        st = Stats()
+        rc = fn(self.h, ctypes.byref(cam), _ptr(Im1), _ptr(dm1), _ptr(Im2), _ptr(dm2), _ptr(sigma1), W, H,
+                ctypes.byref(params), _ptr(u), _ptr(v), _ptr(w), ctypes.byref(st))
+        self._check(rc)
+        return u, v, w, st
+
+    def scene_flow_multiscale(self, cam, Im1, dm1, Im2, dm2, sigma1, params):
+        """OpticalFlow::sceneFlowMultiscale on DImage-style FP64 buffers; returns (u, v, w, stats)."""
+        return self._dimage_call(self.lib.rgbdflow_scene_flow_multiscale, cam, Im1, dm1, Im2, dm2, sigma1, params)
+
+    def scene_flow_with_init(self, cam, Im1, dm1, Im2, dm2, sigma1, params, u, v, w):
+        """OpticalFlow::sceneFlowWithInit: one full-resolution level from the estimate (u, v, w)."""
+        return self._dimage_call(self.lib.rgbdflow_scene_flow_with_init, cam, Im1, dm1, Im2, dm2, sigma1, params,
+                                 u, v, w)
+
     def scene_flow_single_scale(self, cam, Im1, dm1, Im2, dm2, warpIm2, warpDm2, u, v, w, colorW, ddw, alpha, dsw,
                                 gamma, mag, regw, nOuter, nInner, nSOR, allowEarly, params=None):
         Im1, Im2 = _c(Im1, np.float64), _c(Im2, np.float64)
@@ -259,6 +319,41 @@ class Context:
             ctypes.byref(st))
         self._check(rc)
         return u, v, w, warpIm2, warpDm2, st
+
+    def last_launch_count(self):
+        return self.lib.rgbdflow_ctx_last_launch_count(self.h)
+
+    def synchronize(self):
+        self._check(self.lib.rgbdflow_ctx_synchronize(self.h))
+
+    def profile(self, enable):
+        self._check(self.lib.rgbdflow_profile(self.h, int(enable)))
+
+    def profile_read(self):
+        """{kernel class: (launches, ms, algorithmic bytes)} accumulated while profiling."""
+        buf = (KernelStat * 32)()
+        n = self.lib.rgbdflow_profile_read(self.h, buf, 32)
+        return {buf[i].name.decode(): (buf[i].launches, buf[i].ms, buf[i].bytes) for i in range(min(n, 32))}
+
+    def scene_flow_batch_device(self, pairs, params, stream=None):
+        """Device-pointer batch: pairs hold torch CUDA tensors (bgr1/bgr2 uint8 HxWx3, depth1/depth2
+        float32 HxW, out float32 HxWx3, optional est float32 HxWx3).  Enqueued on `stream` (a
+        torch.cuda.Stream, default: torch's current stream); returns without waiting."""
+        import torch
+        arr = (RgbdFlowPair * len(pairs))()
+        for i, p in enumerate(pairs):
+            arr[i].W, arr[i].H, arr[i].cam = p["W"], p["H"], p["cam"]
+            arr[i].bgr1, arr[i].depth1_m = p["bgr1"].data_ptr(), p["depth1"].data_ptr()
+            arr[i].bgr2, arr[i].depth2_m = p["bgr2"].data_ptr(), p["depth2"].data_ptr()
+            arr[i].est_flow = p["est"].data_ptr() if p.get("est") is not None else None
+            arr[i].flow_out = p["out"].data_ptr()
+        s = stream if stream is not None else torch.cuda.current_stream()
+        handle = s.cuda_stream
+        if handle == 0:
+            handle = 1  # torch's default stream is the legacy stream: cudaStreamLegacy, not NULL (NULL = the context's stream)
+        rc = self.lib.rgbdflow_scene_flow_batch_async(self.h, arr, len(pairs), ctypes.byref(params),
+                                                      ctypes.c_void_p(handle))
+        self._check(rc)
 
     def scene_flow_batch(self, pairs, params, stats=True):
         """pairs: list of dicts with W, H, cam (CameraParams), bgr1, depth1, bgr2, depth2[, est_flow].

@@ -245,3 +245,8 @@ def single_scale(f_level, Im1, dm1, Im2, dm2, wI2, wD2, u, v, w, colorW, ddw, al
     if rc != 0:
         raise RuntimeError("oracle: %s" % oracle().sfo_last_error().decode())
     return u, v, w, wI2, wD2, st
+
+
+def stereo_error1():
+    """primesensor::stereoError(1) (src/primesensorUtils.cpp:53-56)."""
+    return 1.0 / (1 / .00285 + 1.0)

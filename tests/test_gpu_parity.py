@@ -1,0 +1,259 @@
+"""Parity of the sm_100a solve (through the C ABI) with the CPU oracle, on a B200.
+
+Tolerances (3-D endpoint error over frame-1 pixels with valid depth, metres):
+  * against the faithful oracle, default hole fill:      mean <= 5e-5 (0.05 mm; the bar is 1 mm)
+  * against the oracle on inputs whose holes are isolated (where the parallel hole fill is exact):
+                                                          mean <= 2e-5
+  * FP64 device solve against the FP64 oracle, isolated holes: mean <= 1e-7
+  * batched result against the same pair solved alone:    bit-identical
+The executed schedule (outer iterations per level, SOR iterations per outer) must equal the
+oracle's on these seeded inputs.
+"""
+import numpy as np
+import pytest
+
+import oracle_binding as ob
+import rgbdflow as rf
+import synthetic as syn
+
+pytestmark = pytest.mark.gpu
+
+
+def cam_of(p):
+    c = p["cam"]
+    return rf.CameraParams.make(p["W"], p["H"], c.f, c.cx, c.cy)
+
+
+def lattice_holes(p, step=4):
+    """Holes only on a lattice: no two holes are 8-neighbours, so every hole has the reference's
+    fill value exactly."""
+    for k in ("depth1", "depth2"):
+        d = p[k].copy()
+        d[d == 0] = 2.0  # remove the generator's holes
+        d[1::step, 1::step] = 0
+        p[k] = d
+    return p
+
+
+def epe(a, b, p):
+    return syn.epe3d(a, b, p["z1_true"], p["cam"], p["depth1"] > 0)
+
+
+@pytest.mark.parametrize("name", ["320x240", "640x480"])
+@pytest.mark.parametrize("fixed", [1, 0])
+def test_two_frames_matches_oracle(ctx, name, fixed):
+    p = syn.make_config_pair(name, seed=1)
+    prm = rf.benchmark_params(p["W"], fixed_schedule=fixed)
+    cam = cam_of(p)
+    gpu, st = ctx.scene_flow_two_frames(cam, p["bgr1"], p["depth1"], p["bgr2"], p["depth2"], prm)
+    ref, rst = ob.two_frames(cam, p["bgr1"], p["depth1"], p["bgr2"], p["depth2"], prm)
+    mean, mx = epe(gpu, ref, p)
+    print("%s fixed=%d: EPE vs oracle mean %.3g mm max %.3g mm" % (name, fixed, mean * 1e3, mx * 1e3))
+    assert np.isfinite(gpu).all()
+    assert mean <= 5e-5
+    assert st.summary() == rst.summary()
+
+
+@pytest.mark.parametrize("name", ["320x240", "640x480"])
+def test_isolated_holes_tight(ctx, name):
+    p = lattice_holes(syn.make_config_pair(name, seed=2))
+    prm = rf.benchmark_params(p["W"], fixed_schedule=1)
+    cam = cam_of(p)
+    gpu, _ = ctx.scene_flow_two_frames(cam, p["bgr1"], p["depth1"], p["bgr2"], p["depth2"], prm)
+    ref, _ = ob.two_frames(cam, p["bgr1"], p["depth1"], p["bgr2"], p["depth2"], prm)
+    mean, mx = epe(gpu, ref, p)
+    print("%s isolated holes: mean %.3g mm max %.3g mm" % (name, mean * 1e3, mx * 1e3))
+    assert mean <= 2e-5
+
+
+def test_fp64_device_matches_fp64_oracle(ctx):
+    p = lattice_holes(syn.make_config_pair("320x240", seed=3))
+    prm = rf.benchmark_params(320, fixed_schedule=1, compute=rf.COMPUTE_FP64)
+    cam = cam_of(p)
+    gpu, _ = ctx.scene_flow_two_frames(cam, p["bgr1"], p["depth1"], p["bgr2"], p["depth2"], prm)
+    ref, _ = ob.two_frames(cam, p["bgr1"], p["depth1"], p["bgr2"], p["depth2"], prm, fp64=True)
+    mean, mx = epe(gpu, ref, p)
+    print("fp64: mean %.3g mm max %.3g mm" % (mean * 1e3, mx * 1e3))
+    assert mean <= 1e-7
+
+
+@pytest.mark.parametrize("W,H", [(97, 61), (33, 17), (130, 47)])
+def test_odd_sizes_and_reference_defaults(ctx, W, H):
+    """Sizes that are not multiples of any tile; the reference's own pyramid defaults (ratio 0.75)."""
+    p = syn.make_pair(W=W, H=H, f=0.8 * W, cx=(W - 1) / 2, cy=(H - 1) / 2, n_patches=2, hole_frac=0.04, seed=W)
+    prm = rf.default_params()
+    prm.regularization = rf.REG_ISOTROPIC
+    prm.min_width = max(4, W // 6)
+    prm.n_outer, prm.n_sor = 4, 27
+    cam = cam_of(p)
+    gpu, st = ctx.scene_flow_two_frames(cam, p["bgr1"], p["depth1"], p["bgr2"], p["depth2"], prm)
+    ref, rst = ob.two_frames(cam, p["bgr1"], p["depth1"], p["bgr2"], p["depth2"], prm)
+    mean, mx = epe(gpu, ref, p)
+    print("%dx%d: levels %d, mean %.3g mm max %.3g mm" % (W, H, st.n_levels, mean * 1e3, mx * 1e3))
+    assert st.n_levels == rst.n_levels
+    assert mean <= 1e-4
+
+
+def test_letouzey_regularisation(ctx):
+    """LETOUZEY weights exp(-((z - z_nbr) / 0.02)^2) (OpticalFlow.cpp:122-124).  On these scenes the
+    reference's own iteration is chaotic with them (decoupled pixels run away: the faithful and the
+    FP64 oracle already differ by tens of mm), so parity is judged against that spread: the device
+    result must be as close to the faithful oracle as the FP64 oracle is."""
+    W, H = 97, 61
+    # LETOUZEY weights are very sensitive to the filled depth of hole pixels, so the holes are put
+    # where the parallel hole fill is exact (an isolated-hole lattice)
+    p = lattice_holes(syn.make_pair(W=W, H=H, f=0.8 * W, cx=(W - 1) / 2, cy=(H - 1) / 2, n_patches=2,
+                                    hole_frac=0.04, seed=W))
+    prm = rf.default_params()
+    prm.regularization = rf.REG_LETOUZEY
+    prm.min_width = 16
+    prm.n_outer, prm.n_sor = 4, 27
+    cam = cam_of(p)
+    gpu, _ = ctx.scene_flow_two_frames(cam, p["bgr1"], p["depth1"], p["bgr2"], p["depth2"], prm)
+    ref, _ = ob.two_frames(cam, p["bgr1"], p["depth1"], p["bgr2"], p["depth2"], prm)
+    ref64, _ = ob.two_frames(cam, p["bgr1"], p["depth1"], p["bgr2"], p["depth2"], prm, fp64=True)
+    spread = epe(ref64, ref, p)[0]
+    mean = epe(gpu, ref, p)[0]
+    print("LETOUZEY: device vs oracle %.3g mm; FP64 oracle vs oracle %.3g mm" % (mean * 1e3, spread * 1e3))
+    assert np.isfinite(gpu).all()
+    assert mean <= 3 * spread + 5e-5
+    # one outer iteration with a tiny step is still in the well-conditioned regime: tight parity
+    prm.n_outer, prm.n_sor = 1, 5
+    gpu, _ = ctx.scene_flow_two_frames(cam, p["bgr1"], p["depth1"], p["bgr2"], p["depth2"], prm)
+    ref, _ = ob.two_frames(cam, p["bgr1"], p["depth1"], p["bgr2"], p["depth2"], prm)
+    assert epe(gpu, ref, p)[0] <= 1e-4
+
+
+def test_batch_equals_solo(ctx):
+    """A pair's result is the same alone and inside a ragged batch."""
+    specs = [("160x120", 4), ("640x480", 5), ("320x240", 6), ("160x120", 7), ("320x240", 8)]
+    pairs = []
+    for name, seed in specs:
+        p = syn.make_config_pair(name, seed=seed)
+        pairs.append(dict(W=p["W"], H=p["H"], cam=cam_of(p), bgr1=p["bgr1"], depth1=p["depth1"], bgr2=p["bgr2"],
+                          depth2=p["depth2"]))
+    outs = []
+    for q in pairs:
+        pp = rf.benchmark_params(640)
+        outs.append(ctx.scene_flow_two_frames(q["cam"], q["bgr1"], q["depth1"], q["bgr2"], q["depth2"], pp)[0])
+    batch, stats = ctx.scene_flow_batch(pairs, rf.benchmark_params(640))
+    for a, b in zip(outs, batch):
+        np.testing.assert_array_equal(a, b)
+
+
+def test_single_scale_seam_matches_oracle(ctx):
+    rng = np.random.default_rng(5)
+    W, H = 72, 50
+    p = syn.make_pair(W=W, H=H, f=60.0, cx=35.5, cy=24.5, n_patches=2, hole_frac=0.0, seed=21)
+    f1 = ob.im2feature(p["bgr1"] / 255.0)
+    f2 = ob.im2feature(p["bgr2"] / 255.0)
+    d1 = p["depth1"].astype(np.float64)
+    d2 = p["depth2"].astype(np.float64)
+    ddw = ob.stereo_error1() / ob.depth_sigma(p["depth1"]).astype(np.float64)
+    dsw = np.full((H, W), 3600.0)
+    mag = (60.0 / d1) ** 2
+    regw = rng.uniform(0.2, 1.0, (H, W, 2))
+    u0 = rng.normal(0, 0.3, (H, W))
+    v0 = rng.normal(0, 0.3, (H, W))
+    w0 = np.zeros((H, W))
+    wi, wd = ob.warp(f1, d1, f2, d2, u0, v0, w0)
+    cam = rf.CameraParams.make(W, H, 60.0, 35.5, 24.5)
+    for early in (0, 1):
+        g = ctx.scene_flow_single_scale(cam, f1, d1, f2, d2, wi, wd, u0, v0, w0, 1.0, ddw, 0.02, dsw, 1e-5, mag, regw,
+                                        5, 1, 30, early)
+        o = ob.single_scale(60.0, f1, d1, f2, d2, wi, wd, u0, v0, w0, 1.0, ddw, 0.02, dsw, 1e-5, mag, regw, 5, 1, 30,
+                            early)
+        o64 = ob.single_scale(60.0, f1, d1, f2, d2, wi, wd, u0, v0, w0, 1.0, ddw, 0.02, dsw, 1e-5, mag, regw, 5, 1,
+                              30, early, fp64=True)
+        # With non-uniform regularisation weights the iteration amplifies rounding: the reference's own
+        # FP32 and FP64 arithmetic already differ by ~1e-4 px here.  The device (FP32, reciprocal
+        # diagonals, contracted multiply-adds) must stay within 4x that spread of the faithful oracle.
+        for k in range(5):  # u, v, w, then the re-warped features and depth
+            spread = np.abs(o[k] - o64[k]).max()
+            np.testing.assert_allclose(g[k], o[k], atol=4 * spread + 1e-6)
+        assert g[5].summary() == o[5].summary()
+
+
+def test_multiscale_and_with_init_dimage_api(ctx):
+    p = syn.make_config_pair("320x240", seed=11)
+    prm = rf.benchmark_params(320)
+    cam = cam_of(p)
+    im1 = p["bgr1"] / 255.0
+    im2 = p["bgr2"] / 255.0
+    sig = ob.depth_sigma(p["depth1"])
+    u, v, w, st = ctx.scene_flow_multiscale(cam, im1, p["depth1"], im2, p["depth2"], sig, prm)
+    ref, rst = ob.two_frames(cam, p["bgr1"], p["depth1"], p["bgr2"], p["depth2"], prm)
+    gpu = np.stack([u, v, w], -1)
+    assert epe(gpu, ref, p)[0] <= 5e-5
+    # warm start from the ground truth motion (sceneFlowWithInit: one level, no early termination)
+    est = p["gt"].astype(np.float32)
+    u, v, w, st = ctx.scene_flow_with_init(cam, im1, p["depth1"], im2, p["depth2"], sig, prm,
+                                           est[..., 0], est[..., 1], est[..., 2])
+    ref, rst = ob.two_frames(cam, p["bgr1"], p["depth1"], p["bgr2"], p["depth2"], prm, est_flow=est)
+    gpu = np.stack([u, v, w], -1)
+    assert st.n_levels == 1 and rst.n_levels == 1
+    assert epe(gpu, ref, p)[0] <= 5e-5
+    assert st.summary() == rst.summary()
+
+
+@pytest.mark.parametrize("storage", [rf.STORE_FP16, rf.STORE_BF16])
+def test_reduced_precision_pyramids(ctx, storage):
+    """FP16 / BF16 storage of the image, depth and gradient planes; flow and Jacobi stay FP32."""
+    p = syn.make_config_pair("640x480", seed=1)
+    cam = cam_of(p)
+    prm32 = rf.benchmark_params(640, fixed_schedule=1)
+    prm = rf.benchmark_params(640, fixed_schedule=1, storage=storage)
+    a, _ = ctx.scene_flow_two_frames(cam, p["bgr1"], p["depth1"], p["bgr2"], p["depth2"], prm32)
+    b, _ = ctx.scene_flow_two_frames(cam, p["bgr1"], p["depth1"], p["bgr2"], p["depth2"], prm)
+    mean, mx = epe(a, b, p)
+    gt = syn.epe3d(b, p["gt"], p["z1_true"], p["cam"], p["depth1"] > 0)
+    print("storage %d: vs fp32 mean %.3g mm max %.3g mm; vs truth %.3g mm" % (storage, mean * 1e3, mx * 1e3, gt[0] * 1e3))
+    assert np.isfinite(b).all()
+    assert mean < 2e-3
+
+
+def test_errors_are_status_codes(ctx):
+    p = syn.make_pair(W=40, H=30, f=33.0, cx=19.5, cy=14.5, n_patches=1, hole_frac=0.0, seed=1)
+    cam = cam_of(p)
+    with pytest.raises(rf.RgbdFlowError) as e:
+        ctx.scene_flow_two_frames(cam, p["bgr1"], p["depth1"], p["bgr2"], p["depth2"], rf.default_params())
+    assert e.value.code == -2  # HPB regularisation is not built
+    small = rf.Context(0, hbm_budget_bytes=1 << 20)
+    with pytest.raises(rf.RgbdFlowError) as e:
+        small.scene_flow_two_frames(cam, p["bgr1"], p["depth1"], p["bgr2"], p["depth2"], rf.benchmark_params(40))
+    assert e.value.code == -4
+    small.close()
+    prm = rf.benchmark_params(40)
+    prm.n_inner = 0
+    with pytest.raises(rf.RgbdFlowError) as e:
+        ctx.scene_flow_two_frames(cam, p["bgr1"], p["depth1"], p["bgr2"], p["depth2"], prm)
+    assert e.value.code == -1
+
+
+@pytest.mark.skipif(not ob.ref_cuda_available(), reason="reference CUDA solver not compiled (oracle/_ref)")
+def test_reference_cuda_solver_pins_oracle():
+    """The reference's own sceneFlowSingleScale, compiled for sm_100a, against the oracle's
+    restatement of it on the same level inputs."""
+    rng = np.random.default_rng(8)
+    W, H = 64, 48
+    p = syn.make_pair(W=W, H=H, f=52.0, cx=31.5, cy=23.5, n_patches=2, hole_frac=0.0, seed=31)
+    f1 = ob.im2feature(p["bgr1"] / 255.0)
+    f2 = ob.im2feature(p["bgr2"] / 255.0)
+    d1 = p["depth1"].astype(np.float64)
+    d2 = p["depth2"].astype(np.float64)
+    ddw = ob.stereo_error1() / ob.depth_sigma(p["depth1"]).astype(np.float64)
+    dsw = np.full((H, W), 52.0 ** 2)
+    mag = (52.0 / d1) ** 2
+    regw = np.ones((H, W, 2))
+    regw[:, -1, 0] = 0
+    regw[-1, :, 1] = 0
+    u0 = rng.normal(0, 0.2, (H, W))
+    v0 = rng.normal(0, 0.2, (H, W))
+    w0 = np.zeros((H, W))
+    wi, wd = ob.warp(f1, d1, f2, d2, u0, v0, w0)
+    args = (52.0, f1, d1, f2, d2, wi, wd, u0, v0, w0, 1.0, ddw, 0.02, dsw, 1e-5, mag, regw, 4, 1, 30, 1)
+    r = ob.single_scale(*args, impl="ref")
+    o = ob.single_scale(*args)
+    np.testing.assert_allclose(o[0], r[0], atol=2e-5)
+    np.testing.assert_allclose(o[1], r[1], atol=2e-5)
+    np.testing.assert_allclose(o[2], r[2], atol=1e-6)
