@@ -155,6 +155,11 @@ def main():
     ap.add_argument("--batch", type=int, default=16)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--serve-frames", type=int, default=150)
+    ap.add_argument("--serve-unique", type=int, default=8)
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -177,15 +182,13 @@ def main():
         if world > 1:
             dist.barrier()
 
+    import replicas
+
     def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.max_over_ranks(x, device="cuda")
 
     B = args.batch
-    host = make_pairs(B, 1000 * rank)
+    host = make_pairs(B, replicas.pair_seed(rank, 0))
     prm = rf.benchmark_params(W)
     ctx = rf.Context(local)
     dev = []
@@ -219,7 +222,7 @@ def main():
     clk = clocks.stop()
     ms = max_over_ranks(e0.elapsed_time(e1))
     step_ms = [step_ev[i].elapsed_time(step_ev[i + 1]) for i in range(args.steps)]
-    value = B * args.steps * world / (ms / 1e3)
+    value = replicas.aggregate_rate(B * args.steps, world, ms / 1e3)
 
     # ---- batched result check: pair 0 of the batch equals the same pair solved alone
     solo = torch.empty((H, W, 3), dtype=torch.float32, device="cuda")
@@ -231,7 +234,7 @@ def main():
 
     # ---- plain: one pair per call (the drop-in form), per-call latency
     lat = []
-    for s in range(max(args.warmup, 2) + 20):
+    for s in range(0 if args.no_plain else max(args.warmup, 2) + 20):
         a = torch.cuda.Event(enable_timing=True)
         b = torch.cuda.Event(enable_timing=True)
         a.record(stream)
@@ -240,21 +243,30 @@ def main():
         torch.cuda.synchronize()
         if s >= max(args.warmup, 2):
             lat.append(a.elapsed_time(b))
-    plain = {"pairs_per_s": 1e3 / float(np.mean(lat)), "p50_ms": float(np.percentile(lat, 50)),
-             "p99_ms": float(np.percentile(lat, 99)), "calls": len(lat)}
+    plain = None
+    if lat:
+        plain = {"pairs_per_s": 1e3 / float(np.mean(lat)), "p50_ms": float(np.percentile(lat, 50)),
+                 "p99_ms": float(np.percentile(lat, 99)), "calls": len(lat)}
 
     # ---- e2e: host buffers through the synchronous C ABI call
-    hp = [dict(W=W, H=H, cam=cam_of(rf, p), bgr1=p["bgr1"], depth1=p["depth1"], bgr2=p["bgr2"], depth2=p["depth2"])
-          for p in host]
-    for _ in range(args.warmup):
-        flows = ctx.scene_flow_batch(hp, prm, stats=False)
-    barrier()
-    t = time.perf_counter()
-    for _ in range(args.steps):
-        flows = ctx.scene_flow_batch(hp, prm, stats=False)
-    e2e_s = max_over_ranks(time.perf_counter() - t)
-    e2e = {"value": B * args.steps * world / e2e_s, "unit": "pairs/s",
-           "h2d_bytes_per_step": B * W * H * (3 + 3 + 4 + 4), "d2h_bytes_per_step": B * W * H * 12}
+    # inputs and outputs in page-locked host memory: the library DMAs them directly
+    def pinned(a):
+        t = torch.from_numpy(a).pin_memory()
+        return t.numpy()
+    hp = [dict(W=W, H=H, cam=cam_of(rf, p), bgr1=pinned(p["bgr1"]), depth1=pinned(p["depth1"]),
+               bgr2=pinned(p["bgr2"]), depth2=pinned(p["depth2"])) for p in host]
+    pouts = [torch.empty((H, W, 3), dtype=torch.float32).pin_memory().numpy() for _ in host]
+    e2e = None
+    if not args.no_e2e:
+        for _ in range(args.warmup):
+            flows = ctx.scene_flow_batch(hp, prm, stats=False, outs=pouts)
+        barrier()
+        t = time.perf_counter()
+        for _ in range(args.steps):
+            flows = ctx.scene_flow_batch(hp, prm, stats=False, outs=pouts)
+        e2e_s = max_over_ranks(time.perf_counter() - t)
+        e2e = {"value": B * args.steps * world / e2e_s, "unit": "pairs/s",
+               "h2d_bytes_per_step": B * W * H * (3 + 3 + 4 + 4), "d2h_bytes_per_step": B * W * H * 12}
 
     # ---- roofline of the dominant kernel from a profiled pass of the same workload
     ctx.profile(1)
@@ -265,18 +277,54 @@ def main():
     ctx.profile(0)
     peak, peak_kind = peaks()
     n_sor, sor_ms, sor_bytes = kst.get("sor", (0, 0.0, 0.0))
-    tot_ms = sum(v[1] for v in kst.values())
     achieved = sor_bytes / (sor_ms / 1e3) / 1e9 if sor_ms > 0 else 0.0
     tr = ncu_traffic()
-    roofline = {"kernel": "k_sor (red-black SOR, 5 iterations per launch)", "bound": "hbm", "achieved": achieved,
+    base_ms = sum(v[1] for k, v in kst.items() if not k.startswith("sor_level"))
+    tot_ms = base_ms
+    abpl = sor_bytes / max(n_sor, 1)
+    roofline = {"kernel": "k_sor (red-black SOR, temporal blocking, K sweeps per launch chosen per level)",
+                "bound": "hbm", "achieved": achieved,
                 "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
-                "traffic": (tr["dram_bytes_per_launch"] if tr else None),
-                "algorithmic_bytes_per_launch": sor_bytes / max(n_sor, 1),
+                "traffic": (tr["dram_bytes_per_algorithmic_byte"] * abpl if tr else None),
+                "algorithmic_bytes_per_launch": abpl,
                 "avg_launch_us": 1e3 * sor_ms / max(n_sor, 1), "launches": n_sor,
                 "share_of_device_time": sor_ms / tot_ms if tot_ms else None,
                 "kernel_ms": {k: round(v[1], 3) for k, v in kst.items()}}
     if tr:
         roofline["traffic_note"] = tr.get("note", "")
+
+    # ---- served: camera streams at 30 fps (Poisson arrivals) through the continuous-batching
+    # server, warm starts from each stream's previous flow
+    served = None
+    if not args.no_serve:
+        import serving
+        streams = serving.make_streams(n_unique=args.serve_unique, seed0=500 + 100 * rank)
+        srv = rf.Server(ctx, prm, max_streams=len(streams), max_batch=len(streams), hbm_budget_bytes=20 << 30,
+                        warm_start=True, warm_early_termination=True)
+        serving.simulate(srv, rf, streams, n_frames=2 * args.serve_unique, fps=30.0, seed=1)  # warm-up: graphs
+        r = serving.simulate(srv, rf, streams, n_frames=args.serve_frames, fps=30.0, seed=2, keep_stream=0, keep_n=6)
+        lat = np.array(r["latencies_ms"])
+        sat = serving.simulate(srv, rf, streams, n_frames=args.serve_unique * 3, fps=30.0, seed=3, time_scale=0.0)
+        srv.close()
+        # matched EPE: the served (warm-started) flows against the plain coarse-to-fine solve of the same pairs
+        seq = streams[0]
+        epes = []
+        for rid, flow in r["kept"]:
+            n = len(seq["frames"])
+            f1 = seq["frames"][serving.frame_index(rid - 1, n)]
+            f2 = seq["frames"][serving.frame_index(rid, n)]
+            camp = rf.CameraParams.make(seq["W"], seq["H"], seq["cam"].f, seq["cam"].cx, seq["cam"].cy)
+            plain_f = ctx.scene_flow_two_frames(camp, f1["bgr"], f1["depth"], f2["bgr"], f2["depth"], prm, stats=False)
+            z = np.where(f1["depth"] > 0, f1["depth"], 2.0).astype(np.float64)
+            epes.append(syn.epe3d(flow, plain_f, z, seq["cam"], f1["depth"] > 0)[0])
+        served = {"streams": "5 x 640x480 + 3 x 320x240 at 30 fps, Poisson arrivals, warm starts from the "
+                             "previous flow (full-resolution level, early termination allowed)",
+                  "pairs": r["pairs"], "pairs_per_s": r["pairs"] / r["wall_s"],
+                  "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                  "max_ms": float(lat.max()),
+                  "saturated_pairs_per_s": sat["pairs"] / sat["wall_s"],
+                  "epe_vs_plain_mm": 1e3 * float(np.mean(epes)) if epes else None,
+                  "hbm_budget_gb": 20}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -296,7 +344,7 @@ def main():
                            "global_batch": B * world, "parallelism": "replicas x%d" % world,
                            "l2": "inputs larger than L2 (working set %.2f GB per GPU)" % (ctx.device_bytes() / 1e9)},
                 "p50_ms": float(np.percentile(step_ms, 50)), "p99_ms": float(np.percentile(step_ms, 99)),
-                "plain": plain, "batch_equals_solo": same,
+                "plain": plain, "batch_equals_solo": same, "served": served,
                 "gpu_launches": launches_per_step * args.steps,
                 "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk}
         print(json.dumps(line), flush=True)

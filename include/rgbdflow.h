@@ -268,7 +268,10 @@ typedef struct rgbdflow_server_config {
     int    max_streams;        /* distinct camera streams */
     int    max_batch;          /* pairs solved per device step */
     size_t hbm_budget_bytes;   /* admission budget for resident state + in-flight pairs */
-    int    warm_start;         /* 1: initialise each pair from the stream's previous flow */
+    int    warm_start;         /* 1: initialise each pair from the stream's previous flow and solve it at
+                                  full resolution only (sceneFlowWithInit, src/sceneFlowWithInit.cpp:7-81) */
+    int    warm_early_termination; /* 1: warm-started pairs may stop their outer iterations early (the
+                                  reference's with-init path never does, sceneFlowWithInit.cpp:74) */
     rgbdflow_params params;
 } rgbdflow_server_config;
 

@@ -98,7 +98,8 @@ struct PairSpec {
     const double* ddw = nullptr; const double* dsw = nullptr; const double* mag = nullptr;
     const double* regw = nullptr;               // W*H*2
     float f_level = 0;
-    int allow_early = 0;
+    int allow_early = 0;        // kind 2; and for kinds 0/1 warm starts when warm_early is set
+    int warm_early = 0;         // warm-started pair may stop its outer iterations early
     // outputs
     float* out = nullptr;                       // kind 0: W*H*3 interleaved float
     double* out_u = nullptr; double* out_v = nullptr; double* out_w = nullptr;  // kinds 1, 2
@@ -154,7 +155,7 @@ static inline SorConfig choose_sor_config(const HostParams& hp, long level_px)
     SorConfig c;
     c.K = hp.K > 0 ? hp.K : (level_px >= (1L << 20) ? 2 : 5);
     c.nbuf = hp.sor_nbuf > 0 ? hp.sor_nbuf : 1;
-    c.ilp = hp.sor_ilp > 0 ? hp.sor_ilp : 2;
+    c.ilp = hp.sor_ilp > 0 ? hp.sor_ilp : 1;
     while (c.K > 1 && !sor_cfg_fits<T>(c)) {
         if (c.nbuf == 2) c.nbuf = 1;
         else c.K--;
@@ -433,6 +434,7 @@ static Plan<T, S> make_plan(const std::vector<PairSpec>& pairs, const HostParams
             const double sf = (double)s.w[k] / pairs[p].xres_full;
             it.f_level = (T)(float)(pairs[p].f_full * sf);
             if (P.kind == 2) { it.allow_early = pairs[p].allow_early; it.f_level = (T)pairs[p].f_level; }
+            else if (pairs[p].warm() && pairs[p].warm_early) it.allow_early = 1;
             it.ctl = (PairCtl*)(P.ctl_off + sizeof(PairCtl) * p);
             for (int c = 0; c < 10; c++) it.pyr[c] = (T*)m.pyr[c];
             for (int c = 0; c < 5; c++) { it.I1[c] = (S*)m.I1[c]; it.I2[c] = (S*)m.I2[c]; }

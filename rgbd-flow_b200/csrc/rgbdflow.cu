@@ -15,6 +15,7 @@
 
 #include "../../include/rgbdflow.h"
 #include "pipeline.cuh"
+#include "server.cuh"
 
 using namespace rgbdflow;
 
@@ -59,6 +60,14 @@ void drop_graphs(rgbdflow_ctx* c)
         if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
     }
     c->graphs.clear();
+}
+
+// page-locked (cudaMallocHost / cudaHostRegister) host memory can be copied by DMA directly
+bool is_pinned(const void* p)
+{
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) { cudaGetLastError(); return false; }
+    return a.type == cudaMemoryTypeHost;
 }
 
 void wait_idle(rgbdflow_ctx* c)
@@ -148,7 +157,7 @@ std::string plan_key(const std::vector<PairSpec>& ps, const HostParams& hp, int 
 {
     std::string k = std::to_string(tag) + ":";
     for (const auto& p : ps)
-        k += std::to_string(p.kind) + "k" + std::to_string(p.W) + "x" + std::to_string(p.H) + (p.warm() ? "e" : "") +
+        k += std::to_string(p.kind) + "k" + std::to_string(p.W) + "x" + std::to_string(p.H) + (p.warm() ? (p.warm_early ? "E" : "e") : "") +
              (p.kind == 2 ? "a" + std::to_string(p.allow_early) + "g" + std::to_string(p.f_level) : std::string()) + "f" + std::to_string(p.f_full) +
              "r" + std::to_string(p.xres_full) + ",";
     char buf[512];
@@ -223,18 +232,35 @@ void run_batch(rgbdflow_ctx* c, const std::vector<PairSpec>& pairs, const HostPa
     char* pin_desc = pin_in + in_b;
     char* pin_out = pin_desc + align_up(P.desc_bytes, 256);
     char* pin_ctl = pin_out + out_b;
+    // host inputs: page-locked caller buffers are copied by DMA directly, others through staging
+    std::vector<std::pair<const void*, std::pair<size_t, size_t>>> direct;  // (src, (arena off, bytes))
     if (!dev)
         for (int p = 0; p < P.n; p++) {
             const auto segs = pairs[p].inputs();
             for (size_t q = 0; q < segs.size(); q++) {
                 if (!segs[q].first) throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "pair " + std::to_string(p) + ": null input buffer");
-                std::memcpy(pin_in + (P.in_seg[p][q] - P.in_off), segs[q].first, segs[q].second);
+                if (is_pinned(segs[q].first)) direct.push_back({segs[q].first, {P.in_seg[p][q], segs[q].second}});
+                else std::memcpy(pin_in + (P.in_seg[p][q] - P.in_off), segs[q].first, segs[q].second);
             }
         }
     std::memcpy(pin_desc, P.desc.data(), P.desc_bytes);
     cudaStream_t st = dev ? user_stream : c->stream;
     if (c->pending) RF_CUDA(cudaStreamWaitEvent(st, c->done, 0));  // arena reuse across streams
-    if (!dev) RF_CUDA(cudaMemcpyAsync(c->arena + P.in_off, pin_in, P.in_bytes, cudaMemcpyHostToDevice, st));
+    if (!dev) {
+        if (direct.empty()) {
+            RF_CUDA(cudaMemcpyAsync(c->arena + P.in_off, pin_in, P.in_bytes, cudaMemcpyHostToDevice, st));
+        } else {
+            for (int p = 0; p < P.n; p++) {
+                const auto segs = pairs[p].inputs();
+                for (size_t q = 0; q < segs.size(); q++)
+                    if (!is_pinned(segs[q].first))
+                        RF_CUDA(cudaMemcpyAsync(c->arena + P.in_seg[p][q], pin_in + (P.in_seg[p][q] - P.in_off),
+                                                segs[q].second, cudaMemcpyHostToDevice, st));
+            }
+            for (const auto& d : direct)
+                RF_CUDA(cudaMemcpyAsync(c->arena + d.second.first, d.first, d.second.second, cudaMemcpyHostToDevice, st));
+        }
+    }
     RF_CUDA(cudaMemcpyAsync(c->arena + P.desc_off, pin_desc, P.desc_bytes, cudaMemcpyHostToDevice, st));
     RF_CUDA(cudaEventRecord(c->desc_up, st));
     RF_CUDA(cudaEventRecord(c->e0, st));
@@ -266,7 +292,20 @@ void run_batch(rgbdflow_ctx* c, const std::vector<PairSpec>& pairs, const HostPa
         c->last_launches = enqueue_solve(P, c->arena, st, c->prof.get());
     }
     RF_CUDA(cudaEventRecord(c->e1, st));
-    if (!dev) RF_CUDA(cudaMemcpyAsync(pin_out, c->arena + P.out_off, P.out_bytes, cudaMemcpyDeviceToHost, st));
+    // outputs: FP32 flows into page-locked caller buffers by DMA directly, the rest through staging
+    std::vector<char> out_direct(P.n, 0);
+    if (!dev) {
+        bool all_direct = true;
+        for (int p = 0; p < P.n; p++) {
+            out_direct[p] = (sizeof(T) == 4 && pairs[p].out && !pairs[p].out_u && is_pinned(pairs[p].out)) ? 1 : 0;
+            all_direct = all_direct && out_direct[p];
+        }
+        for (int p = 0; p < P.n; p++)
+            if (out_direct[p])
+                RF_CUDA(cudaMemcpyAsync(pairs[p].out, c->arena + P.out_pair_off[p], (size_t)pairs[p].W * pairs[p].H * 12,
+                                        cudaMemcpyDeviceToHost, st));
+        if (!all_direct) RF_CUDA(cudaMemcpyAsync(pin_out, c->arena + P.out_off, P.out_bytes, cudaMemcpyDeviceToHost, st));
+    }
     const bool want_ctl = stats || c->prof;
     if (want_ctl) RF_CUDA(cudaMemcpyAsync(pin_ctl, c->arena + P.ctl_off, ctl_bytes, cudaMemcpyDeviceToHost, st));
     RF_CUDA(cudaEventRecord(c->done, st));
@@ -288,7 +327,7 @@ void run_batch(rgbdflow_ctx* c, const std::vector<PairSpec>& pairs, const HostPa
             const size_t N = (size_t)pairs[p].W * pairs[p].H;
             const T* o = (const T*)(pin_out + (P.out_pair_off[p] - P.out_off));
             const PairSpec& q = pairs[p];
-            if (q.out)
+            if (q.out && !out_direct[p])
                 for (size_t z = 0; z < N * 3; z++) q.out[z] = (float)o[z];
             if (q.out_u)
                 for (size_t z = 0; z < N; z++) { q.out_u[z] = (double)o[z * 3]; q.out_v[z] = (double)o[z * 3 + 1]; q.out_w[z] = (double)o[z * 3 + 2]; }
@@ -667,22 +706,242 @@ int rgbdflow_profile_read(rgbdflow_ctx* c, rgbdflow_kernel_stat* out, int max)
     return k;
 }
 
-int rgbdflow_server_create(rgbdflow_ctx* c, const rgbdflow_server_config*, rgbdflow_server** out)
+int rgbdflow_server_create(rgbdflow_ctx* c, const rgbdflow_server_config* cfg, rgbdflow_server** out)
 {
-    if (out) *out = nullptr;
-    return fail(c, RGBDFLOW_ERR_UNSUPPORTED, "serving is not built yet");
+    if (!c || !cfg || !out) return RGBDFLOW_ERR_INVALID_ARG;
+    *out = nullptr;
+    API_BEGIN
+    validate(&cfg->params);
+    if (cfg->params.compute == RGBDFLOW_COMPUTE_FP64) throw ArgError(RGBDFLOW_ERR_UNSUPPORTED, "serving runs the FP32 solve");
+    if (cfg->max_streams <= 0 || cfg->max_batch <= 0) throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "max_streams and max_batch must be > 0");
+    RF_CUDA(cudaSetDevice(c->device));
+    std::unique_ptr<rgbdflow_server> s(new rgbdflow_server());
+    s->ctx = c;
+    s->cfg = *cfg;
+    RF_CUDA(cudaStreamCreateWithFlags(&s->upload, cudaStreamNonBlocking));
+    for (auto& sl : s->slots) {
+        const int rc = rgbdflow_ctx_create(c->device, 0, &sl.ctx);
+        if (rc != RGBDFLOW_OK) throw ArgError(rc, "slot context creation failed");
+        sl.st = sl.ctx->stream;
+        RF_CUDA(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming));
+    }
+    *out = s.release();
+    return RGBDFLOW_OK;
+    API_END(c)
 }
-int rgbdflow_server_destroy(rgbdflow_server*) { return RGBDFLOW_ERR_UNSUPPORTED; }
-int rgbdflow_server_submit(rgbdflow_server*, int, uint64_t, const rgbdflow_camera_params*, const uint8_t*, const float*,
-                           int, int, float*)
+
+int rgbdflow_server_destroy(rgbdflow_server* s)
 {
-    return RGBDFLOW_ERR_UNSUPPORTED;
+    if (!s) return RGBDFLOW_ERR_INVALID_ARG;
+    for (auto& sl : s->slots) {
+        if (sl.busy) cudaEventSynchronize(sl.done);
+        sl.reqs.clear();
+        if (sl.done) cudaEventDestroy(sl.done);
+        if (sl.pin_out) cudaFreeHost(sl.pin_out);
+        if (sl.ctx) rgbdflow_ctx_destroy(sl.ctx);
+    }
+    if (s->upload) cudaStreamSynchronize(s->upload);
+    s->queue.clear();
+    for (auto& kv : s->streams) {
+        kv.second.prev.reset();
+        if (kv.second.flow) cudaFree(kv.second.flow);
+    }
+    s->pool.release_all();
+    if (s->upload) cudaStreamDestroy(s->upload);
+    delete s;
+    return RGBDFLOW_OK;
 }
-int rgbdflow_server_step(rgbdflow_server*, int, rgbdflow_result*, int, int* n)
+
+int rgbdflow_server_submit(rgbdflow_server* s, int stream_id, uint64_t request_id, const rgbdflow_camera_params* cam,
+                           const uint8_t* bgr, const float* depth_m, int W, int H, float* flow_out)
 {
-    if (n) *n = 0;
-    return RGBDFLOW_ERR_UNSUPPORTED;
+    if (!s) return RGBDFLOW_ERR_INVALID_ARG;
+    rgbdflow_ctx* c = s->ctx;
+    API_BEGIN
+    if (!cam || !bgr || !depth_m || W < 2 || H < 2) throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "bad frame");
+    if (cam->xRes == 0 || !(cam->focalLength > 0)) throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "bad camera");
+    auto it = s->streams.find(stream_id);
+    if (it == s->streams.end()) {
+        if ((int)s->streams.size() >= s->cfg.max_streams) throw ArgError(RGBDFLOW_ERR_BUSY, "too many streams");
+        it = s->streams.emplace(stream_id, StreamState()).first;
+    }
+    StreamState& ss = it->second;
+    const size_t N = (size_t)W * H;
+    const size_t fbytes = N * 3 + N * 4;
+    if (s->cfg.hbm_budget_bytes && s->resident_bytes + fbytes + N * 12 > s->cfg.hbm_budget_bytes)
+        throw ArgError(RGBDFLOW_ERR_BUDGET, "frame does not fit the HBM budget");
+    s->pool.resident = &s->resident_bytes;
+    RF_CUDA(cudaSetDevice(c->device));
+    auto f = std::make_shared<DevFrame>();
+    f->W = W; f->H = H; f->cam = *cam;
+    f->bufs = s->pool.get(N);
+    f->pool = &s->pool;
+    f->bgr = f->bufs.dev;
+    f->depth = (float*)(f->bufs.dev + align_up(N * 3, 256));
+    f->ready = f->bufs.ready;
+    // the pinned staging may still feed this buffer set's previous upload
+    RF_CUDA(cudaEventSynchronize(f->ready));
+    std::memcpy(f->bufs.pin, bgr, N * 3);
+    std::memcpy(f->bufs.pin + N * 3, depth_m, N * 4);
+    RF_CUDA(cudaMemcpyAsync(f->bgr, f->bufs.pin, N * 3, cudaMemcpyHostToDevice, s->upload));
+    RF_CUDA(cudaMemcpyAsync(f->depth, f->bufs.pin + N * 3, N * 4, cudaMemcpyHostToDevice, s->upload));
+    RF_CUDA(cudaEventRecord(f->ready, s->upload));
+    if (ss.prev && (ss.W != W || ss.H != H)) {  // a resolution change restarts the stream
+        ss.has_flow = false;
+        ss.prev.reset();
+    }
+    if (!ss.flow || ss.W != W || ss.H != H) {
+        if (ss.flow) { RF_CUDA(cudaFree(ss.flow)); s->resident_bytes -= (size_t)ss.W * ss.H * 12; }
+        RF_CUDA(cudaMalloc(&ss.flow, N * 12));
+        s->resident_bytes += N * 12;
+        ss.has_flow = false;
+    }
+    ss.W = W; ss.H = H;
+    if (ss.prev) {
+        ServerReq r;
+        r.stream = stream_id; r.id = request_id; r.W = W; r.H = H;
+        r.f1 = ss.prev; r.f2 = f; r.out_host = flow_out; r.t_submit = mono_now();
+        s->queue.push_back(r);
+    }
+    ss.prev = f;
+    return RGBDFLOW_OK;
+    API_END(c)
 }
-int rgbdflow_server_pending(const rgbdflow_server*) { return 0; }
+
+namespace {
+
+void server_retire(rgbdflow_server* s, ServerSlot& sl)
+{
+    const double now = mono_now();
+    for (size_t i = 0; i < sl.reqs.size(); i++) {
+        ServerReq& r = sl.reqs[i];
+        const size_t N = (size_t)r.W * r.H;
+        if (r.out_host) std::memcpy(r.out_host, sl.pin_out + sl.out_off[i], N * 12);
+        rgbdflow_result res;
+        res.stream_id = r.stream; res.request_id = r.id; res.W = r.W; res.H = r.H; res.flow = r.out_host;
+        res.submit_time_s = r.t_submit; res.done_time_s = now; res.status = RGBDFLOW_OK;
+        s->ready.push_back(res);
+        StreamState& ss = s->streams[r.stream];
+        ss.in_flight = false;
+        ss.has_flow = true;
+        // frames no longer referenced by any pair or stream return to the pool
+        r.f1.reset();
+        r.f2.reset();
+    }
+    sl.reqs.clear();
+    sl.busy = false;
+}
+
+size_t slot_arena_need(const std::vector<PairSpec>& ps, const HostParams& hp, int storage)
+{
+    if (storage == RGBDFLOW_STORE_FP16) return make_plan<float, __half>(ps, hp).arena_bytes;
+    if (storage == RGBDFLOW_STORE_BF16) return make_plan<float, __nv_bfloat16>(ps, hp).arena_bytes;
+    return make_plan<float, float>(ps, hp).arena_bytes;
+}
+
+void server_launch(rgbdflow_server* s, ServerSlot& sl)
+{
+    // admit queued requests in arrival order: one pair per stream in flight, max_batch per slot,
+    // the slot's solve memory inside the HBM budget
+    const HostParams hp = host_params(s->cfg.params);
+    std::vector<ServerReq> take;
+    std::vector<PairSpec> specs;
+    const size_t other = s->slots[0].ctx == sl.ctx ? s->slots[1].ctx->arena_cap : s->slots[0].ctx->arena_cap;
+    for (auto it = s->queue.begin(); it != s->queue.end() && (int)take.size() < s->cfg.max_batch;) {
+        StreamState& ss = s->streams[it->stream];
+        bool dup = false;
+        for (const auto& t : take) dup = dup || t.stream == it->stream;
+        if (ss.in_flight || dup) { ++it; continue; }
+        PairSpec q;
+        q.W = it->W; q.H = it->H;
+        resized_cam(it->f1->cam, it->W, q.f_full, q.xres_full);
+        q.bgr1 = it->f1->bgr; q.depth1 = it->f1->depth; q.bgr2 = it->f2->bgr; q.depth2 = it->f2->depth;
+        q.est = (s->cfg.warm_start && ss.has_flow) ? ss.flow : nullptr;
+        q.warm_early = s->cfg.warm_early_termination;
+        q.out = ss.flow;
+        specs.push_back(q);
+        if (s->cfg.hbm_budget_bytes &&
+            s->resident_bytes + other + slot_arena_need(specs, hp, s->cfg.params.storage) > s->cfg.hbm_budget_bytes) {
+            specs.pop_back();
+            break;  // the budget is full: later requests wait for memory
+        }
+        take.push_back(*it);
+        it = s->queue.erase(it);
+    }
+    if (take.empty()) return;
+    // canonical order (largest first) so recurring size mixes reuse one cached graph
+    std::vector<size_t> order(take.size());
+    for (size_t i = 0; i < order.size(); i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) {
+        return (long)specs[a].W * specs[a].H > (long)specs[b].W * specs[b].H ||
+               ((long)specs[a].W * specs[a].H == (long)specs[b].W * specs[b].H && (specs[a].est != nullptr) < (specs[b].est != nullptr));
+    });
+    std::vector<PairSpec> ps;
+    sl.reqs.clear();
+    for (size_t i : order) { ps.push_back(specs[i]); sl.reqs.push_back(take[i]); }
+    for (const auto& r : sl.reqs) {
+        s->streams[r.stream].in_flight = true;
+        RF_CUDA(cudaStreamWaitEvent(sl.st, r.f1->ready, 0));
+        RF_CUDA(cudaStreamWaitEvent(sl.st, r.f2->ready, 0));
+    }
+    size_t total = 0;
+    sl.out_off.clear();
+    for (const auto& r : sl.reqs) { sl.out_off.push_back(total); total += align_up((size_t)r.W * r.H * 12, 256); }
+    if (sl.pin_cap < total) {
+        if (sl.pin_out) RF_CUDA(cudaFreeHost(sl.pin_out));
+        RF_CUDA(cudaMallocHost(&sl.pin_out, total));
+        sl.pin_cap = total;
+    }
+    dispatch(sl.ctx, ps, s->cfg.params, nullptr, sl.st);
+    for (size_t i = 0; i < sl.reqs.size(); i++)
+        RF_CUDA(cudaMemcpyAsync(sl.pin_out + sl.out_off[i], ps[i].out, (size_t)ps[i].W * ps[i].H * 12,
+                                cudaMemcpyDeviceToHost, sl.st));
+    RF_CUDA(cudaEventRecord(sl.done, sl.st));
+    sl.busy = true;
+}
+
+}  // namespace
+
+int rgbdflow_server_step(rgbdflow_server* s, int wait, rgbdflow_result* out, int max, int* n_out)
+{
+    if (!s || !n_out) return RGBDFLOW_ERR_INVALID_ARG;
+    *n_out = 0;
+    rgbdflow_ctx* c = s->ctx;
+    API_BEGIN
+    RF_CUDA(cudaSetDevice(c->device));
+    // retire finished slots; with `wait`, block on the oldest busy slot if nothing finished
+    bool any = false;
+    for (auto& sl : s->slots)
+        if (sl.busy && cudaEventQuery(sl.done) == cudaSuccess) { server_retire(s, sl); any = true; }
+    cudaGetLastError();
+    if (wait && !any) {
+        ServerSlot* oldest = nullptr;
+        for (auto& sl : s->slots)
+            if (sl.busy) { oldest = &sl; break; }
+        if (oldest) {
+            RF_CUDA(cudaEventSynchronize(oldest->done));
+            server_retire(s, *oldest);
+        }
+    }
+    // launch into free slots
+    for (auto& sl : s->slots)
+        if (!sl.busy && !s->queue.empty()) server_launch(s, sl);
+    int n = 0;
+    while (!s->ready.empty() && n < max) {
+        out[n++] = s->ready.front();
+        s->ready.pop_front();
+    }
+    *n_out = n;
+    return RGBDFLOW_OK;
+    API_END(c)
+}
+
+int rgbdflow_server_pending(const rgbdflow_server* s)
+{
+    if (!s) return 0;
+    int n = (int)s->queue.size() + (int)s->ready.size();
+    for (const auto& sl : s->slots) n += (int)sl.reqs.size();
+    return n;
+}
 
 }  // extern "C"

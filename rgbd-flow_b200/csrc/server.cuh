@@ -1,0 +1,121 @@
+// server.cuh — the served form: continuous batching of frame pairs from camera streams.
+//
+// Frames are uploaded once, when submitted, into device buffers that two consecutive pairs of a
+// stream share (the frame is frame 2 of one pair and frame 1 of the next).  Each stream keeps its
+// last flow on the device; with warm starts a pair is initialised from it and solved at full
+// resolution only (sceneFlowWithInit semantics, src/sceneFlowWithInit.cpp:7-81).  Two solve slots,
+// each with its own context (arena, stream, graphs), keep the device busy: while one slot's batch
+// runs, requests that arrive are admitted into the other slot's batch as soon as it is free and
+// the HBM budget allows, so their uploads and solves overlap the running batch.
+#pragma once
+#include <time.h>
+
+#include <deque>
+#include <memory>
+#include <unordered_map>
+
+namespace rgbdflow {
+
+static inline double mono_now()
+{
+    timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return ts.tv_sec + 1e-9 * ts.tv_nsec;
+}
+
+// Device + pinned buffers of one uploaded frame.  They come from, and go back to, the server's
+// pool (no allocation, hence no implicit device synchronisation, in the steady state).
+struct FrameBufs {
+    uint8_t* dev = nullptr;   // bgr (W*H*3, 256-aligned) then depth (W*H float)
+    char* pin = nullptr;
+    cudaEvent_t ready = nullptr;
+    size_t bytes = 0;
+};
+
+struct FramePool {
+    std::unordered_map<size_t, std::vector<FrameBufs>> free_;
+    size_t* resident = nullptr;
+    FrameBufs get(size_t n_px)
+    {
+        auto& v = free_[n_px];
+        if (!v.empty()) {
+            FrameBufs b = v.back();
+            v.pop_back();
+            return b;
+        }
+        FrameBufs b;
+        b.bytes = align_up(n_px * 3, 256) + n_px * 4;
+        RF_CUDA(cudaMalloc(&b.dev, b.bytes));
+        RF_CUDA(cudaMallocHost(&b.pin, n_px * 7));
+        RF_CUDA(cudaEventCreateWithFlags(&b.ready, cudaEventDisableTiming));
+        *resident += b.bytes;
+        return b;
+    }
+    void put(size_t n_px, const FrameBufs& b) { free_[n_px].push_back(b); }
+    void release_all()
+    {
+        for (auto& kv : free_)
+            for (auto& b : kv.second) {
+                cudaFree(b.dev);
+                cudaFreeHost(b.pin);
+                cudaEventDestroy(b.ready);
+            }
+        free_.clear();
+    }
+};
+
+struct DevFrame {
+    int W = 0, H = 0;
+    rgbdflow_camera_params cam{};
+    uint8_t* bgr = nullptr;   // device, W*H*3
+    float* depth = nullptr;   // device, W*H
+    cudaEvent_t ready = nullptr;
+    FrameBufs bufs;
+    FramePool* pool = nullptr;
+    ~DevFrame()
+    {
+        if (pool) pool->put((size_t)W * H, bufs);
+    }
+};
+
+struct ServerReq {
+    int stream = 0;
+    uint64_t id = 0;
+    int W = 0, H = 0;
+    std::shared_ptr<DevFrame> f1, f2;
+    float* out_host = nullptr;
+    double t_submit = 0;
+};
+
+struct StreamState {
+    std::shared_ptr<DevFrame> prev;
+    float* flow = nullptr;    // device W*H*3: the last solved flow (warm-start source)
+    int W = 0, H = 0;
+    bool has_flow = false;
+    bool in_flight = false;
+};
+
+struct ServerSlot {
+    rgbdflow_ctx* ctx = nullptr;
+    cudaStream_t st = nullptr;
+    cudaEvent_t done = nullptr;
+    std::vector<ServerReq> reqs;
+    bool busy = false;
+    char* pin_out = nullptr;
+    size_t pin_cap = 0;
+    std::vector<size_t> out_off;
+};
+
+}  // namespace rgbdflow
+
+struct rgbdflow_server {
+    rgbdflow_ctx* ctx = nullptr;  // the owning context (device, last error)
+    rgbdflow_server_config cfg{};
+    cudaStream_t upload = nullptr;
+    std::unordered_map<int, rgbdflow::StreamState> streams;
+    std::deque<rgbdflow::ServerReq> queue;
+    rgbdflow::ServerSlot slots[2];
+    size_t resident_bytes = 0;    // frame pool + stream flows held on the device
+    rgbdflow::FramePool pool;
+    std::deque<rgbdflow_result> ready;
+};

@@ -135,7 +135,8 @@ class RgbdFlowPair(ctypes.Structure):
 
 class ServerConfig(ctypes.Structure):
     _fields_ = [("max_streams", ctypes.c_int), ("max_batch", ctypes.c_int),
-                ("hbm_budget_bytes", ctypes.c_size_t), ("warm_start", ctypes.c_int), ("params", Params)]
+                ("hbm_budget_bytes", ctypes.c_size_t), ("warm_start", ctypes.c_int),
+                ("warm_early_termination", ctypes.c_int), ("params", Params)]
 
 
 class Result(ctypes.Structure):
@@ -355,17 +356,19 @@ class Context:
                                                       ctypes.c_void_p(handle))
         self._check(rc)
 
-    def scene_flow_batch(self, pairs, params, stats=True):
+    def scene_flow_batch(self, pairs, params, stats=True, outs=None):
         """pairs: list of dicts with W, H, cam (CameraParams), bgr1, depth1, bgr2, depth2[, est_flow].
+        outs: optional preallocated (H,W,3) float32 arrays (page-locked ones are filled by DMA).
         Returns the list of (H,W,3) float32 flows (and Stats list)."""
         keep = []
         arr = (RgbdFlowPair * len(pairs))()
+        given = outs
         outs = []
         for i, p in enumerate(pairs):
             b1, b2 = _c(p["bgr1"], np.uint8), _c(p["bgr2"], np.uint8)
             d1, d2 = _c(p["depth1"], np.float32), _c(p["depth2"], np.float32)
             est = _c(p["est_flow"], np.float32) if p.get("est_flow") is not None else None
-            out = np.zeros((p["H"], p["W"], 3), np.float32)
+            out = given[i] if given is not None else np.zeros((p["H"], p["W"], 3), np.float32)
             keep += [b1, b2, d1, d2, est, out]
             outs.append(out)
             arr[i].W, arr[i].H, arr[i].cam = p["W"], p["H"], p["cam"]
@@ -377,3 +380,63 @@ class Context:
         rc = self.lib.rgbdflow_scene_flow_batch(self.h, arr, len(pairs), ctypes.byref(params), st)
         self._check(rc)
         return (outs, list(st)) if stats else outs
+
+
+class Server:
+    """Continuous-batching server over camera streams (rgbdflow_server_*).  A frame submitted on a
+    stream forms a pair with that stream's previous frame; its flow (previous -> this frame) lands
+    in an array owned by this object until the request completes."""
+
+    def __init__(self, ctx, params, max_streams=8, max_batch=8, hbm_budget_bytes=20 << 30, warm_start=True,
+                 warm_early_termination=False):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        cfg = ServerConfig()
+        cfg.max_streams, cfg.max_batch = max_streams, max_batch
+        cfg.hbm_budget_bytes = hbm_budget_bytes
+        cfg.warm_start = int(bool(warm_start))
+        cfg.warm_early_termination = int(bool(warm_early_termination))
+        cfg.params = params
+        h = ctypes.c_void_p()
+        rc = self.lib.rgbdflow_server_create(ctx.h, ctypes.byref(cfg), ctypes.byref(h))
+        ctx._check(rc)
+        self.h = h
+        self._live = {}  # (stream, id) -> (out array, input arrays kept alive until the upload is staged)
+        self._res = (Result * 64)()
+
+    def submit(self, stream, req_id, cam, bgr, depth):
+        bgr = _c(bgr, np.uint8)
+        depth = _c(depth, np.float32)
+        H, W = depth.shape
+        out = np.empty((H, W, 3), np.float32)
+        rc = self.lib.rgbdflow_server_submit(self.h, stream, req_id, ctypes.byref(cam), _ptr(bgr), _ptr(depth), W, H,
+                                             _ptr(out))
+        self.ctx._check(rc)
+        self._live[(stream, req_id)] = out
+        return out
+
+    def step(self, wait=False):
+        """Advance the device; returns [(stream, id, flow, submit_s, done_s, status)] of completed pairs."""
+        n = ctypes.c_int()
+        rc = self.lib.rgbdflow_server_step(self.h, int(wait), self._res, 64, ctypes.byref(n))
+        self.ctx._check(rc)
+        out = []
+        for i in range(n.value):
+            r = self._res[i]
+            flow = self._live.pop((r.stream_id, r.request_id), None)
+            out.append((r.stream_id, r.request_id, flow, r.submit_time_s, r.done_time_s, r.status))
+        return out
+
+    def pending(self):
+        return self.lib.rgbdflow_server_pending(self.h)
+
+    def close(self):
+        if self.h:
+            self.lib.rgbdflow_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

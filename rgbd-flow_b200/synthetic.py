@@ -185,6 +185,30 @@ def make_pair(W=640, H=480, f=525.0, cx=319.5, cy=239.5, n_patches=6, hole_frac=
                 W=W, H=H, seed=seed)
 
 
+def make_sequence(W=640, H=480, f=525.0, cx=319.5, cy=239.5, n_patches=6, hole_frac=0.08, n_frames=16, seed=0,
+                  color_noise=2.0, depth_noise=1.45e-3):
+    """Frames of one camera stream: every patch follows a smooth rigid trajectory (a fixed per-frame
+    rotation <= 3 deg about its centre and translation <= 3 cm, so frame t+1 relates to frame t like
+    the two frames of make_pair).  Returns a list of dicts with bgr (H,W,3 uint8) and depth (H,W
+    float32 m, 0 = invalid)."""
+    rng = np.random.default_rng(seed)
+    cam = Camera(f, cx, cy)
+    ext = 3.0 / f * max(W, H) + 0.5
+    bg_tex = _Texture(rng, (-ext, ext), (-ext, ext), cells=(0.12, 0.05, 0.02))
+    patches = [_Patch(rng, cam, W, H) for _ in range(n_patches)]
+    frames = []
+    cur = patches
+    for t in range(n_frames):
+        col, z, _, _ = _render(cam, W, H, cur, bg_tex)
+        c = np.clip(np.rint(col + rng.normal(0, color_noise, col.shape)), 0, 255).astype(np.uint8)
+        zn = z + rng.normal(0, 1, z.shape) * depth_noise * z * z
+        dep = (np.clip(np.rint(zn * 1000.0), 0, 65535).astype(np.uint16) * 0.001).astype(np.float32)
+        dep[_holes(rng, H, W, hole_frac)] = 0
+        frames.append(dict(bgr=c, depth=dep))
+        cur = [p.moved() for p in cur]
+    return dict(frames=frames, cam=cam, W=W, H=H)
+
+
 def make_config_pair(name, seed=0):
     c = dict(CONFIGS[name])
     return make_pair(seed=seed, **c)

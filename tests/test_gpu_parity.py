@@ -218,7 +218,7 @@ def test_errors_are_status_codes(ctx):
     with pytest.raises(rf.RgbdFlowError) as e:
         ctx.scene_flow_two_frames(cam, p["bgr1"], p["depth1"], p["bgr2"], p["depth2"], rf.default_params())
     assert e.value.code == -2  # HPB regularisation is not built
-    small = rf.Context(0, hbm_budget_bytes=1 << 20)
+    small = rf.Context(0, hbm_budget_bytes=64 << 10)
     with pytest.raises(rf.RgbdFlowError) as e:
         small.scene_flow_two_frames(cam, p["bgr1"], p["depth1"], p["bgr2"], p["depth2"], rf.benchmark_params(40))
     assert e.value.code == -4
