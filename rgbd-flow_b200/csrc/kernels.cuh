@@ -123,6 +123,16 @@ template <> __device__ __forceinline__ __nv_bfloat16 fromT<__nv_bfloat16>(float 
 template <class S, class T> __device__ __forceinline__ S stS(T v) { return fromT<S>((float)v); }
 template <> __device__ __forceinline__ double stS<double, double>(double v) { return v; }
 
+// Typed math: explicit float / double entry points so FP32 code never widens to FP64.
+__device__ __forceinline__ float minT(float a, float b) { return fminf(a, b); }
+__device__ __forceinline__ double minT(double a, double b) { return ::fmin(a, b); }
+__device__ __forceinline__ float maxT(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ double maxT(double a, double b) { return ::fmax(a, b); }
+__device__ __forceinline__ float absT(float a) { return fabsf(a); }
+__device__ __forceinline__ double absT(double a) { return ::fabs(a); }
+__device__ __forceinline__ float expT(float a) { return expf(a); }
+__device__ __forceinline__ double expT(double a) { return ::exp(a); }
+
 template <class T> __device__ __forceinline__ T rsqrtT(T v);
 template <> __device__ __forceinline__ float rsqrtT<float>(float v) { return 1.0f / sqrtf(v); }
 template <> __device__ __forceinline__ double rsqrtT<double>(double v) { return 1.0 / sqrt(v); }
@@ -426,8 +436,8 @@ __global__ void k_level_setup(const LevelItem<T, S>* items, const Tile* tiles, i
     }
     T rh = 0, rv = 0;
     if (regtype == 1) {
-        if (j < W - 1) { const T d = (z1 - it.pyr[6][l + 1]) / (T).02; rh = exp(-(d * d)); }
-        if (i < H - 1) { const T d = (z1 - it.pyr[6][l + W]) / (T).02; rv = exp(-(d * d)); }
+        if (j < W - 1) { const T d = (z1 - it.pyr[6][l + 1]) / (T).02; rh = expT(-(d * d)); }
+        if (i < H - 1) { const T d = (z1 - it.pyr[6][l + W]) / (T).02; rv = expT(-(d * d)); }
     } else {
         rh = (j < W - 1) ? (T)1 : (T)0;
         rv = (i < H - 1) ? (T)1 : (T)0;
@@ -578,9 +588,9 @@ k_linearize(const LevelItem<T, S>* items, const Tile* tiles, SolveConst<T> k, in
         Iy[c] = sy / (T)12;
         It[c] = sDT[c][ry][rx];
     }
-    Ix[5] = fmin(fmax(Ix[5], -k.max_grad), k.max_grad);
-    Iy[5] = fmin(fmax(Iy[5], -k.max_grad), k.max_grad);
-    It[5] = fmin(fmax(It[5], -k.max_grad), k.max_grad);
+    Ix[5] = minT(maxT(Ix[5], -k.max_grad), k.max_grad);
+    Iy[5] = minT(maxT(Iy[5], -k.max_grad), k.max_grad);
+    It[5] = minT(maxT(It[5], -k.max_grad), k.max_grad);
     const T U0 = sU[0][ry][rx], U1 = sU[1][ry][rx], U2 = sU[2][ry][rx];
     const T du0 = sUD[0][ry][rx] - U0, du1 = sUD[1][ry][rx] - U1, du2 = sUD[2][ry][rx] - U2;
     const T z1 = ldS<T, S>(it.D1 + l);
@@ -621,7 +631,7 @@ k_linearize(const LevelItem<T, S>* items, const Tile* tiles, SolveConst<T> k, in
         if (hasL) lv += (uc - sU[c][ry][rx - 1]) * phiL * rhL;
         if (hasD) lv -= (sU[c][ry + 1][rx] - uc) * phi * rvl;
         if (hasU) lv += (uc - sU[c][ry - 1][rx]) * phiU * rvU;
-        lap[c] = (fabs(nrm) < (T)1e-5) ? (T)0 : lv / (nrm / (T)cnt);
+        lap[c] = (absT(nrm) < (T)1e-5) ? (T)0 : lv / (nrm / (T)cnt);
     }
     const T s = it.pyr[9][l];
     const T sL = hasL ? it.pyr[9][l - 1] : (T)0, sU_ = hasU ? it.pyr[9][l - W] : (T)0;
@@ -696,7 +706,7 @@ __device__ __forceinline__ void sor_point(const T* c, T aL, T aU, T aR, T aD, T 
     v -= c[3] * xp[1]; v -= c[4] * xp[2];
     v *= c[0];
     T r = omega * v + ((T)1 - omega) * xp[0];
-    out[0] = fmin(fmax(r, xp[0] - step), xp[0] + step);
+    out[0] = minT(maxT(r, xp[0] - step), xp[0] + step);
     // v row
     v = 0;
     v -= aL * xl[1]; v -= aU * xu[1]; v -= aR * xr[1]; v -= aD * xd[1];
@@ -704,7 +714,7 @@ __device__ __forceinline__ void sor_point(const T* c, T aL, T aU, T aR, T aD, T 
     v -= c[3] * xp[0]; v -= c[5] * xp[2];
     v *= c[1];
     r = omega * v + ((T)1 - omega) * xp[1];
-    out[1] = fmin(fmax(r, xp[1] - step), xp[1] + step);
+    out[1] = minT(maxT(r, xp[1] - step), xp[1] + step);
     // w row: neighbour coefficients carry the depth-smoothness weight of the edge's source pixel
     v = 0;
     v -= (aL * sL) * xl[2]; v -= (aU * sU) * xu[2]; v -= (aR * s) * xr[2]; v -= (aD * s) * xd[2];
@@ -712,7 +722,7 @@ __device__ __forceinline__ void sor_point(const T* c, T aL, T aU, T aR, T aD, T 
     v -= c[4] * xp[0]; v -= c[5] * xp[1];
     v *= c[2];
     r = omega * v + ((T)1 - omega) * xp[2];
-    out[2] = fmin(fmax(r, xp[2] - step), xp[2] + step);
+    out[2] = minT(maxT(r, xp[2] - step), xp[2] + step);
 }
 
 // Region of a tile: global columns [ws, ws + RW), rows [y0, y0 + RH); ws a multiple of 8 so
@@ -726,22 +736,34 @@ __device__ __forceinline__ void sor_load(const LevelItem<T, S>& it, const Tile& 
 {
     typedef SorGeom<T, K, NBUF> G;
     constexpr int CH = 16 / sizeof(T), NCH = G::HRW / CH;
+    if (it.ctl->level_done) return;  // the pair finished this level: its tiles are skipped unread
     const int W = it.W, H = it.H, hw = it.hwp;
     const int m0 = sor_ws<T, K>(t.tx) / 2;
     const int y0 = t.ty * kSorTH - 2 * K;
-    const T* const* xin = it.x[L.xin];
-    for (int q = threadIdx.x; q < G::NPL * G::RH * 2 * NCH; q += G::NT) {
-        const int ch = q % NCH, c = (q / NCH) & 1, rr = (q / (2 * NCH)) % G::RH, pl = q / (2 * NCH * G::RH);
+    const T* base[G::NPL];
+#pragma unroll
+    for (int pl = 0; pl < 12; pl++) base[pl] = it.sys[pl];
+#pragma unroll
+    for (int v = 0; v < 3; v++) base[12 + v] = it.x[L.xin][v];
+    const int npl = L.xin_zero ? 12 : G::NPL;  // a zero increment is not read
+    // one 16-byte chunk position per pass; all planes of that position in a row
+    for (int q = threadIdx.x; q < G::RH * 2 * NCH; q += G::NT) {
+        const int ch = q % NCH, c = (q / NCH) & 1, rr = q / (2 * NCH);
         const int gi = y0 + rr, m = m0 + ch * CH;
         // pixels of colour c in row gi: columns (c ^ (gi & 1)) + 2m', m' < count
         const int cnt = (W + 1 - (c ^ (gi & 1))) >> 1;
         int nb = 0;
-        const T* src = it.sys[0];  // any valid address when nothing is read
-        if (gi >= 0 && gi < H && m >= 0 && m < cnt && !(pl >= 12 && L.xin_zero)) {
+        size_t off = 0;
+        if (gi >= 0 && gi < H && m >= 0 && m < cnt) {
             nb = min(CH, cnt - m) * (int)sizeof(T);
-            src = (pl < 12 ? it.sys[pl] : xin[pl - 12]) + (size_t)gi * 2 * hw + c * hw + m;
+            off = (size_t)gi * 2 * hw + c * hw + m;
         }
-        cp_async16(buf + (((size_t)pl * G::RH + rr) * 2 + c) * G::HRW + ch * CH, src, nb);
+        T* dst = buf + ((size_t)rr * 2 + c) * G::HRW + ch * CH;
+#pragma unroll
+        for (int pl = 0; pl < G::NPL; pl++) {
+            const bool rd = nb > 0 && pl < npl;
+            cp_async16(dst + (size_t)pl * G::RH * G::RW, rd ? base[pl] + off : base[0], rd ? nb : 0);
+        }
     }
 }
 
@@ -792,57 +814,55 @@ k_sor(const LevelItem<T, S>* items, const Tile* tiles, int ntiles, SolveConst<T>
             for (int hs = 0; hs < 2 * nit; hs++) {
                 const int color = hs & 1;
                 const bool chk = L.check && hs >= 2 * nit - 2;
-                for (int q0 = threadIdx.x; q0 < RH * HRW; q0 += ILP * G::NT) {
-                    T c[ILP][9], xl[ILP][3], xu[ILP][3], xr[ILP][3], xd[ILP][3], xp[ILP][3], nv[ILP][3];
-                    T aL[ILP], aU[ILP], aR[ILP], aD[ILP], sL[ILP], sU[ILP], sC[ILP];
-                    int o[ILP];
-                    bool ok[ILP], in_int[ILP];
+                // half-sweep hs only has to be right within h = 2 nit - 1 - hs of the interior: later
+                // half-sweeps read it there and nowhere else, so the window shrinks to the interior
+                // and never touches the region's outermost ring (no index clamping needed)
+                const int h = 2 * nit - 1 - hs;
+                const int r0 = max(iy0 - h, 0), r1 = min(iy0 + kSorTH + h, H);
+                const int cl = max(ix0 - h, 0), chh = min(ix0 + kSorTW + h, W);
+                const int NM = (chh - cl + 2) >> 1;                 // colour pixels per row (upper bound)
+                const int nq = (r1 - r0) * NM;
+                const unsigned magic = ((1u << 20) + NM - 1) / NM;  // q / NM = (q * magic) >> 20, exact here
+                for (int q = threadIdx.x; q < nq; q += G::NT) {
+                    const int ro = (int)__umulhi((unsigned)q << 12, magic);
+                    const int mo = q - ro * NM;
+                    const int gi = r0 + ro;
+                    const int b = color ^ (gi & 1);                 // column parity of this colour in row gi
+                    const int m = ((cl - ws - b + 1) >> 1) + mo;
+                    if (m >= ((chh - ws - b + 1) >> 1)) continue;   // past this row's last pixel
+                    const int rw = gi - y0;
+                    const int own = (rw * 2 + color) * HRW + m;
+                    const int oth = (rw * 2 + (color ^ 1)) * HRW + m;
+                    const int ol = oth - 1 + b, orr = oth + b, ou = oth - 2 * HRW, od = oth + 2 * HRW;
+                    T c[9], xl[3], xu[3], xr[3], xd[3], xp[3], nv[3];
 #pragma unroll
-                    for (int u = 0; u < ILP; u++) {
-                        const int q = q0 + u * G::NT;
-                        const int rr = q / HRW, m = q % HRW;
-                        const int gi = y0 + rr;
-                        const int b = color ^ (gi & 1);           // column parity of this colour in row gi
-                        const int gj = ws + 2 * m + b;
-                        ok[u] = q < RH * HRW && gi >= 0 && gi < H && gj >= 0 && gj < W;
-                        in_int[u] = gi >= iy0 && gi < iy0 + kSorTH && gj >= ix0 && gj < ix0 + kSorTW;
-                        const int rq = ok[u] ? rr : 0, mq = ok[u] ? m : 0;
-                        // own pixel: colour `color`; neighbours: the other colour
-                        const int own = (rq * 2 + color) * HRW + mq;
-                        const int oth = (rq * 2 + (color ^ 1)) * HRW;
-                        const int ml = clampi(mq - 1 + b, 0, HRW - 1), mr = clampi(mq + b, 0, HRW - 1);
-                        const int ru = rq > 0 ? rq - 1 : rq, rd = rq < RH - 1 ? rq + 1 : rq;
-                        const int ol = oth + ml, orr = oth + mr;
-                        const int ou = (ru * 2 + (color ^ 1)) * HRW + mq, od = (rd * 2 + (color ^ 1)) * HRW + mq;
-                        o[u] = own;
+                    for (int z = 0; z < 9; z++) c[z] = buf[z * PL + own];
 #pragma unroll
-                        for (int z = 0; z < 9; z++) c[u][z] = buf[z * PL + own];
-#pragma unroll
-                        for (int v = 0; v < 3; v++) {
-                            const T* xv = buf + (12 + v) * PL;
-                            xl[u][v] = xv[ol]; xr[u][v] = xv[orr]; xu[u][v] = xv[ou]; xd[u][v] = xv[od]; xp[u][v] = xv[own];
-                        }
-                        aL[u] = buf[9 * PL + ol]; aU[u] = buf[10 * PL + ou]; aR[u] = buf[9 * PL + own];
-                        aD[u] = buf[10 * PL + own]; sL[u] = buf[11 * PL + ol]; sU[u] = buf[11 * PL + ou];
-                        sC[u] = buf[11 * PL + own];
+                    for (int v = 0; v < 3; v++) {
+                        const T* xv = buf + (12 + v) * PL;
+                        xl[v] = xv[ol]; xr[v] = xv[orr]; xu[v] = xv[ou]; xd[v] = xv[od]; xp[v] = xv[own];
                     }
+                    sor_point<T>(c, buf[9 * PL + ol], buf[10 * PL + ou], buf[9 * PL + own], buf[10 * PL + own],
+                                 buf[11 * PL + ol], buf[11 * PL + ou], buf[11 * PL + own], xl, xu, xr, xd, xp,
+                                 k.omega, k.step, nv);
 #pragma unroll
-                    for (int u = 0; u < ILP; u++)
-                        sor_point<T>(c[u], aL[u], aU[u], aR[u], aD[u], sL[u], sU[u], sC[u], xl[u], xu[u], xr[u], xd[u],
-                                     xp[u], k.omega, k.step, nv[u]);
-#pragma unroll
-                    for (int u = 0; u < ILP; u++) {
-                        if (!ok[u]) continue;
-#pragma unroll
-                        for (int v = 0; v < 3; v++) buf[(12 + v) * PL + o[u]] = nv[u][v];
-                        if (chk && in_int[u])
-                            for (int v = 0; v < 3; v++) md = fmax(md, fabs(nv[u][v] - xp[u][v]));
+                    for (int v = 0; v < 3; v++) buf[(12 + v) * PL + own] = nv[v];
+                    if (chk) {
+                        const int gj = ws + 2 * m + b;
+                        if (gi >= iy0 && gi < iy0 + kSorTH && gj >= ix0 && gj < ix0 + kSorTW)
+                            for (int v = 0; v < 3; v++) md = maxT(md, absT(nv[v] - xp[v]));
                     }
                 }
                 __syncthreads();
             }
             // interior out: x to the other buffer, or the fold u += x with the statistic partial
             T part = 0;
+            T* const o0 = L.final_fold ? it.u[0] : it.x[L.xin ^ 1][0];
+            T* const o1 = L.final_fold ? it.u[1] : it.x[L.xin ^ 1][1];
+            T* const o2 = L.final_fold ? it.u[2] : it.x[L.xin ^ 1][2];
+            const T* const dep = it.pyr[6];
+            const int pitch = it.pitch, hwp = it.hwp;
+            const T fl = it.f_level;
             for (int q = threadIdx.x; q < kSorTW * kSorTH; q += G::NT) {
                 const int gi = iy0 + q / kSorTW, gj = ix0 + q % kSorTW;
                 if (gi >= H || gj >= W) continue;
@@ -850,14 +870,13 @@ k_sor(const LevelItem<T, S>* items, const Tile* tiles, int ntiles, SolveConst<T>
                 const int o = ((gi - y0) * 2 + cl) * HRW + ((gj - ws) >> 1);
                 const T a = buf[12 * PL + o], bq = buf[13 * PL + o], cz = buf[14 * PL + o];
                 if (L.final_fold) {
-                    const size_t lp = (size_t)gi * it.pitch + gj;
-                    it.u[0][lp] += a; it.u[1][lp] += bq; it.u[2][lp] += cz;
-                    const T wz = it.f_level / it.pyr[6][(size_t)gi * W + gj];
+                    const size_t lp = (size_t)gi * pitch + gj;
+                    o0[lp] += a; o1[lp] += bq; o2[lp] += cz;
+                    const T wz = fl / dep[(size_t)gi * W + gj];
                     part += a * a + bq * bq + (cz * cz) * wz;
                 } else {
-                    T* const* xo = it.x[L.xin ^ 1];
-                    const int lc = cs_idx(gi, gj, it.hwp);
-                    xo[0][lc] = a; xo[1][lc] = bq; xo[2][lc] = cz;
+                    const int lc = cs_idx(gi, gj, hwp);
+                    o0[lc] = a; o1[lc] = bq; o2[lc] = cz;
                 }
             }
             if (L.check && nit > 0) {
