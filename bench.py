@@ -126,6 +126,129 @@ def oracle_pairs_per_s(pairs, steps):
     return steps / sum(ts), threads, outs, ts
 
 
+def device_pair(rf, torch, p):
+    return dict(W=p["W"], H=p["H"], cam=cam_of(rf, p),
+                bgr1=torch.from_numpy(p["bgr1"]).cuda(), bgr2=torch.from_numpy(p["bgr2"]).cuda(),
+                depth1=torch.from_numpy(p["depth1"]).cuda(), depth2=torch.from_numpy(p["depth2"]).cuda(),
+                out=torch.empty((p["H"], p["W"], 3), dtype=torch.float32, device="cuda"))
+
+
+def run_ncu_case(n_pairs, rf, torch):
+    """One batched solve of n_pairs 640x480 pairs through the device-pointer API, graphs off."""
+    ctx = rf.Context(0)
+    dev = [device_pair(rf, torch, p) for p in make_pairs(n_pairs, 0)]
+    ctx.scene_flow_batch_device(dev, rf.benchmark_params(W))
+    torch.cuda.synchronize()
+    ctx.close()
+
+
+def run_served(ctx, rf, serving, streams, prm, args, warm):
+    """Camera streams through the server: pairs/s, latency percentiles and the 3-D EPE of the
+    served flows against the plain solve of the same pairs (stream 0, a few kept results)."""
+    srv = rf.Server(ctx, prm, max_streams=len(streams), max_batch=len(streams), hbm_budget_bytes=20 << 30,
+                    warm_start=warm, warm_early_termination=warm)
+    serving.simulate(srv, rf, streams, n_frames=2 * args.serve_unique, fps=30.0, seed=1)  # warm-up: graphs
+    r = serving.simulate(srv, rf, streams, n_frames=args.serve_frames, fps=30.0, seed=2, keep_stream=0, keep_n=6)
+    lat = np.array(r["latencies_ms"])
+    sat = serving.simulate(srv, rf, streams, n_frames=args.serve_unique * 3, fps=30.0, seed=3, time_scale=0.0)
+    srv.close()
+    seq = streams[0]
+    epes = []
+    for rid, flow in r["kept"]:
+        n = len(seq["frames"])
+        f1 = seq["frames"][serving.frame_index(rid - 1, n)]
+        f2 = seq["frames"][serving.frame_index(rid, n)]
+        camp = rf.CameraParams.make(seq["W"], seq["H"], seq["cam"].f, seq["cam"].cx, seq["cam"].cy)
+        plain_f = ctx.scene_flow_two_frames(camp, f1["bgr"], f1["depth"], f2["bgr"], f2["depth"], prm, stats=False)
+        z = np.where(f1["depth"] > 0, f1["depth"], 2.0).astype(np.float64)
+        epes.append(syn.epe3d(flow, plain_f, z, seq["cam"], f1["depth"] > 0)[0])
+    how = ("warm starts from the stream's previous flow (full-resolution level, early termination allowed)"
+           if warm else "cold: the full coarse-to-fine solve per pair (flows equal the plain call's)")
+    return {"streams": "5 x 640x480 + 3 x 320x240 at 30 fps, Poisson arrivals; " + how,
+            "pairs": r["pairs"], "pairs_per_s": r["pairs"] / r["wall_s"],
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "max_ms": float(lat.max()),
+            "saturated_pairs_per_s": sat["pairs"] / sat["wall_s"],
+            "epe_vs_plain_mm": 1e3 * float(np.mean(epes)) if epes else None,
+            "hbm_budget_gb": 20}
+
+
+MIX = [(160, 120, 24), (320, 240, 24), (640, 480, 16)]
+
+
+def run_mixed(ctx, rf, torch, stream, prm, args, rank):
+    """64 uneven pairs per step, device-resident, CUDA events on the launching stream."""
+    dev = []
+    for (w, h, n) in MIX:
+        name = "%dx%d" % (w, h)
+        for i in range(n):
+            dev.append(device_pair(rf, torch, syn.make_config_pair(name, seed=3000 + 97 * rank + 1000 * w + i)))
+    for _ in range(args.warmup):
+        ctx.scene_flow_batch_device(dev, prm)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    steps = max(1, min(args.steps, 10))
+    e0.record(stream)
+    for _ in range(steps):
+        ctx.scene_flow_batch_device(dev, prm)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    px = sum(w * h * n for (w, h, n) in MIX)
+    return {"pairs": len(dev), "mix": "24 x 160x120 + 24 x 320x240 + 16 x 640x480", "ms_per_step": ms,
+            "pairs_per_s": 1e3 * len(dev) / ms, "equiv_640x480_pairs_per_s": 1e3 * px / (640 * 480) / ms,
+            "launches_per_step": ctx.last_launch_count()}
+
+
+def run_precision(ctx, rf, torch, stream, dev, pairs, args):
+    """FP16 / BF16 pyramid storage against the FP32 and FP64 device solves of the same pairs."""
+    n = min(4, len(dev))
+    host = [dict(W=p["W"], H=p["H"], cam=cam_of(rf, p), bgr1=p["bgr1"], depth1=p["depth1"], bgr2=p["bgr2"],
+                 depth2=p["depth2"]) for p in pairs[:n]]
+
+    def epes(fl, ref):
+        return [syn.epe3d(a, b, p["z1_true"], p["cam"], p["depth1"] > 0) for a, b, p in zip(fl, ref, pairs)]
+
+    p64 = rf.benchmark_params(W)
+    p64.compute = rf.COMPUTE_FP64
+    f64 = ctx.scene_flow_batch(host, p64, stats=False)
+    p32 = rf.benchmark_params(W)
+    f32 = ctx.scene_flow_batch(host, p32, stats=False)
+    dev = [dict(d, out=torch.empty_like(d["out"])) for d in dev]  # keep the FP32 outputs of the caller
+    out = {"pairs": n, "reference": "FP64 device solve of the same schedule (the only FP64 path)"}
+    for name, st in (("fp32", rf.STORE_FP32), ("fp16", rf.STORE_FP16), ("bf16", rf.STORE_BF16)):
+        prm = rf.benchmark_params(W)
+        prm.storage = st
+        fl = ctx.scene_flow_batch(host, prm, stats=False)
+        e64, e32 = epes(fl, f64), epes(fl, f32)
+        # device-resident throughput and per-kernel-class GB/s of the stored type
+        for _ in range(2):
+            ctx.scene_flow_batch_device(dev, prm)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(3):
+            ctx.scene_flow_batch_device(dev, prm)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 3
+        ctx.profile(1)
+        ctx.scene_flow_batch_device(dev, prm)
+        torch.cuda.synchronize()
+        kst = ctx.profile_read()
+        ctx.profile(0)
+        gbs = {k: kst[k][2] / (kst[k][1] / 1e3) / 1e9 for k in ("sor", "linearize") if k in kst and kst[k][1] > 0}
+        out[name] = {"pairs_per_s": 1e3 * len(dev) / ms,
+                     "epe_vs_fp64_mm": {"mean": 1e3 * float(np.mean([e[0] for e in e64])),
+                                        "max": 1e3 * float(np.max([e[1] for e in e64]))},
+                     "epe_vs_fp32_mm": {"mean": 1e3 * float(np.mean([e[0] for e in e32])),
+                                        "max": 1e3 * float(np.max([e[1] for e in e32]))},
+                     "algorithmic_gbs": gbs}
+    return out
+
+
 def run_reference(args, rank, world):
     """The reference arm: the reference has no CPU implementation of its 3-D solver, so its
     restatement (oracle/, the same arithmetic and schedule) runs on the host cores."""
@@ -158,8 +281,13 @@ def main():
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-precision", action="store_true")
     ap.add_argument("--serve-frames", type=int, default=150)
     ap.add_argument("--serve-unique", type=int, default=8)
+    ap.add_argument("--ncu-case", type=int, default=0, metavar="NP",
+                    help="profiling case: one batched solve of NP 640x480 pairs with graphs off "
+                         "(every launch visible to a profiler), then exit; prints no bench line")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -169,11 +297,16 @@ def main():
         run_reference(args, rank, world)
         return
 
+    if args.ncu_case:
+        os.environ["RGBDFLOW_NO_GRAPHS"] = "1"  # read when the context is created
     import torch
     import torch.distributed as dist
     import rgbdflow as rf
 
     torch.cuda.set_device(local)
+    if args.ncu_case:
+        run_ncu_case(args.ncu_case, rf, torch)
+        return
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
@@ -191,12 +324,7 @@ def main():
     host = make_pairs(B, replicas.pair_seed(rank, 0))
     prm = rf.benchmark_params(W)
     ctx = rf.Context(local)
-    dev = []
-    for p in host:
-        dev.append(dict(W=W, H=H, cam=cam_of(rf, p),
-                        bgr1=torch.from_numpy(p["bgr1"]).cuda(), bgr2=torch.from_numpy(p["bgr2"]).cuda(),
-                        depth1=torch.from_numpy(p["depth1"]).cuda(), depth2=torch.from_numpy(p["depth2"]).cuda(),
-                        out=torch.empty((H, W, 3), dtype=torch.float32, device="cuda")))
+    dev = [device_pair(rf, torch, p) for p in host]
     stream = torch.cuda.Stream()  # the stream every solve below is enqueued on and timed on
     torch.cuda.set_stream(stream)
 
@@ -294,37 +422,22 @@ def main():
         roofline["traffic_note"] = tr.get("note", "")
 
     # ---- served: camera streams at 30 fps (Poisson arrivals) through the continuous-batching
-    # server, warm starts from each stream's previous flow
-    served = None
+    # server.  Headline: cold pairs (the full coarse-to-fine solve, the same flow as the plain
+    # call); beside it, warm starts from each stream's previous flow.
+    served = served_warm = None
     if not args.no_serve:
         import serving
         streams = serving.make_streams(n_unique=args.serve_unique, seed0=500 + 100 * rank)
-        srv = rf.Server(ctx, prm, max_streams=len(streams), max_batch=len(streams), hbm_budget_bytes=20 << 30,
-                        warm_start=True, warm_early_termination=True)
-        serving.simulate(srv, rf, streams, n_frames=2 * args.serve_unique, fps=30.0, seed=1)  # warm-up: graphs
-        r = serving.simulate(srv, rf, streams, n_frames=args.serve_frames, fps=30.0, seed=2, keep_stream=0, keep_n=6)
-        lat = np.array(r["latencies_ms"])
-        sat = serving.simulate(srv, rf, streams, n_frames=args.serve_unique * 3, fps=30.0, seed=3, time_scale=0.0)
-        srv.close()
-        # matched EPE: the served (warm-started) flows against the plain coarse-to-fine solve of the same pairs
-        seq = streams[0]
-        epes = []
-        for rid, flow in r["kept"]:
-            n = len(seq["frames"])
-            f1 = seq["frames"][serving.frame_index(rid - 1, n)]
-            f2 = seq["frames"][serving.frame_index(rid, n)]
-            camp = rf.CameraParams.make(seq["W"], seq["H"], seq["cam"].f, seq["cam"].cx, seq["cam"].cy)
-            plain_f = ctx.scene_flow_two_frames(camp, f1["bgr"], f1["depth"], f2["bgr"], f2["depth"], prm, stats=False)
-            z = np.where(f1["depth"] > 0, f1["depth"], 2.0).astype(np.float64)
-            epes.append(syn.epe3d(flow, plain_f, z, seq["cam"], f1["depth"] > 0)[0])
-        served = {"streams": "5 x 640x480 + 3 x 320x240 at 30 fps, Poisson arrivals, warm starts from the "
-                             "previous flow (full-resolution level, early termination allowed)",
-                  "pairs": r["pairs"], "pairs_per_s": r["pairs"] / r["wall_s"],
-                  "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-                  "max_ms": float(lat.max()),
-                  "saturated_pairs_per_s": sat["pairs"] / sat["wall_s"],
-                  "epe_vs_plain_mm": 1e3 * float(np.mean(epes)) if epes else None,
-                  "hbm_budget_gb": 20}
+        served = run_served(ctx, rf, serving, streams, prm, args, warm=False)
+        served_warm = run_served(ctx, rf, serving, streams, prm, args, warm=True)
+
+    # ---- batching: the uneven mix of 64 pairs (24 x 160x120, 24 x 320x240, 16 x 640x480) in one
+    # persistent launch per pyramid level
+    mixed = None if args.no_mixed else run_mixed(ctx, rf, torch, stream, prm, args, rank)
+
+    # ---- precision: pyramids stored in FP16 / BF16 (flow and Jacobi accumulation in FP32),
+    # against the FP32 and the FP64 device solves of the same pairs
+    precision = None if args.no_precision else run_precision(ctx, rf, torch, stream, dev, host, args)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -344,7 +457,8 @@ def main():
                            "global_batch": B * world, "parallelism": "replicas x%d" % world,
                            "l2": "inputs larger than L2 (working set %.2f GB per GPU)" % (ctx.device_bytes() / 1e9)},
                 "p50_ms": float(np.percentile(step_ms, 50)), "p99_ms": float(np.percentile(step_ms, 99)),
-                "plain": plain, "batch_equals_solo": same, "served": served,
+                "plain": plain, "batch_equals_solo": same, "served": served, "served_warm": served_warm,
+                "mixed_batch": mixed, "precision": precision,
                 "gpu_launches": launches_per_step * args.steps,
                 "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk}
         print(json.dumps(line), flush=True)

@@ -725,6 +725,75 @@ __device__ __forceinline__ void sor_point(const T* c, T aL, T aU, T aR, T aD, T 
     out[2] = minT(maxT(r, xp[2] - step), xp[2] + step);
 }
 
+// Two same-colour neighbours of one row as one aligned vector access (even index).
+template <class T> struct Vec2;
+template <> struct Vec2<float> { typedef float2 t; };
+template <> struct Vec2<double> { typedef double2 t; };
+template <class T> __device__ __forceinline__ typename Vec2<T>::t ld2(const T* p)
+{
+    return *reinterpret_cast<const typename Vec2<T>::t*>(p);
+}
+template <class T> __device__ __forceinline__ void st2(T* p, T a, T b)
+{
+    typename Vec2<T>::t v;
+    v.x = a;
+    v.y = b;
+    *reinterpret_cast<typename Vec2<T>::t*>(p) = v;
+}
+
+// One pair of same-colour pixels (half-row positions m, m + 1; m even) of region row rw: loads
+// with 2-wide shared accesses, both updates, 2-wide stores.  b = column parity of the colour in
+// this row: the left neighbour of position m is other-colour position m - 1 + b, the right one
+// m + b.  Returns the largest |x_new - x_old| over the pair's interior pixels (imask bit 0 / 1).
+template <class T, int PL, int HRW>
+__device__ __forceinline__ T sor_pair(T* buf, int rw, int color, int m, int b, T omega, T step, int imask)
+{
+    const int own = (rw * 2 + color) * HRW + m;
+    const int oth = (rw * 2 + (color ^ 1)) * HRW + m;
+    const int ou = oth - 2 * HRW, od = oth + 2 * HRW;
+    // left / right neighbours of the two pixels from one 2-wide and one scalar access
+    T l0[5], l1[5], r0[5], r1[5];
+    const int pls[5] = {9, 11, 12, 13, 14};
+#pragma unroll
+    for (int z = 0; z < 5; z++) {
+        const T* pb = buf + pls[z] * PL;
+        const typename Vec2<T>::t v = ld2<T>(pb + oth);
+        if (b) {
+            const T e = pb[oth + 2];
+            l0[z] = v.x; l1[z] = v.y; r0[z] = v.y; r1[z] = e;
+        } else {
+            const T e = pb[oth - 1];
+            l0[z] = e; l1[z] = v.x; r0[z] = v.x; r1[z] = v.y;
+        }
+    }
+    T c0[9], c1[9];
+#pragma unroll
+    for (int z = 0; z < 9; z++) {
+        const typename Vec2<T>::t v = ld2<T>(buf + z * PL + own);
+        c0[z] = v.x; c1[z] = v.y;
+    }
+    const typename Vec2<T>::t aR = ld2<T>(buf + 9 * PL + own), aD = ld2<T>(buf + 10 * PL + own);
+    const typename Vec2<T>::t sO = ld2<T>(buf + 11 * PL + own);
+    const typename Vec2<T>::t aU = ld2<T>(buf + 10 * PL + ou), sU = ld2<T>(buf + 11 * PL + ou);
+    T xu0[3], xu1[3], xd0[3], xd1[3], xp0[3], xp1[3], n0[3], n1[3];
+#pragma unroll
+    for (int v = 0; v < 3; v++) {
+        const T* xv = buf + (12 + v) * PL;
+        const typename Vec2<T>::t u = ld2<T>(xv + ou), d = ld2<T>(xv + od), q = ld2<T>(xv + own);
+        xu0[v] = u.x; xu1[v] = u.y; xd0[v] = d.x; xd1[v] = d.y; xp0[v] = q.x; xp1[v] = q.y;
+    }
+    sor_point<T>(c0, l0[0], aU.x, aR.x, aD.x, l0[1], sU.x, sO.x, l0 + 2, xu0, r0 + 2, xd0, xp0, omega, step, n0);
+    sor_point<T>(c1, l1[0], aU.y, aR.y, aD.y, l1[1], sU.y, sO.y, l1 + 2, xu1, r1 + 2, xd1, xp1, omega, step, n1);
+#pragma unroll
+    for (int v = 0; v < 3; v++) st2<T>(buf + (12 + v) * PL + own, n0[v], n1[v]);
+    T md = 0;
+    if (imask & 1)
+        for (int v = 0; v < 3; v++) md = maxT(md, absT(n0[v] - xp0[v]));
+    if (imask & 2)
+        for (int v = 0; v < 3; v++) md = maxT(md, absT(n1[v] - xp1[v]));
+    return md;
+}
+
 // Region of a tile: global columns [ws, ws + RW), rows [y0, y0 + RH); ws a multiple of 8 so
 // each checkerboard half-row segment starts 16-byte aligned.  Shared layout per plane:
 // [RH rows][2 colours][HRW], colour = parity of (global row + column).
@@ -820,6 +889,34 @@ k_sor(const LevelItem<T, S>* items, const Tile* tiles, int ntiles, SolveConst<T>
                 const int h = 2 * nit - 1 - hs;
                 const int r0 = max(iy0 - h, 0), r1 = min(iy0 + kSorTH + h, H);
                 const int cl = max(ix0 - h, 0), chh = min(ix0 + kSorTW + h, W);
+                if constexpr (ILP == 2) {
+                    // pair lanes: a half-warp per row, each lane two adjacent same-colour pixels; the
+                    // two rows of a warp have one parity (no divergence on b).  A pixel of a pair that
+                    // falls outside the window is updated too, which is harmless: the window already
+                    // tolerates stale values outside it, errors travel one pixel per half-sweep, and
+                    // every access stays inside the shared buffer (window rows are >= 1 row inside
+                    // the region; positions m - 1 and m + 2 fall in the neighbouring half-rows).
+                    const int mlo = (cl - ws) >> 1, mhi = (chh - ws + 1) >> 1;
+                    const int plo = mlo & ~1;
+                    const int np = min((mhi - plo + 1) >> 1, (HRW - plo) >> 1);
+                    const int l16 = threadIdx.x & 15, hw = threadIdx.x >> 4, wq = hw >> 1;
+                    const int kofs = ((wq >> 1) << 2) + (wq & 1) + 2 * (hw & 1);
+                    if (l16 < np)
+                        for (int kk = kofs; kk < r1 - r0; kk += G::NT / 16) {
+                            const int gi = r0 + kk;
+                            const int b = color ^ (gi & 1);
+                            const int m = plo + 2 * l16;
+                            int imask = 0;
+                            if (chk && gi >= iy0 && gi < iy0 + kSorTH) {
+                                const int gj = ws + 2 * m + b;
+                                imask = (gj >= ix0 && gj < ix0 + kSorTW ? 1 : 0) | (gj + 2 >= ix0 && gj + 2 < ix0 + kSorTW ? 2 : 0);
+                            }
+                            const T d = sor_pair<T, PL, HRW>(buf, gi - y0, color, m, b, k.omega, k.step, imask);
+                            md = maxT(md, d);
+                        }
+                    __syncthreads();
+                    continue;
+                }
                 const int NM = (chh - cl + 2) >> 1;                 // colour pixels per row (upper bound)
                 const int nq = (r1 - r0) * NM;
                 const unsigned magic = ((1u << 20) + NM - 1) / NM;  // q / NM = (q * magic) >> 20, exact here

@@ -23,6 +23,7 @@ struct GraphEntry {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int launches = 0;
+    std::string exact;  // the batch (sizes, cameras) the executable graph currently holds
 };
 
 struct rgbdflow_ctx {
@@ -88,7 +89,9 @@ void ensure_arena(rgbdflow_ctx* c, size_t need)
     if (c->arena) RF_CUDA(cudaFree(c->arena));
     c->arena = nullptr;
     c->arena_cap = 0;
-    const size_t cap = align_up(need + need / 8, 1 << 20);
+    // grow at least 2x: a server's batches grow step by step, and every reallocation waits for the
+    // device and drops the cached graphs
+    const size_t cap = align_up(std::max(need + need / 8, 2 * c->arena_cap), 1 << 20);
     const size_t want = (c->budget && cap > c->budget) ? need : cap;
     RF_CUDA(cudaMalloc(&c->arena, want));
     c->arena_cap = want;
@@ -166,6 +169,21 @@ std::string plan_key(const std::vector<PairSpec>& ps, const HostParams& hp, int 
                   hp.n_sor, hp.max_dist, hp.fill_holes, hp.fixed, hp.omega, hp.step, hp.eps_d, hp.eps_z, hp.eps_s,
                   hp.sor_tol, hp.outer_tol, hp.occ_margin, hp.occ_penalty, hp.max_grad, hp.period, hp.K * 100 + hp.sor_ilp * 10 + hp.sor_nbuf, hp.fill_rounds);
     return k + buf;
+}
+
+// What decides the sequence of launches (and so the shape of a captured graph), without the
+// pair sizes: the kind of solve, level count, which steps have pairs, hole fill, warm starts,
+// the SOR configuration per step and every parameter of the schedule.
+template <class T, class S>
+std::string topo_key(const Plan<T, S>& P, const HostParams& hp, int tag, bool dev)
+{
+    std::string k = std::to_string(tag) + (dev ? "d" : "h") + std::to_string(P.kind) + "L" + std::to_string(P.Lmax) +
+                    "p" + std::to_string(P.pyr.size()) + "w" + std::to_string((int)P.any_warm) + "s";
+    for (size_t i = 0; i < P.steps.size(); i++)
+        k += std::to_string(P.steps[i].n_items > 0) + std::to_string(P.sor_cfg[i].K) + std::to_string(P.sor_cfg[i].nbuf) +
+             std::to_string(P.sor_cfg[i].ilp) + ".";
+    const std::vector<PairSpec> none;
+    return k + plan_key(none, hp, tag);
 }
 
 void fill_stats(const PairCtl& c, int L, const PyrShape& s, double ms, rgbdflow_stats* st)
@@ -266,10 +284,14 @@ void run_batch(rgbdflow_ctx* c, const std::vector<PairSpec>& pairs, const HostPa
     RF_CUDA(cudaEventRecord(c->e0, st));
     const bool graphs = c->use_graphs && !c->prof;
     if (graphs) {
-        const std::string key = plan_key(pairs, hp, slot) + (dev ? "|dev" : "");
-        auto it = c->graphs.find(key);
-        if (it == c->graphs.end()) {
-            GraphEntry g;
+        // One executable graph per launch topology.  A batch of other sizes with the same topology
+        // is captured again and written into that executable (cudaGraphExecUpdate: new grids and
+        // arguments, no re-instantiation), so changing batch mixes cost a capture, not a build.
+        const std::string exact = plan_key(pairs, hp, slot) + (dev ? "|dev" : "");
+        const std::string topo = topo_key(P, hp, slot, dev);
+        auto it = c->graphs.find(topo);
+        if (it == c->graphs.end() || it->second.exact != exact) {
+            cudaGraph_t graph = nullptr;
             RF_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
             int launches = 0;
             try {
@@ -280,11 +302,30 @@ void run_batch(rgbdflow_ctx* c, const std::vector<PairSpec>& pairs, const HostPa
                 if (tmp) cudaGraphDestroy(tmp);
                 throw;
             }
-            RF_CUDA(cudaStreamEndCapture(c->stream, &g.graph));
-            RF_CUDA(cudaGraphInstantiate(&g.exec, g.graph, 0));
-            g.launches = launches;
-            if (c->graphs.size() > 32) drop_graphs(c);
-            it = c->graphs.emplace(key, g).first;
+            RF_CUDA(cudaStreamEndCapture(c->stream, &graph));
+            bool updated = false;
+            if (it != c->graphs.end()) {
+                cudaGraphExecUpdateResultInfo info;
+                if (cudaGraphExecUpdate(it->second.exec, graph, &info) == cudaSuccess) {
+                    cudaGraphDestroy(it->second.graph);
+                    it->second.graph = graph;
+                    updated = true;
+                } else {
+                    cudaGetLastError();
+                    cudaGraphExecDestroy(it->second.exec);
+                    cudaGraphDestroy(it->second.graph);
+                    c->graphs.erase(it);
+                }
+            }
+            if (!updated) {
+                GraphEntry g;
+                g.graph = graph;
+                RF_CUDA(cudaGraphInstantiate(&g.exec, g.graph, 0));
+                if (c->graphs.size() > 32) drop_graphs(c);
+                it = c->graphs.emplace(topo, g).first;
+            }
+            it->second.exact = exact;
+            it->second.launches = launches;
         }
         RF_CUDA(cudaGraphLaunch(it->second.exec, st));
         c->last_launches = it->second.launches;
@@ -945,3 +986,4 @@ int rgbdflow_server_pending(const rgbdflow_server* s)
 }
 
 }  // extern "C"
+
