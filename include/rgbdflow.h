@@ -298,6 +298,32 @@ int rgbdflow_server_step(rgbdflow_server* srv, int wait, rgbdflow_result* out, i
 /* Requests queued or in flight. */
 int rgbdflow_server_pending(const rgbdflow_server* srv);
 
+/* ---------------------------------------------------------------------------------------------
+ * Allocation-free solve (no counterpart in the reference).  For callers that must not allocate
+ * once they run: a real-time loop with a fixed memory footprint, a process whose device memory
+ * belongs to another allocator, or code that cannot take the implicit device synchronisation of
+ * cudaMalloc / cudaFree.  This call allocates no device and no page-locked host memory (its host
+ * bookkeeping is ordinary heap memory) and needs no context: its workspace is a 40 MiB array in
+ * the library's static device memory, present on every device the library is loaded on.
+ *   Limit: one pair whose workspace fits in 40 MiB, i.e. up to 320 x 240 pixels at pyramid ratio
+ *   0.75 or below, FP32 storage and compute.  A larger pair is rejected with
+ *   RGBDFLOW_ERR_BUDGET, other storage or compute types with RGBDFLOW_ERR_UNSUPPORTED, and
+ *   nothing is enqueued then.
+ *   pair: DEVICE pointers, with the meaning of rgbdflow_scene_flow_batch_async (same solve, same
+ *   result; est_flow NULL or a warm start).  stream: a cudaStream_t as void*, NULL = the legacy
+ *   default stream.  Runs on the current device and returns after enqueue.
+ *   Set-up: the first call on each device looks up the workspace address and sets kernel
+ *   attributes; make that first call before any stream capture.
+ *   Zeroing: nothing in the workspace has to start at zero; every call clears, on the stream, the
+ *   counters it relies on.
+ *   Overlap: all calls on a device share the one workspace.  Two calls whose work overlaps on
+ *   the device (different streams, or threads without ordering) race and corrupt each other's
+ *   results; keep them on one stream, or order them with events.
+ *   err / err_len: NULL or a buffer that receives the error message.
+ * ------------------------------------------------------------------------------------------- */
+int rgbdflow_scene_flow_noalloc(const rgbdflow_pair* pair, const rgbdflow_params* params, void* stream,
+                                char* err, size_t err_len);
+
 #ifdef __cplusplus
 }
 #endif

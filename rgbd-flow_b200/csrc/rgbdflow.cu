@@ -987,3 +987,102 @@ int rgbdflow_server_pending(const rgbdflow_server* s)
 
 }  // extern "C"
 
+// ------------------------------------------------------------------------------------------
+// Allocation-free solve: the workspace of one pair lives in this file's static device array.
+// The plan is the one rgbdflow_scene_flow_batch_async builds for a batch of one, bound to the
+// array instead of a context's arena, and its launches go straight onto the caller's stream.
+// ------------------------------------------------------------------------------------------
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = size_t(40) << 20;  // one 320 x 240 pair at pyramid ratio <= 0.75
+__device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+struct NoAllocDevice {
+    char* scratch = nullptr;  // device address of g_noalloc_scratch on this device
+    int sms = 0;
+};
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+NoAllocDevice g_noalloc_dev[kNoAllocMaxDevices];
+
+// Once per device, with that device current: the workspace address and the kernel attributes.
+const NoAllocDevice& noalloc_setup(int dev)
+{
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    NoAllocDevice& d = g_noalloc_dev[dev];
+    if (d.scratch) return d;
+    void* p = nullptr;
+    RF_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    int sms = 0;
+    RF_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    set_kernel_attrs<float, float>();
+    d.sms = sms;
+    d.scratch = (char*)p;
+    return d;
+}
+
+int noalloc_fail(char* err, size_t err_len, int code, const std::string& m)
+{
+    if (err && err_len) {
+        const size_t n = std::min(m.size(), err_len - 1);
+        std::memcpy(err, m.data(), n);
+        err[n] = 0;
+    }
+    return code;
+}
+
+}  // namespace
+
+extern "C" int rgbdflow_scene_flow_noalloc(const rgbdflow_pair* pair, const rgbdflow_params* params, void* stream,
+                                           char* err, size_t err_len)
+{
+    try {
+        if (err && err_len) err[0] = 0;
+        validate(params);
+        if (params->storage != RGBDFLOW_STORE_FP32 || params->compute != RGBDFLOW_COMPUTE_FP32)
+            throw ArgError(RGBDFLOW_ERR_UNSUPPORTED, "the allocation-free solve stores and computes in FP32 only");
+        if (!pair) throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "no pair");
+        const rgbdflow_pair& q = *pair;
+        if (q.W < 2 || q.H < 2 || !q.bgr1 || !q.bgr2 || !q.depth1_m || !q.depth2_m || !q.flow_out)
+            throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "bad size or null buffer");
+        if (q.cam.xRes == 0 || !(q.cam.focalLength > 0)) throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "bad camera");
+        PairSpec s;
+        s.W = q.W; s.H = q.H;
+        resized_cam(q.cam, q.W, s.f_full, s.xres_full);
+        s.bgr1 = q.bgr1; s.depth1 = q.depth1_m; s.bgr2 = q.bgr2; s.depth2 = q.depth2_m;
+        s.est = q.est_flow; s.out = q.flow_out;
+        const std::vector<PairSpec> ps(1, s);
+        const HostParams hp = host_params(*params);
+        Plan<float, float> P = make_plan<float, float>(ps, hp);
+        if (P.arena_bytes > kNoAllocScratchBytes)
+            throw ArgError(RGBDFLOW_ERR_BUDGET, "a " + std::to_string(q.W) + "x" + std::to_string(q.H) + " pair needs " +
+                                                    std::to_string(P.arena_bytes) + " workspace bytes; the static workspace holds " +
+                                                    std::to_string(kNoAllocScratchBytes) + " (one 320x240 pair)");
+        int dev = 0;
+        const cudaError_t ge = cudaGetDevice(&dev);
+        if (ge != cudaSuccess) { cudaGetLastError(); throw ArgError(RGBDFLOW_ERR_NO_DEVICE, "no CUDA device"); }
+        if (dev < 0 || dev >= kNoAllocMaxDevices) throw ArgError(RGBDFLOW_ERR_UNSUPPORTED, "device index above 63");
+        const NoAllocDevice& d = noalloc_setup(dev);
+        P.sms = d.sms;
+        bind_plan(P, d.scratch);
+        unsigned char* db = P.desc.data();
+        PrepItem<float>* prep = (PrepItem<float>*)(db + P.prep_items_off);
+        prep[0].bgr[0] = q.bgr1; prep[0].bgr[1] = q.bgr2;
+        prep[0].depth[0] = q.depth1_m; prep[0].depth[1] = q.depth2_m;
+        ((float**)(db + P.out_ptrs_off))[0] = q.flow_out;
+        ((EstSrc*)(db + P.est_src_off))[0].f = q.est_flow;
+        const cudaStream_t st = (cudaStream_t)stream;
+        // pageable source: the copy is staged before cudaMemcpyAsync returns, so P may go out of scope
+        RF_CUDA(cudaMemcpyAsync(d.scratch + P.desc_off, P.desc.data(), P.desc_bytes, cudaMemcpyHostToDevice, st));
+        enqueue_solve(P, d.scratch, st);
+        return RGBDFLOW_OK;
+    } catch (const ArgError& e) {
+        return noalloc_fail(err, err_len, e.code, e.what());
+    } catch (const CudaError& e) {
+        return noalloc_fail(err, err_len, RGBDFLOW_ERR_CUDA, e.what());
+    } catch (const std::exception& e) {
+        return noalloc_fail(err, err_len, RGBDFLOW_ERR_INTERNAL, e.what());
+    } catch (...) {
+        return noalloc_fail(err, err_len, RGBDFLOW_ERR_INTERNAL, "unknown error");
+    }
+}

@@ -181,6 +181,7 @@ SIGNATURES = {
     "rgbdflow_server_submit": (_i, [_vp, _i, ctypes.c_uint64, _P(CameraParams), _vp, _vp, _i, _i, _vp]),
     "rgbdflow_server_step": (_i, [_vp, _i, _P(Result), _i, _P(_i)]),
     "rgbdflow_server_pending": (_i, [_vp]),
+    "rgbdflow_scene_flow_noalloc": (_i, [_P(RgbdFlowPair), _P(Params), _vp, ctypes.c_char_p, ctypes.c_size_t]),
 }
 
 
@@ -230,6 +231,26 @@ def batch_device_bytes(sizes, params, warm=None):
     if rc != OK:
         raise RgbdFlowError(rc, "rgbdflow_batch_device_bytes failed")
     return out.value
+
+
+def scene_flow_noalloc(pair, params, stream=None):
+    """Allocation-free solve of one pair of torch CUDA tensors (keys as in
+    Context.scene_flow_batch_device) in the library's static workspace, enqueued on `stream`
+    (a torch.cuda.Stream, default: torch's current stream); returns without waiting."""
+    import torch
+    lib = load()
+    arr = RgbdFlowPair()
+    arr.W, arr.H, arr.cam = pair["W"], pair["H"], pair["cam"]
+    arr.bgr1, arr.depth1_m = pair["bgr1"].data_ptr(), pair["depth1"].data_ptr()
+    arr.bgr2, arr.depth2_m = pair["bgr2"].data_ptr(), pair["depth2"].data_ptr()
+    arr.est_flow = pair["est"].data_ptr() if pair.get("est") is not None else None
+    arr.flow_out = pair["out"].data_ptr()
+    s = stream if stream is not None else torch.cuda.current_stream()
+    err = ctypes.create_string_buffer(512)
+    rc = lib.rgbdflow_scene_flow_noalloc(ctypes.byref(arr), ctypes.byref(params), ctypes.c_void_p(s.cuda_stream),
+                                         err, len(err))
+    if rc != OK:
+        raise RgbdFlowError(rc, err.value.decode())
 
 
 class Context:
