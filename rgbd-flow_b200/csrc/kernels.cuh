@@ -103,6 +103,7 @@ struct SorLaunch {
     int prev_check;    // the previous launch ended with a check: decide here whether to stop
     int prev_check_idx;
     int outer;         // outer iteration index (stats)
+    int seq;           // index of this launch among the level's SOR launches (strip kernel tickets)
 };
 
 // ------------------------------------------------------------------------------------------
@@ -139,6 +140,28 @@ template <> __device__ __forceinline__ double rsqrtT<double>(double v) { return 
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
+// Explicitly rounded arithmetic: the SOR update and the early-termination statistic are written
+// with these so that no contraction choice of the compiler can make two kernels that share them
+// (the tile and the strip SOR) round differently.
+__device__ __forceinline__ float fmaR(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fmaR(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float mulR(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mulR(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float addR(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double addR(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float subR(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double subR(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float divR(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ double divR(double a, double b) { return __ddiv_rn(a, b); }
+
+// One pixel's term of the outer early-termination statistic: du^2 + dv^2 + dw^2 * f / depth1
+// (sceneFlowSingleScaleJacobiCUDA.cu:943-951).
+template <class T>
+__device__ __forceinline__ T stat_px(T a, T b, T c, T fl, T dep)
+{
+    return addR(addR(mulR(a, a), mulR(b, b)), mulR(mulR(c, c), divR(fl, dep)));
+}
+
 // Checkerboard ("colour-split") layout of the SOR's planes (system and increment): every row
 // holds its (i + j) even pixels first, then its odd ones, each half hwp long, so one colour's
 // pixels -- and their other-colour neighbours -- are contiguous.
@@ -166,7 +189,6 @@ struct PrepItem {
     T f2;               // focal length squared (calculateDepthSmoothnessTermWeights)
     T dvc;              // depthVsColorDataWeight
     int max_dist;       // depth-sigma boundary radius
-    int* unfilled;      // per round: unfilled pixels left (both frames), for the early exit
     int tiles_x, tile0;
 };
 
@@ -267,54 +289,80 @@ __global__ void k_sigma(const PrepItem<T>* items, const Tile* tiles)
 // holes get exactly the reference's value; inside larger holes the order (and so the value)
 // can differ from the reference's hash-set order.
 template <class T>
-__global__ void k_fill_round(const PrepItem<T>* items, const Tile* tiles, int round)
+__global__ void k_fill_round(const PrepItem<T>* items, const Tile* tiles, int n_tiles, int* left, int* tleft, int round)
 {
-    const Tile t = tiles[blockIdx.x];
-    const PrepItem<T>& it = items[t.item];
-    if (round > 1 && it.unfilled[round - 1] == 0) return;
-    const int j = t.tx * LTW + (threadIdx.x % LTW), i = t.ty * LTH + (threadIdx.x / LTW);
-    const int W = it.W, H = it.H;
-    const bool inside = (i < H && j < W);
-    int left = 0;
-    for (int f = 0; f < 2 && inside; f++) {
-        const int l = i * W + j;
-        uint8_t* st = it.stamp[f];
-        if (st[l] != 255) continue;  // valid or already filled
-        auto known = [&](int ii, int jj) { const int s = st[ii * W + jj]; return s < round; };
-        auto count = [&](int ci, int cj) {
-            int c = 0;
-            for (int ii = max(0, ci - 1); ii <= min(H - 1, ci + 1); ii++)
-                for (int jj = max(0, cj - 1); jj <= min(W - 1, cj + 1); jj++)
-                    if (!(ii == ci && jj == cj) && known(ii, jj)) c++;
-            return c;
-        };
-        const int c = count(i, j);
-        bool fill = c > 0;
-        for (int ii = max(0, i - 1); ii <= min(H - 1, i + 1) && fill; ii++)
-            for (int jj = max(0, j - 1); jj <= min(W - 1, j + 1); jj++) {
-                if (ii == i && jj == j) continue;
-                const int s = st[ii * W + jj];
-                if (s >= round && count(ii, jj) > c) { fill = false; break; }
-            }
-        if (!fill) { left++; continue; }
-        float v[8];
-        int n = 0;
-        for (int ii = max(0, i - 1); ii <= min(H - 1, i + 1); ii++)
-            for (int jj = max(0, j - 1); jj <= min(W - 1, j + 1); jj++)
-                if (!(ii == i && jj == j) && known(ii, jj)) {
-                    float x = (float)it.dep[f][ii * W + jj];
-                    int k = n++;
-                    while (k > 0 && v[k - 1] > x) { v[k] = v[k - 1]; k--; }
-                    v[k] = x;
+    // left[r]: hole pixels (all pairs, both frames) still unfilled after round r; tleft[ti]: nonzero
+    // while tile ti holds one.  A block takes the tiles blockIdx.x + k gridDim.x; after round 1 it
+    // gathers, 32 at a time, only those that still hold holes, and once every hole is filled the
+    // remaining rounds end after one load.
+    __shared__ int s_list[32];
+    __shared__ int s_n;
+    if (round > 1 && left[round - 1] == 0) return;
+    const int per = (n_tiles - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
+    for (int k0 = 0; k0 < per; k0 += 32) {
+        if (threadIdx.x < 32) {
+            const int k = k0 + threadIdx.x;
+            const int ti = blockIdx.x + k * gridDim.x;
+            const bool has = k < per && (round == 1 || tleft[ti] != 0);
+            const unsigned m = __ballot_sync(0xffffffffu, has);
+            if (has) s_list[__popc(m & ((1u << threadIdx.x) - 1))] = ti;
+            if (threadIdx.x == 0) s_n = __popc(m);
+        }
+        __syncthreads();
+        const int n = s_n;
+        for (int q = 0; q < n; q++) {
+        const int ti = s_list[q];
+        const Tile t = tiles[ti];
+        const PrepItem<T>& it = items[t.item];
+        const int j = t.tx * LTW + (threadIdx.x % LTW), i = t.ty * LTH + (threadIdx.x / LTW);
+        const int W = it.W, H = it.H;
+        const bool inside = (i < H && j < W);
+        int nleft = 0;
+        for (int f = 0; f < 2 && inside; f++) {
+            const int l = i * W + j;
+            uint8_t* st = it.stamp[f];
+            if (st[l] != 255) continue;  // valid or already filled
+            auto known = [&](int ii, int jj) { const int s = st[ii * W + jj]; return s < round; };
+            auto count = [&](int ci, int cj) {
+                int c = 0;
+                for (int ii = max(0, ci - 1); ii <= min(H - 1, ci + 1); ii++)
+                    for (int jj = max(0, cj - 1); jj <= min(W - 1, cj + 1); jj++)
+                        if (!(ii == ci && jj == cj) && known(ii, jj)) c++;
+                return c;
+            };
+            const int c = count(i, j);
+            bool fill = c > 0;
+            for (int ii = max(0, i - 1); ii <= min(H - 1, i + 1) && fill; ii++)
+                for (int jj = max(0, j - 1); jj <= min(W - 1, j + 1); jj++) {
+                    if (ii == i && jj == j) continue;
+                    const int s = st[ii * W + jj];
+                    if (s >= round && count(ii, jj) > c) { fill = false; break; }
                 }
-        it.dep[f][l] = (T)v[n / 2];
-        st[l] = (uint8_t)round;
+            if (!fill) { nleft++; continue; }
+            float v[8];
+            int n = 0;
+            for (int ii = max(0, i - 1); ii <= min(H - 1, i + 1); ii++)
+                for (int jj = max(0, j - 1); jj <= min(W - 1, j + 1); jj++)
+                    if (!(ii == i && jj == j) && known(ii, jj)) {
+                        float x = (float)it.dep[f][ii * W + jj];
+                        int k = n++;
+                        while (k > 0 && v[k - 1] > x) { v[k] = v[k - 1]; k--; }
+                        v[k] = x;
+                    }
+            it.dep[f][l] = (T)v[n / 2];
+            st[l] = (uint8_t)round;
+        }
+        // pixels still unfilled after this round: all pairs (early exit of later rounds) and per
+        // tile (later rounds skip the tile when none is left)
+        const int any = __syncthreads_count(nleft > 0);
+        const unsigned m = __ballot_sync(0xffffffffu, nleft > 0);
+        int tot = nleft;
+        for (int o = 16; o > 0; o >>= 1) tot += __shfl_down_sync(0xffffffffu, tot, o);
+        if ((threadIdx.x & 31) == 0 && m) atomicAdd(&left[round], tot);
+        if (threadIdx.x == 0) tleft[ti] = any;
+        }
+        __syncthreads();  // s_list is refilled
     }
-    // count pixels still unfilled after this round (warp aggregate)
-    const unsigned m = __ballot_sync(0xffffffffu, left > 0);
-    int tot = left;
-    for (int o = 16; o > 0; o >>= 1) tot += __shfl_down_sync(0xffffffffu, tot, o);
-    if ((threadIdx.x & 31) == 0 && m) atomicAdd(&it.unfilled[round], tot);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -699,30 +747,33 @@ __device__ __forceinline__ void sor_point(const T* c, T aL, T aU, T aR, T aD, T 
                                           const T* xl, const T* xu, const T* xr, const T* xd, const T* xp,
                                           T omega, T step, T* out)
 {
+    // Each row: v = (rhs - sum of neighbour terms - the other two unknowns' terms) / diag, relaxed
+    // and clamped; every product-subtract is one fused multiply-add, in the reference's order.
+    const T omc = (T)1 - omega;
     // u row
-    T v = 0;
-    v -= aL * xl[0]; v -= aU * xu[0]; v -= aR * xr[0]; v -= aD * xd[0];
-    v += c[6];
-    v -= c[3] * xp[1]; v -= c[4] * xp[2];
-    v *= c[0];
-    T r = omega * v + ((T)1 - omega) * xp[0];
-    out[0] = minT(maxT(r, xp[0] - step), xp[0] + step);
+    T v = -mulR(aL, xl[0]);
+    v = fmaR(-aU, xu[0], v); v = fmaR(-aR, xr[0], v); v = fmaR(-aD, xd[0], v);
+    v = addR(v, c[6]);
+    v = fmaR(-c[3], xp[1], v); v = fmaR(-c[4], xp[2], v);
+    v = mulR(v, c[0]);
+    T r = fmaR(omega, v, mulR(omc, xp[0]));
+    out[0] = minT(maxT(r, subR(xp[0], step)), addR(xp[0], step));
     // v row
-    v = 0;
-    v -= aL * xl[1]; v -= aU * xu[1]; v -= aR * xr[1]; v -= aD * xd[1];
-    v += c[7];
-    v -= c[3] * xp[0]; v -= c[5] * xp[2];
-    v *= c[1];
-    r = omega * v + ((T)1 - omega) * xp[1];
-    out[1] = minT(maxT(r, xp[1] - step), xp[1] + step);
+    v = -mulR(aL, xl[1]);
+    v = fmaR(-aU, xu[1], v); v = fmaR(-aR, xr[1], v); v = fmaR(-aD, xd[1], v);
+    v = addR(v, c[7]);
+    v = fmaR(-c[3], xp[0], v); v = fmaR(-c[5], xp[2], v);
+    v = mulR(v, c[1]);
+    r = fmaR(omega, v, mulR(omc, xp[1]));
+    out[1] = minT(maxT(r, subR(xp[1], step)), addR(xp[1], step));
     // w row: neighbour coefficients carry the depth-smoothness weight of the edge's source pixel
-    v = 0;
-    v -= (aL * sL) * xl[2]; v -= (aU * sU) * xu[2]; v -= (aR * s) * xr[2]; v -= (aD * s) * xd[2];
-    v += c[8];
-    v -= c[4] * xp[0]; v -= c[5] * xp[1];
-    v *= c[2];
-    r = omega * v + ((T)1 - omega) * xp[2];
-    out[2] = minT(maxT(r, xp[2] - step), xp[2] + step);
+    v = -mulR(mulR(aL, sL), xl[2]);
+    v = fmaR(-mulR(aU, sU), xu[2], v); v = fmaR(-mulR(aR, s), xr[2], v); v = fmaR(-mulR(aD, s), xd[2], v);
+    v = addR(v, c[8]);
+    v = fmaR(-c[4], xp[0], v); v = fmaR(-c[5], xp[1], v);
+    v = mulR(v, c[2]);
+    r = fmaR(omega, v, mulR(omc, xp[2]));
+    out[2] = minT(maxT(r, subR(xp[2], step)), addR(xp[2], step));
 }
 
 // Two same-colour neighbours of one row as one aligned vector access (even index).
@@ -745,12 +796,12 @@ template <class T> __device__ __forceinline__ void st2(T* p, T a, T b)
 // with 2-wide shared accesses, both updates, 2-wide stores.  b = column parity of the colour in
 // this row: the left neighbour of position m is other-colour position m - 1 + b, the right one
 // m + b.  Returns the largest |x_new - x_old| over the pair's interior pixels (imask bit 0 / 1).
-template <class T, int PL, int HRW>
-__device__ __forceinline__ T sor_pair(T* buf, int rw, int color, int m, int b, T omega, T step, int imask)
+// The offsets name the pair's own half-row position (own), the other colour's half-row of the
+// same row at the same position (oth), and the other colour's half-rows of the rows above (ou)
+// and below (od); planes are PL elements apart.
+template <class T, int PL>
+__device__ __forceinline__ T sor_pair_at(T* buf, int own, int oth, int ou, int od, int b, T omega, T step, int imask)
 {
-    const int own = (rw * 2 + color) * HRW + m;
-    const int oth = (rw * 2 + (color ^ 1)) * HRW + m;
-    const int ou = oth - 2 * HRW, od = oth + 2 * HRW;
     // left / right neighbours of the two pixels from one 2-wide and one scalar access
     T l0[5], l1[5], r0[5], r1[5];
     const int pls[5] = {9, 11, 12, 13, 14};
@@ -792,6 +843,14 @@ __device__ __forceinline__ T sor_pair(T* buf, int rw, int color, int m, int b, T
     if (imask & 2)
         for (int v = 0; v < 3; v++) md = maxT(md, absT(n1[v] - xp1[v]));
     return md;
+}
+
+template <class T, int PL, int HRW>
+__device__ __forceinline__ T sor_pair(T* buf, int rw, int color, int m, int b, T omega, T step, int imask)
+{
+    const int own = (rw * 2 + color) * HRW + m;
+    const int oth = (rw * 2 + (color ^ 1)) * HRW + m;
+    return sor_pair_at<T, PL>(buf, own, oth, oth - 2 * HRW, oth + 2 * HRW, b, omega, step, imask);
 }
 
 // Region of a tile: global columns [ws, ws + RW), rows [y0, y0 + RH); ws a multiple of 8 so
@@ -968,9 +1027,8 @@ k_sor(const LevelItem<T, S>* items, const Tile* tiles, int ntiles, SolveConst<T>
                 const T a = buf[12 * PL + o], bq = buf[13 * PL + o], cz = buf[14 * PL + o];
                 if (L.final_fold) {
                     const size_t lp = (size_t)gi * pitch + gj;
-                    o0[lp] += a; o1[lp] += bq; o2[lp] += cz;
-                    const T wz = fl / dep[(size_t)gi * W + gj];
-                    part += a * a + bq * bq + (cz * cz) * wz;
+                    o0[lp] = addR(o0[lp], a); o1[lp] = addR(o1[lp], bq); o2[lp] = addR(o2[lp], cz);
+                    part = addR(part, stat_px<T>(a, bq, cz, fl, dep[(size_t)gi * W + gj]));
                 } else {
                     const int lc = cs_idx(gi, gj, hwp);
                     o0[lc] = a; o1[lc] = bq; o2[lc] = cz;
@@ -1001,6 +1059,318 @@ k_sor(const LevelItem<T, S>* items, const Tile* tiles, int ntiles, SolveConst<T>
         cur ^= (NBUF - 1);
     }
     cp_async_wait<0>();
+}
+
+// ------------------------------------------------------------------------------------------
+// Red-black SOR over column strips, the rows streamed through a shared-memory ring (wavefront
+// temporal blocking).
+//
+// A work unit is one item's strip of 64 interior columns [x0, x0 + 64) over a band of rows
+// [ya, yb) (ya a multiple of 32; yb a multiple of 32 or H).  Shared memory holds the strip plus
+// 16 columns each side (the 2K-pixel halo of K <= 5 iterations, widened to whole 16-byte chunks)
+// for a ring of 32 rows, all 15 planes, in the checkerboard layout.  The 2 nit half-sweeps of
+// the launch run as a pipeline of stages: at step t, stage s (colour s & 1) updates row t - 2s.
+// The lag of two rows per stage makes the in-place update exact: when stage s writes row r,
+// stage s - 1 has finished every row <= r + 1 in earlier steps and stage s + 1 has not yet read
+// any row >= r - 1, so each update sees exactly the values of a whole-image red-black sweep.  As
+// in the tile kernel, stage s only has to be right within h = 2 nit - 1 - s pixels of the unit's
+// interior, so its window is the interior widened by h (clipped to the image).
+//
+// Every step: each thread issues one cp.async of the row 2 + P steps ahead (P = 8 rows in
+// flight; only the threads that own a load position issue them); threads 0..479 run the stages
+// (48 lanes a stage, one pixel a lane); threads 480..511 write the row that left the pipeline (x
+// to the other ping-pong buffer, or the fold u += x with the statistic); one barrier.  Units come from a ticket counter, so a pair that has finished its
+// level costs nothing and the SMs stay balanced.  Results equal the tile kernel's bit for bit:
+// the same pixel update, and the same statistic partial per 32 x 32 tile summed in the same order
+// (rows r and r + 16 paired, a warp tree over the 32 columns, then the 16 row pairs in order).
+constexpr int kStripW = 64, kStripRW = 96, kStripHRW = 48, kStripNR = 32, kStripNU = 16, kStripP = 8;
+constexpr int kStripNT = 512, kStripLanes = 48, kStripOutT = 480, kStripMaxNit = 5;
+constexpr int kStripPL = kStripNR * kStripRW;  // ring plane stride (elements)
+constexpr int kStripUPL = kStripNU * kStripW;  // fold ring plane stride: u (3 planes) and depth 1
+template <class T> constexpr size_t strip_smem_bytes()
+{
+    return sizeof(T) * ((size_t)15 * kStripPL + 4 * kStripUPL + 2 * 16 * 32);
+}
+static_assert(4 * kStripMaxNit + 1 + kStripP < kStripNR, "ring too short for the pipeline depth");
+static_assert(kStripNU > kStripP + 1, "fold ring too short for the prefetch depth");
+static_assert(2 * kStripMaxNit * kStripLanes <= kStripOutT && kStripOutT + 32 == kStripNT,
+              "stage lanes and the output warp exceed the block");
+static_assert(kStripLanes >= (kStripW + 2 * (2 * kStripMaxNit - 1)) / 2 + 1, "too few lanes for a stage row");
+static_assert(15 * 2 * (kStripHRW / 4) + 3 * (kStripW / 4) + kStripW <= kStripNT, "one load per thread per row");
+
+struct StripUnit {
+    int item;
+    int x0;      // first interior column (a multiple of 64)
+    int ya, yb;  // interior rows
+};
+
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem, int src_bytes)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(sa), "l"(gmem), "r"(src_bytes) : "memory");
+}
+
+template <class T, class S>
+__global__ void __launch_bounds__(kStripNT, 1)
+k_sor_strip(const LevelItem<T, S>* items, const StripUnit* units, int n_units, int* ticket, SolveConst<T> k,
+            SorLaunch L)
+{
+    static_assert(sizeof(T) == 4, "the strip SOR holds FP32 planes (16-byte chunks of 4 values)");
+    constexpr int RW = kStripRW, HRW = kStripHRW, PL = kStripPL, UPL = kStripUPL, NRM = kStripNR - 1;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* const ring = reinterpret_cast<T*>(smem_raw);
+    T* const uring = ring + 15 * PL;
+    T* const sacc = uring + 4 * UPL;  // [2 tile columns][16 rows][32 lanes]
+    __shared__ int s_unit, s_nit;
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int tbase = L.seq * (n_units + (int)gridDim.x);  // the tickets of this launch
+    const int s = tid / kStripLanes, j = tid % kStripLanes;  // stage and lane (threads < 480)
+    const bool outw = tid >= kStripOutT;
+    for (;;) {
+        if (tid == 0) {
+            const int u = atomicAdd(ticket, 1) - tbase;
+            int nit = -1;  // -1: nothing to do for this unit
+            if (u < n_units) {
+                const StripUnit su = units[u];
+                PairCtl* ctl = items[su.item].ctl;
+                if (!ctl->level_done) {
+                    nit = L.nit;
+                    bool stopped = ctl->sor_stop != 0;
+                    if (!stopped && L.prev_check) {
+                        const float md = __uint_as_float(ctl->maxdiff[L.prev_check_idx]);
+                        if ((double)md < k.sor_tol || (T)md >= k.step) {
+                            stopped = true;
+                            if (su.x0 == 0 && su.ya == 0) { ctl->sor_stop = 1; ctl->sor_stop_iter = L.it0; }
+                        }
+                    }
+                    if (stopped) nit = 0;
+                }
+            }
+            s_unit = u;
+            s_nit = nit;
+        }
+        __syncthreads();
+        const int u = s_unit, nit = s_nit;
+        __syncthreads();  // s_unit and s_nit are rewritten only after every thread has read them
+        if (u >= n_units) break;
+        if (nit < 0) continue;
+
+        const StripUnit su = units[u];
+        const LevelItem<T, S>& it = items[su.item];
+        const int W = it.W, H = it.H, hw = it.hwp, pitch = it.pitch;
+        const int x0 = su.x0, ya = su.ya, yb = su.yb;
+        const int wsh = x0 / 2 - 8;  // the region's first half-row position (column x0 - 16)
+        const int S2 = 2 * nit;
+        const int t0 = nit > 0 ? max(0, ya - S2 + 1) : ya - 1;
+        const int t1 = yb + 4 * nit - 1;           // the last step outputs row yb - 1
+        const int rhi_load = min(yb + S2 - 1, H);  // rows read by the stages: [t0 - 1, rhi_load]
+        const bool fold = L.final_fold != 0;
+
+        // ---- this thread's load of every row, a fixed position: kind 1 a system / increment
+        // chunk, 2 a u chunk (fold), 3 a depth element (fold), 0 none.  Rows are loaded in order
+        // t0 - 1, t0, t0 + 1, ...; the row R of the next load, its source and its ring address
+        // advance by one row per load.
+        int lkind = 0, nb0 = 0, nb1 = 0;  // valid bytes of the chunk in even / odd rows
+        const T* lbase = nullptr;         // a valid address for zero-filled copies
+        const T* lsrc = nullptr;          // source of row lR (meaningful only where it is in range)
+        size_t lstride = 0;
+        unsigned ldst = 0, lwrap = 0, lring = 0;  // shared address of row lR's slot; ring span
+        int lR = t0 - 1, lU = 0;
+        if (tid < 360) {
+            const int pl = tid / 24, rem = tid % 24, ch = rem % 12, lc = rem / 12;
+            const int lm = wsh + 4 * ch;
+            lbase = pl < 12 ? it.sys[pl] : it.x[L.xin][pl - 12];
+            lkind = 1;
+            if (!(pl >= 12 && L.xin_zero) && lm >= 0) {
+                const int cnt0 = (W + 1 - lc) >> 1, cnt1 = (W + 1 - (lc ^ 1)) >> 1;
+                nb0 = lm < cnt0 ? min(4, cnt0 - lm) * (int)sizeof(T) : 0;
+                nb1 = lm < cnt1 ? min(4, cnt1 - lm) * (int)sizeof(T) : 0;
+            }
+            lstride = (size_t)2 * hw;
+            lsrc = lbase + lc * hw + lm + (ptrdiff_t)lR * (ptrdiff_t)lstride;
+            const unsigned a0 = (unsigned)__cvta_generic_to_shared(ring + pl * PL + lc * HRW + 4 * ch);
+            lring = kStripNR * RW * sizeof(T);
+            lwrap = a0 + lring;
+            ldst = a0 + (unsigned)((lR & NRM) * RW * sizeof(T));
+        } else if (fold && tid < 472) {
+            const bool dep = tid >= 408;
+            const int col = dep ? x0 + (tid - 408) : x0 + 4 * ((tid - 360) % 16);
+            const int pl = dep ? 0 : (tid - 360) / 16;
+            nb0 = dep ? (col < W ? (int)sizeof(T) : 0) : max(0, min(4, W - col)) * (int)sizeof(T);
+            lbase = dep ? it.pyr[6] : it.u[pl];
+            lstride = dep ? (size_t)W : (size_t)pitch;
+            lU = lR - 4 * nit;
+            lsrc = lbase + col + (ptrdiff_t)lU * (ptrdiff_t)lstride;
+            const unsigned a0 = (unsigned)__cvta_generic_to_shared(uring + (dep ? 3 : pl) * UPL + (col - x0));
+            lring = kStripNU * kStripW * sizeof(T);
+            lwrap = a0 + lring;
+            ldst = a0 + (unsigned)((lU & (kStripNU - 1)) * kStripW * sizeof(T));
+            lkind = dep ? 3 : 2;
+        }
+        auto load_next = [&]() {
+            if (lkind == 1) {
+                if (lR <= rhi_load) {
+                    const int nb = (lR >= 0 && lR < H) ? ((lR & 1) ? nb1 : nb0) : 0;
+                    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(ldst), "l"(nb ? lsrc : lbase),
+                                 "r"(nb) : "memory");
+                }
+            } else if (lkind) {
+                // the fold row written when row lR enters the ring
+                if (lU >= ya && lU < yb) {
+                    const T* sp = nb0 ? lsrc : lbase;
+                    if (lkind == 2)
+                        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(ldst), "l"(sp), "r"(nb0) : "memory");
+                    else
+                        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(ldst), "l"(sp), "r"(nb0) : "memory");
+                }
+                lU++;
+            }
+            lR++;
+            lsrc += lstride;
+            ldst += (unsigned)(lkind == 1 ? RW * sizeof(T) : kStripW * sizeof(T));
+            if (ldst >= lwrap) ldst -= lring;
+        };
+
+        // ---- this thread's stage: window, and per b (the column parity of this colour in a row)
+        // its pixel's half-row position, whether it is in the window, whether it is interior
+        const bool stage = tid < 2 * kStripMaxNit * kStripLanes && s < S2;
+        const int colour = s & 1, h = S2 - 1 - s;
+        const int cl = max(x0 - h, 0), chh = min(x0 + kStripW + h, W);
+        const int rlo = max(ya - h, 0), rhi = min(yb + h, H);
+        const bool chk = L.check && s >= S2 - 2;
+        const int m0 = ((cl + 1) >> 1) + j, m1 = (cl >> 1) + j;
+        const bool pv0 = 2 * m0 < chh, pv1 = 2 * m1 + 1 < chh;
+        const int pp0 = m0 - wsh, pp1 = m1 - wsh;
+        const bool in0 = 2 * m0 >= x0 && 2 * m0 < x0 + kStripW, in1 = 2 * m1 + 1 >= x0 && 2 * m1 + 1 < x0 + kStripW;
+        // output pointers in registers: the asm memory clobbers of cp.async would otherwise make
+        // every step reload them from the item descriptor
+        T* const xo0 = fold ? it.u[0] : it.x[L.xin ^ 1][0];
+        T* const xo1 = fold ? it.u[1] : it.x[L.xin ^ 1][1];
+        T* const xo2 = fold ? it.u[2] : it.x[L.xin ^ 1][2];
+        T* const statp = it.stat_part;
+        const T fl = it.f_level;
+        const int sx = (W + kSorTW - 1) / kSorTW;
+        T md = 0, tot0 = 0, tot1 = 0;
+
+        if (lkind) {
+            load_next();  // rows t0 - 1, t0, t0 + 1: the first group
+            load_next();
+            load_next();
+            cp_async_commit();
+#pragma unroll 1
+            for (int i = 2; i <= kStripP + 1; i++) {
+                load_next();  // row t0 + i
+                cp_async_commit();
+            }
+            cp_async_wait<kStripP>();
+        }
+        __syncthreads();
+#pragma unroll 1
+        for (int t = t0; t < t1; t++) {
+            if (lkind) {
+                load_next();  // row t + 2 + P
+                cp_async_commit();
+            }
+            if (stage) {
+                const int r = t - 2 * s;
+                const int b = colour ^ (r & 1);  // column parity of this colour in row r
+                if (r >= rlo && r < rhi && (b ? pv1 : pv0)) {
+                    const int p = b ? pp1 : pp0;
+                    const int oc = (colour ^ 1) * HRW + p;
+                    const int rs = (r & NRM) * RW;
+                    const int own = rs + colour * HRW + p, oth = rs + oc;
+                    const int ol = oth - 1 + b, orr = oth + b;
+                    const int ou = ((r - 1) & NRM) * RW + oc, od = ((r + 1) & NRM) * RW + oc;
+                    T c[9], xl[3], xu[3], xr[3], xd[3], xp[3], nv[3];
+#pragma unroll
+                    for (int z = 0; z < 9; z++) c[z] = ring[z * PL + own];
+#pragma unroll
+                    for (int v = 0; v < 3; v++) {
+                        const T* xv = ring + (12 + v) * PL;
+                        xl[v] = xv[ol]; xr[v] = xv[orr]; xu[v] = xv[ou]; xd[v] = xv[od]; xp[v] = xv[own];
+                    }
+                    sor_point<T>(c, ring[9 * PL + ol], ring[10 * PL + ou], ring[9 * PL + own], ring[10 * PL + own],
+                                 ring[11 * PL + ol], ring[11 * PL + ou], ring[11 * PL + own], xl, xu, xr, xd, xp,
+                                 k.omega, k.step, nv);
+#pragma unroll
+                    for (int v = 0; v < 3; v++) ring[(12 + v) * PL + own] = nv[v];
+                    if (chk && r >= ya && r < yb && (b ? in1 : in0))
+                        for (int v = 0; v < 3; v++) md = maxT(md, absT(nv[v] - xp[v]));
+                }
+            } else if (outw) {
+                const int ro = t - 4 * nit + 1;  // the row the last stage finished in the previous step
+                if (ro >= ya && ro < yb) {
+                    const int rs = (ro & NRM) * RW;
+                    T val[2];
+#pragma unroll
+                    for (int kk = 0; kk < 2; kk++) {
+                        const int gj = x0 + lane + 32 * kk;
+                        val[kk] = 0;
+                        if (gj < W) {
+                            const int o = rs + ((ro + gj) & 1) * HRW + ((gj >> 1) - wsh);
+                            const T a = ring[12 * PL + o], bq = ring[13 * PL + o], cz = ring[14 * PL + o];
+                            if (fold) {
+                                const int ui = (ro & (kStripNU - 1)) * kStripW + lane + 32 * kk;
+                                const size_t lp = (size_t)ro * pitch + gj;
+                                xo0[lp] = addR(uring[ui], a);
+                                xo1[lp] = addR(uring[UPL + ui], bq);
+                                xo2[lp] = addR(uring[2 * UPL + ui], cz);
+                                val[kk] = stat_px<T>(a, bq, cz, fl, uring[3 * UPL + ui]);
+                            } else {
+                                const int lcx = cs_idx(ro, gj, hw);
+                                xo0[lcx] = a; xo1[lcx] = bq; xo2[lcx] = cz;
+                            }
+                        }
+                    }
+                    if (fold) {
+                        // statistic partials of the (up to) two 32 x 32 tiles this row crosses
+                        const int rl = ro & 31;
+                        if (rl < 16) {
+                            sacc[rl * 32 + lane] = val[0];
+                            sacc[(16 + rl) * 32 + lane] = val[1];
+                        } else {
+                            T p0 = addR(sacc[(rl - 16) * 32 + lane], val[0]);
+                            T p1 = addR(sacc[rl * 32 + lane], val[1]);
+                            for (int off = 16; off > 0; off >>= 1) {
+                                p0 = addR(p0, __shfl_down_sync(0xffffffffu, p0, off));
+                                p1 = addR(p1, __shfl_down_sync(0xffffffffu, p1, off));
+                            }
+                            tot0 = addR(tot0, p0);
+                            tot1 = addR(tot1, p1);
+                        }
+                        if (rl == 31 || ro == yb - 1) {
+                            const int nrows = rl + 1;  // rows r2 whose row r2 + 16 does not exist
+                            for (int r2 = max(0, nrows - 16); r2 < min(16, nrows); r2++) {
+                                T p0 = sacc[r2 * 32 + lane], p1 = sacc[(16 + r2) * 32 + lane];
+                                for (int off = 16; off > 0; off >>= 1) {
+                                    p0 = addR(p0, __shfl_down_sync(0xffffffffu, p0, off));
+                                    p1 = addR(p1, __shfl_down_sync(0xffffffffu, p1, off));
+                                }
+                                tot0 = addR(tot0, p0);
+                                tot1 = addR(tot1, p1);
+                            }
+                            if (lane == 0) {
+                                const int tb = (ro >> 5) * sx + (x0 >> 5);
+                                statp[tb] = tot0;
+                                if (x0 + 32 < W) statp[tb + 1] = tot1;
+                            }
+                            tot0 = 0;
+                            tot1 = 0;
+                        }
+                    }
+                }
+            }
+            if (lkind) cp_async_wait<kStripP>();
+            __syncthreads();
+        }
+        cp_async_wait<0>();
+        if (L.check && nit > 0) {
+            float mm = (float)md;
+            for (int off = 16; off > 0; off >>= 1) mm = fmaxf(mm, __shfl_xor_sync(0xffffffffu, mm, off));
+            if (lane == 0 && mm > 0) atomicMax(&items[su.item].ctl->maxdiff[L.check_idx], __float_as_uint(mm));
+        }
+        __syncthreads();  // the ring is refilled by the next unit
+    }
 }
 
 // After each outer iteration: the early-termination statistic of the pair (mean over 3N of

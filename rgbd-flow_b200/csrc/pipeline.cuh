@@ -132,6 +132,9 @@ struct HostParams {
     double omega, step, eps_d, eps_z, eps_s, sor_tol, outer_tol, occ_margin, occ_penalty, max_grad;
     int period, K, fill_rounds;
     int sor_ilp, sor_nbuf;  // 0 = automatic
+    int sor_strip;          // strip SOR for large FP32 levels (0: tiles everywhere)
+    int strip_min_w, strip_min_h, strip_seg;  // strip eligibility and band height (0: automatic)
+    long strip_min_px;                        // strips only for steps with this many eligible pixels
 };
 
 // Row pitch of the u planes, and the checkerboard half-row length of the x / sys planes (16-byte
@@ -167,6 +170,52 @@ static inline SorConfig choose_sor_config(const HostParams& hp, long level_px)
     return c;
 }
 
+// Whether an item's level may run on the strip SOR: FP32 planes, at most 5 sweeps per launch, and
+// a level large enough that its strips carry many rows (the pipeline fill costs about 6 nit rows).
+// Measured on the 640x480 benchmark: strips beat tiles on the 640-wide level of a 16-pair batch,
+// tie at 320 and lose at 160; with a single pair the 640-wide level has too few strip units to
+// fill the SMs, so a step only uses strips when its eligible items add up to enough pixels.
+template <class T>
+static inline bool use_strip(const HostParams& hp, int W, int H)
+{
+    if (sizeof(T) != 4 || !hp.sor_strip || hp.K > kStripMaxNit) return false;
+    return W >= (hp.strip_min_w > 0 ? hp.strip_min_w : 400) && H >= (hp.strip_min_h > 0 ? hp.strip_min_h : 96);
+}
+
+// Work units of the strip SOR: every item's strips of 64 columns, cut into bands of rows (a
+// multiple of 32 high; the last band of a strip takes the remainder).  The band height aims at
+// about four units per SM over the step, so units of pairs that finish early leave no SM idle
+// for long, and at no fewer than 64 rows, so the pipeline fill stays a small share.  Units are
+// ordered band-major, then strip, then item: consecutive tickets spread over the pairs.
+template <class X>
+static std::vector<StripUnit> strip_units(const std::vector<X>& items, const std::vector<int>& which,
+                                          const HostParams& hp, int sms)
+{
+    std::vector<StripUnit> v;
+    if (which.empty()) return v;
+    long rows = 0;
+    for (int i : which) rows += (long)((items[i].W + kStripW - 1) / kStripW) * items[i].H;
+    int seg = hp.strip_seg;
+    if (seg <= 0) {
+        const double want = (double)rows / (4.0 * sms);
+        seg = (int)((want + 16) / 32) * 32;
+        seg = std::max(64, std::min(seg, 512));
+    }
+    seg = std::max(32, seg & ~31);
+    int max_bands = 0;
+    for (int i : which) max_bands = std::max(max_bands, (items[i].H + seg - 1) / seg);
+    int max_strips = 0;
+    for (int i : which) max_strips = std::max(max_strips, (items[i].W + kStripW - 1) / kStripW);
+    for (int b = 0; b < max_bands; b++)
+        for (int sx = 0; sx < max_strips; sx++)
+            for (int i : which) {
+                const int W = items[i].W, H = items[i].H;
+                if (sx * kStripW >= W || b * seg >= H) continue;
+                v.push_back(StripUnit{i, sx * kStripW, b * seg, std::min(H, (b + 1) * seg)});
+            }
+    return v;
+}
+
 // Bump allocator over a byte range.
 struct Bump {
     size_t off = 0;
@@ -187,6 +236,7 @@ struct Plan {
     size_t in_off = 0, in_bytes = 0;    // inputs uploaded each call (bgr, depth, est)
     size_t out_off = 0, out_bytes = 0;  // flows read back
     size_t ctl_off = 0;                 // PairCtl[n]
+    size_t ctr_off = 0;                 // int[16]: strip SOR ticket counter per step (zeroed with ctl)
     size_t desc_off = 0, desc_bytes = 0;
     int kind = 0;
     std::vector<std::vector<size_t>> in_seg;  // per pair: arena offset of each input segment
@@ -199,14 +249,17 @@ struct Plan {
         long level_px;  // pixels of this level summed over the step's pairs
         size_t items_off; int n_items;
         size_t lin_tiles_off; int n_lin;
-        size_t sor_tiles_off; int n_sor;
+        size_t sor_tiles_off; int n_sor;      // tile SOR work list (items not on the strip kernel)
+        size_t strip_units_off; int n_units;  // strip SOR work list
+        int strip_grid;
     };
     std::vector<StepDesc> steps;
     struct PyrLevelDesc { size_t jobs_off; int n_jobs; size_t src_tiles_off; int n_src; size_t dst_tiles_off; int n_dst; size_t g_off; };
     std::vector<PyrLevelDesc> pyr;
     size_t prep_items_off = 0, prep_tiles_off = 0; int n_prep_tiles = 0;
     size_t out_ptrs_off = 0;
-    size_t unfilled_off = 0;            // int[n][256]
+    size_t unfilled_off = 0;            // int[256]: hole pixels left after each fill round
+    size_t tleft_off = 0;               // int[prep tiles]: the tile still holds a hole
     std::vector<std::vector<std::vector<SorLaunch>>> sor_sched;  // [step][inner iteration]
     std::vector<std::vector<int>> n_checks;                     // [step][inner iteration]
     std::vector<std::vector<size_t>> u_off;         // per pair per level: offset of u[0] (for warm-start upload)
@@ -285,7 +338,13 @@ static Plan<T, S> make_plan(const std::vector<PairSpec>& pairs, const HostParams
         }
     Bump A;
     P.ctl_off = A.take(sizeof(PairCtl) * P.n);
-    P.unfilled_off = A.take(sizeof(int) * 256 * P.n);
+    P.ctr_off = A.take(sizeof(int) * 16);
+    P.unfilled_off = A.take(sizeof(int) * 256);
+    {
+        size_t nt = 0;
+        for (const auto& p : pairs) nt += (size_t)((p.W + LTW - 1) / LTW) * ((p.H + LTH - 1) / LTH);
+        P.tleft_off = A.take(sizeof(int) * std::max<size_t>(nt, 1));
+    }
     const size_t in0 = A.off;
     for (int p = 0; p < P.n; p++) {
         std::vector<size_t> seg;
@@ -362,7 +421,6 @@ static Plan<T, S> make_plan(const std::vector<PairSpec>& pairs, const HostParams
         it.f2 = (T)((double)pairs[p].f_full * (double)pairs[p].f_full);
         it.dvc = (T)hp.dvc;
         it.max_dist = hp.max_dist;
-        it.unfilled = (int*)(P.unfilled_off + sizeof(int) * 256 * p);
         it.tiles_x = (s.w[0] + LTW - 1) / LTW;
         it.tile0 = (int)prep_tiles.size();
         const int ty = (s.h[0] + LTH - 1) / LTH;
@@ -465,18 +523,30 @@ static Plan<T, S> make_plan(const std::vector<PairSpec>& pairs, const HostParams
                 for (int x = 0; x < it.lin_tiles_x; x++) lt.push_back(Tile{iid, x, y, y * it.lin_tiles_x + x});
             items.push_back(it);
         }
+        std::vector<int> strip_items;
+        long strip_px = 0;
+        for (const auto& x : items)
+            if (use_strip<T>(hp, x.W, x.H)) strip_px += (long)x.W * x.H;
+        const bool strips = strip_px >= (hp.strip_min_px > 0 ? hp.strip_min_px : 2000000L);
         for (auto& x : items) {
             const int sx = (x.W + kSorTW - 1) / kSorTW, sy = (x.H + kSorTH - 1) / kSorTH;
             x.n_sor_tiles = sx * sy;
+            if (strips && use_strip<T>(hp, x.W, x.H)) {
+                strip_items.push_back((int)(&x - items.data()));
+                continue;
+            }
             for (int y = 0; y < sy; y++)
                 for (int xx = 0; xx < sx; xx++) stt.push_back(Tile{(int)(&x - items.data()), xx, y, y * sx + xx});
         }
+        const std::vector<StripUnit> units = strip_units(items, strip_items, hp, P.sms);
         typename Plan<T, S>::StepDesc d;
         d.level_px = 0;
         for (const auto& x : items) d.level_px += (long)x.W * x.H;
         d.items_off = P.put(items); d.n_items = (int)items.size();
         d.lin_tiles_off = P.put(lt); d.n_lin = (int)lt.size();
         d.sor_tiles_off = P.put(stt); d.n_sor = (int)stt.size();
+        d.strip_units_off = P.put(units); d.n_units = (int)units.size();
+        d.strip_grid = std::min(P.sms, d.n_units);
         P.steps.push_back(d);
     }
     // output pointers (one per pair, in the order of the finest step's items = pair order)
@@ -541,7 +611,7 @@ static void bind_plan(Plan<T, S>& P, char* base)
                 rebase(it[p].dep[f], base); rebase(it[p].stamp[f], base);
             }
             rebase_nz(it[p].sigma_in, base);
-            rebase(it[p].bmask, base); rebase(it[p].ddw, base); rebase(it[p].dsw, base); rebase(it[p].unfilled, base);
+            rebase(it[p].bmask, base); rebase(it[p].ddw, base); rebase(it[p].dsw, base);
         }
     }
     for (auto& lv : P.pyr) {
@@ -683,6 +753,17 @@ static void launch_sor(const SorConfig& c, const LevelItem<T, S>* items, const T
     }
 }
 
+template <class T, class S>
+static void launch_sor_strip(const LevelItem<T, S>* items, const StripUnit* units, int n_units, int grid, int* ticket,
+                             const SolveConst<T>& k, const SorLaunch& L, cudaStream_t st)
+{
+    if constexpr (sizeof(T) == 4) {
+        k_sor_strip<T, S><<<grid, kStripNT, strip_smem_bytes<T>(), st>>>(items, units, n_units, ticket, k, L);
+    } else {
+        throw ArgError(-2, "the strip SOR holds FP32 planes only");
+    }
+}
+
 template <class T, class S, int K, int NB, int ILP>
 static void sor_attr1()
 {
@@ -711,6 +792,9 @@ static void set_kernel_attrs()
     sor_attr<T, S, 4>();
     sor_attr<T, S, 5>();
     sor_attr<T, S, 6>();
+    if constexpr (sizeof(T) == 4)
+        RF_CUDA(cudaFuncSetAttribute(k_sor_strip<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)strip_smem_bytes<T>()));
 }
 
 // Whether configuration c fits shared memory for type T.
@@ -738,6 +822,9 @@ static int enqueue_level(const Plan<T, S>& P, char* base, int sidx, cudaStream_t
     const LevelItem<T, S>* items = (const LevelItem<T, S>*)(base + P.desc_off + d.items_off);
     const Tile* lt = (const Tile*)(base + P.desc_off + d.lin_tiles_off);
     const Tile* stt = (const Tile*)(base + P.desc_off + d.sor_tiles_off);
+    const StripUnit* units = (const StripUnit*)(base + P.desc_off + d.strip_units_off);
+    int* ticket = (int*)(base + P.ctr_off) + sidx;
+    int seq = 0;
     const SolveConst<T> k = solve_const<T>(P.hp);
     if (setup) {
         RF_PROF_B(pf, KC_SETUP, st);
@@ -757,10 +844,17 @@ static int enqueue_level(const Plan<T, S>& P, char* base, int sidx, cudaStream_t
             const int lvl = P.Lmax - 1 - sidx;
             for (SorLaunch L : sched) {
                 L.outer = outer;
+                L.seq = seq++;
                 RF_PROF_B(pf, KC_SOR_LEVEL0 + lvl, st);
-                launch_sor<T, S>(P.sor_cfg[sidx], items, stt, d.n_sor, P.sms, k, L, st);
+                if (d.n_sor) {
+                    launch_sor<T, S>(P.sor_cfg[sidx], items, stt, d.n_sor, P.sms, k, L, st);
+                    launches++;
+                }
+                if (d.n_units) {
+                    launch_sor_strip<T, S>(items, units, d.n_units, d.strip_grid, ticket, k, L, st);
+                    launches++;
+                }
                 RF_PROF_E(pf, st);
-                launches++;
             }
         }
         const int wpb = 4;
@@ -780,7 +874,7 @@ static int enqueue_solve(const Plan<T, S>& P, char* base, cudaStream_t st, Prof*
 {
     int launches = 0;
     char* db = base + P.desc_off;
-    RF_CUDA(cudaMemsetAsync(base + P.ctl_off, 0, sizeof(PairCtl) * P.n, st));
+    RF_CUDA(cudaMemsetAsync(base + P.ctl_off, 0, P.ctr_off + sizeof(int) * 16 - P.ctl_off, st));  // ctl + tickets
     const auto& fin = P.steps.back();
     const LevelItem<T, S>* fin_items = (const LevelItem<T, S>*)(db + fin.items_off);
     const Tile* fin_tiles = (const Tile*)(db + fin.lin_tiles_off);
@@ -795,7 +889,7 @@ static int enqueue_solve(const Plan<T, S>& P, char* base, cudaStream_t st, Prof*
         RF_PROF_E(pf, st);
         launches++;
     } else {
-        RF_CUDA(cudaMemsetAsync(base + P.unfilled_off, 0, sizeof(int) * 256 * P.n, st));
+        RF_CUDA(cudaMemsetAsync(base + P.unfilled_off, 0, sizeof(int) * 256, st));
         const PrepItem<T>* prep = (const PrepItem<T>*)(db + P.prep_items_off);
         const Tile* pt = (const Tile*)(db + P.prep_tiles_off);
         RF_PROF_B(pf, KC_PREP, st);
@@ -808,7 +902,8 @@ static int enqueue_solve(const Plan<T, S>& P, char* base, cudaStream_t st, Prof*
         if (P.hp.fill_holes)
             for (int r = 1; r <= P.hp.fill_rounds; r++) {
                 RF_PROF_B(pf, KC_FILL, st);
-                k_fill_round<T><<<P.n_prep_tiles, LTW * LTH, 0, st>>>(prep, pt, r);
+                k_fill_round<T><<<std::min(P.n_prep_tiles, 8 * P.sms), LTW * LTH, 0, st>>>(
+                    prep, pt, P.n_prep_tiles, (int*)(base + P.unfilled_off), (int*)(base + P.tleft_off), r);
                 RF_PROF_E(pf, st);
                 launches++;
             }
