@@ -295,8 +295,10 @@ __global__ void k_fill_round(const PrepItem<T>* items, const Tile* tiles, int n_
     // while tile ti holds one.  A block takes the tiles blockIdx.x + k gridDim.x; after round 1 it
     // gathers, 32 at a time, only those that still hold holes, and once every hole is filled the
     // remaining rounds end after one load.
+    constexpr int FH = LTH + 4, FW = LTW + 4;
     __shared__ int s_list[32];
     __shared__ int s_n;
+    __shared__ uint8_t s_st[2][FH][FW];
     if (round > 1 && left[round - 1] == 0) return;
     const int per = (n_tiles - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
     for (int k0 = 0; k0 < per; k0 += 32) {
@@ -311,55 +313,63 @@ __global__ void k_fill_round(const PrepItem<T>* items, const Tile* tiles, int n_
         __syncthreads();
         const int n = s_n;
         for (int q = 0; q < n; q++) {
-        const int ti = s_list[q];
-        const Tile t = tiles[ti];
-        const PrepItem<T>& it = items[t.item];
-        const int j = t.tx * LTW + (threadIdx.x % LTW), i = t.ty * LTH + (threadIdx.x / LTW);
-        const int W = it.W, H = it.H;
-        const bool inside = (i < H && j < W);
-        int nleft = 0;
-        for (int f = 0; f < 2 && inside; f++) {
-            const int l = i * W + j;
-            uint8_t* st = it.stamp[f];
-            if (st[l] != 255) continue;  // valid or already filled
-            auto known = [&](int ii, int jj) { const int s = st[ii * W + jj]; return s < round; };
-            auto count = [&](int ci, int cj) {
-                int c = 0;
-                for (int ii = max(0, ci - 1); ii <= min(H - 1, ci + 1); ii++)
-                    for (int jj = max(0, cj - 1); jj <= min(W - 1, cj + 1); jj++)
-                        if (!(ii == ci && jj == cj) && known(ii, jj)) c++;
-                return c;
-            };
-            const int c = count(i, j);
-            bool fill = c > 0;
-            for (int ii = max(0, i - 1); ii <= min(H - 1, i + 1) && fill; ii++)
-                for (int jj = max(0, j - 1); jj <= min(W - 1, j + 1); jj++) {
-                    if (ii == i && jj == j) continue;
-                    const int s = st[ii * W + jj];
-                    if (s >= round && count(ii, jj) > c) { fill = false; break; }
-                }
-            if (!fill) { nleft++; continue; }
-            float v[8];
-            int n = 0;
-            for (int ii = max(0, i - 1); ii <= min(H - 1, i + 1); ii++)
-                for (int jj = max(0, j - 1); jj <= min(W - 1, j + 1); jj++)
-                    if (!(ii == i && jj == j) && known(ii, jj)) {
-                        float x = (float)it.dep[f][ii * W + jj];
-                        int k = n++;
-                        while (k > 0 && v[k - 1] > x) { v[k] = v[k - 1]; k--; }
-                        v[k] = x;
+            const int ti = s_list[q];
+            const Tile t = tiles[ti];
+            const PrepItem<T>& it = items[t.item];
+            const int W = it.W, H = it.H;
+            const int i0 = t.ty * LTH, j0 = t.tx * LTW;
+            // the tile's stamps with a 2-pixel halo, both frames (254: outside the image).  Every
+            // decision of a round reads the state at the round's start: a stamp another block
+            // sets to `round` meanwhile reads like 255 (neither is known, both are candidates).
+            for (int e = threadIdx.x; e < 2 * FH * FW; e += LTW * LTH) {
+                const int f = e / (FH * FW), rr = (e / FW) % FH, cc = e % FW;
+                const int gi = i0 - 2 + rr, gj = j0 - 2 + cc;
+                s_st[f][rr][cc] = (gi >= 0 && gi < H && gj >= 0 && gj < W) ? it.stamp[f][gi * W + gj] : (uint8_t)254;
+            }
+            __syncthreads();
+            const int tx = threadIdx.x % LTW, ty = threadIdx.x / LTW;
+            const int j = j0 + tx, i = i0 + ty;
+            int nleft = 0;
+            for (int f = 0; f < 2 && i < H && j < W; f++) {
+                if (s_st[f][ty + 2][tx + 2] != 255) continue;  // valid or already filled
+                auto known = [&](int r, int c) { return s_st[f][r][c] < round; };
+                auto count = [&](int r, int c) {
+                    int kn = 0;
+                    for (int a = -1; a <= 1; a++)
+                        for (int b = -1; b <= 1; b++)
+                            if ((a | b) && known(r + a, c + b)) kn++;
+                    return kn;
+                };
+                const int c = count(ty + 2, tx + 2);
+                bool fill = c > 0;
+                for (int a = -1; a <= 1 && fill; a++)
+                    for (int b = -1; b <= 1; b++) {
+                        if (!(a | b)) continue;
+                        const int sn = s_st[f][ty + 2 + a][tx + 2 + b];
+                        if (sn >= round && sn != 254 && count(ty + 2 + a, tx + 2 + b) > c) { fill = false; break; }
                     }
-            it.dep[f][l] = (T)v[n / 2];
-            st[l] = (uint8_t)round;
-        }
-        // pixels still unfilled after this round: all pairs (early exit of later rounds) and per
-        // tile (later rounds skip the tile when none is left)
-        const int any = __syncthreads_count(nleft > 0);
-        const unsigned m = __ballot_sync(0xffffffffu, nleft > 0);
-        int tot = nleft;
-        for (int o = 16; o > 0; o >>= 1) tot += __shfl_down_sync(0xffffffffu, tot, o);
-        if ((threadIdx.x & 31) == 0 && m) atomicAdd(&left[round], tot);
-        if (threadIdx.x == 0) tleft[ti] = any;
+                if (!fill) { nleft++; continue; }
+                float v[8];
+                int nv = 0;
+                for (int a = -1; a <= 1; a++)
+                    for (int b = -1; b <= 1; b++)
+                        if ((a | b) && known(ty + 2 + a, tx + 2 + b)) {  // row-major neighbour order
+                            const float x = (float)it.dep[f][(i + a) * W + (j + b)];
+                            int kk = nv++;
+                            while (kk > 0 && v[kk - 1] > x) { v[kk] = v[kk - 1]; kk--; }
+                            v[kk] = x;
+                        }
+                it.dep[f][i * W + j] = (T)v[nv / 2];
+                it.stamp[f][i * W + j] = (uint8_t)round;
+            }
+            // pixels still unfilled after this round: all pairs (early exit of later rounds) and
+            // per tile (later rounds skip the tile when none is left)
+            const int any = __syncthreads_count(nleft > 0);
+            const unsigned m = __ballot_sync(0xffffffffu, nleft > 0);
+            int tot = nleft;
+            for (int o = 16; o > 0; o >>= 1) tot += __shfl_down_sync(0xffffffffu, tot, o);
+            if ((threadIdx.x & 31) == 0 && m) atomicAdd(&left[round], tot);
+            if (threadIdx.x == 0) tleft[ti] = any;
         }
         __syncthreads();  // s_list is refilled
     }
