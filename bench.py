@@ -44,7 +44,8 @@ def peaks():
 
 
 def ncu_traffic():
-    """DRAM bytes per SOR launch from the committed ncu summary (profiles/), if present."""
+    """DRAM bytes of a level-0 strip-SOR launch per pair, from the committed ncu summary
+    (profiles/sor_traffic.json), if present."""
     try:
         d = json.load(open(os.path.join(ROOT, "profiles", "sor_traffic.json")))
         return d
@@ -147,14 +148,17 @@ def run_served(ctx, rf, serving, streams, prm, args, warm):
     served flows against the plain solve of the same pairs (stream 0, a few kept results)."""
     srv = rf.Server(ctx, prm, max_streams=len(streams), max_batch=len(streams), hbm_budget_bytes=20 << 30,
                     warm_start=warm, warm_early_termination=warm)
-    serving.simulate(srv, rf, streams, n_frames=2 * args.serve_unique, fps=30.0, seed=1)  # warm-up: graphs
-    r = serving.simulate(srv, rf, streams, n_frames=args.serve_frames, fps=30.0, seed=2, keep_stream=0, keep_n=6)
+    # warm-up: the slots' graphs for the batch mixes that recur (about a second of traffic)
+    serving.simulate(srv, rf, streams, n_frames=4 * args.serve_unique, fps=30.0, seed=1)
+    r = serving.simulate(srv, rf, streams, n_frames=args.serve_frames, fps=30.0, seed=2, keep_stream=0, keep_n=7)
     lat = np.array(r["latencies_ms"])
     sat = serving.simulate(srv, rf, streams, n_frames=args.serve_unique * 3, fps=30.0, seed=3, time_scale=0.0)
     srv.close()
     seq = streams[0]
     epes = []
     for rid, flow in r["kept"]:
+        if rid == 0:
+            continue  # its first frame is the last frame of the warm-up run, not frame_index(-1)
         n = len(seq["frames"])
         f1 = seq["frames"][serving.frame_index(rid - 1, n)]
         f2 = seq["frames"][serving.frame_index(rid, n)]
@@ -396,7 +400,8 @@ def main():
         e2e = {"value": B * args.steps * world / e2e_s, "unit": "pairs/s",
                "h2d_bytes_per_step": B * W * H * (3 + 3 + 4 + 4), "d2h_bytes_per_step": B * W * H * 12}
 
-    # ---- roofline of the dominant kernel from a profiled pass of the same workload
+    # ---- roofline of the dominant kernel from a profiled pass of the same workload: the SOR of
+    # the 640x480 level (the strip kernel), algorithmic bytes / live CUDA-event time
     ctx.profile(1)
     for _ in range(2):
         ctx.scene_flow_batch_device(dev, prm)
@@ -404,19 +409,22 @@ def main():
     kst = ctx.profile_read()
     ctx.profile(0)
     peak, peak_kind = peaks()
+    n0, ms0, b0 = kst.get("sor_level0", (0, 0.0, 0.0))
     n_sor, sor_ms, sor_bytes = kst.get("sor", (0, 0.0, 0.0))
-    achieved = sor_bytes / (sor_ms / 1e3) / 1e9 if sor_ms > 0 else 0.0
+    achieved = b0 / (ms0 / 1e3) / 1e9 if ms0 > 0 else 0.0
     tr = ncu_traffic()
-    base_ms = sum(v[1] for k, v in kst.items() if not k.startswith("sor_level"))
-    tot_ms = base_ms
-    abpl = sor_bytes / max(n_sor, 1)
-    roofline = {"kernel": "k_sor (red-black SOR, temporal blocking, K sweeps per launch chosen per level)",
-                "bound": "hbm", "achieved": achieved,
-                "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
-                "traffic": (tr["dram_bytes_per_algorithmic_byte"] * abpl if tr else None),
-                "algorithmic_bytes_per_launch": abpl,
-                "avg_launch_us": 1e3 * sor_ms / max(n_sor, 1), "launches": n_sor,
-                "share_of_device_time": sor_ms / tot_ms if tot_ms else None,
+    tot_ms = sum(v[1] for k, v in kst.items() if not k.startswith("sor_level"))
+    roofline = {"kernel": "k_sor_strip: red-black SOR of the 640x480 level over 64-column strips, rows streamed "
+                          "through a shared-memory ring, 5 sweeps per launch",
+                "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_source": peak_kind,
+                "traffic": (tr["dram_bytes_per_launch_per_pair"] * B if tr else None),
+                "algorithmic_bytes_per_launch": b0 / max(n0, 1),
+                "avg_launch_us": 1e3 * ms0 / max(n0, 1), "launches": n0,
+                "share_of_device_time": ms0 / tot_ms if tot_ms else None,
+                "all_sor_levels": {"achieved_gbs": sor_bytes / (sor_ms / 1e3) / 1e9 if sor_ms > 0 else 0.0,
+                                   "frac": (sor_bytes / (sor_ms / 1e3) / 1e9) / peak if sor_ms > 0 else 0.0,
+                                   "share_of_device_time": sor_ms / tot_ms if tot_ms else None},
                 "kernel_ms": {k: round(v[1], 3) for k, v in kst.items()}}
     if tr:
         roofline["traffic_note"] = tr.get("note", "")

@@ -942,17 +942,22 @@ static int enqueue_solve(const Plan<T, S>& P, char* base, cudaStream_t st, Prof*
 //        3 flow, 5 weights; the 12 feature/depth values in the storage type) plus the 12-float
 //        system written.
 template <class T, class S>
-static void executed_bytes(const Plan<T, S>& P, const PairCtl* ctl, double* sor_bytes, double* lin_bytes)
+static void executed_bytes(const Plan<T, S>& P, const PairCtl* ctl, double* sor_bytes, double* lin_bytes,
+                           double* sor_level = nullptr)
 {
     *sor_bytes = 0;
     *lin_bytes = 0;
+    if (sor_level)
+        for (int k = 0; k < 16; k++) sor_level[k] = 0;
     const double lin_px = 12.0 * sizeof(S) + 8.0 * sizeof(T) + 12.0 * sizeof(T);
     for (int p = 0; p < P.n; p++)
         for (int k = 0; k < P.L[p]; k++) {
             const double N = (double)P.shapes[p].w[k] * P.shapes[p].h[k];
             const int O = std::min(ctl[p].outer_exec[k], 64);
             for (int o = 0; o < O; o++) {
-                *sor_bytes += N * (ctl[p].sor_exec[k][o] * 72.0 * sizeof(T) / 4.0 + 24.0 * sizeof(T) / 4.0);
+                const double b = N * (ctl[p].sor_exec[k][o] * 72.0 * sizeof(T) / 4.0 + 24.0 * sizeof(T) / 4.0);
+                *sor_bytes += b;
+                if (sor_level) sor_level[k] += b;
                 *lin_bytes += N * lin_px * P.hp.n_inner;
             }
         }

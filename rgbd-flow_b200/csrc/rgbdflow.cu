@@ -23,8 +23,10 @@ struct GraphEntry {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int launches = 0;
-    std::string exact;  // the batch (sizes, cameras) the executable graph currently holds
+    std::string topo;       // its launch topology (executables of one topology can be updated in place)
+    uint64_t last_use = 0;  // for least-recently-used eviction
 };
+constexpr size_t kGraphCache = 48;  // executable graphs kept per context
 
 struct rgbdflow_ctx {
     int device = 0;
@@ -36,7 +38,8 @@ struct rgbdflow_ctx {
     char* pin = nullptr;
     size_t pin_cap = 0;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
-    std::map<std::string, GraphEntry> graphs;
+    std::map<std::string, GraphEntry> graphs;  // by exact batch (sizes, cameras, parameters)
+    uint64_t graph_clock = 0;
     bool attrs[4] = {false, false, false, false};
     int last_launches = 0;
     int sms = 148;
@@ -297,13 +300,15 @@ void run_batch(rgbdflow_ctx* c, const std::vector<PairSpec>& pairs, const HostPa
     RF_CUDA(cudaEventRecord(c->e0, st));
     const bool graphs = c->use_graphs && !c->prof;
     if (graphs) {
-        // One executable graph per launch topology.  A batch of other sizes with the same topology
-        // is captured again and written into that executable (cudaGraphExecUpdate: new grids and
-        // arguments, no re-instantiation), so changing batch mixes cost a capture, not a build.
+        // One executable graph per exact batch (sizes, cameras, parameters), least recently used
+        // evicted beyond kGraphCache: recurring batch mixes (a server's) launch without any
+        // capture.  A new batch is captured once; when the cache is full it is written into an
+        // evicted executable of the same launch topology (cudaGraphExecUpdate: new grids and
+        // arguments, no re-instantiation) where one exists.
         const std::string exact = plan_key(pairs, hp, slot) + (dev ? "|dev" : "");
-        const std::string topo = topo_key(P, hp, slot, dev);
-        auto it = c->graphs.find(topo);
-        if (it == c->graphs.end() || it->second.exact != exact) {
+        auto it = c->graphs.find(exact);
+        if (it == c->graphs.end()) {
+            const std::string topo = topo_key(P, hp, slot, dev);
             cudaGraph_t graph = nullptr;
             RF_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
             int launches = 0;
@@ -316,30 +321,36 @@ void run_batch(rgbdflow_ctx* c, const std::vector<PairSpec>& pairs, const HostPa
                 throw;
             }
             RF_CUDA(cudaStreamEndCapture(c->stream, &graph));
+            GraphEntry g;
+            g.graph = graph;
+            g.topo = topo;
+            g.launches = launches;
             bool updated = false;
-            if (it != c->graphs.end()) {
+            if (c->graphs.size() >= kGraphCache) {
+                // the victim: the least recently used executable of this topology, else of any
+                auto victim = c->graphs.end();
+                for (auto j = c->graphs.begin(); j != c->graphs.end(); ++j) {
+                    const bool same = j->second.topo == topo;
+                    if (victim == c->graphs.end() || (same && victim->second.topo != topo) ||
+                        (same == (victim->second.topo == topo) && j->second.last_use < victim->second.last_use))
+                        victim = j;
+                }
+                GraphEntry old = victim->second;
+                c->graphs.erase(victim);
                 cudaGraphExecUpdateResultInfo info;
-                if (cudaGraphExecUpdate(it->second.exec, graph, &info) == cudaSuccess) {
-                    cudaGraphDestroy(it->second.graph);
-                    it->second.graph = graph;
+                if (old.topo == topo && cudaGraphExecUpdate(old.exec, graph, &info) == cudaSuccess) {
+                    g.exec = old.exec;
                     updated = true;
                 } else {
                     cudaGetLastError();
-                    cudaGraphExecDestroy(it->second.exec);
-                    cudaGraphDestroy(it->second.graph);
-                    c->graphs.erase(it);
+                    cudaGraphExecDestroy(old.exec);
                 }
+                cudaGraphDestroy(old.graph);
             }
-            if (!updated) {
-                GraphEntry g;
-                g.graph = graph;
-                RF_CUDA(cudaGraphInstantiate(&g.exec, g.graph, 0));
-                if (c->graphs.size() > 32) drop_graphs(c);
-                it = c->graphs.emplace(topo, g).first;
-            }
-            it->second.exact = exact;
-            it->second.launches = launches;
+            if (!updated) RF_CUDA(cudaGraphInstantiate(&g.exec, g.graph, 0));
+            it = c->graphs.emplace(exact, g).first;
         }
+        it->second.last_use = ++c->graph_clock;
         RF_CUDA(cudaGraphLaunch(it->second.exec, st));
         c->last_launches = it->second.launches;
     } else {
@@ -371,10 +382,11 @@ void run_batch(rgbdflow_ctx* c, const std::vector<PairSpec>& pairs, const HostPa
     RF_CUDA(cudaEventElapsedTime(&ms, c->e0, c->e1));
     if (c->prof) {
         c->prof->collect(c->prof_ms, c->prof_n);
-        double sb, lb;
-        executed_bytes(P, (const PairCtl*)pin_ctl, &sb, &lb);
+        double sb, lb, sl[16];
+        executed_bytes(P, (const PairCtl*)pin_ctl, &sb, &lb, sl);
         c->prof_bytes[KC_SOR] += sb;
         c->prof_bytes[KC_LIN] += lb;
+        for (int k = 0; k < 16; k++) c->prof_bytes[KC_SOR_LEVEL0 + k] += sl[k];
     }
     if (!dev)
         for (int p = 0; p < P.n; p++) {
@@ -806,6 +818,11 @@ int rgbdflow_server_destroy(rgbdflow_server* s)
     return RGBDFLOW_OK;
 }
 
+namespace {
+void server_presize(rgbdflow_server* s);
+constexpr int kServerFramesPerStream = 8;  // frame buffer sets stocked per stream (a backlog of ~6 pairs)
+}
+
 int rgbdflow_server_submit(rgbdflow_server* s, int stream_id, uint64_t request_id, const rgbdflow_camera_params* cam,
                            const uint8_t* bgr, const float* depth_m, int W, int H, float* flow_out)
 {
@@ -825,6 +842,16 @@ int rgbdflow_server_submit(rgbdflow_server* s, int stream_id, uint64_t request_i
     if (s->cfg.hbm_budget_bytes && s->resident_bytes + fbytes + N * 12 > s->cfg.hbm_budget_bytes)
         throw ArgError(RGBDFLOW_ERR_BUDGET, "frame does not fit the HBM budget");
     s->pool.resident = &s->resident_bytes;
+    if (!ss.flow || ss.W != W || ss.H != H) {
+        // a new stream (or size): stock its frame buffers while the budget allows
+        const size_t fb = align_up(N * 3, 256) + N * 4;
+        int stock = kServerFramesPerStream;
+        while (stock > 0 && s->cfg.hbm_budget_bytes &&
+               s->resident_bytes + stock * fb + N * 12 > s->cfg.hbm_budget_bytes / 2)
+            stock--;
+        RF_CUDA(cudaSetDevice(c->device));
+        s->pool.reserve(N, stock);
+    }
     RF_CUDA(cudaSetDevice(c->device));
     auto f = std::make_shared<DevFrame>();
     f->W = W; f->H = H; f->cam = *cam;
@@ -844,13 +871,15 @@ int rgbdflow_server_submit(rgbdflow_server* s, int stream_id, uint64_t request_i
         ss.has_flow = false;
         ss.prev.reset();
     }
-    if (!ss.flow || ss.W != W || ss.H != H) {
+    const bool resized = !ss.flow || ss.W != W || ss.H != H;
+    if (resized) {
         if (ss.flow) { RF_CUDA(cudaFree(ss.flow)); s->resident_bytes -= (size_t)ss.W * ss.H * 12; }
         RF_CUDA(cudaMalloc(&ss.flow, N * 12));
         s->resident_bytes += N * 12;
         ss.has_flow = false;
     }
     ss.W = W; ss.H = H;
+    if (resized) server_presize(s);
     if (ss.prev) {
         ServerReq r;
         r.stream = stream_id; r.id = request_id; r.W = W; r.H = H;
@@ -886,11 +915,79 @@ void server_retire(rgbdflow_server* s, ServerSlot& sl)
     sl.busy = false;
 }
 
+// Device arena and pinned descriptor staging of a slot's batch.
+struct SlotNeed {
+    size_t arena = 0, pin = 0;
+};
+SlotNeed slot_need(const std::vector<PairSpec>& ps, const HostParams& hp, int storage)
+{
+    // the storage type changes plane sizes only, not the descriptor count
+    size_t arena = 0, desc = 0;
+    if (storage == RGBDFLOW_STORE_FP16) {
+        const auto P = make_plan<float, __half>(ps, hp);
+        arena = P.arena_bytes; desc = P.desc_bytes;
+    } else if (storage == RGBDFLOW_STORE_BF16) {
+        const auto P = make_plan<float, __nv_bfloat16>(ps, hp);
+        arena = P.arena_bytes; desc = P.desc_bytes;
+    } else {
+        const auto P = make_plan<float, float>(ps, hp);
+        arena = P.arena_bytes; desc = P.desc_bytes;
+    }
+    return SlotNeed{arena, align_up(desc, 256) + sizeof(PairCtl) * ps.size()};
+}
 size_t slot_arena_need(const std::vector<PairSpec>& ps, const HostParams& hp, int storage)
 {
-    if (storage == RGBDFLOW_STORE_FP16) return make_plan<float, __half>(ps, hp).arena_bytes;
-    if (storage == RGBDFLOW_STORE_BF16) return make_plan<float, __nv_bfloat16>(ps, hp).arena_bytes;
-    return make_plan<float, float>(ps, hp).arena_bytes;
+    return slot_need(ps, hp, storage).arena;
+}
+
+// Arena bytes of a batch for admission: the sum of its pairs' single-pair arenas (an upper bound:
+// each single-pair plan carries its own control blocks and alignment), cached per pair shape.
+size_t admit_need(rgbdflow_server* s, const std::vector<PairSpec>& ps, const HostParams& hp)
+{
+    static thread_local std::map<std::string, size_t> cache;
+    size_t tot = 0;
+    for (const auto& q : ps) {
+        const std::string key = std::to_string(q.W) + "x" + std::to_string(q.H) + (q.warm() ? "w" : "c") +
+                                std::to_string(s->cfg.params.storage) + plan_key({}, hp, 0);
+        auto it = cache.find(key);
+        if (it == cache.end()) it = cache.emplace(key, slot_arena_need({q}, hp, s->cfg.params.storage)).first;
+        tot += it->second;
+    }
+    return tot;
+}
+
+// When a stream registers or changes size: size both slots' solve memory once for a full batch
+// (max_batch cold pairs of the largest registered size) as far as the HBM budget allows, so that
+// serving never regrows an arena (which waits for the device and drops the slot's graphs).
+void server_presize(rgbdflow_server* s)
+{
+    int W = 0, H = 0;
+    for (const auto& kv : s->streams)
+        if ((long)kv.second.W * kv.second.H > (long)W * H) { W = kv.second.W; H = kv.second.H; }
+    if (W < 2 || H < 2) return;
+    PairSpec q;
+    q.W = W; q.H = H;
+    q.f_full = 0.8f * W;
+    q.xres_full = (unsigned)W;
+    const int nb = std::max(1, std::min(s->cfg.max_batch, s->cfg.max_streams));
+    std::vector<PairSpec> ps(nb, q);
+    const SlotNeed need = slot_need(ps, host_params(s->cfg.params), s->cfg.params.storage);
+    for (auto& sl : s->slots) {
+        if (sl.busy) continue;  // grown on its next launch instead
+        const size_t other = (&sl == &s->slots[0]) ? s->slots[1].ctx->arena_cap : s->slots[0].ctx->arena_cap;
+        if (sl.ctx->arena_cap < need.arena &&
+            !(s->cfg.hbm_budget_bytes && s->resident_bytes + other + need.arena > s->cfg.hbm_budget_bytes))
+            ensure_arena(sl.ctx, need.arena);
+        // pinned staging: the slot's descriptors and its results (cudaFreeHost / cudaMallocHost on
+        // growth would synchronise the device mid-serving)
+        ensure_pin(sl.ctx, need.pin);
+        const size_t out = (size_t)nb * align_up((size_t)W * H * 12, 256);
+        if (sl.pin_cap < out) {
+            if (sl.pin_out) RF_CUDA(cudaFreeHost(sl.pin_out));
+            RF_CUDA(cudaMallocHost(&sl.pin_out, out));
+            sl.pin_cap = out;
+        }
+    }
 }
 
 void server_launch(rgbdflow_server* s, ServerSlot& sl)
@@ -914,8 +1011,7 @@ void server_launch(rgbdflow_server* s, ServerSlot& sl)
         q.warm_early = s->cfg.warm_early_termination;
         q.out = ss.flow;
         specs.push_back(q);
-        if (s->cfg.hbm_budget_bytes &&
-            s->resident_bytes + other + slot_arena_need(specs, hp, s->cfg.params.storage) > s->cfg.hbm_budget_bytes) {
+        if (s->cfg.hbm_budget_bytes && s->resident_bytes + other + admit_need(s, specs, hp) > s->cfg.hbm_budget_bytes) {
             specs.pop_back();
             break;  // the budget is full: later requests wait for memory
         }

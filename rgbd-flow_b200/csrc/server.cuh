@@ -35,6 +35,24 @@ struct FrameBufs {
 struct FramePool {
     std::unordered_map<size_t, std::vector<FrameBufs>> free_;
     size_t* resident = nullptr;
+    static FrameBufs make(size_t n_px, size_t* resident)
+    {
+        FrameBufs b;
+        b.bytes = align_up(n_px * 3, 256) + n_px * 4;
+        RF_CUDA(cudaMalloc(&b.dev, b.bytes));
+        RF_CUDA(cudaMallocHost(&b.pin, n_px * 7));
+        RF_CUDA(cudaEventCreateWithFlags(&b.ready, cudaEventDisableTiming));
+        *resident += b.bytes;
+        return b;
+    }
+    // Stock `count` more buffer sets of this size up front: allocating them while serving (device
+    // and page-locked memory) stalls the request loop for milliseconds to a hundred and more,
+    // exactly when a burst of arrivals keeps more frames alive.
+    void reserve(size_t n_px, int count)
+    {
+        auto& v = free_[n_px];
+        for (int i = 0; i < count; i++) v.push_back(make(n_px, resident));
+    }
     FrameBufs get(size_t n_px)
     {
         auto& v = free_[n_px];
@@ -43,13 +61,7 @@ struct FramePool {
             v.pop_back();
             return b;
         }
-        FrameBufs b;
-        b.bytes = align_up(n_px * 3, 256) + n_px * 4;
-        RF_CUDA(cudaMalloc(&b.dev, b.bytes));
-        RF_CUDA(cudaMallocHost(&b.pin, n_px * 7));
-        RF_CUDA(cudaEventCreateWithFlags(&b.ready, cudaEventDisableTiming));
-        *resident += b.bytes;
-        return b;
+        return make(n_px, resident);
     }
     void put(size_t n_px, const FrameBufs& b) { free_[n_px].push_back(b); }
     void release_all()
