@@ -232,6 +232,18 @@ int rgbdflow_scene_flow_batch(rgbdflow_ctx* ctx, const rgbdflow_pair* pairs, int
 int rgbdflow_scene_flow_batch_async(rgbdflow_ctx* ctx, const rgbdflow_pair* pairs, int n,
                                     const rgbdflow_params* params, void* stream);
 
+/* Same as rgbdflow_scene_flow_batch (HOST buffers), but returns once the work is enqueued on the
+ * context's stream: the inputs' upload, the solve and the flows' download run while the caller
+ * goes on, and rgbdflow_ctx_synchronize(ctx) waits for them.  No reference counterpart: a caller
+ * that alternates two contexts overlaps one batch's PCIe transfers with the other's solve.
+ *   flow_out must be page-locked host memory (cudaMallocHost / cudaHostRegister): the flows are
+ *   DMA'd straight into it; RGBDFLOW_ERR_INVALID_ARG otherwise.  Inputs may be pageable (they are
+ *   staged before the call returns) or page-locked (DMA'd directly; keep them unchanged until the
+ *   context is synchronised).  FP32 compute only (RGBDFLOW_ERR_UNSUPPORTED for FP64).  The flows
+ *   of a submitted batch equal rgbdflow_scene_flow_batch's bit for bit. */
+int rgbdflow_scene_flow_batch_submit(rgbdflow_ctx* ctx, const rgbdflow_pair* pairs, int n,
+                                     const rgbdflow_params* params);
+
 /* Wait for every solve this context enqueued (on any stream). */
 int rgbdflow_ctx_synchronize(rgbdflow_ctx* ctx);
 

@@ -234,7 +234,7 @@ void ensure_attrs(rgbdflow_ctx* c, int slot)
 //                           user_stream and the call returns without waiting.
 template <class T, class S>
 void run_batch(rgbdflow_ctx* c, const std::vector<PairSpec>& pairs, const HostParams& hp, rgbdflow_stats* stats, int slot,
-               cudaStream_t user_stream = nullptr)
+               cudaStream_t user_stream = nullptr, bool host_async = false)
 {
     ensure_attrs<T, S>(c, slot);
     const bool dev = user_stream != nullptr;
@@ -375,6 +375,12 @@ void run_batch(rgbdflow_ctx* c, const std::vector<PairSpec>& pairs, const HostPa
     if (want_ctl) RF_CUDA(cudaMemcpyAsync(pin_ctl, c->arena + P.ctl_off, ctl_bytes, cudaMemcpyDeviceToHost, st));
     RF_CUDA(cudaEventRecord(c->done, st));
     c->pending = true;
+    if (host_async) {
+        for (int p = 0; p < P.n; p++)
+            if (!out_direct[p]) throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "submitted pair " + std::to_string(p) +
+                                                                        ": flow_out must be page-locked host memory");
+        return;
+    }
     if (dev && !want_ctl) return;
     RF_CUDA(cudaEventSynchronize(c->done));
     c->pending = false;
@@ -410,9 +416,17 @@ void run_batch(rgbdflow_ctx* c, const std::vector<PairSpec>& pairs, const HostPa
 
 
 static void dispatch(rgbdflow_ctx* c, const std::vector<PairSpec>& ps, const rgbdflow_params& p, rgbdflow_stats* stats,
-                     cudaStream_t user_stream = nullptr)
+                     cudaStream_t user_stream = nullptr, bool host_async = false)
 {
     const HostParams hp = host_params(p);
+    if (host_async) {
+        if (p.compute == RGBDFLOW_COMPUTE_FP64)
+            throw ArgError(RGBDFLOW_ERR_UNSUPPORTED, "the FP64 device solve has no submitted form");
+        if (p.storage == RGBDFLOW_STORE_FP16) run_batch<float, __half>(c, ps, hp, nullptr, 2, nullptr, true);
+        else if (p.storage == RGBDFLOW_STORE_BF16) run_batch<float, __nv_bfloat16>(c, ps, hp, nullptr, 3, nullptr, true);
+        else run_batch<float, float>(c, ps, hp, nullptr, 0, nullptr, true);
+        return;
+    }
     if (p.compute == RGBDFLOW_COMPUTE_FP64) {
         if (user_stream) throw ArgError(RGBDFLOW_ERR_UNSUPPORTED, "the FP64 device solve has no device-pointer form");
         run_batch<double, double>(c, ps, hp, stats, 1);
@@ -692,6 +706,34 @@ int rgbdflow_scene_flow_single_scale(rgbdflow_ctx* c, const rgbdflow_camera_para
     s.out_u = u; s.out_v = v; s.out_w = w;
     s.out_warpI = warpIm2; s.out_warpD = warpDm2;
     dispatch(c, {s}, p, stats);
+    return RGBDFLOW_OK;
+    API_END(c)
+}
+
+int rgbdflow_scene_flow_batch_submit(rgbdflow_ctx* c, const rgbdflow_pair* pairs, int n, const rgbdflow_params* params)
+{
+    if (!c) return RGBDFLOW_ERR_INVALID_ARG;
+    API_BEGIN
+    validate(params);
+    if (!pairs || n <= 0) throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "no pairs");
+    RF_CUDA(cudaSetDevice(c->device));
+    std::vector<PairSpec> ps;
+    for (int i = 0; i < n; i++) {
+        const rgbdflow_pair& q = pairs[i];
+        if (q.W < 2 || q.H < 2 || !q.bgr1 || !q.bgr2 || !q.depth1_m || !q.depth2_m || !q.flow_out)
+            throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "pair " + std::to_string(i) + ": bad size or null buffer");
+        if (q.cam.xRes == 0 || !(q.cam.focalLength > 0))
+            throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "pair " + std::to_string(i) + ": bad camera");
+        if (!is_pinned(q.flow_out))
+            throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "pair " + std::to_string(i) + ": flow_out must be page-locked host memory");
+        PairSpec s;
+        s.W = q.W; s.H = q.H;
+        resized_cam(q.cam, q.W, s.f_full, s.xres_full);
+        s.bgr1 = q.bgr1; s.depth1 = q.depth1_m; s.bgr2 = q.bgr2; s.depth2 = q.depth2_m;
+        s.est = q.est_flow; s.out = q.flow_out;
+        ps.push_back(s);
+    }
+    dispatch(c, ps, *params, nullptr, nullptr, true);
     return RGBDFLOW_OK;
     API_END(c)
 }

@@ -172,6 +172,7 @@ SIGNATURES = {
                                               _vp, _vp, _i, _i, _i, _i, _P(Params), _P(Stats)]),
     "rgbdflow_scene_flow_batch": (_i, [_vp, _P(RgbdFlowPair), _i, _P(Params), _P(Stats)]),
     "rgbdflow_scene_flow_batch_async": (_i, [_vp, _P(RgbdFlowPair), _i, _P(Params), _vp]),
+    "rgbdflow_scene_flow_batch_submit": (_i, [_vp, _P(RgbdFlowPair), _i, _P(Params)]),
     "rgbdflow_ctx_synchronize": (_i, [_vp]),
     "rgbdflow_ctx_last_launch_count": (_i, [_vp]),
     "rgbdflow_profile": (_i, [_vp, _i]),
@@ -401,6 +402,27 @@ class Context:
         rc = self.lib.rgbdflow_scene_flow_batch(self.h, arr, len(pairs), ctypes.byref(params), st)
         self._check(rc)
         return (outs, list(st)) if stats else outs
+
+    def scene_flow_batch_submit(self, pairs, params, outs):
+        """Host-buffer batch that returns once enqueued (rgbdflow_scene_flow_batch_submit).  outs:
+        page-locked (H,W,3) float32 arrays the flows are DMA'd into; the input arrays and outs must
+        stay alive and unchanged until synchronize().  Returns outs."""
+        keep = []
+        arr = (RgbdFlowPair * len(pairs))()
+        for i, p in enumerate(pairs):
+            b1, b2 = _c(p["bgr1"], np.uint8), _c(p["bgr2"], np.uint8)
+            d1, d2 = _c(p["depth1"], np.float32), _c(p["depth2"], np.float32)
+            est = _c(p["est_flow"], np.float32) if p.get("est_flow") is not None else None
+            keep += [b1, b2, d1, d2, est]
+            arr[i].W, arr[i].H, arr[i].cam = p["W"], p["H"], p["cam"]
+            arr[i].bgr1, arr[i].depth1_m = b1.ctypes.data, d1.ctypes.data
+            arr[i].bgr2, arr[i].depth2_m = b2.ctypes.data, d2.ctypes.data
+            arr[i].est_flow = est.ctypes.data if est is not None else None
+            arr[i].flow_out = outs[i].ctypes.data
+        rc = self.lib.rgbdflow_scene_flow_batch_submit(self.h, arr, len(pairs), ctypes.byref(params))
+        self._check(rc)
+        self._submitted = keep  # the staged / DMA'd inputs stay referenced until the next call
+        return outs
 
 
 class Server:

@@ -141,6 +141,40 @@ def test_batch_equals_solo(ctx):
         np.testing.assert_array_equal(a, b)
 
 
+def test_batch_submit_equals_batch(ctx):
+    """The submitted host-buffer batch (returns once enqueued; two contexts alternating) gives the
+    synchronous call's flows bit for bit, and refuses pageable outputs."""
+    import torch
+    pairs = []
+    for name, seed in (("320x240", 31), ("160x120", 32), ("320x240", 33)):
+        p = syn.make_config_pair(name, seed=seed)
+        pairs.append(dict(W=p["W"], H=p["H"], cam=cam_of(p), bgr1=p["bgr1"], depth1=p["depth1"], bgr2=p["bgr2"],
+                          depth2=p["depth2"]))
+    prm = rf.benchmark_params(320)
+    ref = ctx.scene_flow_batch(pairs, prm, stats=False)
+    other = rf.Context(0)
+    try:
+        outs = [[torch.empty((q["H"], q["W"], 3), dtype=torch.float32).pin_memory().numpy() for q in pairs]
+                for _ in range(2)]
+        ctxs = [ctx, other]
+        for s in range(4):  # two submits in flight, then each context reused after a synchronize
+            if s >= 2:
+                ctxs[s % 2].synchronize()
+                for a, b in zip(outs[s % 2], ref):
+                    np.testing.assert_array_equal(a, b)
+            ctxs[s % 2].scene_flow_batch_submit(pairs, prm, outs[s % 2])
+        for c in ctxs:
+            c.synchronize()
+        for o in outs:
+            for a, b in zip(o, ref):
+                np.testing.assert_array_equal(a, b)
+        with pytest.raises(rf.RgbdFlowError) as e:
+            other.scene_flow_batch_submit(pairs, prm, [np.zeros((q["H"], q["W"], 3), np.float32) for q in pairs])
+        assert e.value.code == -1  # RGBDFLOW_ERR_INVALID_ARG
+    finally:
+        other.close()
+
+
 @pytest.mark.parametrize("name,seg", [("320x240", 0), ("640x480", 0), ("640x480", 64), ("160x120", 32)])
 def test_strip_and_tile_sor_agree_bitwise(ctx, monkeypatch, name, seg):
     """The strip SOR (rows streamed through a shared-memory ring) and the tile SOR (32 x 32 tiles
