@@ -89,6 +89,7 @@ struct SolveConst {
     double outer_tol;
     int fixed;
     int n_sor;
+    int period;         // SOR convergence check period (iterations)
 };
 
 // One SOR launch of the host schedule.
@@ -104,6 +105,7 @@ struct SorLaunch {
     int prev_check_idx;
     int outer;         // outer iteration index (stats)
     int seq;           // index of this launch among the level's SOR launches (strip kernel tickets)
+    int xout;          // whole-level kernel: ping-pong buffer that receives x (non-final inner iterations)
 };
 
 // ------------------------------------------------------------------------------------------
@@ -1382,6 +1384,141 @@ k_sor_strip(const LevelItem<T, S>* items, const StripUnit* units, int n_units, i
         __syncthreads();  // the ring is refilled by the next unit
     }
 }
+
+// ------------------------------------------------------------------------------------------
+// Whole-level SOR for levels that fit one CTA's shared memory (the coarsest, e.g. 40 x 30): one
+// CTA per pair stages the level's system and increment once and runs every SOR iteration of the
+// inner iteration in one launch.  The convergence check (iteration it with it % period ==
+// period - 1, .cu:905-921) is a block reduction and the stop decision is taken in the kernel
+// with the tile kernels' rule, so the executed schedule and the result equal theirs: the same
+// pixel update (sor_point), whole-image red-black half-sweeps, the same statistic partial per
+// 32 x 32 tile summed in the same order.  Replaces the tile kernel's six latency-bound launches
+// per inner iteration at these levels.
+//
+// Shared layout: 15 planes of [H + 2 rows][2 colours][hwp + 2 positions] (checkerboard, one
+// zero row / position of padding on every side, so neighbours never need a bounds test).
+template <class T> __host__ __device__ constexpr size_t level_smem_bytes(int H, int hwp)
+{
+    return sizeof(T) * ((size_t)15 * (H + 2) * 2 * (hwp + 2) + 64);
+}
+
+template <class T, class S>
+__global__ void __launch_bounds__(512)
+k_sor_level(const LevelItem<T, S>* items, const int* which, SolveConst<T> k, SorLaunch L)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* const buf = reinterpret_cast<T*>(smem_raw);
+    __shared__ int s_stop;
+    const LevelItem<T, S>& it = items[which[blockIdx.x]];
+    PairCtl* ctl = it.ctl;
+    if (ctl->level_done) return;
+    const int W = it.W, H = it.H, hw = it.hwp, RP = hw + 2;
+    const int PLS = (H + 2) * 2 * RP;
+    T* const red = buf + 15 * PLS;
+    const int tid = threadIdx.x, NT = blockDim.x;
+    // stage: valid pixels from global, zero everywhere else (padding, positions past a row's count)
+    for (int e = tid; e < 15 * PLS; e += NT) {
+        const int z = e / PLS, rem = e % PLS, rr = rem / (2 * RP) - 1, c = (rem / RP) & 1, p = rem % RP - 1;
+        T v = 0;
+        if (rr >= 0 && rr < H && p >= 0 && p < ((W + 1 - (c ^ (rr & 1))) >> 1)) {
+            const size_t g = (size_t)rr * 2 * hw + c * hw + p;
+            if (z < 12) v = it.sys[z][g];
+            else if (!L.xin_zero) v = it.x[L.xin][z - 12][g];
+        }
+        buf[e] = v;
+    }
+    if (tid == 0) s_stop = 0;
+    __syncthreads();
+    int executed = k.n_sor;
+    for (int itn = 0; itn < k.n_sor; itn++) {
+        const bool chk = !k.fixed && (itn % k.period == k.period - 1);
+        T md = 0;
+        for (int color = 0; color < 2; color++) {
+            for (int q = tid; q < H * hw; q += NT) {
+                const int i = q / hw, m = q % hw;
+                const int b = color ^ (i & 1);
+                if (m >= ((W + 1 - b) >> 1)) continue;
+                const int own = ((i + 1) * 2 + color) * RP + m + 1;
+                const int oth = ((i + 1) * 2 + (color ^ 1)) * RP + m + 1;
+                const int ol = oth - 1 + b, orr = oth + b, ou = oth - 2 * RP, od = oth + 2 * RP;
+                T c[9], xl[3], xu[3], xr[3], xd[3], xp[3], nv[3];
+#pragma unroll
+                for (int z = 0; z < 9; z++) c[z] = buf[z * PLS + own];
+#pragma unroll
+                for (int v = 0; v < 3; v++) {
+                    const T* xv = buf + (12 + v) * PLS;
+                    xl[v] = xv[ol]; xr[v] = xv[orr]; xu[v] = xv[ou]; xd[v] = xv[od]; xp[v] = xv[own];
+                }
+                sor_point<T>(c, buf[9 * PLS + ol], buf[10 * PLS + ou], buf[9 * PLS + own], buf[10 * PLS + own],
+                             buf[11 * PLS + ol], buf[11 * PLS + ou], buf[11 * PLS + own], xl, xu, xr, xd, xp,
+                             k.omega, k.step, nv);
+#pragma unroll
+                for (int v = 0; v < 3; v++) buf[(12 + v) * PLS + own] = nv[v];
+                if (chk)
+                    for (int v = 0; v < 3; v++) md = maxT(md, absT(nv[v] - xp[v]));
+            }
+            __syncthreads();
+        }
+        if (chk) {
+            // the check: max |dx| of this iteration over the level (float bits, as the tile kernels)
+            float mm = (float)md;
+            for (int off = 16; off > 0; off >>= 1) mm = fmaxf(mm, __shfl_xor_sync(0xffffffffu, mm, off));
+            if ((tid & 31) == 0) red[tid >> 5] = (T)mm;
+            __syncthreads();
+            if (tid == 0) {
+                float g = 0;
+                for (int w = 0; w < NT / 32; w++) g = fmaxf(g, (float)red[w]);
+                const int ci = min(itn / k.period, kMaxChecks - 1);
+                if (g > 0) ctl->maxdiff[ci] = __float_as_uint(g);
+                if ((double)g < k.sor_tol || (T)g >= k.step) {
+                    s_stop = 1;
+                    ctl->sor_stop = 1;
+                    ctl->sor_stop_iter = itn + 1;
+                }
+            }
+            __syncthreads();
+            if (s_stop) { executed = itn + 1; break; }
+        }
+    }
+    (void)executed;
+    // out: the fold u += x with the statistic partial per 32 x 32 tile (the tile kernels' order),
+    // or x into the ping-pong buffer the next inner iteration reads
+    const int sx = (W + kSorTW - 1) / kSorTW, sy = (H + kSorTH - 1) / kSorTH;
+    if (L.final_fold) {
+        const int pitch = it.pitch;
+        const T fl = it.f_level;
+        for (int ti = 0; ti < sx * sy; ti++) {
+            const int ix0 = (ti % sx) * kSorTW, iy0 = (ti / sx) * kSorTH;
+            T part = 0;
+            for (int q = tid; q < kSorTW * kSorTH; q += NT) {
+                const int gi = iy0 + q / kSorTW, gj = ix0 + q % kSorTW;
+                if (gi >= H || gj >= W) continue;
+                const int o = ((gi + 1) * 2 + ((gi + gj) & 1)) * RP + (gj >> 1) + 1;
+                const T a = buf[12 * PLS + o], bq = buf[13 * PLS + o], cz = buf[14 * PLS + o];
+                const size_t lp = (size_t)gi * pitch + gj;
+                it.u[0][lp] = addR(it.u[0][lp], a); it.u[1][lp] = addR(it.u[1][lp], bq); it.u[2][lp] = addR(it.u[2][lp], cz);
+                part = addR(part, stat_px<T>(a, bq, cz, fl, it.pyr[6][(size_t)gi * W + gj]));
+            }
+            for (int off = 16; off > 0; off >>= 1) part += __shfl_down_sync(0xffffffffu, part, off);
+            if ((tid & 31) == 0) red[tid >> 5] = part;
+            __syncthreads();
+            if (tid == 0) {
+                T tot = 0;
+                for (int w = 0; w < NT / 32; w++) tot += red[w];
+                it.stat_part[ti] = tot;
+            }
+            __syncthreads();
+        }
+    } else {
+        for (int q = tid; q < H * W; q += NT) {
+            const int gi = q / W, gj = q % W;
+            const int o = ((gi + 1) * 2 + ((gi + gj) & 1)) * RP + (gj >> 1) + 1;
+            const int lc = cs_idx(gi, gj, hw);
+            for (int v = 0; v < 3; v++) it.x[L.xout][v][lc] = buf[(12 + v) * PLS + o];
+        }
+    }
+}
+
 
 // After each outer iteration: the early-termination statistic of the pair (mean over 3N of
 // sqr(du) * (1, 1, f / depth1), .cu:943-951), the stop decision and the executed-schedule record.

@@ -135,6 +135,7 @@ struct HostParams {
     int sor_strip;          // strip SOR for large FP32 levels (0: tiles everywhere)
     int strip_min_w, strip_min_h, strip_seg;  // strip eligibility and band height (0: automatic)
     long strip_min_px;                        // strips only for steps with this many eligible pixels
+    int sor_level;                            // whole-level SOR for levels that fit one CTA (0: off)
 };
 
 // Row pitch of the u planes, and the checkerboard half-row length of the x / sys planes (16-byte
@@ -216,6 +217,16 @@ static std::vector<StripUnit> strip_units(const std::vector<X>& items, const std
     return v;
 }
 
+// Whether an item's level runs on the whole-level SOR: the level's 15 planes fit one CTA's shared
+// memory (the coarsest levels, e.g. 40 x 30).
+constexpr size_t kLevelSmemMax = 200 * 1024;
+template <class T>
+static inline bool use_level(const HostParams& hp, int W, int H, int hwp)
+{
+    (void)W;
+    return hp.sor_level && level_smem_bytes<T>(H, hwp) <= kLevelSmemMax;
+}
+
 // Bump allocator over a byte range.
 struct Bump {
     size_t off = 0;
@@ -252,6 +263,8 @@ struct Plan {
         size_t sor_tiles_off; int n_sor;      // tile SOR work list (items not on the strip kernel)
         size_t strip_units_off; int n_units;  // strip SOR work list
         int strip_grid;
+        size_t level_items_off; int n_level;  // whole-level SOR: items (one CTA each)
+        size_t level_smem;
     };
     std::vector<StepDesc> steps;
     struct PyrLevelDesc { size_t jobs_off; int n_jobs; size_t src_tiles_off; int n_src; size_t dst_tiles_off; int n_dst; size_t g_off; };
@@ -523,7 +536,8 @@ static Plan<T, S> make_plan(const std::vector<PairSpec>& pairs, const HostParams
                 for (int x = 0; x < it.lin_tiles_x; x++) lt.push_back(Tile{iid, x, y, y * it.lin_tiles_x + x});
             items.push_back(it);
         }
-        std::vector<int> strip_items;
+        std::vector<int> strip_items, level_items;
+        size_t level_smem = 0;
         long strip_px = 0;
         for (const auto& x : items)
             if (use_strip<T>(hp, x.W, x.H)) strip_px += (long)x.W * x.H;
@@ -531,6 +545,11 @@ static Plan<T, S> make_plan(const std::vector<PairSpec>& pairs, const HostParams
         for (auto& x : items) {
             const int sx = (x.W + kSorTW - 1) / kSorTW, sy = (x.H + kSorTH - 1) / kSorTH;
             x.n_sor_tiles = sx * sy;
+            if (use_level<T>(hp, x.W, x.H, x.hwp)) {
+                level_items.push_back((int)(&x - items.data()));
+                level_smem = std::max(level_smem, level_smem_bytes<T>(x.H, x.hwp));
+                continue;
+            }
             if (strips && use_strip<T>(hp, x.W, x.H)) {
                 strip_items.push_back((int)(&x - items.data()));
                 continue;
@@ -547,6 +566,8 @@ static Plan<T, S> make_plan(const std::vector<PairSpec>& pairs, const HostParams
         d.sor_tiles_off = P.put(stt); d.n_sor = (int)stt.size();
         d.strip_units_off = P.put(units); d.n_units = (int)units.size();
         d.strip_grid = std::min(P.sms, d.n_units);
+        d.level_items_off = P.put(level_items); d.n_level = (int)level_items.size();
+        d.level_smem = level_smem;
         P.steps.push_back(d);
     }
     // output pointers (one per pair, in the order of the finest step's items = pair order)
@@ -656,7 +677,7 @@ static SolveConst<T> solve_const(const HostParams& hp)
     k.omega = (T)hp.omega; k.step = (T)hp.step;
     k.occ_margin = (T)hp.occ_margin; k.occ_penalty = (T)hp.occ_penalty; k.max_grad = (T)hp.max_grad;
     k.sor_tol = hp.sor_tol; k.outer_tol = hp.outer_tol;
-    k.fixed = hp.fixed; k.n_sor = hp.n_sor;
+    k.fixed = hp.fixed; k.n_sor = hp.n_sor; k.period = hp.period;
     return k;
 }
 
@@ -795,6 +816,7 @@ static void set_kernel_attrs()
     if constexpr (sizeof(T) == 4)
         RF_CUDA(cudaFuncSetAttribute(k_sor_strip<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)strip_smem_bytes<T>()));
+    RF_CUDA(cudaFuncSetAttribute(k_sor_level<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLevelSmemMax));
 }
 
 // Whether configuration c fits shared memory for type T.
@@ -823,6 +845,7 @@ static int enqueue_level(const Plan<T, S>& P, char* base, int sidx, cudaStream_t
     const Tile* lt = (const Tile*)(base + P.desc_off + d.lin_tiles_off);
     const Tile* stt = (const Tile*)(base + P.desc_off + d.sor_tiles_off);
     const StripUnit* units = (const StripUnit*)(base + P.desc_off + d.strip_units_off);
+    const int* level_items = (const int*)(base + P.desc_off + d.level_items_off);
     int* ticket = (int*)(base + P.ctr_off) + sidx;
     int seq = 0;
     const SolveConst<T> k = solve_const<T>(P.hp);
@@ -842,9 +865,23 @@ static int enqueue_level(const Plan<T, S>& P, char* base, int sidx, cudaStream_t
             RF_PROF_E(pf, st);
             launches++;
             const int lvl = P.Lmax - 1 - sidx;
+            if (d.n_level) {
+                // the whole-level items: every SOR iteration of this inner iteration in one launch
+                SorLaunch L{};
+                L.it0 = 0; L.nit = P.hp.n_sor; L.outer = outer;
+                L.xin = sched.front().xin;
+                L.xin_zero = (hh == 0);
+                L.final_fold = (hh == P.hp.n_inner - 1);
+                L.xout = L.final_fold ? 0 : P.sor_sched[sidx][hh + 1].front().xin;
+                RF_PROF_B(pf, KC_SOR_LEVEL0 + lvl, st);
+                k_sor_level<T, S><<<d.n_level, 512, d.level_smem, st>>>(items, level_items, k, L);
+                RF_PROF_E(pf, st);
+                launches++;
+            }
             for (SorLaunch L : sched) {
                 L.outer = outer;
                 L.seq = seq++;
+                if (!d.n_sor && !d.n_units) continue;
                 RF_PROF_B(pf, KC_SOR_LEVEL0 + lvl, st);
                 if (d.n_sor) {
                     launch_sor<T, S>(P.sor_cfg[sidx], items, stt, d.n_sor, P.sms, k, L, st);

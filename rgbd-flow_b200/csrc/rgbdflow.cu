@@ -138,6 +138,8 @@ HostParams host_params(const rgbdflow_params& p)
     h.strip_seg = e ? std::atoi(e) : 0;
     e = std::getenv("RGBDFLOW_STRIP_MIN_PX");
     h.strip_min_px = e ? std::atol(e) : 0;
+    e = std::getenv("RGBDFLOW_SOR_LEVEL");
+    h.sor_level = e ? std::atoi(e) : 1;
     h.fill_rounds = 64;
     return h;
 }
@@ -182,8 +184,8 @@ std::string plan_key(const std::vector<PairSpec>& ps, const HostParams& hp, int 
                   hp.n_sor, hp.max_dist, hp.fill_holes, hp.fixed, hp.omega, hp.step, hp.eps_d, hp.eps_z, hp.eps_s,
                   hp.sor_tol, hp.outer_tol, hp.occ_margin, hp.occ_penalty, hp.max_grad, hp.period, hp.K * 100 + hp.sor_ilp * 10 + hp.sor_nbuf, hp.fill_rounds);
     k += buf;
-    std::snprintf(buf, sizeof buf, " strip %d %d %d %d %ld", hp.sor_strip, hp.strip_min_w, hp.strip_min_h, hp.strip_seg,
-                  hp.strip_min_px);
+    std::snprintf(buf, sizeof buf, " strip %d %d %d %d %ld level %d", hp.sor_strip, hp.strip_min_w, hp.strip_min_h,
+                  hp.strip_seg, hp.strip_min_px, hp.sor_level);
     return k + buf;
 }
 
@@ -197,7 +199,8 @@ std::string topo_key(const Plan<T, S>& P, const HostParams& hp, int tag, bool de
                     "p" + std::to_string(P.pyr.size()) + "w" + std::to_string((int)P.any_warm) + "s";
     for (size_t i = 0; i < P.steps.size(); i++)
         k += std::to_string(P.steps[i].n_items > 0) + std::to_string(P.sor_cfg[i].K) + std::to_string(P.sor_cfg[i].nbuf) +
-             std::to_string(P.sor_cfg[i].ilp) + (P.steps[i].n_sor > 0 ? "t" : "") + (P.steps[i].n_units > 0 ? "s" : "") + ".";
+             std::to_string(P.sor_cfg[i].ilp) + (P.steps[i].n_sor > 0 ? "t" : "") + (P.steps[i].n_units > 0 ? "s" : "") +
+             (P.steps[i].n_level > 0 ? "l" : "") + ".";
     const std::vector<PairSpec> none;
     return k + plan_key(none, hp, tag);
 }

@@ -196,6 +196,23 @@ def test_strip_and_tile_sor_agree_bitwise(ctx, monkeypatch, name, seg):
     np.testing.assert_array_equal(tile, strip)
 
 
+@pytest.mark.parametrize("name,n_inner", [("640x480", 1), ("160x120", 1), ("320x240", 2)])
+def test_whole_level_sor_agrees_bitwise(ctx, monkeypatch, name, n_inner):
+    """The whole-level SOR (one CTA runs all iterations of a level that fits its shared memory)
+    and the tile SOR give the same flow and executed schedule, bit for bit, also with two inner
+    iterations (the increment handed on between them)."""
+    p = syn.make_config_pair(name, seed=13)
+    prm = rf.benchmark_params(p["W"])
+    prm.n_inner = n_inner
+    args = (cam_of(p), p["bgr1"], p["depth1"], p["bgr2"], p["depth2"], prm)
+    monkeypatch.setenv("RGBDFLOW_SOR_LEVEL", "0")
+    tile, st_tile = ctx.scene_flow_two_frames(*args)
+    monkeypatch.setenv("RGBDFLOW_SOR_LEVEL", "1")
+    whole, st_whole = ctx.scene_flow_two_frames(*args)
+    assert st_tile.summary() == st_whole.summary()
+    np.testing.assert_array_equal(tile, whole)
+
+
 def test_single_scale_seam_matches_oracle(ctx):
     rng = np.random.default_rng(5)
     W, H = 72, 50
