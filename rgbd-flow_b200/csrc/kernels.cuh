@@ -391,8 +391,10 @@ struct PyrJob {
     const T* src[10];
     T* tmp[10];
     T* dst[10];
-    int tiles_x_src, tile0_src;  // tiles over the source (horizontal pass)
+    int tiles_x_src, tile0_src;  // tiles over the computed source columns (horizontal pass)
     int tiles_x_dst, tile0_dst;  // tiles over the destination
+    int hstep, hoff;             // horizontal pass computes columns hoff + hstep * k only: the ones the
+                                 // resample reads with a nonzero weight (every other one at ratio 0.5)
 };
 
 constexpr int kMaxTaps = 33;
@@ -402,7 +404,7 @@ __global__ void k_hfilter(const PyrJob<T>* jobs, const Tile* tiles, const T* __r
 {
     const Tile t = tiles[blockIdx.x];
     const PyrJob<T>& jb = jobs[t.item];
-    const int j = t.tx * LTW + (threadIdx.x % LTW), i = t.ty * LTH + (threadIdx.x / LTW);
+    const int j = jb.hoff + jb.hstep * (t.tx * LTW + (threadIdx.x % LTW)), i = t.ty * LTH + (threadIdx.x / LTW);
     if (i >= jb.sH || j >= jb.sW) return;
     const T* g = gall + t.item * kMaxTaps;
     const int fs = jb.fs, W = jb.sW;
@@ -439,13 +441,15 @@ __global__ void k_vresize(const PyrJob<T>* jobs, const Tile* tiles, const T* __r
     const int v0 = clampi(yy, 0, jb.sH - 1), v1 = clampi(yy + 1, 0, jb.sH - 1);
     const T s00 = (T)(fabs(1 - dx) * fabs(1 - dy)), s01 = (T)(fabs(1 - dx) * fabs(dy));
     const T s10 = (T)(fabs(dx) * fabs(1 - dy)), s11 = (T)(fabs(dx) * fabs(dy));
+    // a corner of weight 0 adds exactly 0 (every pyramid value is finite): it is skipped, which at
+    // ratio 0.5 (samples on source pixels) leaves one corner of four
     for (int p = 0; p < jb.nplanes; p++) {
         const T* tp = jb.tmp[p];
         T acc = 0;
         acc += vtap(tp, jb.sW, jb.sH, u0, v0, g, jb.fs) * s00;
-        acc += vtap(tp, jb.sW, jb.sH, u0, v1, g, jb.fs) * s01;
-        acc += vtap(tp, jb.sW, jb.sH, u1, v0, g, jb.fs) * s10;
-        acc += vtap(tp, jb.sW, jb.sH, u1, v1, g, jb.fs) * s11;
+        if (s01 != (T)0) acc += vtap(tp, jb.sW, jb.sH, u0, v1, g, jb.fs) * s01;
+        if (s10 != (T)0) acc += vtap(tp, jb.sW, jb.sH, u1, v0, g, jb.fs) * s10;
+        if (s11 != (T)0) acc += vtap(tp, jb.sW, jb.sH, u1, v1, g, jb.fs) * s11;
         jb.dst[p][(size_t)i * jb.dW + j] = acc;
     }
 }
@@ -1401,9 +1405,13 @@ template <class T> __host__ __device__ constexpr size_t level_smem_bytes(int H, 
 {
     return sizeof(T) * ((size_t)15 * (H + 2) * 2 * (hwp + 2) + 64);
 }
+__host__ __device__ constexpr int level_threads(int H, int hwp)
+{
+    return (H * hwp + 31) / 32 * 32 > 1024 ? 1024 : ((H * hwp + 31) / 32 * 32 < 64 ? 64 : (H * hwp + 31) / 32 * 32);
+}
 
 template <class T, class S>
-__global__ void __launch_bounds__(512)
+__global__ void __launch_bounds__(1024)
 k_sor_level(const LevelItem<T, S>* items, const int* which, SolveConst<T> k, SorLaunch L)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1430,12 +1438,16 @@ k_sor_level(const LevelItem<T, S>* items, const int* which, SolveConst<T> k, Sor
     if (tid == 0) s_stop = 0;
     __syncthreads();
     int executed = k.n_sor;
+    // the block is launched with about one thread per position (H x hwp); a thread's positions and
+    // their rows are fixed across the half-sweeps
+    const int q0 = tid, q1 = tid + NT;
+    const int i0 = q0 / hw, m0 = q0 % hw, i1 = q1 / hw, m1 = q1 % hw;
     for (int itn = 0; itn < k.n_sor; itn++) {
         const bool chk = !k.fixed && (itn % k.period == k.period - 1);
         T md = 0;
         for (int color = 0; color < 2; color++) {
-            for (int q = tid; q < H * hw; q += NT) {
-                const int i = q / hw, m = q % hw;
+            for (int r = 0, q = q0; q < H * hw; r++, q += NT) {
+                const int i = r == 0 ? i0 : (r == 1 ? i1 : q / hw), m = r == 0 ? m0 : (r == 1 ? m1 : q % hw);
                 const int b = color ^ (i & 1);
                 if (m >= ((W + 1 - b) >> 1)) continue;
                 const int own = ((i + 1) * 2 + color) * RP + m + 1;
@@ -1487,24 +1499,31 @@ k_sor_level(const LevelItem<T, S>* items, const int* which, SolveConst<T> k, Sor
     if (L.final_fold) {
         const int pitch = it.pitch;
         const T fl = it.f_level;
+        // the partials are summed exactly as a 512-thread tile CTA sums them: "virtual thread" vt
+        // (0..511) takes pixels vt and vt + 512 of the tile, a warp tree per virtual warp, then
+        // the 16 virtual warps in order; a real warp takes virtual warps w, w + NT / 32, ...
+        const int lane = tid & 31;
         for (int ti = 0; ti < sx * sy; ti++) {
             const int ix0 = (ti % sx) * kSorTW, iy0 = (ti / sx) * kSorTH;
-            T part = 0;
-            for (int q = tid; q < kSorTW * kSorTH; q += NT) {
-                const int gi = iy0 + q / kSorTW, gj = ix0 + q % kSorTW;
-                if (gi >= H || gj >= W) continue;
-                const int o = ((gi + 1) * 2 + ((gi + gj) & 1)) * RP + (gj >> 1) + 1;
-                const T a = buf[12 * PLS + o], bq = buf[13 * PLS + o], cz = buf[14 * PLS + o];
-                const size_t lp = (size_t)gi * pitch + gj;
-                it.u[0][lp] = addR(it.u[0][lp], a); it.u[1][lp] = addR(it.u[1][lp], bq); it.u[2][lp] = addR(it.u[2][lp], cz);
-                part = addR(part, stat_px<T>(a, bq, cz, fl, it.pyr[6][(size_t)gi * W + gj]));
+            for (int vw = tid >> 5; vw < 16; vw += NT >> 5) {
+                T part = 0;
+                for (int q = vw * 32 + lane; q < kSorTW * kSorTH; q += 512) {
+                    const int gi = iy0 + q / kSorTW, gj = ix0 + q % kSorTW;
+                    if (gi >= H || gj >= W) continue;
+                    const int o = ((gi + 1) * 2 + ((gi + gj) & 1)) * RP + (gj >> 1) + 1;
+                    const T a = buf[12 * PLS + o], bq = buf[13 * PLS + o], cz = buf[14 * PLS + o];
+                    const size_t lp = (size_t)gi * pitch + gj;
+                    it.u[0][lp] = addR(it.u[0][lp], a); it.u[1][lp] = addR(it.u[1][lp], bq);
+                    it.u[2][lp] = addR(it.u[2][lp], cz);
+                    part = addR(part, stat_px<T>(a, bq, cz, fl, it.pyr[6][(size_t)gi * W + gj]));
+                }
+                for (int off = 16; off > 0; off >>= 1) part += __shfl_down_sync(0xffffffffu, part, off);
+                if (lane == 0) red[vw] = part;
             }
-            for (int off = 16; off > 0; off >>= 1) part += __shfl_down_sync(0xffffffffu, part, off);
-            if ((tid & 31) == 0) red[tid >> 5] = part;
             __syncthreads();
             if (tid == 0) {
                 T tot = 0;
-                for (int w = 0; w < NT / 32; w++) tot += red[w];
+                for (int w = 0; w < 16; w++) tot += red[w];
                 it.stat_part[ti] = tot;
             }
             __syncthreads();

@@ -265,6 +265,7 @@ struct Plan {
         int strip_grid;
         size_t level_items_off; int n_level;  // whole-level SOR: items (one CTA each)
         size_t level_smem;
+        int level_threads;
     };
     std::vector<StepDesc> steps;
     struct PyrLevelDesc { size_t jobs_off; int n_jobs; size_t src_tiles_off; int n_src; size_t dst_tiles_off; int n_dst; size_t g_off; };
@@ -466,7 +467,18 @@ static Plan<T, S> make_plan(const std::vector<PairSpec>& pairs, const HostParams
                 jb.dst[c] = (T*)mem[p][i].pyr[c];
             }
             const int jid = (int)jobs.size();
-            jb.tiles_x_src = (jb.sW + LTW - 1) / LTW;
+            // columns the resample reads with a nonzero weight: at rate 0.5 the samples fall on
+            // source pixels x = 2j + 1 (weight 1 on column 2j + 1, 0 on its neighbour)
+            bool odd_only = true;
+            for (int jj = 0; jj < jb.dW && odd_only; jj++) {
+                const double x = (double)(jj + 1) / jb.rate - 1;
+                const int xx = (int)x;
+                odd_only = (x == (double)xx) && (xx & 1) && xx < jb.sW;
+            }
+            jb.hstep = odd_only ? 2 : 1;
+            jb.hoff = odd_only ? 1 : 0;
+            const int hcols = odd_only ? jb.sW / 2 : jb.sW;
+            jb.tiles_x_src = (hcols + LTW - 1) / LTW;
             jb.tile0_src = (int)st.size();
             for (int y = 0; y < (jb.sH + LTH - 1) / LTH; y++)
                 for (int x = 0; x < jb.tiles_x_src; x++) st.push_back(Tile{jid, x, y, 0});
@@ -538,6 +550,7 @@ static Plan<T, S> make_plan(const std::vector<PairSpec>& pairs, const HostParams
         }
         std::vector<int> strip_items, level_items;
         size_t level_smem = 0;
+        int level_thr = 64;
         long strip_px = 0;
         for (const auto& x : items)
             if (use_strip<T>(hp, x.W, x.H)) strip_px += (long)x.W * x.H;
@@ -548,6 +561,7 @@ static Plan<T, S> make_plan(const std::vector<PairSpec>& pairs, const HostParams
             if (use_level<T>(hp, x.W, x.H, x.hwp)) {
                 level_items.push_back((int)(&x - items.data()));
                 level_smem = std::max(level_smem, level_smem_bytes<T>(x.H, x.hwp));
+                level_thr = std::max(level_thr, level_threads(x.H, x.hwp));
                 continue;
             }
             if (strips && use_strip<T>(hp, x.W, x.H)) {
@@ -568,6 +582,7 @@ static Plan<T, S> make_plan(const std::vector<PairSpec>& pairs, const HostParams
         d.strip_grid = std::min(P.sms, d.n_units);
         d.level_items_off = P.put(level_items); d.n_level = (int)level_items.size();
         d.level_smem = level_smem;
+        d.level_threads = level_thr;
         P.steps.push_back(d);
     }
     // output pointers (one per pair, in the order of the finest step's items = pair order)
@@ -874,7 +889,7 @@ static int enqueue_level(const Plan<T, S>& P, char* base, int sidx, cudaStream_t
                 L.final_fold = (hh == P.hp.n_inner - 1);
                 L.xout = L.final_fold ? 0 : P.sor_sched[sidx][hh + 1].front().xin;
                 RF_PROF_B(pf, KC_SOR_LEVEL0 + lvl, st);
-                k_sor_level<T, S><<<d.n_level, 512, d.level_smem, st>>>(items, level_items, k, L);
+                k_sor_level<T, S><<<d.n_level, d.level_threads, d.level_smem, st>>>(items, level_items, k, L);
                 RF_PROF_E(pf, st);
                 launches++;
             }
