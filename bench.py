@@ -152,7 +152,9 @@ def run_served(ctx, rf, serving, streams, prm, args, warm):
                     warm_start=warm, warm_early_termination=warm)
     # warm-up: the slots' graphs for the batch mixes that recur (about a second of traffic)
     serving.simulate(srv, rf, streams, n_frames=4 * args.serve_unique, fps=30.0, seed=1)
+    srv.counters(reset=True)
     r = serving.simulate(srv, rf, streams, n_frames=args.serve_frames, fps=30.0, seed=2, keep_stream=0, keep_n=7)
+    counters = srv.counters()
     lat = np.array(r["latencies_ms"])
     sat = serving.simulate(srv, rf, streams, n_frames=args.serve_unique * 3, fps=30.0, seed=3, time_scale=0.0)
     srv.close()
@@ -176,7 +178,10 @@ def run_served(ctx, rf, serving, streams, prm, args, warm):
             "max_ms": float(lat.max()),
             "saturated_pairs_per_s": sat["pairs"] / sat["wall_s"],
             "epe_vs_plain_mm": 1e3 * float(np.mean(epes)) if epes else None,
-            "hbm_budget_gb": 20}
+            "hbm_budget_gb": 20,
+            # what the timed run spent on the host outside the solve: server counters (allocations,
+            # graph captures, longest calls) and the request loop's longest iteration and calls
+            "host": {"server": counters, "loop_ms": r["host"]}}
 
 
 MIX = [(160, 120, 24), (320, 240, 24), (640, 480, 16)]

@@ -310,6 +310,22 @@ int rgbdflow_server_step(rgbdflow_server* srv, int wait, rgbdflow_result* out, i
 /* Requests queued or in flight. */
 int rgbdflow_server_pending(const rgbdflow_server* srv);
 
+/* Where a served request's latency can go besides the device solve.  Counts and maxima since the
+ * server was created or last read with reset = 1.  The server captures the graphs of the batches
+ * its registered streams can form when a stream registers (up to 40 per solve slot), so in the
+ * steady state graphs_built, arena_grows and frames_allocated stay 0. */
+typedef struct rgbdflow_server_counters {
+    uint64_t frames_allocated;  /* frame buffer sets allocated after the streams' stock ran out */
+    uint64_t graphs_built;      /* solve graphs captured (first sight of a batch composition) */
+    uint64_t arena_grows;       /* slot solve-memory reallocations (each waits for the device) */
+    uint64_t launches;          /* device steps launched */
+    double   max_submit_ms;     /* longest host time inside one submit call */
+    double   max_launch_ms;     /* longest host time to admit and enqueue one device step */
+    double   max_retire_ms;     /* longest host time to hand one finished step's flows back */
+    double   max_graph_build_ms; /* longest capture + instantiation of one solve graph */
+} rgbdflow_server_counters;
+int rgbdflow_server_counters_read(rgbdflow_server* srv, int reset, rgbdflow_server_counters* out);
+
 /* ---------------------------------------------------------------------------------------------
  * Allocation-free solve (no counterpart in the reference).  For callers that must not allocate
  * once they run: a real-time loop with a fixed memory footprint, a process whose device memory

@@ -40,6 +40,8 @@ struct rgbdflow_ctx {
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     std::map<std::string, GraphEntry> graphs;  // by exact batch (sizes, cameras, parameters)
     uint64_t graph_clock = 0;
+    uint64_t n_graph_builds = 0, n_arena_grows = 0;  // captures and arena reallocations, for counters
+    double max_build_ms = 0;                            // longest capture + instantiation, for counters
     bool attrs[4] = {false, false, false, false};
     int last_launches = 0;
     int sms = 148;
@@ -97,6 +99,7 @@ void ensure_arena(rgbdflow_ctx* c, size_t need)
     const size_t cap = align_up(std::max(need + need / 8, 2 * c->arena_cap), 1 << 20);
     const size_t want = (c->budget && cap > c->budget) ? need : cap;
     RF_CUDA(cudaMalloc(&c->arena, want));
+    c->n_arena_grows++;
     c->arena_cap = want;
 }
 
@@ -174,10 +177,11 @@ void resized_cam(const rgbdflow_camera_params& c, int W, float& f, unsigned& xre
 std::string plan_key(const std::vector<PairSpec>& ps, const HostParams& hp, int tag)
 {
     std::string k = std::to_string(tag) + ":";
+    // cameras are left out: they reach the kernels only through the item descriptors, which every
+    // call uploads, so batches that differ only in their cameras share one graph
     for (const auto& p : ps)
         k += std::to_string(p.kind) + "k" + std::to_string(p.W) + "x" + std::to_string(p.H) + (p.warm() ? (p.warm_early ? "E" : "e") : "") +
-             (p.kind == 2 ? "a" + std::to_string(p.allow_early) + "g" + std::to_string(p.f_level) : std::string()) + "f" + std::to_string(p.f_full) +
-             "r" + std::to_string(p.xres_full) + ",";
+             (p.kind == 2 ? "a" + std::to_string(p.allow_early) : std::string()) + ",";
     char buf[512];
     std::snprintf(buf, sizeof buf, "|%d %.17g %.17g %.17g %.17g %.17g %d %d %d %d %d %d %d %.17g %.17g %.17g %.17g %.17g %.17g %.17g %.17g %.17g %.17g %d %d %d",
                   hp.regularization, hp.color_w, hp.dvc, hp.alpha, hp.gamma, hp.ratio, hp.min_width, hp.n_outer, hp.n_inner,
@@ -229,6 +233,73 @@ void ensure_attrs(rgbdflow_ctx* c, int slot)
     if (c->attrs[slot]) return;
     set_kernel_attrs<T, S>();
     c->attrs[slot] = true;
+}
+
+// Key of a batch's executable graph: the exact batch (sizes, kinds, warm starts, parameters), the
+// storage slot and the input form.
+std::string graph_key(const std::vector<PairSpec>& pairs, const HostParams& hp, int slot, bool dev)
+{
+    return plan_key(pairs, hp, slot) + (dev ? "|dev" : "");
+}
+
+// The executable graph of plan P (bound to the context's arena) for `pairs`: from the cache, or
+// captured on the context's stream now, without running it.  One executable graph per exact
+// batch, least recently used evicted beyond kGraphCache: recurring batch mixes (a server's)
+// launch without any capture.  When the cache is full a new batch is written into an evicted
+// executable of the same launch topology (cudaGraphExecUpdate: new grids and arguments, no
+// re-instantiation) where one exists.
+template <class T, class S>
+GraphEntry& graph_for(rgbdflow_ctx* c, const Plan<T, S>& P, const std::vector<PairSpec>& pairs, const HostParams& hp,
+                      int slot, bool dev)
+{
+    const std::string exact = graph_key(pairs, hp, slot, dev);
+    auto it = c->graphs.find(exact);
+    if (it == c->graphs.end()) {
+        MaxTimer timer(&c->max_build_ms);
+        const std::string topo = topo_key(P, hp, slot, dev);
+        cudaGraph_t graph = nullptr;
+        RF_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        int launches = 0;
+        try {
+            launches = enqueue_solve(P, c->arena, c->stream);
+        } catch (...) {
+            cudaGraph_t tmp = nullptr;
+            cudaStreamEndCapture(c->stream, &tmp);
+            if (tmp) cudaGraphDestroy(tmp);
+            throw;
+        }
+        RF_CUDA(cudaStreamEndCapture(c->stream, &graph));
+        c->n_graph_builds++;
+        GraphEntry g;
+        g.graph = graph;
+        g.topo = topo;
+        g.launches = launches;
+        bool updated = false;
+        if (c->graphs.size() >= kGraphCache) {
+            // the victim: the least recently used executable of this topology, else of any
+            auto victim = c->graphs.end();
+            for (auto j = c->graphs.begin(); j != c->graphs.end(); ++j) {
+                const bool same = j->second.topo == topo;
+                if (victim == c->graphs.end() || (same && victim->second.topo != topo) ||
+                    (same == (victim->second.topo == topo) && j->second.last_use < victim->second.last_use))
+                    victim = j;
+            }
+            GraphEntry old = victim->second;
+            c->graphs.erase(victim);
+            cudaGraphExecUpdateResultInfo info;
+            if (old.topo == topo && cudaGraphExecUpdate(old.exec, graph, &info) == cudaSuccess) {
+                g.exec = old.exec;
+                updated = true;
+            } else {
+                cudaGetLastError();
+                cudaGraphExecDestroy(old.exec);
+            }
+            cudaGraphDestroy(old.graph);
+        }
+        if (!updated) RF_CUDA(cudaGraphInstantiate(&g.exec, g.graph, 0));
+        it = c->graphs.emplace(exact, g).first;
+    }
+    return it->second;
 }
 
 // Runs a batch through one graph launch.
@@ -303,59 +374,10 @@ void run_batch(rgbdflow_ctx* c, const std::vector<PairSpec>& pairs, const HostPa
     RF_CUDA(cudaEventRecord(c->e0, st));
     const bool graphs = c->use_graphs && !c->prof;
     if (graphs) {
-        // One executable graph per exact batch (sizes, cameras, parameters), least recently used
-        // evicted beyond kGraphCache: recurring batch mixes (a server's) launch without any
-        // capture.  A new batch is captured once; when the cache is full it is written into an
-        // evicted executable of the same launch topology (cudaGraphExecUpdate: new grids and
-        // arguments, no re-instantiation) where one exists.
-        const std::string exact = plan_key(pairs, hp, slot) + (dev ? "|dev" : "");
-        auto it = c->graphs.find(exact);
-        if (it == c->graphs.end()) {
-            const std::string topo = topo_key(P, hp, slot, dev);
-            cudaGraph_t graph = nullptr;
-            RF_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-            int launches = 0;
-            try {
-                launches = enqueue_solve(P, c->arena, c->stream);
-            } catch (...) {
-                cudaGraph_t tmp = nullptr;
-                cudaStreamEndCapture(c->stream, &tmp);
-                if (tmp) cudaGraphDestroy(tmp);
-                throw;
-            }
-            RF_CUDA(cudaStreamEndCapture(c->stream, &graph));
-            GraphEntry g;
-            g.graph = graph;
-            g.topo = topo;
-            g.launches = launches;
-            bool updated = false;
-            if (c->graphs.size() >= kGraphCache) {
-                // the victim: the least recently used executable of this topology, else of any
-                auto victim = c->graphs.end();
-                for (auto j = c->graphs.begin(); j != c->graphs.end(); ++j) {
-                    const bool same = j->second.topo == topo;
-                    if (victim == c->graphs.end() || (same && victim->second.topo != topo) ||
-                        (same == (victim->second.topo == topo) && j->second.last_use < victim->second.last_use))
-                        victim = j;
-                }
-                GraphEntry old = victim->second;
-                c->graphs.erase(victim);
-                cudaGraphExecUpdateResultInfo info;
-                if (old.topo == topo && cudaGraphExecUpdate(old.exec, graph, &info) == cudaSuccess) {
-                    g.exec = old.exec;
-                    updated = true;
-                } else {
-                    cudaGetLastError();
-                    cudaGraphExecDestroy(old.exec);
-                }
-                cudaGraphDestroy(old.graph);
-            }
-            if (!updated) RF_CUDA(cudaGraphInstantiate(&g.exec, g.graph, 0));
-            it = c->graphs.emplace(exact, g).first;
-        }
-        it->second.last_use = ++c->graph_clock;
-        RF_CUDA(cudaGraphLaunch(it->second.exec, st));
-        c->last_launches = it->second.launches;
+        GraphEntry& g = graph_for(c, P, pairs, hp, slot, dev);
+        g.last_use = ++c->graph_clock;
+        RF_CUDA(cudaGraphLaunch(g.exec, st));
+        c->last_launches = g.launches;
     } else {
         c->last_launches = enqueue_solve(P, c->arena, st, c->prof.get());
     }
@@ -436,6 +458,32 @@ static void dispatch(rgbdflow_ctx* c, const std::vector<PairSpec>& ps, const rgb
     } else if (p.storage == RGBDFLOW_STORE_FP16) run_batch<float, __half>(c, ps, hp, stats, 2, user_stream);
     else if (p.storage == RGBDFLOW_STORE_BF16) run_batch<float, __nv_bfloat16>(c, ps, hp, stats, 3, user_stream);
     else run_batch<float, float>(c, ps, hp, stats, 0, user_stream);
+}
+
+// Captures the graph of a batch of device-pointer pairs (the served form) ahead of its first
+// launch; nothing runs.  Returns false, capturing nothing, when the batch would need more solve
+// memory than the context holds: its first launch reallocates, which drops the cached graphs.
+template <class T, class S>
+static bool prepare_batch(rgbdflow_ctx* c, const std::vector<PairSpec>& pairs, const HostParams& hp, int slot)
+{
+    if (!c->use_graphs || c->prof) return false;
+    if (c->graphs.count(graph_key(pairs, hp, slot, true))) return true;
+    ensure_attrs<T, S>(c, slot);
+    Plan<T, S> P = make_plan<T, S>(pairs, hp);
+    P.sms = c->sms;
+    if (!c->arena || P.arena_bytes > c->arena_cap) return false;
+    bind_plan(P, c->arena);
+    graph_for(c, P, pairs, hp, slot, true);
+    return true;
+}
+
+// prepare_batch with dispatch's choice of types (the FP32 solve: serving has no FP64 form).
+static bool prepare_dispatch(rgbdflow_ctx* c, const std::vector<PairSpec>& ps, const rgbdflow_params& p)
+{
+    const HostParams hp = host_params(p);
+    if (p.storage == RGBDFLOW_STORE_FP16) return prepare_batch<float, __half>(c, ps, hp, 2);
+    if (p.storage == RGBDFLOW_STORE_BF16) return prepare_batch<float, __nv_bfloat16>(c, ps, hp, 3);
+    return prepare_batch<float, float>(c, ps, hp, 0);
 }
 
 static int fail(rgbdflow_ctx* c, int code, const std::string& m)
@@ -864,8 +912,10 @@ int rgbdflow_server_destroy(rgbdflow_server* s)
 }
 
 namespace {
-void server_presize(rgbdflow_server* s);
+void server_prepare(rgbdflow_server* s);
+void server_prepare_slot(rgbdflow_server* s, ServerSlot& sl);
 constexpr int kServerFramesPerStream = 8;  // frame buffer sets stocked per stream (a backlog of ~6 pairs)
+constexpr int kServerPrecapture = 40;      // batch graphs captured ahead per slot (within kGraphCache)
 }
 
 int rgbdflow_server_submit(rgbdflow_server* s, int stream_id, uint64_t request_id, const rgbdflow_camera_params* cam,
@@ -874,6 +924,7 @@ int rgbdflow_server_submit(rgbdflow_server* s, int stream_id, uint64_t request_i
     if (!s) return RGBDFLOW_ERR_INVALID_ARG;
     rgbdflow_ctx* c = s->ctx;
     API_BEGIN
+    MaxTimer timer(&s->counters.max_submit_ms);
     if (!cam || !bgr || !depth_m || W < 2 || H < 2) throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "bad frame");
     if (cam->xRes == 0 || !(cam->focalLength > 0)) throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "bad camera");
     auto it = s->streams.find(stream_id);
@@ -924,7 +975,7 @@ int rgbdflow_server_submit(rgbdflow_server* s, int stream_id, uint64_t request_i
         ss.has_flow = false;
     }
     ss.W = W; ss.H = H;
-    if (resized) server_presize(s);
+    if (resized) server_prepare(s);
     if (ss.prev) {
         ServerReq r;
         r.stream = stream_id; r.id = request_id; r.W = W; r.H = H;
@@ -940,6 +991,7 @@ namespace {
 
 void server_retire(rgbdflow_server* s, ServerSlot& sl)
 {
+    MaxTimer timer(&s->counters.max_retire_ms);
     const double now = mono_now();
     for (size_t i = 0; i < sl.reqs.size(); i++) {
         ServerReq& r = sl.reqs[i];
@@ -1001,10 +1053,10 @@ size_t admit_need(rgbdflow_server* s, const std::vector<PairSpec>& ps, const Hos
     return tot;
 }
 
-// When a stream registers or changes size: size both slots' solve memory once for a full batch
-// (max_batch cold pairs of the largest registered size) as far as the HBM budget allows, so that
-// serving never regrows an arena (which waits for the device and drops the slot's graphs).
-void server_presize(rgbdflow_server* s)
+// Sizes a slot's solve memory once for a full batch (max_batch cold pairs of the largest
+// registered size) as far as the HBM budget allows, so that serving never regrows an arena
+// (which waits for the device and drops the slot's graphs).
+void server_presize_slot(rgbdflow_server* s, ServerSlot& sl)
 {
     int W = 0, H = 0;
     for (const auto& kv : s->streams)
@@ -1017,21 +1069,79 @@ void server_presize(rgbdflow_server* s)
     const int nb = std::max(1, std::min(s->cfg.max_batch, s->cfg.max_streams));
     std::vector<PairSpec> ps(nb, q);
     const SlotNeed need = slot_need(ps, host_params(s->cfg.params), s->cfg.params.storage);
+    const size_t other = (&sl == &s->slots[0]) ? s->slots[1].ctx->arena_cap : s->slots[0].ctx->arena_cap;
+    if (sl.ctx->arena_cap < need.arena &&
+        !(s->cfg.hbm_budget_bytes && s->resident_bytes + other + need.arena > s->cfg.hbm_budget_bytes))
+        ensure_arena(sl.ctx, need.arena);
+    // pinned staging: the slot's descriptors and its results (cudaFreeHost / cudaMallocHost on
+    // growth would synchronise the device mid-serving)
+    ensure_pin(sl.ctx, need.pin);
+    const size_t out = (size_t)nb * align_up((size_t)W * H * 12, 256);
+    if (sl.pin_cap < out) {
+        if (sl.pin_out) RF_CUDA(cudaFreeHost(sl.pin_out));
+        RF_CUDA(cudaMallocHost(&sl.pin_out, out));
+        sl.pin_cap = out;
+    }
+}
+
+// The batches the registered streams can form in the steady state: per frame size any count from
+// 0 to the number of streams of that size, max_batch pairs at most, all warm-started when the
+// server warm-starts (the cold first pairs of new streams are captured when they come), pairs in
+// server_launch's canonical order (larger frames first).  Empty when there are more than
+// kServerPrecapture.
+std::vector<std::vector<PairSpec>> server_batches(const rgbdflow_server* s)
+{
+    std::map<std::pair<int, int>, int> count;  // (W, H) -> registered streams
+    for (const auto& kv : s->streams)
+        if (kv.second.W >= 2 && kv.second.H >= 2) count[{kv.second.W, kv.second.H}]++;
+    std::vector<std::pair<std::pair<int, int>, int>> sizes(count.begin(), count.end());
+    std::stable_sort(sizes.begin(), sizes.end(), [](const auto& a, const auto& b) {
+        return (long)a.first.first * a.first.second > (long)b.first.first * b.first.second;
+    });
+    static const float kNoFlow = 0;  // marks a pair warm-started; never read (nothing runs)
+    std::vector<std::vector<PairSpec>> batches;
+    std::vector<int> n(sizes.size(), 0);
+    for (;;) {  // an odometer over the per-size counts
+        size_t i = 0;
+        while (i < n.size() && ++n[i] > sizes[i].second) n[i++] = 0;
+        if (i == n.size()) break;
+        int pairs = 0;
+        for (int v : n) pairs += v;
+        if (pairs > s->cfg.max_batch) continue;
+        if ((int)batches.size() == kServerPrecapture) return {};
+        std::vector<PairSpec> ps;
+        for (size_t k = 0; k < sizes.size(); k++)
+            for (int j = 0; j < n[k]; j++) {
+                PairSpec q;
+                q.W = sizes[k].first.first;
+                q.H = sizes[k].first.second;
+                q.f_full = 0.8f * q.W;
+                q.xres_full = (unsigned)q.W;
+                q.est = s->cfg.warm_start ? &kNoFlow : nullptr;
+                q.warm_early = s->cfg.warm_early_termination;
+                ps.push_back(q);
+            }
+        batches.push_back(std::move(ps));
+    }
+    return batches;
+}
+
+// Readies a slot for the registered streams: its solve memory (server_presize_slot), then the graph
+// of every batch of server_batches, captured without running.
+void server_prepare_slot(rgbdflow_server* s, ServerSlot& sl)
+{
+    sl.prepare = false;
+    server_presize_slot(s, sl);
+    for (const auto& ps : server_batches(s)) prepare_dispatch(sl.ctx, ps, s->cfg.params);
+}
+
+// When a stream registers or changes size: ready each idle slot now; a busy slot is readied before
+// its next launch (server_step), so the request path neither reallocates nor captures.
+void server_prepare(rgbdflow_server* s)
+{
     for (auto& sl : s->slots) {
-        if (sl.busy) continue;  // grown on its next launch instead
-        const size_t other = (&sl == &s->slots[0]) ? s->slots[1].ctx->arena_cap : s->slots[0].ctx->arena_cap;
-        if (sl.ctx->arena_cap < need.arena &&
-            !(s->cfg.hbm_budget_bytes && s->resident_bytes + other + need.arena > s->cfg.hbm_budget_bytes))
-            ensure_arena(sl.ctx, need.arena);
-        // pinned staging: the slot's descriptors and its results (cudaFreeHost / cudaMallocHost on
-        // growth would synchronise the device mid-serving)
-        ensure_pin(sl.ctx, need.pin);
-        const size_t out = (size_t)nb * align_up((size_t)W * H * 12, 256);
-        if (sl.pin_cap < out) {
-            if (sl.pin_out) RF_CUDA(cudaFreeHost(sl.pin_out));
-            RF_CUDA(cudaMallocHost(&sl.pin_out, out));
-            sl.pin_cap = out;
-        }
+        if (sl.busy) sl.prepare = true;
+        else server_prepare_slot(s, sl);
     }
 }
 
@@ -1039,6 +1149,7 @@ void server_launch(rgbdflow_server* s, ServerSlot& sl)
 {
     // admit queued requests in arrival order: one pair per stream in flight, max_batch per slot,
     // the slot's solve memory inside the HBM budget
+    MaxTimer timer(&s->counters.max_launch_ms);
     const HostParams hp = host_params(s->cfg.params);
     std::vector<ServerReq> take;
     std::vector<PairSpec> specs;
@@ -1093,6 +1204,7 @@ void server_launch(rgbdflow_server* s, ServerSlot& sl)
                                 cudaMemcpyDeviceToHost, sl.st));
     RF_CUDA(cudaEventRecord(sl.done, sl.st));
     sl.busy = true;
+    s->counters.launches++;
 }
 
 }  // namespace
@@ -1118,9 +1230,11 @@ int rgbdflow_server_step(rgbdflow_server* s, int wait, rgbdflow_result* out, int
             server_retire(s, *oldest);
         }
     }
-    // launch into free slots
-    for (auto& sl : s->slots)
+    // launch into free slots (after readying them for streams registered while they ran)
+    for (auto& sl : s->slots) {
+        if (!sl.busy && sl.prepare) server_prepare_slot(s, sl);
         if (!sl.busy && !s->queue.empty()) server_launch(s, sl);
+    }
     int n = 0;
     while (!s->ready.empty() && n < max) {
         out[n++] = s->ready.front();
@@ -1137,6 +1251,30 @@ int rgbdflow_server_pending(const rgbdflow_server* s)
     int n = (int)s->queue.size() + (int)s->ready.size();
     for (const auto& sl : s->slots) n += (int)sl.reqs.size();
     return n;
+}
+
+int rgbdflow_server_counters_read(rgbdflow_server* s, int reset, rgbdflow_server_counters* out)
+{
+    if (!s || !out) return RGBDFLOW_ERR_INVALID_ARG;
+    uint64_t graphs = 0, grows = 0;
+    for (const auto& sl : s->slots) {
+        graphs += sl.ctx->n_graph_builds;
+        grows += sl.ctx->n_arena_grows;
+    }
+    rgbdflow_server_counters k = s->counters;
+    for (const auto& sl : s->slots) k.max_graph_build_ms = std::max(k.max_graph_build_ms, sl.ctx->max_build_ms);
+    k.frames_allocated = s->pool.misses - s->base_frames;
+    k.graphs_built = graphs - s->base_graphs;
+    k.arena_grows = grows - s->base_grows;
+    *out = k;
+    if (reset) {
+        s->counters = rgbdflow_server_counters{};
+        for (auto& sl : s->slots) sl.ctx->max_build_ms = 0;
+        s->base_frames = s->pool.misses;
+        s->base_graphs = graphs;
+        s->base_grows = grows;
+    }
+    return RGBDFLOW_OK;
 }
 
 }  // extern "C"

@@ -23,6 +23,18 @@ static inline double mono_now()
     return ts.tv_sec + 1e-9 * ts.tv_nsec;
 }
 
+// Keeps in *slot the longest duration (milliseconds) of the scopes it times.
+struct MaxTimer {
+    double* slot;
+    double t0;
+    explicit MaxTimer(double* s) : slot(s), t0(mono_now()) {}
+    ~MaxTimer()
+    {
+        const double ms = 1e3 * (mono_now() - t0);
+        if (ms > *slot) *slot = ms;
+    }
+};
+
 // Device + pinned buffers of one uploaded frame.  They come from, and go back to, the server's
 // pool (no allocation, hence no implicit device synchronisation, in the steady state).
 struct FrameBufs {
@@ -35,6 +47,7 @@ struct FrameBufs {
 struct FramePool {
     std::unordered_map<size_t, std::vector<FrameBufs>> free_;
     size_t* resident = nullptr;
+    uint64_t misses = 0;  // buffer sets allocated because the stock of their size was empty
     static FrameBufs make(size_t n_px, size_t* resident)
     {
         FrameBufs b;
@@ -61,6 +74,7 @@ struct FramePool {
             v.pop_back();
             return b;
         }
+        misses++;
         return make(n_px, resident);
     }
     void put(size_t n_px, const FrameBufs& b) { free_[n_px].push_back(b); }
@@ -113,6 +127,7 @@ struct ServerSlot {
     cudaEvent_t done = nullptr;
     std::vector<ServerReq> reqs;
     bool busy = false;
+    bool prepare = false;  // streams registered while busy: size memory and capture graphs when idle
     char* pin_out = nullptr;
     size_t pin_cap = 0;
     std::vector<size_t> out_off;
@@ -130,4 +145,7 @@ struct rgbdflow_server {
     size_t resident_bytes = 0;    // frame pool + stream flows held on the device
     rgbdflow::FramePool pool;
     std::deque<rgbdflow_result> ready;
+    // rgbdflow_server_counters_read: running maxima and step count, and the totals of the last reset
+    rgbdflow_server_counters counters{};
+    uint64_t base_frames = 0, base_graphs = 0, base_grows = 0;
 };

@@ -145,6 +145,13 @@ class Result(ctypes.Structure):
                 ("done_time_s", ctypes.c_double), ("status", ctypes.c_int)]
 
 
+class ServerCounters(ctypes.Structure):
+    _fields_ = [("frames_allocated", ctypes.c_uint64), ("graphs_built", ctypes.c_uint64),
+                ("arena_grows", ctypes.c_uint64), ("launches", ctypes.c_uint64),
+                ("max_submit_ms", ctypes.c_double), ("max_launch_ms", ctypes.c_double),
+                ("max_retire_ms", ctypes.c_double), ("max_graph_build_ms", ctypes.c_double)]
+
+
 _lib = None
 
 _P = ctypes.POINTER
@@ -182,6 +189,7 @@ SIGNATURES = {
     "rgbdflow_server_submit": (_i, [_vp, _i, ctypes.c_uint64, _P(CameraParams), _vp, _vp, _i, _i, _vp]),
     "rgbdflow_server_step": (_i, [_vp, _i, _P(Result), _i, _P(_i)]),
     "rgbdflow_server_pending": (_i, [_vp]),
+    "rgbdflow_server_counters_read": (_i, [_vp, _i, _P(ServerCounters)]),
     "rgbdflow_scene_flow_noalloc": (_i, [_P(RgbdFlowPair), _P(Params), _vp, ctypes.c_char_p, ctypes.c_size_t]),
 }
 
@@ -472,6 +480,15 @@ class Server:
 
     def pending(self):
         return self.lib.rgbdflow_server_pending(self.h)
+
+    def counters(self, reset=False):
+        """Host-side events that add to served latency (rgbdflow_server_counters_read): frame
+        buffers allocated beyond the stock, graphs captured, arena reallocations, device steps, and
+        the longest host time of a submit, a step launch, a step retirement and a graph capture +
+        instantiation (ms)."""
+        k = ServerCounters()
+        self.ctx._check(self.lib.rgbdflow_server_counters_read(self.h, int(bool(reset)), ctypes.byref(k)))
+        return {name: getattr(k, name) for name, _ in ServerCounters._fields_}
 
     def close(self):
         if self.h:

@@ -32,8 +32,9 @@ def frame_index(t, n_unique):
 
 def simulate(server, rf, streams, n_frames=300, fps=30.0, seed=0, time_scale=1.0, keep_stream=None, keep_n=0):
     """Submit n_frames per stream at `fps` (exponential inter-arrival times, mean 1/fps) and
-    collect every result.  Returns dict(latencies_ms, pairs, wall_s, kept) where kept holds up to
-    keep_n (frame index, flow) results of stream keep_stream."""
+    collect every result.  Returns dict(latencies_ms, pairs, wall_s, kept, host) where kept holds
+    up to keep_n (frame index, flow) results of stream keep_stream and host the longest host times
+    (ms) of one loop iteration (its sleep excluded), one submit call and one step call."""
     rng = np.random.default_rng(seed)
     arrivals = []
     for s, seq in enumerate(streams):
@@ -45,17 +46,25 @@ def simulate(server, rf, streams, n_frames=300, fps=30.0, seed=0, time_scale=1.0
     cams = [rf.CameraParams.make(seq["W"], seq["H"], seq["cam"].f, seq["cam"].cx, seq["cam"].cy) for seq in streams]
     lat, done, kept = [], 0, []
     expected = len(streams) * (n_frames - 1)
+    host = dict(iter_ms=0.0, submit_ms=0.0, step_ms=0.0)
     t0 = time.perf_counter()
     i = 0
     while done < expected:
-        now = time.perf_counter() - t0
+        t_iter = time.perf_counter()
+        now = t_iter - t0
         while i < len(arrivals) and arrivals[i][0] <= now:
             _, s, k = arrivals[i]
             seq = streams[s]
             fr = seq["frames"][frame_index(k, len(seq["frames"]))]
+            t = time.perf_counter()
             server.submit(s, k, cams[s], fr["bgr"], fr["depth"])
+            host["submit_ms"] = max(host["submit_ms"], 1e3 * (time.perf_counter() - t))
             i += 1
-        res = server.step(wait=(i >= len(arrivals)))
+        wait = i >= len(arrivals)
+        t = time.perf_counter()
+        res = server.step(wait=wait)
+        if not wait:
+            host["step_ms"] = max(host["step_ms"], 1e3 * (time.perf_counter() - t))
         for (sid, rid, flow, ts, td, st) in res:
             if st != 0:
                 raise RuntimeError("request failed: %d" % st)
@@ -63,9 +72,11 @@ def simulate(server, rf, streams, n_frames=300, fps=30.0, seed=0, time_scale=1.0
             done += 1
             if sid == keep_stream and len(kept) < keep_n:
                 kept.append((rid, flow))
+        if not wait:
+            host["iter_ms"] = max(host["iter_ms"], 1e3 * (time.perf_counter() - t_iter))
         if not res and i < len(arrivals):
             nxt = arrivals[i][0] - (time.perf_counter() - t0)
             if nxt > 0:
                 time.sleep(min(nxt, 0.0005))
     wall = time.perf_counter() - t0
-    return dict(latencies_ms=lat, pairs=done, wall_s=wall, kept=kept)
+    return dict(latencies_ms=lat, pairs=done, wall_s=wall, kept=kept, host=host)

@@ -141,6 +141,26 @@ def test_batch_equals_solo(ctx):
         np.testing.assert_array_equal(a, b)
 
 
+def test_graph_shared_across_cameras_gives_the_fresh_result(ctx):
+    """Solve graphs are keyed without the camera (it reaches the kernels only through the uploaded
+    item descriptors): a pair solved with another camera, reusing the graph a same-sized pair has
+    just captured, equals the same pair solved in a fresh context, whose first call captures."""
+    p = syn.make_config_pair("320x240", seed=21)
+    prm = rf.benchmark_params(640)
+    other = rf.CameraParams.make(p["W"], p["H"], 0.9 * p["cam"].f, p["cam"].cx + 3.0, p["cam"].cy - 2.0)
+    ctx.scene_flow_two_frames(cam_of(p), p["bgr1"], p["depth1"], p["bgr2"], p["depth2"], prm, stats=False)
+    reused = ctx.scene_flow_two_frames(other, p["bgr1"], p["depth1"], p["bgr2"], p["depth2"], prm, stats=False)
+    fresh_ctx = rf.Context(0)
+    try:
+        fresh = fresh_ctx.scene_flow_two_frames(other, p["bgr1"], p["depth1"], p["bgr2"], p["depth2"], prm,
+                                                stats=False)
+    finally:
+        fresh_ctx.close()
+    assert not np.array_equal(reused, ctx.scene_flow_two_frames(cam_of(p), p["bgr1"], p["depth1"], p["bgr2"],
+                                                                  p["depth2"], prm, stats=False))
+    np.testing.assert_array_equal(reused, fresh)
+
+
 def test_batch_submit_equals_batch(ctx):
     """The submitted host-buffer batch (returns once enqueued; two contexts alternating) gives the
     synchronous call's flows bit for bit, and refuses pageable outputs."""

@@ -73,3 +73,62 @@ def test_admission_respects_the_hbm_budget(ctx):
         srv.submit(1, 0, _cam(streams[1]), fr["bgr"], fr["depth"])  # a 320x240 frame + flow exceed 1 MB
     assert e.value.code == -4
     srv.close()
+
+
+def test_graphs_are_captured_when_a_stream_registers(ctx):
+    """Registering a stream captures, on both solve slots, the graph of every batch the registered
+    streams can form; the pairs that follow launch cached graphs only: the counters read no
+    capture, no reallocation and no frame allocation, and one device step per pair."""
+    seq = _streams()[0]
+    srv = rf.Server(ctx, rf.benchmark_params(640), max_streams=4, max_batch=4, warm_start=False)
+    fr = seq["frames"][0]
+    srv.submit(0, 0, _cam(seq), fr["bgr"], fr["depth"])  # the stream's first frame registers it
+    reg = srv.counters(reset=True)
+    assert reg["graphs_built"] == 2 and reg["launches"] == 0 and reg["max_graph_build_ms"] > 0
+    for k in range(1, 6):
+        fr = seq["frames"][k % len(seq["frames"])]
+        srv.submit(0, k, _cam(seq), fr["bgr"], fr["depth"])
+        while srv.pending():
+            for r in srv.step(wait=True):
+                assert r[5] == 0
+    c = srv.counters()
+    assert c["graphs_built"] == 0 and c["arena_grows"] == 0 and c["frames_allocated"] == 0
+    assert c["launches"] == 5
+    assert c["max_submit_ms"] > 0 and c["max_launch_ms"] > 0 and c["max_retire_ms"] > 0
+    srv.close()
+
+
+def test_a_stream_registered_while_a_slot_runs_is_captured_before_its_next_launch(ctx):
+    """A slot that is busy when a stream registers sizes its solve memory for that stream and
+    captures its batches before it next launches (or at once, if it is idle by then): with a
+    160x120 and a 320x240 stream, three batches per slot, and the mixed pairs that follow neither
+    capture nor reallocate."""
+    streams = _streams()
+    srv = rf.Server(ctx, rf.benchmark_params(640), max_streams=4, max_batch=4, warm_start=False)
+
+    def submit(s, k):
+        fr = streams[s]["frames"][k]
+        srv.submit(s, k, _cam(streams[s]), fr["bgr"], fr["depth"])
+
+    def drain():
+        while srv.pending():
+            for r in srv.step(wait=True):
+                assert r[5] == 0
+
+    submit(0, 0)
+    submit(0, 1)
+    srv.step(wait=False)  # launches the first pair of stream 0 on a slot
+    submit(1, 0)          # registers stream 1, most likely while that slot runs
+    drain()
+    start = srv.counters(reset=True)
+    # per slot: the 160x120 batch when stream 0 registers; then its memory grows for the 320x240
+    # stream (which drops its graphs) and it captures the three batches of the two streams
+    assert start["graphs_built"] == 2 * (1 + 3) and start["arena_grows"] == 2 * 2
+    for k in range(1, 5):
+        submit(1, k)
+        if k + 1 < 5:
+            submit(0, k + 1)
+        drain()
+    c = srv.counters()
+    assert c["graphs_built"] == 0 and c["arena_grows"] == 0 and c["launches"] == 4
+    srv.close()
