@@ -43,6 +43,8 @@ extern "C" {
 #define RGBDFLOW_ERR_NO_DEVICE    (-6)
 #define RGBDFLOW_ERR_BUSY         (-7) /* no free slot; retry later */
 #define RGBDFLOW_ERR_INTERNAL     (-8)
+#define RGBDFLOW_ERR_IO           (-9)  /* a file could not be opened, read or written in full */
+#define RGBDFLOW_ERR_FORMAT       (-10) /* a file is not in the expected format */
 
 /* regularisation types (OpticalFlow::sceneFlowRegularizationType, OpticalFlow.h:99-104) */
 #define RGBDFLOW_REG_ISOTROPIC 0
@@ -351,6 +353,21 @@ int rgbdflow_server_counters_read(rgbdflow_server* srv, int reset, rgbdflow_serv
  * ------------------------------------------------------------------------------------------- */
 int rgbdflow_scene_flow_noalloc(const rgbdflow_pair* pair, const rgbdflow_params* params, void* stream,
                                 char* err, size_t err_len);
+
+/* ---------------------------------------------------------------------------------------------
+ * .flo3 scene-flow files: readSceneFlow / writeSceneFlow (src/sceneFlowIO.cpp:18-61), the format
+ * the reference's demo writes its result in (src/main.cpp:126).  Layout: the 8 bytes
+ * 237 159 43 26 202 94 218 68, int32 width, int32 height, then width*height (u, v, w) float32
+ * triples, rows top to bottom; numbers little-endian (the reference writes host order, which is
+ * little-endian on its platforms).  Host-only: no device, no context.
+ * err / err_len: NULL or a buffer that receives the message of a failure.
+ * ------------------------------------------------------------------------------------------- */
+/* Writes W*H*3 floats.  A file that cannot be opened or written in full: RGBDFLOW_ERR_IO. */
+int rgbdflow_flo3_write(const char* path, const float* flow, int W, int H, char* err, size_t err_len);
+/* Reads the size into *W, *H and, with flow != NULL, the W*H*3 values (n_floats >= W*H*3, else
+ * RGBDFLOW_ERR_INVALID_ARG).  A file that cannot be opened or ends early: RGBDFLOW_ERR_IO; another
+ * magic number or a size below 1: RGBDFLOW_ERR_FORMAT.  Bytes after the last value are ignored. */
+int rgbdflow_flo3_read(const char* path, float* flow, size_t n_floats, int* W, int* H, char* err, size_t err_len);
 
 #ifdef __cplusplus
 }

@@ -16,6 +16,7 @@
 #include "../../include/rgbdflow.h"
 #include "pipeline.cuh"
 #include "server.cuh"
+#include "flo3.h"
 
 using namespace rgbdflow;
 
@@ -1374,6 +1375,36 @@ extern "C" int rgbdflow_scene_flow_noalloc(const rgbdflow_pair* pair, const rgbd
         return noalloc_fail(err, err_len, RGBDFLOW_ERR_CUDA, e.what());
     } catch (const std::exception& e) {
         return noalloc_fail(err, err_len, RGBDFLOW_ERR_INTERNAL, e.what());
+    } catch (...) {
+        return noalloc_fail(err, err_len, RGBDFLOW_ERR_INTERNAL, "unknown error");
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// .flo3 files (host-only)
+// ------------------------------------------------------------------------------------------
+extern "C" int rgbdflow_flo3_write(const char* path, const float* flow, int W, int H, char* err, size_t err_len)
+{
+    if (err && err_len) err[0] = 0;
+    try {
+        flo3_write(path, flow, W, H);
+        return RGBDFLOW_OK;
+    } catch (const Flo3Error& e) {
+        return noalloc_fail(err, err_len, e.code, e.msg);
+    } catch (...) {
+        return noalloc_fail(err, err_len, RGBDFLOW_ERR_INTERNAL, "unknown error");
+    }
+}
+
+extern "C" int rgbdflow_flo3_read(const char* path, float* flow, size_t n_floats, int* W, int* H, char* err,
+                                  size_t err_len)
+{
+    if (err && err_len) err[0] = 0;
+    try {
+        flo3_read(path, flow, n_floats, W, H);
+        return RGBDFLOW_OK;
+    } catch (const Flo3Error& e) {
+        return noalloc_fail(err, err_len, e.code, e.msg);
     } catch (...) {
         return noalloc_fail(err, err_len, RGBDFLOW_ERR_INTERNAL, "unknown error");
     }

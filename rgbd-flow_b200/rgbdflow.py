@@ -27,7 +27,7 @@ MAX_LEVELS, MAX_OUTER = 16, 64
 
 OK = 0
 ERR_NAMES = {-1: "INVALID_ARG", -2: "UNSUPPORTED", -3: "CUDA", -4: "BUDGET", -5: "TIMEOUT",
-             -6: "NO_DEVICE", -7: "BUSY", -8: "INTERNAL"}
+             -6: "NO_DEVICE", -7: "BUSY", -8: "INTERNAL", -9: "IO", -10: "FORMAT"}
 
 
 class RgbdFlowError(RuntimeError):
@@ -191,6 +191,9 @@ SIGNATURES = {
     "rgbdflow_server_pending": (_i, [_vp]),
     "rgbdflow_server_counters_read": (_i, [_vp, _i, _P(ServerCounters)]),
     "rgbdflow_scene_flow_noalloc": (_i, [_P(RgbdFlowPair), _P(Params), _vp, ctypes.c_char_p, ctypes.c_size_t]),
+    "rgbdflow_flo3_write": (_i, [ctypes.c_char_p, _vp, _i, _i, ctypes.c_char_p, ctypes.c_size_t]),
+    "rgbdflow_flo3_read": (_i, [ctypes.c_char_p, _vp, ctypes.c_size_t, _P(_i), _P(_i), ctypes.c_char_p,
+                                ctypes.c_size_t]),
 }
 
 
@@ -240,6 +243,35 @@ def batch_device_bytes(sizes, params, warm=None):
     if rc != OK:
         raise RgbdFlowError(rc, "rgbdflow_batch_device_bytes failed")
     return out.value
+
+
+def write_flo3(path, flow):
+    """Write an (H, W, 3) float32 flow (u px, v px, w m) as a .flo3 file (rgbdflow_flo3_write;
+    writeSceneFlow, src/sceneFlowIO.cpp:49-61).  Host-only."""
+    flow = np.ascontiguousarray(flow, dtype=np.float32)
+    if flow.ndim != 3 or flow.shape[2] != 3:
+        raise RgbdFlowError(-1, "flow must be (H, W, 3)")
+    err = ctypes.create_string_buffer(512)
+    rc = load().rgbdflow_flo3_write(os.fsencode(path), _ptr(flow), flow.shape[1], flow.shape[0], err, len(err))
+    if rc != OK:
+        raise RgbdFlowError(rc, err.value.decode())
+
+
+def read_flo3(path):
+    """Read a .flo3 file into an (H, W, 3) float32 array (rgbdflow_flo3_read; readSceneFlow,
+    src/sceneFlowIO.cpp:23-44).  Host-only."""
+    lib = load()
+    err = ctypes.create_string_buffer(512)
+    W, H = ctypes.c_int(), ctypes.c_int()
+    rc = lib.rgbdflow_flo3_read(os.fsencode(path), None, 0, ctypes.byref(W), ctypes.byref(H), err, len(err))
+    if rc != OK:
+        raise RgbdFlowError(rc, err.value.decode())
+    flow = np.empty((H.value, W.value, 3), np.float32)
+    rc = lib.rgbdflow_flo3_read(os.fsencode(path), _ptr(flow), flow.size, ctypes.byref(W), ctypes.byref(H), err,
+                                len(err))
+    if rc != OK:
+        raise RgbdFlowError(rc, err.value.decode())
+    return flow
 
 
 def scene_flow_noalloc(pair, params, stream=None):
