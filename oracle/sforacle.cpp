@@ -794,6 +794,252 @@ void multiscale(const rgbdflow_camera_params& cam, const rgbdflow_params& p, con
 
 using namespace sfo;
 
+/* ------------------------------------------------------------------------------------------ */
+/* 2-D optical flow: Ce Liu's coarse-to-fine solver, the demo's flow type 1
+ * (OpticalFlow::Coarse2FineFlow, src/opticalFlowMultiscale.cpp:4-146, CELIU variant:
+ * OpticalFlow::SmoothFlowSOR, src/SmoothFlowSOR.cpp:8-247).  All FP64, like the reference, with
+ * its lexicographic SOR order, so the result equals the reference's bit for bit. */
+
+/* Image::dx / Image::dy without the advanced filter (Image.h:955-1019): forward differences;
+ * the last column (dx) or row (dy) is 0. */
+static void fwd_dx(const std::vector<double>& in, int W, int H, std::vector<double>& out)
+{
+    out.assign((size_t)W * H, 0.0);
+    for (int i = 0; i < H; i++)
+        for (int j = 0; j < W - 1; j++) out[(size_t)i * W + j] = in[(size_t)i * W + j + 1] - in[(size_t)i * W + j];
+}
+static void fwd_dy(const std::vector<double>& in, int W, int H, std::vector<double>& out)
+{
+    out.assign((size_t)W * H, 0.0);
+    for (int i = 0; i < H - 1; i++)
+        for (int j = 0; j < W; j++) out[(size_t)i * W + j] = in[(size_t)(i + 1) * W + j] - in[(size_t)i * W + j];
+}
+
+/* getDxs (src/opticalFlowUtils.cpp:18-53): spatial derivatives of 0.4 im1 + 0.6 im2 with the
+ * 5-tap {1,-8,0,8,-1}/12 filter (Image::dx/dy advanced), temporal derivative im2 - im1. */
+static void get_dxs(const Img& im1, const Img& im2, Img& dx, Img& dy, Img& dt)
+{
+    Img m = im1;
+    for (size_t z = 0; z < m.n(); z++) m.d[z] *= 0.4;
+    for (size_t z = 0; z < m.n(); z++) m.d[z] += im2.d[z] * 0.6;
+    double f[5] = {1, -8, 0, 8, -1};
+    for (int i = 0; i < 5; i++) f[i] /= 12;
+    hfilter(m, dx, f, 2);
+    vfilter(m, dy, f, 2);
+    dt.alloc(im1.w, im1.h, im1.c);
+    for (size_t z = 0; z < dt.n(); z++) dt.d[z] = im2.d[z] - im1.d[z];
+}
+
+/* warpFL, bilinear (src/opticalFlowUtils.cpp:62-67; ImageProcessing::warpImage,
+ * ImageProcessing.h:472-491): Im2 at (j + u, i + v), Im1 where that falls outside the image. */
+static void warp_fl(const Img& Im1, const Img& Im2, const std::vector<double>& u, const std::vector<double>& v, Img& out)
+{
+    const int W = Im2.w, H = Im2.h, C = Im2.c;
+    out.alloc(W, H, C);
+    for (int i = 0; i < H; i++)
+        for (int j = 0; j < W; j++) {
+            const int o = i * W + j;
+            const double x = j + u[o], y = i + v[o];
+            if (x < 0 || x > W - 1 || y < 0 || y > H - 1)
+                for (int k = 0; k < C; k++) out.d[(size_t)o * C + k] = Im1.d[(size_t)o * C + k];
+            else
+                bilinear_acc(Im2.data(), W, H, C, x, y, out.data() + (size_t)o * C);
+        }
+}
+
+/* Laplacian with normalising weights (src/opticalFlowUtils.cpp:252-313) as SmoothFlowSOR calls
+ * it (SmoothFlowSOR.cpp:144): with the 1-channel phi as the 2-channel weight image.  Channel k of
+ * pixel (i, j) of a 1-channel image is element i * W + j + k (Image::operator(), Image.h:76), so
+ * the "down" weight of (i, j) is phi at (i, j + 1). */
+static void laplacian_phi(const std::vector<double>& in, const std::vector<double>& phi, int W, int H,
+                          std::vector<double>& out)
+{
+    auto nw = [&](int i, int j, int k) { return phi[(size_t)i * W + j + k]; };
+    out.assign((size_t)W * H, 0.0);
+    std::vector<double> foo((size_t)W * H, 0.0);
+    for (int i = 0; i < H; i++)
+        for (int j = 0; j < W - 1; j++) {
+            const size_t o = (size_t)i * W + j;
+            foo[o] = (in[o + 1] - in[o]) * nw(i, j, 0);
+        }
+    for (int i = 0; i < H; i++)
+        for (int j = 0; j < W; j++) {
+            const size_t o = (size_t)i * W + j;
+            if (j < W - 1) out[o] -= foo[o];
+            if (j > 0) out[o] += foo[o - 1];
+        }
+    std::fill(foo.begin(), foo.end(), 0.0);
+    for (int i = 0; i < H - 1; i++)
+        for (int j = 0; j < W; j++) {
+            const size_t o = (size_t)i * W + j;
+            foo[o] = (in[o + W] - in[o]) * nw(i, j, 1);
+        }
+    for (int i = 0; i < H; i++)
+        for (int j = 0; j < W; j++) {
+            const size_t o = (size_t)i * W + j;
+            if (i < H - 1) out[o] -= foo[o];
+            if (i > 0) out[o] += foo[o - W];
+        }
+    for (int i = 0; i < H; i++)
+        for (int j = 0; j < W; j++) {
+            const size_t o = (size_t)i * W + j;
+            double norm = 0;
+            int count = 0;
+            if (j < W - 1) { norm += nw(i, j, 0); count++; }
+            if (j > 0) { norm += nw(i, j - 1, 0); count++; }
+            if (i < H - 1) { norm += nw(i, j, 1); count++; }
+            if (i > 0) { norm += nw(i - 1, j, 1); count++; }
+            if (std::fabs(norm) < 1e-5) out[o] = 0;
+            else out[o] /= (norm / count);
+        }
+}
+
+/* estLaplacianNoise (src/opticalFlowUtils.cpp:155-190): per channel, the mean of the absolute
+ * differences in (0, 1e6), 0.001 when there are none.  The solve reads it only to reject a
+ * value below 1e-20 (SmoothFlowSOR.cpp:113-117). */
+static void est_laplacian_noise(const Img& a, const Img& b, std::vector<double>& para)
+{
+    const int C = a.c;
+    para.assign(C, 0.0);
+    std::vector<double> total(C, 0.0);
+    for (size_t i = 0; i < (size_t)a.w * a.h; i++)
+        for (int k = 0; k < C; k++) {
+            const double t = std::fabs(a.d[i * C + k] - b.d[i * C + k]);
+            if (t > 0 && t < 1000000) { para[k] += t; total[k]++; }
+        }
+    for (int k = 0; k < C; k++) para[k] = total[k] == 0 ? 0.001 : para[k] / total[k];
+}
+
+/* OpticalFlow::SmoothFlowSOR (src/SmoothFlowSOR.cpp:8-247), Laplacian noise model, bilinear warps. */
+static void smooth_flow_sor(const Img& Im1, const Img& Im2, Img& warpIm2, std::vector<double>& u,
+                            std::vector<double>& v, double alpha, int nOuter, int nInner, int nSOR,
+                            std::vector<double>& lap)
+{
+    const int W = Im1.w, H = Im1.h, C = Im1.c;
+    const size_t N = (size_t)W * H;
+    const double eps_phi = std::pow(0.001, 2), eps_psi = std::pow(0.001, 2);
+    Img imdx, imdy, imdt;
+    std::vector<double> du(N), dv(N), uu, vv, ux, uy, vx, vy, phi(N), psi(N * C);
+    std::vector<double> dxy(N), dx2(N), dy2(N), dtdx(N), dtdy(N), foo1, foo2;
+    for (int count = 0; count < nOuter; count++) {
+        get_dxs(Im1, warpIm2, imdx, imdy, imdt);
+        std::fill(du.begin(), du.end(), 0.0);
+        std::fill(dv.begin(), dv.end(), 0.0);
+        for (int hh = 0; hh < nInner; hh++) {
+            uu = u;
+            vv = v;
+            if (hh > 0)
+                for (size_t i = 0; i < N; i++) { uu[i] = u[i] + du[i]; vv[i] = v[i] + dv[i]; }
+            fwd_dx(uu, W, H, ux);
+            fwd_dy(uu, W, H, uy);
+            fwd_dx(vv, W, H, vx);
+            fwd_dy(vv, W, H, vy);
+            for (size_t i = 0; i < N; i++) {
+                const double t = ux[i] * ux[i] + uy[i] * uy[i] + vx[i] * vx[i] + vy[i] * vy[i];
+                phi[i] = 0.5 / std::sqrt(t + eps_phi);
+            }
+            for (size_t i = 0; i < N; i++)
+                for (int k = 0; k < C; k++) {
+                    const size_t o = i * C + k;
+                    double t = imdt.d[o] + imdx.d[o] * du[i] + imdy.d[o] * dv[i];
+                    t *= t;
+                    if (lap[k] < 1E-20) throw std::runtime_error("bad lap para");
+                    psi[o] = 1 / (2 * std::sqrt(t + eps_psi));
+                }
+            // Image::Multiply (Image.h:1697-1710) then Image::collapse, channel mean (Image.h:1480-1516)
+            for (size_t i = 0; i < N; i++) {
+                double sxy = 0, sx2 = 0, sy2 = 0, stx = 0, sty = 0;
+                for (int k = 0; k < C; k++) {
+                    const size_t o = i * C + k;
+                    const double a = imdx.d[o], b = imdy.d[o], c = imdt.d[o];
+                    if (C > 1) {
+                        sxy += psi[o] * a * b; sx2 += psi[o] * a * a; sy2 += psi[o] * b * b;
+                        stx += psi[o] * a * c; sty += psi[o] * b * c;
+                    } else {
+                        sxy = psi[o] * a * b; sx2 = psi[o] * a * a; sy2 = psi[o] * b * b;
+                        stx = psi[o] * a * c; sty = psi[o] * b * c;
+                    }
+                }
+                if (C > 1) { sxy /= C; sx2 /= C; sy2 /= C; stx /= C; sty /= C; }
+                dxy[i] = sxy; dx2[i] = sx2; dy2[i] = sy2; dtdx[i] = stx; dtdy[i] = sty;
+            }
+            laplacian_phi(u, phi, W, H, foo1);
+            laplacian_phi(v, phi, W, H, foo2);
+            for (size_t i = 0; i < N; i++) {
+                dtdx[i] = -dtdx[i] - alpha * foo1[i];
+                dtdy[i] = -dtdy[i] - alpha * foo2[i];
+            }
+            const double omega = 1.8;
+            std::fill(du.begin(), du.end(), 0.0);
+            std::fill(dv.begin(), dv.end(), 0.0);
+            bool converged = false;
+            for (int k = 0; k < nSOR && !converged; k++) {
+                double maxDiff = 0;
+                for (int i = 0; i < H; i++)
+                    for (int j = 0; j < W; j++) {
+                        const size_t o = (size_t)i * W + j;
+                        double sigmaU = 0, sigmaV = 0, weightSum = 0, w;
+                        if (j > 0) { w = phi[o - 1]; sigmaU += w * du[o - 1]; sigmaV += w * dv[o - 1]; weightSum += w; }
+                        if (j < W - 1) { w = phi[o]; sigmaU += w * du[o + 1]; sigmaV += w * dv[o + 1]; weightSum += w; }
+                        if (i > 0) { w = phi[o - W]; sigmaU += w * du[o - W]; sigmaV += w * dv[o - W]; weightSum += w; }
+                        if (i < H - 1) { w = phi[o]; sigmaU += w * du[o + W]; sigmaV += w * dv[o + W]; weightSum += w; }
+                        sigmaU *= -alpha;
+                        sigmaV *= -alpha;
+                        weightSum *= alpha;
+                        const double prevDU = du[o], prevDV = dv[o];
+                        sigmaU += dxy[o] * dv[o];
+                        du[o] = (1 - omega) * du[o] + omega / (dx2[o] + weightSum) * (dtdx[o] - sigmaU);
+                        sigmaV += dxy[o] * du[o];
+                        dv[o] = (1 - omega) * dv[o] + omega / (dy2[o] + weightSum) * (dtdy[o] - sigmaV);
+                        maxDiff = std::max(maxDiff, std::max(std::fabs(du[o] - prevDU), std::fabs(dv[o] - prevDV)));
+                    }
+                converged = maxDiff < 1e-5;
+            }
+        }
+        for (size_t i = 0; i < N; i++) { u[i] += du[i]; v[i] += dv[i]; }
+        warp_fl(Im1, Im2, u, v, warpIm2);
+        est_laplacian_noise(Im1, warpIm2, lap);
+    }
+}
+
+/* OpticalFlow::Coarse2FineFlow (src/opticalFlowMultiscale.cpp:4-146) on two 3-channel images,
+ * CELIU variant, no depth maps: per level, coarsest first, the 5-channel features, the flow
+ * resized from the coarser level and scaled by 1 / ratio, the warp, SmoothFlowSOR with
+ * nOuter + k outer and nSOR + 3 k SOR iterations at level k. */
+void coarse2fine_flow(const Img& im1, const Img& im2, double alpha, double ratio, int min_width, int nOuter, int nInner,
+                      int nSOR, std::vector<double>& u, std::vector<double>& v)
+{
+    std::vector<Img> p1, p2;
+    build_pyramid(im1, ratio, min_width, p1);
+    build_pyramid(im2, ratio, min_width, p2);
+    std::vector<double> lap(im1.c + 2, 0.02);
+    Img warp;
+    const int L = (int)p1.size();
+    for (int k = L - 1; k >= 0; k--) {
+        Img f1, f2;
+        im2feature(p1[k], f1);
+        im2feature(p2[k], f2);
+        const int W = p1[k].w, H = p1[k].h;
+        if (k == L - 1) {
+            u.assign((size_t)W * H, 0.0);
+            v.assign((size_t)W * H, 0.0);
+            warp = f2;
+        } else {
+            Img uin, vin, uo, vo;
+            uin.w = vin.w = p1[k + 1].w; uin.h = vin.h = p1[k + 1].h; uin.c = vin.c = 1;
+            uin.d = u; vin.d = v;
+            resize_dims(uin, uo, W, H);
+            resize_dims(vin, vo, W, H);
+            const double s = 1 / ratio;
+            u = uo.d; v = vo.d;
+            for (auto& x : u) x *= s;
+            for (auto& x : v) x *= s;
+            warp_fl(f1, f2, u, v, warp);
+        }
+        smooth_flow_sor(f1, f2, warp, u, v, alpha, nOuter + k, nInner, nSOR + k * 3, lap);
+    }
+}
+
 static thread_local std::string g_err;
 
 extern "C" {
@@ -1023,6 +1269,25 @@ int sfo_scene_flow_two_frames(int fp64, const rgbdflow_camera_params* camFull, c
             flow_out[l * 3] = (float)u.d[l]; flow_out[l * 3 + 1] = (float)v.d[l]; flow_out[l * 3 + 2] = (float)w.d[l];
         }
         trace_to_stats(t, stats);
+        return 0;
+    } catch (const std::exception& e) { g_err = e.what(); return -1; }
+}
+
+/* 2-D optical flow of two BGR8 images (the demo's flow type 1, runFlowTwoFramesCeLiu,
+ * src/runFlowTwoFrames.cpp:30-45): colour / 255 as cv2liuBGR (src/ceLiuOpticalFlow.cpp:19-37),
+ * then Coarse2FineFlow with the given parameters.  u, v: W*H doubles. */
+int sfo_optical_flow_2d(const uint8_t* bgr1, const uint8_t* bgr2, int W, int H, double alpha, double ratio,
+                        int min_width, int n_outer, int n_inner, int n_sor, double* u, double* v)
+{
+    try {
+        Img I1, I2;
+        I1.alloc(W, H, 3);
+        I2.alloc(W, H, 3);
+        for (size_t z = 0; z < (size_t)W * H * 3; z++) { I1.d[z] = bgr1[z] / 255.0; I2.d[z] = bgr2[z] / 255.0; }
+        std::vector<double> uu, vv;
+        coarse2fine_flow(I1, I2, alpha, ratio, min_width, n_outer, n_inner, n_sor, uu, vv);
+        std::memcpy(u, uu.data(), sizeof(double) * uu.size());
+        std::memcpy(v, vv.data(), sizeof(double) * vv.size());
         return 0;
     } catch (const std::exception& e) { g_err = e.what(); return -1; }
 }

@@ -1,5 +1,6 @@
 """ctypes bindings of the CPU restatement (oracle/libsforacle.so) and of the reference's own
-code compiled in place (oracle/_ref/libref_cpu.so, oracle/_ref/libref_cuda.so).
+code compiled in place (oracle/_ref/libref_cpu.so, oracle/_ref/libref_cuda.so,
+oracle/_ref/libref_flow2d.so).
 
 Test infrastructure only: the checker side of the parity tests, the smoke check and the CPU
 baseline of the benchmark.  The product path never imports this module.
@@ -15,6 +16,7 @@ ORACLE_DIR = os.path.join(ROOT, "oracle")
 ORACLE_SO = os.path.join(ORACLE_DIR, "libsforacle.so")
 REF_CPU_SO = os.path.join(ORACLE_DIR, "_ref", "libref_cpu.so")
 REF_CUDA_SO = os.path.join(ORACLE_DIR, "_ref", "libref_cuda.so")
+REF_FLOW2D_SO = os.path.join(ORACLE_DIR, "_ref", "libref_flow2d.so")
 
 _P = ctypes.POINTER
 _d = ctypes.c_double
@@ -76,6 +78,7 @@ def oracle():
                                          _i, _i, _i, _i, ctypes.c_void_p, ctypes.c_void_p])
         lib.sfo_scene_flow_two_frames.argtypes = [_i, ctypes.c_void_p, _pu8, _pf, _pu8, _pf, _i, _i,
                                                   ctypes.c_void_p, _pf, _pf, ctypes.c_void_p]
+        lib.sfo_optical_flow_2d.argtypes = [_pu8, _pu8, _i, _i, _d, _d, _i, _i, _i, _i, _pd, _pd]
         lib.sfo_last_error.restype = ctypes.c_char_p
         lib.sfo_set_threads.argtypes = [_i]
         _oracle = lib
@@ -116,6 +119,46 @@ def ref_cuda():
         lib.ref_single_scale.argtypes = ([_f] + [_pd] * 9 + [_i, _i, _i, _d, _pd, _d, _pd, _d, _pd, _pd, _i, _i, _i, _i])
         _ref_cuda = lib
     return _ref_cuda
+
+
+_ref_flow2d = None
+
+
+def ref_flow2d_available():
+    return os.path.exists(REF_FLOW2D_SO)
+
+
+def ref_flow2d():
+    global _ref_flow2d
+    if _ref_flow2d is None:
+        lib = ctypes.CDLL(REF_FLOW2D_SO)
+        lib.ref_coarse2fine_flow.argtypes = [_pd, _pd, _i, _i, _i, _d, _d, _i, _i, _i, _i, _pd, _pd,
+                                             ctypes.c_char_p, _i]
+        _ref_flow2d = lib
+    return _ref_flow2d
+
+
+def optical_flow_2d(bgr1, bgr2, alpha=0.02, ratio=0.75, min_width=20, n_outer=10, n_inner=1, n_sor=400,
+                    impl="oracle"):
+    """2-D optical flow (u, v) of two (H, W, 3) uint8 BGR images: the demo's flow type 1 with its
+    defaults (runFlowTwoFramesCeLiu, src/runFlowTwoFrames.cpp:30-45; opticalFlowParams ratio
+    0.75, minWidth 20).  impl "oracle" (the restatement) or "ref" (the reference, compiled)."""
+    b1, b2 = _cont(bgr1, np.uint8), _cont(bgr2, np.uint8)
+    H, W = b1.shape[:2]
+    u = np.zeros((H, W)); v = np.zeros((H, W))
+    if impl == "ref":
+        d1, d2 = b1.astype(np.float64) / 255.0, b2.astype(np.float64) / 255.0
+        err = ctypes.create_string_buffer(256)
+        rc = ref_flow2d().ref_coarse2fine_flow(dptr(d1), dptr(d2), W, H, 0, alpha, ratio, min_width, n_outer, n_inner,
+                                               n_sor, dptr(u), dptr(v), err, len(err))
+        if rc != 0:
+            raise RuntimeError("reference Coarse2FineFlow: " + err.value.decode())
+    else:
+        rc = oracle().sfo_optical_flow_2d(u8ptr(b1), u8ptr(b2), W, H, alpha, ratio, min_width, n_outer, n_inner, n_sor,
+                                          dptr(u), dptr(v))
+        if rc != 0:
+            raise RuntimeError("oracle 2-D flow: " + oracle().sfo_last_error().decode())
+    return u, v
 
 
 # ---------------------------------------------------------------------------------------------
