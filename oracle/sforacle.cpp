@@ -910,10 +910,88 @@ static void est_laplacian_noise(const Img& a, const Img& b, std::vector<double>&
     for (int k = 0; k < C; k++) para[k] = total[k] == 0 ? 0.001 : para[k] / total[k];
 }
 
-/* OpticalFlow::SmoothFlowSOR (src/SmoothFlowSOR.cpp:8-247), Laplacian noise model, bilinear warps. */
+/* One SOR update of pixel (i, j) (SmoothFlowSOR.cpp:166-215): new values of the left and upper
+ * neighbours come from (nu, nv), old values of the right and lower ones and of the pixel itself
+ * from (ou, ov); writes (wu, wv)[o] and returns max(|du change|, |dv change|). */
+struct Sor2dSys {
+    int W, H;
+    double alpha;
+    const double *phi, *dxy, *dx2, *dy2, *dtdx, *dtdy;
+};
+static inline double sor2d_update(const Sor2dSys& q, int i, int j, const double* nu, const double* nv, const double* ou,
+                                  const double* ov, double* wu, double* wv)
+{
+    const int W = q.W, H = q.H;
+    const size_t o = (size_t)i * W + j;
+    const double omega = 1.8;
+    double sigmaU = 0, sigmaV = 0, weightSum = 0, w;
+    if (j > 0) { w = q.phi[o - 1]; sigmaU += w * nu[o - 1]; sigmaV += w * nv[o - 1]; weightSum += w; }
+    if (j < W - 1) { w = q.phi[o]; sigmaU += w * ou[o + 1]; sigmaV += w * ov[o + 1]; weightSum += w; }
+    if (i > 0) { w = q.phi[o - W]; sigmaU += w * nu[o - W]; sigmaV += w * nv[o - W]; weightSum += w; }
+    if (i < H - 1) { w = q.phi[o]; sigmaU += w * ou[o + W]; sigmaV += w * ov[o + W]; weightSum += w; }
+    sigmaU *= -q.alpha;
+    sigmaV *= -q.alpha;
+    weightSum *= q.alpha;
+    const double prevDU = ou[o], prevDV = ov[o];
+    sigmaU += q.dxy[o] * prevDV;
+    const double nDU = (1 - omega) * prevDU + omega / (q.dx2[o] + weightSum) * (q.dtdx[o] - sigmaU);
+    sigmaV += q.dxy[o] * nDU;
+    const double nDV = (1 - omega) * prevDV + omega / (q.dy2[o] + weightSum) * (q.dtdy[o] - sigmaV);
+    wu[o] = nDU;
+    wv[o] = nDV;
+    return std::max(std::fabs(nDU - prevDU), std::fabs(nDV - prevDV));
+}
+
+/* The same SOR iterations in the order a device runs them, for checking that order on the CPU.
+ * Each sweep walks the anti-diagonals d = i + j in turn: every pixel of one diagonal depends only
+ * on the diagonal before it in this sweep and the one after it in the previous sweep, exactly as
+ * in the lexicographic order.  Consecutive sweeps overlap, each starting two steps after the
+ * previous one.  Sweep s writes ring slot s % D and reads the previous sweep's values from slot
+ * (s - 1) % D; a sweep starts only after sweep s - D has finished without converging, so the slot
+ * of the sweep that converges is never overwritten.  Returns the slot of the last sweep (the
+ * first that converged, or sweep nSOR - 1). */
+static int sor2d_wavefront(const Sor2dSys& q, int nSOR, int D, std::vector<std::vector<double>>& ru,
+                           std::vector<std::vector<double>>& rv)
+{
+    const int W = q.W, H = q.H, ndiag = W + H - 1, lag = 2;
+    const size_t N = (size_t)W * H;
+    ru.assign(D, std::vector<double>(N, 0.0));
+    rv.assign(D, std::vector<double>(N, 0.0));
+    std::vector<long> start(nSOR, -1);
+    std::vector<double> maxd(nSOR, 0.0);
+    int done = -1;  // last sweep that finished
+    int stop = -1;  // sweep that converged
+    int next = 0;   // next sweep to start
+    for (long t = 0; stop < 0 && done < nSOR - 1; t++) {
+        if (next < nSOR && (next == 0 || t >= start[next - 1] + lag) && (next < D || done >= next - D)) {
+            start[next] = t;
+            next++;
+        }
+        for (int s = done + 1; s < next; s++) {
+            const long d = t - start[s];
+            if (d < 0 || d >= ndiag) continue;
+            const int cur = s % D, prv = (s + D - 1) % D;
+            for (long i = std::max(0L, d - (W - 1)); i <= std::min((long)H - 1, d); i++) {
+                const double m = sor2d_update(q, (int)i, (int)(d - i), ru[cur].data(), rv[cur].data(), ru[prv].data(),
+                                              rv[prv].data(), ru[cur].data(), rv[cur].data());
+                maxd[s] = std::max(maxd[s], m);
+            }
+        }
+        // the sweeps that finished at this step, in order: the first converged one ends the iterations
+        while (done + 1 < next && t - start[done + 1] == ndiag - 1) {
+            done++;
+            if (maxd[done] < 1e-5) { stop = done; break; }
+        }
+    }
+    return (stop >= 0 ? stop : nSOR - 1) % D;
+}
+
+/* OpticalFlow::SmoothFlowSOR (src/SmoothFlowSOR.cpp:8-247), Laplacian noise model, bilinear warps.
+ * ring > 0 runs the SOR iterations in the device order of sor2d_wavefront with a ring of that
+ * many slots; 0 runs them in the reference's lexicographic order. */
 static void smooth_flow_sor(const Img& Im1, const Img& Im2, Img& warpIm2, std::vector<double>& u,
                             std::vector<double>& v, double alpha, int nOuter, int nInner, int nSOR,
-                            std::vector<double>& lap)
+                            std::vector<double>& lap, int ring = 0)
 {
     const int W = Im1.w, H = Im1.h, C = Im1.c;
     const size_t N = (size_t)W * H;
@@ -969,9 +1047,17 @@ static void smooth_flow_sor(const Img& Im1, const Img& Im2, Img& warpIm2, std::v
                 dtdx[i] = -dtdx[i] - alpha * foo1[i];
                 dtdy[i] = -dtdy[i] - alpha * foo2[i];
             }
-            const double omega = 1.8;
             std::fill(du.begin(), du.end(), 0.0);
             std::fill(dv.begin(), dv.end(), 0.0);
+            if (ring > 0) {
+                const Sor2dSys q{W, H, alpha, phi.data(), dxy.data(), dx2.data(), dy2.data(), dtdx.data(), dtdy.data()};
+                std::vector<std::vector<double>> ru, rv;
+                const int slot = sor2d_wavefront(q, nSOR, ring, ru, rv);
+                du = ru[slot];
+                dv = rv[slot];
+                continue;
+            }
+            const double omega = 1.8;
             bool converged = false;
             for (int k = 0; k < nSOR && !converged; k++) {
                 double maxDiff = 0;
@@ -1007,7 +1093,7 @@ static void smooth_flow_sor(const Img& Im1, const Img& Im2, Img& warpIm2, std::v
  * resized from the coarser level and scaled by 1 / ratio, the warp, SmoothFlowSOR with
  * nOuter + k outer and nSOR + 3 k SOR iterations at level k. */
 void coarse2fine_flow(const Img& im1, const Img& im2, double alpha, double ratio, int min_width, int nOuter, int nInner,
-                      int nSOR, std::vector<double>& u, std::vector<double>& v)
+                      int nSOR, std::vector<double>& u, std::vector<double>& v, int ring = 0)
 {
     std::vector<Img> p1, p2;
     build_pyramid(im1, ratio, min_width, p1);
@@ -1036,7 +1122,7 @@ void coarse2fine_flow(const Img& im1, const Img& im2, double alpha, double ratio
             for (auto& x : v) x *= s;
             warp_fl(f1, f2, u, v, warp);
         }
-        smooth_flow_sor(f1, f2, warp, u, v, alpha, nOuter + k, nInner, nSOR + k * 3, lap);
+        smooth_flow_sor(f1, f2, warp, u, v, alpha, nOuter + k, nInner, nSOR + k * 3, lap, ring);
     }
 }
 
@@ -1276,8 +1362,18 @@ int sfo_scene_flow_two_frames(int fp64, const rgbdflow_camera_params* camFull, c
 /* 2-D optical flow of two BGR8 images (the demo's flow type 1, runFlowTwoFramesCeLiu,
  * src/runFlowTwoFrames.cpp:30-45): colour / 255 as cv2liuBGR (src/ceLiuOpticalFlow.cpp:19-37),
  * then Coarse2FineFlow with the given parameters.  u, v: W*H doubles. */
+int sfo_optical_flow_2d_ring(const uint8_t* bgr1, const uint8_t* bgr2, int W, int H, double alpha, double ratio,
+                             int min_width, int n_outer, int n_inner, int n_sor, int ring, double* u, double* v);
 int sfo_optical_flow_2d(const uint8_t* bgr1, const uint8_t* bgr2, int W, int H, double alpha, double ratio,
                         int min_width, int n_outer, int n_inner, int n_sor, double* u, double* v)
+{
+    return sfo_optical_flow_2d_ring(bgr1, bgr2, W, H, alpha, ratio, min_width, n_outer, n_inner, n_sor, 0, u, v);
+}
+
+/* sfo_optical_flow_2d with the SOR iterations in the device order of sor2d_wavefront (ring > 0
+ * slots), or the reference's lexicographic order (ring 0). */
+int sfo_optical_flow_2d_ring(const uint8_t* bgr1, const uint8_t* bgr2, int W, int H, double alpha, double ratio,
+                             int min_width, int n_outer, int n_inner, int n_sor, int ring, double* u, double* v)
 {
     try {
         Img I1, I2;
@@ -1285,7 +1381,7 @@ int sfo_optical_flow_2d(const uint8_t* bgr1, const uint8_t* bgr2, int W, int H, 
         I2.alloc(W, H, 3);
         for (size_t z = 0; z < (size_t)W * H * 3; z++) { I1.d[z] = bgr1[z] / 255.0; I2.d[z] = bgr2[z] / 255.0; }
         std::vector<double> uu, vv;
-        coarse2fine_flow(I1, I2, alpha, ratio, min_width, n_outer, n_inner, n_sor, uu, vv);
+        coarse2fine_flow(I1, I2, alpha, ratio, min_width, n_outer, n_inner, n_sor, uu, vv, ring);
         std::memcpy(u, uu.data(), sizeof(double) * uu.size());
         std::memcpy(v, vv.data(), sizeof(double) * vv.size());
         return 0;

@@ -79,6 +79,7 @@ def oracle():
         lib.sfo_scene_flow_two_frames.argtypes = [_i, ctypes.c_void_p, _pu8, _pf, _pu8, _pf, _i, _i,
                                                   ctypes.c_void_p, _pf, _pf, ctypes.c_void_p]
         lib.sfo_optical_flow_2d.argtypes = [_pu8, _pu8, _i, _i, _d, _d, _i, _i, _i, _i, _pd, _pd]
+        lib.sfo_optical_flow_2d_ring.argtypes = [_pu8, _pu8, _i, _i, _d, _d, _i, _i, _i, _i, _i, _pd, _pd]
         lib.sfo_last_error.restype = ctypes.c_char_p
         lib.sfo_set_threads.argtypes = [_i]
         _oracle = lib
@@ -139,10 +140,12 @@ def ref_flow2d():
 
 
 def optical_flow_2d(bgr1, bgr2, alpha=0.02, ratio=0.75, min_width=20, n_outer=10, n_inner=1, n_sor=400,
-                    impl="oracle"):
+                    impl="oracle", ring=0):
     """2-D optical flow (u, v) of two (H, W, 3) uint8 BGR images: the demo's flow type 1 with its
     defaults (runFlowTwoFramesCeLiu, src/runFlowTwoFrames.cpp:30-45; opticalFlowParams ratio
-    0.75, minWidth 20).  impl "oracle" (the restatement) or "ref" (the reference, compiled)."""
+    0.75, minWidth 20).  impl "oracle" (the restatement) or "ref" (the reference, compiled).
+    ring > 0 (oracle only): the SOR iterations in the device order, anti-diagonal wavefronts
+    with overlapping sweeps and a ring of that many slots."""
     b1, b2 = _cont(bgr1, np.uint8), _cont(bgr2, np.uint8)
     H, W = b1.shape[:2]
     u = np.zeros((H, W)); v = np.zeros((H, W))
@@ -154,8 +157,8 @@ def optical_flow_2d(bgr1, bgr2, alpha=0.02, ratio=0.75, min_width=20, n_outer=10
         if rc != 0:
             raise RuntimeError("reference Coarse2FineFlow: " + err.value.decode())
     else:
-        rc = oracle().sfo_optical_flow_2d(u8ptr(b1), u8ptr(b2), W, H, alpha, ratio, min_width, n_outer, n_inner, n_sor,
-                                          dptr(u), dptr(v))
+        rc = oracle().sfo_optical_flow_2d_ring(u8ptr(b1), u8ptr(b2), W, H, alpha, ratio, min_width, n_outer, n_inner,
+                                               n_sor, ring, dptr(u), dptr(v))
         if rc != 0:
             raise RuntimeError("oracle 2-D flow: " + oracle().sfo_last_error().decode())
     return u, v

@@ -7,7 +7,11 @@ src/SmoothFlowSOR.cpp), pinned against the reference's own code:
     on more seeded cases: bit-identical;
   * known answers: identical frames give exactly zero flow; a smooth texture moved by (1.5, 0.5)
     px is recovered to 0.02 px on average away from the borders.
-The reference's 2-D solve is FP64 with a lexicographic SOR order, and so is the restatement."""
+The reference's 2-D solve is FP64 with a lexicographic SOR order, and so is the restatement.
+The order a device can run in parallel and still match the reference, is checked too. It sweeps
+anti-diagonal wavefronts, overlaps consecutive sweeps and keeps a ring of D flow-increment slots.
+It must equal the lexicographic order bit for bit, including on a scene where a red-black order
+moves the flow by more than a pixel."""
 import os
 
 import numpy as np
@@ -61,3 +65,20 @@ def test_translation_is_recovered():
     g = np.load(GOLDEN)
     u, v = ob.optical_flow_2d(g["shift_bgr1"], g["shift_bgr2"], **_golden_params().PARAMS["shift"])
     assert abs(u[8:-8, 8:-8].mean() - 1.5) < 0.02 and abs(v[8:-8, 8:-8].mean() - 0.5) < 0.02
+
+
+@pytest.mark.parametrize("ring", [2, 3, 8])
+def test_wavefront_order_equals_lexicographic(ring):
+    g = np.load(GOLDEN)
+    prm = _golden_params().PARAMS
+    for tag in ("shift", "patch"):
+        u0, v0 = ob.optical_flow_2d(g[tag + "_bgr1"], g[tag + "_bgr2"], **prm[tag])
+        u1, v1 = ob.optical_flow_2d(g[tag + "_bgr1"], g[tag + "_bgr2"], ring=ring, **prm[tag])
+        np.testing.assert_array_equal(u1, u0)
+        np.testing.assert_array_equal(v1, v0)
+    # a scene where a red-black sweep order moves the reference's flow by 1.2 px on average
+    p = syn.make_config_pair("160x120", seed=1)
+    u0, v0 = ob.optical_flow_2d(p["bgr1"], p["bgr2"])
+    u1, v1 = ob.optical_flow_2d(p["bgr1"], p["bgr2"], ring=ring)
+    np.testing.assert_array_equal(u1, u0)
+    np.testing.assert_array_equal(v1, v0)
