@@ -355,6 +355,32 @@ int rgbdflow_scene_flow_noalloc(const rgbdflow_pair* pair, const rgbdflow_params
                                 char* err, size_t err_len);
 
 /* ---------------------------------------------------------------------------------------------
+ * 2-D optical flow: the reference demo's flow type 1, Ce Liu's coarse-to-fine solver
+ * (runFlowTwoFramesCeLiu, src/runFlowTwoFrames.cpp:30-45 -> OpticalFlow::Coarse2FineFlow,
+ * src/opticalFlowMultiscale.cpp, with SmoothFlowSOR, src/SmoothFlowSOR.cpp).  The device solve
+ * keeps the reference's FP64 arithmetic, operation order and lexicographic SOR order, so its flow
+ * equals the reference's.  Its SOR runs as overlapping anti-diagonal sweeps in one thread block
+ * per inner iteration, with sor_ring sweeps in flight.
+ * ------------------------------------------------------------------------------------------- */
+typedef struct rgbdflow_flow2d_params {
+    double alpha;          /* smoothness weight (the demo's -s, 0.02) */
+    double pyramid_ratio;  /* (0.75) */
+    int    min_width;      /* (20) */
+    int    n_outer;        /* outer fixed-point iterations at the finest level, + k at level k (10) */
+    int    n_inner;        /* (1) */
+    int    n_sor;          /* SOR iterations at the finest level, + 3 k at level k (400) */
+    int    sor_ring;       /* SOR sweeps in flight, 2..16 (8); the result does not depend on it */
+} rgbdflow_flow2d_params;
+
+/* The demo's values for flow type 1 (runFlowTwoFramesCeLiu, opticalFlowParams). */
+void rgbdflow_flow2d_params_default(rgbdflow_flow2d_params* p);
+/* Host buffers (BGR8, W*H*3 each), synchronous.  flow_out: W*H*2 floats (u, v in pixels), the
+ * reference's cv::Vec2f result (liu2cvFlow2d).  alpha < 0: RGBDFLOW_ERR_INVALID_ARG (the
+ * reference asserts alpha >= 0). */
+int rgbdflow_optical_flow_2d(rgbdflow_ctx* ctx, const uint8_t* bgr1, const uint8_t* bgr2, int W, int H,
+                             const rgbdflow_flow2d_params* params, float* flow_out);
+
+/* ---------------------------------------------------------------------------------------------
  * .flo3 scene-flow files: readSceneFlow / writeSceneFlow (src/sceneFlowIO.cpp:18-61), the format
  * the reference's demo writes its result in (src/main.cpp:126).  Layout: the 8 bytes
  * 237 159 43 26 202 94 218 68, int32 width, int32 height, then width*height (u, v, w) float32

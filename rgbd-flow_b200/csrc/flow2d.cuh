@@ -1,0 +1,364 @@
+// flow2d.cuh — 2-D optical flow on the device: Ce Liu's coarse-to-fine solver, the reference
+// demo's flow type 1 (OpticalFlow::Coarse2FineFlow, src/opticalFlowMultiscale.cpp:4-146, with
+// OpticalFlow::SmoothFlowSOR, src/SmoothFlowSOR.cpp:8-247).
+//
+// The reference's solver is numerically fragile (lexicographic SOR with omega 1.8): reordering
+// its sweep changes the result by pixels on ordinary scenes.  So this solve keeps the
+// reference's arithmetic exactly: FP64, every operation rounded on its own (explicit __d*_rn
+// intrinsics, no fused multiply-adds), the reference's operation order, and its lexicographic
+// SOR order.  The SOR runs as anti-diagonal wavefronts: pixel (i, j) needs new values only from
+// diagonal i + j - 1 of its own sweep and old values from diagonal i + j + 1 of the previous
+// one, so one diagonal is a parallel step.  Consecutive sweeps overlap, each starting two steps
+// after the previous one; sweep s writes ring slot s % D and reads the previous sweep from slot
+// (s - 1) % D, and starts only after sweep s - D has finished without converging, so the slot of
+// the sweep that converges is never overwritten.
+//
+// Data: planar FP64 per level; colour pyramids 3 channels interleaved (as DImage), features 5
+// channels interleaved.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <vector>
+
+namespace rgbdflow {
+namespace f2d {
+
+constexpr int kThreads = 256;
+constexpr int kSorThreads = 1024;
+constexpr int kMaxRing = 16;
+constexpr int kMaxTaps = 64;
+
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double ddiv(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ int clampi(int x, int n) { return min(max(x, 0), n - 1); }
+// std::max(a, b) of the C++ library: (a < b) ? b : a (a NaN b is dropped, a NaN a is kept)
+__device__ __forceinline__ double cmax(double a, double b) { return (a < b) ? b : a; }
+
+// ImageProcessing::BilinearInterpolate, accumulating form (ImageProcessing.h:128-148)
+__device__ __forceinline__ void bilinear_acc(const double* img, int W, int H, int C, double x, double y, double* out)
+{
+    const int xx = (int)x, yy = (int)y;
+    double dx = dsub(x, (double)xx);
+    if (dx > 1) dx = 1;
+    if (dx < 0) dx = 0;
+    double dy = dsub(y, (double)yy);
+    if (dy > 1) dy = 1;
+    if (dy < 0) dy = 0;
+    for (int m = 0; m <= 1; m++)
+        for (int n = 0; n <= 1; n++) {
+            const int u = clampi(xx + m, W), v = clampi(yy + n, H);
+            const size_t off = ((size_t)v * W + u) * C;
+            const double s = dmul(fabs(dsub((double)(1 - m), dx)), fabs(dsub((double)(1 - n), dy)));
+            for (int l = 0; l < C; l++) out[l] = dadd(out[l], dmul(img[off + l], s));
+        }
+}
+
+// colour / 255 (cv2liuBGR, src/ceLiuOpticalFlow.cpp:19-37)
+__global__ void k_unpack(const uint8_t* __restrict__ bgr, double* __restrict__ out, size_t n)
+{
+    for (size_t z = blockIdx.x * (size_t)blockDim.x + threadIdx.x; z < n; z += (size_t)gridDim.x * blockDim.x)
+        out[z] = ddiv((double)bgr[z], 255.0);
+}
+
+// ImageProcessing::hfiltering / vfiltering with clamp-to-edge (ImageProcessing.h:247-269, 339-358)
+__global__ void k_hfilter(const double* __restrict__ in, double* __restrict__ out, int W, int H, int C,
+                          const double* __restrict__ taps, int fs)
+{
+    const size_t n = (size_t)W * H;
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(p / W), j = (int)(p % W);
+        for (int k = 0; k < C; k++) {
+            double acc = 0;
+            for (int l = -fs; l <= fs; l++)
+                acc = dadd(acc, dmul(in[((size_t)i * W + clampi(j + l, W)) * C + k], taps[l + fs]));
+            out[p * C + k] = acc;
+        }
+    }
+}
+__global__ void k_vfilter(const double* __restrict__ in, double* __restrict__ out, int W, int H, int C,
+                          const double* __restrict__ taps, int fs)
+{
+    const size_t n = (size_t)W * H;
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(p / W), j = (int)(p % W);
+        for (int k = 0; k < C; k++) {
+            double acc = 0;
+            for (int l = -fs; l <= fs; l++)
+                acc = dadd(acc, dmul(in[((size_t)clampi(i + l, H) * W + j) * C + k], taps[l + fs]));
+            out[p * C + k] = acc;
+        }
+    }
+}
+
+// ImageProcessing::ResizeImage (ImageProcessing.h:203-242): dst (j, i) samples src at
+// ((j + 1) / xr - 1, (i + 1) / yr - 1)
+__global__ void k_resize(const double* __restrict__ in, int W, int H, int C, double* __restrict__ out, int DW, int DH,
+                         double xr, double yr)
+{
+    const size_t n = (size_t)DW * DH;
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(p / DW), j = (int)(p % DW);
+        double acc[5] = {0, 0, 0, 0, 0};
+        const double x = dsub(ddiv((double)(j + 1), xr), 1.0), y = dsub(ddiv((double)(i + 1), yr), 1.0);
+        bilinear_acc(in, W, H, C, x, y, acc);
+        for (int k = 0; k < C; k++) out[p * C + k] = acc[k];
+    }
+}
+
+// Image::desaturate (Image.h:1438-1469): .114 B + .587 G + .299 R, channels in BGR order
+__device__ __forceinline__ double gray_at(const double* im, size_t p)
+{
+    return dadd(dadd(dmul(im[p * 3], .114), dmul(im[p * 3 + 1], .587)), dmul(im[p * 3 + 2], .299));
+}
+
+// OpticalFlow::im2feature RGB_WITH_GRADIENT (OpticalFlow.cpp:189-214): gray, its 5-tap dx, dy,
+// G - B, G - R
+__global__ void k_features(const double* __restrict__ im, double* __restrict__ feat, int W, int H,
+                           const double* __restrict__ d5)
+{
+    const size_t n = (size_t)W * H;
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(p / W), j = (int)(p % W);
+        double gx = 0, gy = 0;
+        for (int l = -2; l <= 2; l++) gx = dadd(gx, dmul(gray_at(im, (size_t)i * W + clampi(j + l, W)), d5[l + 2]));
+        for (int l = -2; l <= 2; l++) gy = dadd(gy, dmul(gray_at(im, (size_t)clampi(i + l, H) * W + j), d5[l + 2]));
+        feat[p * 5 + 0] = gray_at(im, p);
+        feat[p * 5 + 1] = gx;
+        feat[p * 5 + 2] = gy;
+        feat[p * 5 + 3] = dsub(im[p * 3 + 1], im[p * 3]);
+        feat[p * 5 + 4] = dsub(im[p * 3 + 1], im[p * 3 + 2]);
+    }
+}
+
+// x *= s (Image::Multiplywith, Image.h:1778-1782)
+__global__ void k_scale(double* __restrict__ x, size_t n, double s)
+{
+    for (size_t z = blockIdx.x * (size_t)blockDim.x + threadIdx.x; z < n; z += (size_t)gridDim.x * blockDim.x)
+        x[z] = dmul(x[z], s);
+}
+
+// warpFL, bilinear (src/opticalFlowUtils.cpp:62-67; ImageProcessing::warpImage,
+// ImageProcessing.h:472-491): Im2 at (j + u, i + v), Im1 where that falls outside
+__global__ void k_warp(const double* __restrict__ f1, const double* __restrict__ f2, const double* __restrict__ u,
+                       const double* __restrict__ v, double* __restrict__ out, int W, int H)
+{
+    const size_t n = (size_t)W * H;
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(p / W), j = (int)(p % W);
+        const double x = dadd((double)j, u[p]), y = dadd((double)i, v[p]);
+        double acc[5] = {0, 0, 0, 0, 0};
+        if (x < 0 || x > W - 1 || y < 0 || y > H - 1) {
+            for (int k = 0; k < 5; k++) acc[k] = f1[p * 5 + k];
+        } else {
+            bilinear_acc(f2, W, H, 5, x, y, acc);
+        }
+        for (int k = 0; k < 5; k++) out[p * 5 + k] = acc[k];
+    }
+}
+
+// One level's per-iteration state.
+struct LevelBufs {
+    const double *f1, *f2;  // features of frames 1 and 2 (5 channels)
+    double* warp;           // frame 2 features warped by the flow (5 channels)
+    double *u, *v, *du, *dv, *phi;
+    double *dxy, *dx2, *dy2, *dtdx, *dtdy;
+    int W, H;
+};
+
+// 0.4 Im1 + 0.6 warp at pixel p, channel k (getDxs, src/opticalFlowUtils.cpp:33-37)
+__device__ __forceinline__ double mix_at(const LevelBufs& b, size_t p, int k)
+{
+    return dadd(dmul(b.f1[p * 5 + k], 0.4), dmul(b.warp[p * 5 + k], 0.6));
+}
+
+// SmoothFlowSOR.cpp:52-139 for one inner iteration: the flow gradient weight phi of u + du
+// (forward differences, Image::dx/dy, Image.h:955-1019), and the robust data weights psi of the
+// derivatives of getDxs (5-tap dx, dy of 0.4 Im1 + 0.6 warp, dt = warp - Im1), multiplied out
+// and averaged over the channels (Image::Multiply, Image::collapse).  first: the inner
+// iteration's uu is u itself.
+// eps: pow(0.001, 2) as the host's pow computes it (SmoothFlowSOR.cpp:30-31).
+__global__ void k_phi_psi(LevelBufs b, const double* __restrict__ d5, int first, double eps)
+{
+    const int W = b.W, H = b.H;
+    const size_t n = (size_t)W * H;
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(p / W), j = (int)(p % W);
+        auto uu = [&](size_t q) { return first ? b.u[q] : dadd(b.u[q], b.du[q]); };
+        auto vv = [&](size_t q) { return first ? b.v[q] : dadd(b.v[q], b.dv[q]); };
+        const double ux = (j < W - 1) ? dsub(uu(p + 1), uu(p)) : 0.0;
+        const double uy = (i < H - 1) ? dsub(uu(p + W), uu(p)) : 0.0;
+        const double vx = (j < W - 1) ? dsub(vv(p + 1), vv(p)) : 0.0;
+        const double vy = (i < H - 1) ? dsub(vv(p + W), vv(p)) : 0.0;
+        const double t = dadd(dadd(dadd(dmul(ux, ux), dmul(uy, uy)), dmul(vx, vx)), dmul(vy, vy));
+        b.phi[p] = ddiv(0.5, __dsqrt_rn(dadd(t, eps)));
+        const double du = first ? 0.0 : b.du[p], dv = first ? 0.0 : b.dv[p];
+        double sxy = 0, sx2 = 0, sy2 = 0, stx = 0, sty = 0;
+        for (int k = 0; k < 5; k++) {
+            double ix = 0, iy = 0;
+            for (int l = -2; l <= 2; l++) ix = dadd(ix, dmul(mix_at(b, (size_t)i * W + clampi(j + l, W), k), d5[l + 2]));
+            for (int l = -2; l <= 2; l++) iy = dadd(iy, dmul(mix_at(b, (size_t)clampi(i + l, H) * W + j, k), d5[l + 2]));
+            const double it = dsub(b.warp[p * 5 + k], b.f1[p * 5 + k]);
+            double r = dadd(dadd(it, dmul(ix, du)), dmul(iy, dv));
+            r = dmul(r, r);
+            const double psi = ddiv(1.0, dmul(2.0, __dsqrt_rn(dadd(r, eps))));
+            sxy = dadd(sxy, dmul(dmul(psi, ix), iy));
+            sx2 = dadd(sx2, dmul(dmul(psi, ix), ix));
+            sy2 = dadd(sy2, dmul(dmul(psi, iy), iy));
+            stx = dadd(stx, dmul(dmul(psi, ix), it));
+            sty = dadd(sty, dmul(dmul(psi, iy), it));
+        }
+        b.dxy[p] = ddiv(sxy, 5.0);
+        b.dx2[p] = ddiv(sx2, 5.0);
+        b.dy2[p] = ddiv(sy2, 5.0);
+        b.dtdx[p] = ddiv(stx, 5.0);
+        b.dtdy[p] = ddiv(sty, 5.0);
+    }
+}
+
+// Laplacian with normalising weights (src/opticalFlowUtils.cpp:252-313) of x at pixel (i, j),
+// weighted by the 1-channel phi read as a 2-channel image, as SmoothFlowSOR.cpp:144 calls it:
+// channel k of (i, j) is element i * W + j + k (Image::operator(), Image.h:76).
+__device__ __forceinline__ double laplacian_phi(const double* x, const double* phi, int W, int H, int i, int j)
+{
+    const size_t o = (size_t)i * W + j;
+    double out = 0;
+    if (j < W - 1) out = dsub(out, dmul(dsub(x[o + 1], x[o]), phi[o]));
+    if (j > 0) out = dadd(out, dmul(dsub(x[o], x[o - 1]), phi[o - 1]));
+    if (i < H - 1) out = dsub(out, dmul(dsub(x[o + W], x[o]), phi[o + 1]));
+    if (i > 0) out = dadd(out, dmul(dsub(x[o], x[o - W]), phi[o - W + 1]));
+    double norm = 0;
+    int count = 0;
+    if (j < W - 1) { norm = dadd(norm, phi[o]); count++; }
+    if (j > 0) { norm = dadd(norm, phi[o - 1]); count++; }
+    if (i < H - 1) { norm = dadd(norm, phi[o + 1]); count++; }
+    if (i > 0) { norm = dadd(norm, phi[o - W + 1]); count++; }
+    if (fabs(norm) < 1e-5) return 0;
+    return ddiv(out, ddiv(norm, (double)count));
+}
+
+// The right-hand sides (SmoothFlowSOR.cpp:144-151): -Itx - alpha * Lap(u), -Ity - alpha * Lap(v)
+__global__ void k_rhs(LevelBufs b, double alpha)
+{
+    const int W = b.W, H = b.H;
+    const size_t n = (size_t)W * H;
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(p / W), j = (int)(p % W);
+        b.dtdx[p] = dsub(-b.dtdx[p], dmul(alpha, laplacian_phi(b.u, b.phi, W, H, i, j)));
+        b.dtdy[p] = dsub(-b.dtdy[p], dmul(alpha, laplacian_phi(b.v, b.phi, W, H, i, j)));
+    }
+}
+
+// One SOR update (SmoothFlowSOR.cpp:166-215) of pixel (i, j): left / upper neighbours new
+// (nu, nv), right / lower neighbours and the pixel itself old (ou, ov); returns the change.
+__device__ __forceinline__ double sor_update(const LevelBufs& b, double alpha, int i, int j, const double* nu,
+                                             const double* nv, const double* ou, const double* ov, double* wu,
+                                             double* wv)
+{
+    const int W = b.W, H = b.H;
+    const size_t o = (size_t)i * W + j;
+    const double omega = 1.8;
+    double sigmaU = 0, sigmaV = 0, weightSum = 0, w;
+    if (j > 0) { w = b.phi[o - 1]; sigmaU = dadd(sigmaU, dmul(w, nu[o - 1])); sigmaV = dadd(sigmaV, dmul(w, nv[o - 1])); weightSum = dadd(weightSum, w); }
+    if (j < W - 1) { w = b.phi[o]; sigmaU = dadd(sigmaU, dmul(w, ou[o + 1])); sigmaV = dadd(sigmaV, dmul(w, ov[o + 1])); weightSum = dadd(weightSum, w); }
+    if (i > 0) { w = b.phi[o - W]; sigmaU = dadd(sigmaU, dmul(w, nu[o - W])); sigmaV = dadd(sigmaV, dmul(w, nv[o - W])); weightSum = dadd(weightSum, w); }
+    if (i < H - 1) { w = b.phi[o]; sigmaU = dadd(sigmaU, dmul(w, ou[o + W])); sigmaV = dadd(sigmaV, dmul(w, ov[o + W])); weightSum = dadd(weightSum, w); }
+    sigmaU = dmul(sigmaU, -alpha);
+    sigmaV = dmul(sigmaV, -alpha);
+    weightSum = dmul(weightSum, alpha);
+    const double prevDU = ou[o], prevDV = ov[o];
+    sigmaU = dadd(sigmaU, dmul(b.dxy[o], prevDV));
+    const double nDU = dadd(dmul(1 - omega, prevDU), dmul(ddiv(omega, dadd(b.dx2[o], weightSum)), dsub(b.dtdx[o], sigmaU)));
+    sigmaV = dadd(sigmaV, dmul(b.dxy[o], nDU));
+    const double nDV = dadd(dmul(1 - omega, prevDV), dmul(ddiv(omega, dadd(b.dy2[o], weightSum)), dsub(b.dtdy[o], sigmaV)));
+    wu[o] = nDU;
+    wv[o] = nDV;
+    return cmax(fabs(dsub(nDU, prevDU)), fabs(dsub(nDV, prevDV)));
+}
+
+// The SOR iterations of one inner iteration (SmoothFlowSOR.cpp:156-226) as overlapping
+// anti-diagonal sweeps, one CTA.  ring: D slots of (u, v) increments, each N doubles.  Leaves the
+// last sweep's increments (the first that converged, max change < 1e-5, or sweep nSOR - 1) in
+// (du, dv) and the number of sweeps run in *sweeps.  status: 0, or 1 when the step bound ran out.
+__global__ void __launch_bounds__(kSorThreads) k_sor_wavefront(LevelBufs b, double alpha, int nSOR, int D,
+                                                               double* ring_u, double* ring_v, int* sweeps, int* status)
+{
+    const int W = b.W, H = b.H, ndiag = W + H - 1, lag = 2;
+    const size_t N = (size_t)W * H;
+    __shared__ long long start[kMaxRing];
+    __shared__ unsigned long long maxd[kMaxRing];
+    __shared__ int s_done, s_stop, s_next;
+    for (size_t p = threadIdx.x; p < N; p += blockDim.x) {
+        ring_u[(size_t)(D - 1) * N + p] = 0;
+        ring_v[(size_t)(D - 1) * N + p] = 0;
+    }
+    if (threadIdx.x == 0) { s_done = -1; s_stop = -1; s_next = 0; }
+    __syncthreads();
+    // every sweep takes ndiag steps and starts within ndiag + lag steps of the previous one
+    const long long t_max = (long long)nSOR * (ndiag + lag) + ndiag + 8;
+    long long t = 0;
+    for (; t < t_max; t++) {
+        if (threadIdx.x == 0) {
+            const int nx = s_next;
+            if (nx < nSOR && (nx == 0 || t >= start[(nx - 1) % D] + lag) && (nx < D || s_done >= nx - D)) {
+                start[nx % D] = t;
+                maxd[nx % D] = 0ull;
+                s_next = nx + 1;
+            }
+        }
+        __syncthreads();
+        const int done = s_done, next = s_next;
+        if (s_stop >= 0 || done >= nSOR - 1) break;
+        for (int s = done + 1; s < next; s++) {
+            const long long d = t - start[s % D];
+            if (d < 0 || d >= ndiag) continue;
+            const int cur = s % D, prv = (s + D - 1) % D;
+            const double* nu = ring_u + (size_t)cur * N;
+            const double* nv = ring_v + (size_t)cur * N;
+            const double* ou = ring_u + (size_t)prv * N;
+            const double* ov = ring_v + (size_t)prv * N;
+            double* wu = ring_u + (size_t)cur * N;
+            double* wv = ring_v + (size_t)cur * N;
+            const int i0 = (int)max(0LL, d - (W - 1)), i1 = (int)min((long long)H - 1, d);
+            for (int i = i0 + threadIdx.x; i <= i1; i += blockDim.x) {
+                const double m = sor_update(b, alpha, i, (int)(d - i), nu, nv, ou, ov, wu, wv);
+                if (m == m) atomicMax(&maxd[s % D], (unsigned long long)__double_as_longlong(m));  // NaN is skipped, as std::max skips it
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            while (s_done + 1 < s_next && t - start[(s_done + 1) % D] == ndiag - 1) {
+                s_done++;
+                if (__longlong_as_double((long long)maxd[s_done % D]) < 1e-5) {
+                    s_stop = s_done;
+                    break;
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        *sweeps = s_done + 1;
+        if (t >= t_max) *status = 1;
+    }
+    const int last = (s_stop >= 0 ? s_stop : nSOR - 1) % D;
+    for (size_t p = threadIdx.x; p < N; p += blockDim.x) {
+        b.du[p] = ring_u[(size_t)last * N + p];
+        b.dv[p] = ring_v[(size_t)last * N + p];
+    }
+}
+
+// u += du, v += dv (Image::Add, SmoothFlowSOR.cpp:227-228)
+__global__ void k_update(LevelBufs b)
+{
+    const size_t n = (size_t)b.W * b.H;
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
+        b.u[p] = dadd(b.u[p], b.du[p]);
+        b.v[p] = dadd(b.v[p], b.dv[p]);
+    }
+}
+
+}  // namespace f2d
+}  // namespace rgbdflow

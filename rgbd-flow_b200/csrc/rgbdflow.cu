@@ -17,6 +17,7 @@
 #include "pipeline.cuh"
 #include "server.cuh"
 #include "flo3.h"
+#include "flow2d.cuh"
 
 using namespace rgbdflow;
 
@@ -487,6 +488,195 @@ static bool prepare_dispatch(rgbdflow_ctx* c, const std::vector<PairSpec>& ps, c
     return prepare_batch<float, float>(c, ps, hp, 0);
 }
 
+// Taps of Image::GaussianSmoothing (Image.h:1179-1199): exp(-i^2 / 2 sigma^2), normalised.
+static std::vector<double> gauss_taps(double sigma, int fsize)
+{
+    std::vector<double> g(2 * fsize + 1);
+    double sum = 0;
+    const double s2 = sigma * sigma * 2;
+    for (int i = -fsize; i <= fsize; i++) {
+        g[i + fsize] = std::exp(-(double)(i * i) / s2);
+        sum += g[i + fsize];
+    }
+    for (auto& x : g) x /= sum;
+    return g;
+}
+
+// The 2-D optical flow of one pair (Coarse2FineFlow, src/opticalFlowMultiscale.cpp:4-146, CELIU
+// variant, no depth maps) on the context's stream; synchronous.
+static void run_flow2d(rgbdflow_ctx* c, const uint8_t* bgr1, const uint8_t* bgr2, int W, int H,
+                       const rgbdflow_flow2d_params& prm, float* flow_out)
+{
+    using namespace rgbdflow::f2d;
+    if (!bgr1 || !bgr2 || !flow_out || W < 2 || H < 2) throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "bad frame");
+    if (!(prm.alpha >= 0)) throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "alpha must be >= 0");
+    if (prm.n_outer < 0 || prm.n_inner < 1 || prm.n_sor < 1 || prm.sor_ring < 2 || prm.sor_ring > kMaxRing)
+        throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "n_inner and n_sor must be >= 1, sor_ring in 2..16");
+    // pyramid geometry (GaussianPyramid::ConstructPyramid, GaussianPyramid.cpp:20-63)
+    double ratio = prm.pyramid_ratio;
+    if (ratio > 0.98 || ratio < 0.4) ratio = 0.75;
+    int L = 1;
+    for (double w = W * ratio; w >= prm.min_width; w *= ratio) L++;
+    const double baseSigma = (1 / ratio - 1);
+    const int nsm = (int)(std::log(0.25) / std::log(ratio));
+    const double nSigma = baseSigma * nsm;
+    struct Lev {
+        int w, h, src, fs;
+        double sigma, rate;
+        size_t taps_off;
+    };
+    std::vector<Lev> lev(L);
+    std::vector<double> taps = {1, -8, 0, 8, -1};
+    for (auto& t : taps) t /= 12;
+    lev[0] = {W, H, -1, 0, 0, 1, 0};
+    for (int i = 1; i < L; i++) {
+        Lev& l = lev[i];
+        if (i <= nsm) {
+            l.sigma = baseSigma * i;
+            l.src = 0;
+            l.rate = std::pow(ratio, i);
+            l.w = (int)((double)W * l.rate);
+            l.h = (int)((double)H * l.rate);
+        } else {
+            l.sigma = nSigma;
+            l.src = i - nsm;
+            l.rate = (double)std::pow(ratio, i) * W / lev[l.src].w;
+            l.w = (int)((double)lev[l.src].w * l.rate);
+            l.h = (int)((double)lev[l.src].h * l.rate);
+        }
+        l.fs = (int)(l.sigma * 3);
+        if (2 * l.fs + 1 > rgbdflow::f2d::kMaxTaps) throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "pyramid filter too wide");
+        l.taps_off = taps.size();
+        const std::vector<double> g = gauss_taps(l.sigma, l.fs);
+        taps.insert(taps.end(), g.begin(), g.end());
+        if (l.w < 1 || l.h < 1) throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "pyramid level below one pixel");
+    }
+    // one stream-ordered allocation, carved
+    const size_t N0 = (size_t)W * H;
+    size_t total = 0;
+    auto reserve = [&](size_t bytes) { const size_t o = total; total += align_up(bytes, 256); return o; };
+    const size_t o_bgr = reserve(N0 * 6);
+    const size_t o_taps = reserve(taps.size() * sizeof(double));
+    const size_t o_ctl = reserve(2 * sizeof(int));
+    std::vector<size_t> o_img[2], o_feat[2], o_u(L), o_v(L);
+    for (int f = 0; f < 2; f++)
+        for (int i = 0; i < L; i++) {
+            o_img[f].push_back(reserve((size_t)lev[i].w * lev[i].h * 3 * sizeof(double)));
+            o_feat[f].push_back(reserve((size_t)lev[i].w * lev[i].h * 5 * sizeof(double)));
+        }
+    for (int i = 0; i < L; i++) {
+        o_u[i] = reserve((size_t)lev[i].w * lev[i].h * sizeof(double));
+        o_v[i] = reserve((size_t)lev[i].w * lev[i].h * sizeof(double));
+    }
+    const size_t o_tmpA = reserve(N0 * 3 * sizeof(double)), o_tmpB = reserve(N0 * 3 * sizeof(double));
+    const size_t o_warp = reserve(N0 * 5 * sizeof(double));
+    size_t o_plane[8];
+    for (auto& o : o_plane) o = reserve(N0 * sizeof(double));
+    const size_t o_ring_u = reserve((size_t)prm.sor_ring * N0 * sizeof(double));
+    const size_t o_ring_v = reserve((size_t)prm.sor_ring * N0 * sizeof(double));
+    if (c->budget && total > c->budget) throw ArgError(RGBDFLOW_ERR_BUDGET, "2-D flow needs " + std::to_string(total) + " device bytes");
+    RF_CUDA(cudaSetDevice(c->device));
+    cudaStream_t st = c->stream;
+    if (c->pending) RF_CUDA(cudaStreamWaitEvent(st, c->done, 0));
+    char* base = nullptr;
+    RF_CUDA(cudaMallocAsync((void**)&base, total, st));
+    struct Free {
+        char* p;
+        cudaStream_t s;
+        ~Free() { if (p) { cudaFreeAsync(p, s); cudaStreamSynchronize(s); } }
+    } release{base, st};
+    auto D = [&](size_t o) { return (double*)(base + o); };
+    int* ctl = (int*)(base + o_ctl);
+    uint8_t* dbgr = (uint8_t*)(base + o_bgr);
+    RF_CUDA(cudaMemcpyAsync(dbgr, bgr1, N0 * 3, cudaMemcpyHostToDevice, st));
+    RF_CUDA(cudaMemcpyAsync(dbgr + N0 * 3, bgr2, N0 * 3, cudaMemcpyHostToDevice, st));
+    RF_CUDA(cudaMemcpyAsync(D(o_taps), taps.data(), taps.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+    RF_CUDA(cudaMemsetAsync(ctl, 0, 2 * sizeof(int), st));
+    const double* d5 = D(o_taps);
+    int launches = 0;
+    auto grid = [&](size_t n) { return (int)std::max<size_t>(1, std::min<size_t>((n + kThreads - 1) / kThreads, (size_t)c->sms * 8)); };
+    for (int f = 0; f < 2; f++) {
+        k_unpack<<<grid(N0 * 3), kThreads, 0, st>>>(dbgr + f * N0 * 3, D(o_img[f][0]), N0 * 3);
+        launches++;
+        for (int i = 1; i < L; i++) {
+            const Lev& l = lev[i];
+            const int sw = lev[l.src].w, sh = lev[l.src].h;
+            const size_t sn = (size_t)sw * sh;
+            k_hfilter<<<grid(sn), kThreads, 0, st>>>(D(o_img[f][l.src]), D(o_tmpA), sw, sh, 3, D(o_taps) + l.taps_off, l.fs);
+            k_vfilter<<<grid(sn), kThreads, 0, st>>>(D(o_tmpA), D(o_tmpB), sw, sh, 3, D(o_taps) + l.taps_off, l.fs);
+            k_resize<<<grid((size_t)l.w * l.h), kThreads, 0, st>>>(D(o_tmpB), sw, sh, 3, D(o_img[f][i]), l.w, l.h, l.rate, l.rate);
+            launches += 3;
+        }
+        for (int i = 0; i < L; i++) {
+            k_features<<<grid((size_t)lev[i].w * lev[i].h), kThreads, 0, st>>>(D(o_img[f][i]), D(o_feat[f][i]), lev[i].w, lev[i].h, d5);
+            launches++;
+        }
+    }
+    const double eps = std::pow(0.001, 2);
+    for (int k = L - 1; k >= 0; k--) {
+        const int w = lev[k].w, h = lev[k].h;
+        const size_t n = (size_t)w * h;
+        LevelBufs b;
+        b.f1 = D(o_feat[0][k]);
+        b.f2 = D(o_feat[1][k]);
+        b.warp = D(o_warp);
+        b.u = D(o_u[k]);
+        b.v = D(o_v[k]);
+        b.du = D(o_plane[0]);
+        b.dv = D(o_plane[1]);
+        b.phi = D(o_plane[2]);
+        b.dxy = D(o_plane[3]);
+        b.dx2 = D(o_plane[4]);
+        b.dy2 = D(o_plane[5]);
+        b.dtdx = D(o_plane[6]);
+        b.dtdy = D(o_plane[7]);
+        b.W = w;
+        b.H = h;
+        if (k == L - 1) {
+            RF_CUDA(cudaMemsetAsync(b.u, 0, n * sizeof(double), st));
+            RF_CUDA(cudaMemsetAsync(b.v, 0, n * sizeof(double), st));
+            RF_CUDA(cudaMemcpyAsync(b.warp, b.f2, n * 5 * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        } else {
+            // the coarser flow resized (Image::imresize(w, h)) and scaled by 1 / ratio, then the warp
+            const int pw = lev[k + 1].w, ph = lev[k + 1].h;
+            const double xr = (double)w / pw, yr = (double)h / ph;
+            k_resize<<<grid(n), kThreads, 0, st>>>(D(o_u[k + 1]), pw, ph, 1, b.u, w, h, xr, yr);
+            k_resize<<<grid(n), kThreads, 0, st>>>(D(o_v[k + 1]), pw, ph, 1, b.v, w, h, xr, yr);
+            const double s = 1 / prm.pyramid_ratio;
+            k_scale<<<grid(n), kThreads, 0, st>>>(b.u, n, s);
+            k_scale<<<grid(n), kThreads, 0, st>>>(b.v, n, s);
+            k_warp<<<grid(n), kThreads, 0, st>>>(b.f1, b.f2, b.u, b.v, b.warp, w, h);
+            launches += 5;
+        }
+        const int nOuter = prm.n_outer + k, nSOR = prm.n_sor + k * 3;
+        for (int count = 0; count < nOuter; count++) {
+            for (int hh = 0; hh < prm.n_inner; hh++) {
+                k_phi_psi<<<grid(n), kThreads, 0, st>>>(b, d5, hh == 0 ? 1 : 0, eps);
+                k_rhs<<<grid(n), kThreads, 0, st>>>(b, prm.alpha);
+                k_sor_wavefront<<<1, kSorThreads, 0, st>>>(b, prm.alpha, nSOR, prm.sor_ring, D(o_ring_u), D(o_ring_v),
+                                                           ctl + 1, ctl);
+                launches += 3;
+            }
+            k_update<<<grid(n), kThreads, 0, st>>>(b);
+            k_warp<<<grid(n), kThreads, 0, st>>>(b.f1, b.f2, b.u, b.v, b.warp, w, h);
+            launches += 2;
+        }
+    }
+    RF_CUDA(cudaGetLastError());
+    std::vector<double> u(N0), v(N0);
+    int hctl[2] = {0, 0};
+    RF_CUDA(cudaMemcpyAsync(u.data(), D(o_u[0]), N0 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    RF_CUDA(cudaMemcpyAsync(v.data(), D(o_v[0]), N0 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    RF_CUDA(cudaMemcpyAsync(hctl, ctl, sizeof(hctl), cudaMemcpyDeviceToHost, st));
+    RF_CUDA(cudaStreamSynchronize(st));
+    c->last_launches = launches;
+    if (hctl[0]) throw ArgError(RGBDFLOW_ERR_INTERNAL, "2-D SOR ran out of its step bound");
+    for (size_t z = 0; z < N0; z++) {
+        flow_out[z * 2] = (float)u[z];
+        flow_out[z * 2 + 1] = (float)v[z];
+    }
+}
+
 static int fail(rgbdflow_ctx* c, int code, const std::string& m)
 {
     if (c) c->err = m;
@@ -827,6 +1017,30 @@ int rgbdflow_ctx_synchronize(rgbdflow_ctx* c)
 }
 
 int rgbdflow_ctx_last_launch_count(const rgbdflow_ctx* c) { return c ? c->last_launches : 0; }
+
+void rgbdflow_flow2d_params_default(rgbdflow_flow2d_params* p)
+{
+    if (!p) return;
+    // runFlowTwoFramesCeLiu (src/runFlowTwoFrames.cpp:36-41) with the demo's smoothness weight
+    // (main.cpp:57) and opticalFlowParams' pyramid (OpticalFlow.h:54)
+    p->alpha = 0.02;
+    p->pyramid_ratio = 0.75;
+    p->min_width = 20;
+    p->n_outer = 10;
+    p->n_inner = 1;
+    p->n_sor = 400;
+    p->sor_ring = 8;
+}
+
+int rgbdflow_optical_flow_2d(rgbdflow_ctx* c, const uint8_t* bgr1, const uint8_t* bgr2, int W, int H,
+                             const rgbdflow_flow2d_params* params, float* flow_out)
+{
+    if (!c || !params) return RGBDFLOW_ERR_INVALID_ARG;
+    API_BEGIN
+    run_flow2d(c, bgr1, bgr2, W, H, *params, flow_out);
+    return RGBDFLOW_OK;
+    API_END(c)
+}
 
 int rgbdflow_profile(rgbdflow_ctx* c, int enable)
 {

@@ -145,6 +145,13 @@ class Result(ctypes.Structure):
                 ("done_time_s", ctypes.c_double), ("status", ctypes.c_int)]
 
 
+class Flow2dParams(ctypes.Structure):
+    """rgbdflow_flow2d_params: the 2-D optical flow's parameters (the demo's flow type 1)."""
+    _fields_ = [("alpha", ctypes.c_double), ("pyramid_ratio", ctypes.c_double), ("min_width", ctypes.c_int),
+                ("n_outer", ctypes.c_int), ("n_inner", ctypes.c_int), ("n_sor", ctypes.c_int),
+                ("sor_ring", ctypes.c_int)]
+
+
 class ServerCounters(ctypes.Structure):
     _fields_ = [("frames_allocated", ctypes.c_uint64), ("graphs_built", ctypes.c_uint64),
                 ("arena_grows", ctypes.c_uint64), ("launches", ctypes.c_uint64),
@@ -191,6 +198,8 @@ SIGNATURES = {
     "rgbdflow_server_pending": (_i, [_vp]),
     "rgbdflow_server_counters_read": (_i, [_vp, _i, _P(ServerCounters)]),
     "rgbdflow_scene_flow_noalloc": (_i, [_P(RgbdFlowPair), _P(Params), _vp, ctypes.c_char_p, ctypes.c_size_t]),
+    "rgbdflow_flow2d_params_default": (None, [_P(Flow2dParams)]),
+    "rgbdflow_optical_flow_2d": (_i, [_vp, _vp, _vp, _i, _i, _P(Flow2dParams), _vp]),
     "rgbdflow_flo3_write": (_i, [ctypes.c_char_p, _vp, _i, _i, ctypes.c_char_p, ctypes.c_size_t]),
     "rgbdflow_flo3_read": (_i, [ctypes.c_char_p, _vp, ctypes.c_size_t, _P(_i), _P(_i), ctypes.c_char_p,
                                 ctypes.c_size_t]),
@@ -243,6 +252,16 @@ def batch_device_bytes(sizes, params, warm=None):
     if rc != OK:
         raise RgbdFlowError(rc, "rgbdflow_batch_device_bytes failed")
     return out.value
+
+
+def flow2d_params(**over):
+    """rgbdflow_flow2d_params_default (the demo's flow type 1: alpha 0.02, ratio 0.75, minWidth 20,
+    10 outer, 1 inner, 400 SOR iterations) with the given fields replaced.  Host-only."""
+    p = Flow2dParams()
+    load().rgbdflow_flow2d_params_default(ctypes.byref(p))
+    for k, v in over.items():
+        setattr(p, k, v)
+    return p
 
 
 def write_flo3(path, flow):
@@ -329,6 +348,18 @@ class Context:
 
     def device_bytes(self):
         return self.lib.rgbdflow_ctx_device_bytes(self.h)
+
+    def optical_flow_2d(self, bgr1, bgr2, params=None):
+        """2-D optical flow (the reference demo's flow type 1; rgbdflow_optical_flow_2d) of two
+        (H, W, 3) uint8 BGR frames: (H, W, 2) float32 (u, v in pixels)."""
+        b1, b2 = _c(bgr1, np.uint8), _c(bgr2, np.uint8)
+        H, W = b1.shape[:2]
+        if b2.shape != b1.shape or b1.ndim != 3 or b1.shape[2] != 3:
+            raise RgbdFlowError(-1, "frames must be two (H, W, 3) uint8 images of one size")
+        out = np.empty((H, W, 2), np.float32)
+        p = params if params is not None else flow2d_params()
+        self._check(self.lib.rgbdflow_optical_flow_2d(self.h, _ptr(b1), _ptr(b2), W, H, ctypes.byref(p), _ptr(out)))
+        return out
 
     def scene_flow_two_frames(self, cam, bgr1, depth1, bgr2, depth2, params, est_flow=None, stats=True):
         bgr1, bgr2 = _c(bgr1, np.uint8), _c(bgr2, np.uint8)

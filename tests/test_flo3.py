@@ -101,3 +101,11 @@ def test_read_reports_the_size_and_checks_the_buffer(tmp_path):
     rc = lib.rgbdflow_flo3_read(g.OUT.encode(), small.ctypes.data, small.size, ctypes.byref(W), ctypes.byref(H),
                                 err, len(err))
     assert rc == -1 and b"fewer" in err.value
+
+
+def test_flow2d_defaults_are_the_demos():
+    """rgbdflow_flow2d_params_default (host-only): runFlowTwoFramesCeLiu's iterations
+    (src/runFlowTwoFrames.cpp:36-41), the demo's smoothness weight and opticalFlowParams' pyramid."""
+    p = rf.flow2d_params()
+    assert (p.alpha, p.pyramid_ratio, p.min_width, p.n_outer, p.n_inner, p.n_sor) == (0.02, 0.75, 20, 10, 1, 400)
+    assert 2 <= p.sor_ring <= 16
