@@ -395,6 +395,14 @@ int rgbdflow_flo3_write(const char* path, const float* flow, int W, int H, char*
  * magic number or a size below 1: RGBDFLOW_ERR_FORMAT.  Bytes after the last value are ignored. */
 int rgbdflow_flo3_read(const char* path, float* flow, size_t n_floats, int* W, int* H, char* err, size_t err_len);
 
+/* Middlebury .flo 2-D flow files: readFlow / writeFlow (src/middleburyFlowIO.cpp:15-65), the
+ * format the reference's demo writes 2-D flows in (src/main.cpp:125).  Layout: the 4 bytes "PIEH"
+ * (the float 202021.25), int32 width, int32 height, then width*height (u, v) float32 pairs, rows
+ * top to bottom, little-endian.  Host-only; arguments, sizes and failures as the .flo3 calls, with
+ * W*H*2 values. */
+int rgbdflow_flo_write(const char* path, const float* flow, int W, int H, char* err, size_t err_len);
+int rgbdflow_flo_read(const char* path, float* flow, size_t n_floats, int* W, int* H, char* err, size_t err_len);
+
 #ifdef __cplusplus
 }
 #endif

@@ -77,4 +77,44 @@ inline void flo3_read(const char* path, float* flow, size_t n_floats, int* W, in
     if (std::fread(flow, 4, n, f.get()) != n) throw Flo3Error{RGBDFLOW_ERR_IO, "can't read pixel values for flow image"};
 }
 
+// Middlebury .flo, the format the reference's demo writes 2-D flows in (readFlow / writeFlow,
+// src/middleburyFlowIO.cpp:15-65; src/main.cpp:125): the 4 bytes "PIEH" (read back as the float
+// 202021.25), int32 width, int32 height, then width * height (u, v) float32 pairs, rows top to
+// bottom, little-endian; failures classed as for .flo3.
+constexpr unsigned char kFloTag[4] = {'P', 'I', 'E', 'H'};
+
+inline void flo_write(const char* path, const float* flow, int W, int H)
+{
+    if (!path || !flow || W < 1 || H < 1) throw Flo3Error{RGBDFLOW_ERR_INVALID_ARG, "flo write: bad arguments"};
+    FILE* raw = std::fopen(path, "wb");
+    if (!raw) throw Flo3Error{RGBDFLOW_ERR_IO, std::string("can't open ") + path + " for writing"};
+    File f(raw);
+    const int32_t wh[2] = {W, H};
+    if (std::fwrite(kFloTag, 1, 4, f.get()) != 4 || std::fwrite(wh, 4, 2, f.get()) != 2)
+        throw Flo3Error{RGBDFLOW_ERR_IO, "can't write metadata for flow image"};
+    const size_t n = (size_t)W * H * 2;
+    if (std::fwrite(flow, 4, n, f.get()) != n) throw Flo3Error{RGBDFLOW_ERR_IO, "can't write pixel values for flow image"};
+    if (std::fclose(f.release()) != 0) throw Flo3Error{RGBDFLOW_ERR_IO, "can't write pixel values for flow image"};
+}
+
+inline void flo_read(const char* path, float* flow, size_t n_floats, int* W, int* H)
+{
+    if (!path || !W || !H) throw Flo3Error{RGBDFLOW_ERR_INVALID_ARG, "flo read: bad arguments"};
+    FILE* raw = std::fopen(path, "rb");
+    if (!raw) throw Flo3Error{RGBDFLOW_ERR_IO, std::string("can't open ") + path};
+    File f(raw);
+    unsigned char tag[4];
+    int32_t wh[2];
+    if (std::fread(tag, 1, 4, f.get()) != 4 || std::fread(wh, 4, 2, f.get()) != 2)
+        throw Flo3Error{RGBDFLOW_ERR_IO, "can't read metadata for flow image"};
+    if (std::memcmp(tag, kFloTag, 4) != 0) throw Flo3Error{RGBDFLOW_ERR_FORMAT, "magic number doesn't match .flo format"};
+    if (wh[0] < 1 || wh[1] < 1) throw Flo3Error{RGBDFLOW_ERR_FORMAT, "flo size below 1"};
+    *W = wh[0];
+    *H = wh[1];
+    if (!flow) return;
+    const size_t n = (size_t)wh[0] * wh[1] * 2;
+    if (n_floats < n) throw Flo3Error{RGBDFLOW_ERR_INVALID_ARG, "flo read: the buffer holds fewer than W*H*2 floats"};
+    if (std::fread(flow, 4, n, f.get()) != n) throw Flo3Error{RGBDFLOW_ERR_IO, "can't read pixel values for flow image"};
+}
+
 }  // namespace rgbdflow

@@ -1623,3 +1623,30 @@ extern "C" int rgbdflow_flo3_read(const char* path, float* flow, size_t n_floats
         return noalloc_fail(err, err_len, RGBDFLOW_ERR_INTERNAL, "unknown error");
     }
 }
+
+extern "C" int rgbdflow_flo_write(const char* path, const float* flow, int W, int H, char* err, size_t err_len)
+{
+    if (err && err_len) err[0] = 0;
+    try {
+        flo_write(path, flow, W, H);
+        return RGBDFLOW_OK;
+    } catch (const Flo3Error& e) {
+        return noalloc_fail(err, err_len, e.code, e.msg);
+    } catch (...) {
+        return noalloc_fail(err, err_len, RGBDFLOW_ERR_INTERNAL, "unknown error");
+    }
+}
+
+extern "C" int rgbdflow_flo_read(const char* path, float* flow, size_t n_floats, int* W, int* H, char* err,
+                                 size_t err_len)
+{
+    if (err && err_len) err[0] = 0;
+    try {
+        flo_read(path, flow, n_floats, W, H);
+        return RGBDFLOW_OK;
+    } catch (const Flo3Error& e) {
+        return noalloc_fail(err, err_len, e.code, e.msg);
+    } catch (...) {
+        return noalloc_fail(err, err_len, RGBDFLOW_ERR_INTERNAL, "unknown error");
+    }
+}

@@ -203,6 +203,9 @@ SIGNATURES = {
     "rgbdflow_flo3_write": (_i, [ctypes.c_char_p, _vp, _i, _i, ctypes.c_char_p, ctypes.c_size_t]),
     "rgbdflow_flo3_read": (_i, [ctypes.c_char_p, _vp, ctypes.c_size_t, _P(_i), _P(_i), ctypes.c_char_p,
                                 ctypes.c_size_t]),
+    "rgbdflow_flo_write": (_i, [ctypes.c_char_p, _vp, _i, _i, ctypes.c_char_p, ctypes.c_size_t]),
+    "rgbdflow_flo_read": (_i, [ctypes.c_char_p, _vp, ctypes.c_size_t, _P(_i), _P(_i), ctypes.c_char_p,
+                               ctypes.c_size_t]),
 }
 
 
@@ -264,33 +267,51 @@ def flow2d_params(**over):
     return p
 
 
+def _write_flow_file(fn, path, flow, C):
+    flow = np.ascontiguousarray(flow, dtype=np.float32)
+    if flow.ndim != 3 or flow.shape[2] != C:
+        raise RgbdFlowError(-1, "flow must be (H, W, %d)" % C)
+    err = ctypes.create_string_buffer(512)
+    rc = fn(os.fsencode(path), _ptr(flow), flow.shape[1], flow.shape[0], err, len(err))
+    if rc != OK:
+        raise RgbdFlowError(rc, err.value.decode())
+
+
+def _read_flow_file(fn, path, C):
+    err = ctypes.create_string_buffer(512)
+    W, H = ctypes.c_int(), ctypes.c_int()
+    rc = fn(os.fsencode(path), None, 0, ctypes.byref(W), ctypes.byref(H), err, len(err))
+    if rc != OK:
+        raise RgbdFlowError(rc, err.value.decode())
+    flow = np.empty((H.value, W.value, C), np.float32)
+    rc = fn(os.fsencode(path), _ptr(flow), flow.size, ctypes.byref(W), ctypes.byref(H), err, len(err))
+    if rc != OK:
+        raise RgbdFlowError(rc, err.value.decode())
+    return flow
+
+
 def write_flo3(path, flow):
     """Write an (H, W, 3) float32 flow (u px, v px, w m) as a .flo3 file (rgbdflow_flo3_write;
     writeSceneFlow, src/sceneFlowIO.cpp:49-61).  Host-only."""
-    flow = np.ascontiguousarray(flow, dtype=np.float32)
-    if flow.ndim != 3 or flow.shape[2] != 3:
-        raise RgbdFlowError(-1, "flow must be (H, W, 3)")
-    err = ctypes.create_string_buffer(512)
-    rc = load().rgbdflow_flo3_write(os.fsencode(path), _ptr(flow), flow.shape[1], flow.shape[0], err, len(err))
-    if rc != OK:
-        raise RgbdFlowError(rc, err.value.decode())
+    _write_flow_file(load().rgbdflow_flo3_write, path, flow, 3)
 
 
 def read_flo3(path):
     """Read a .flo3 file into an (H, W, 3) float32 array (rgbdflow_flo3_read; readSceneFlow,
     src/sceneFlowIO.cpp:23-44).  Host-only."""
-    lib = load()
-    err = ctypes.create_string_buffer(512)
-    W, H = ctypes.c_int(), ctypes.c_int()
-    rc = lib.rgbdflow_flo3_read(os.fsencode(path), None, 0, ctypes.byref(W), ctypes.byref(H), err, len(err))
-    if rc != OK:
-        raise RgbdFlowError(rc, err.value.decode())
-    flow = np.empty((H.value, W.value, 3), np.float32)
-    rc = lib.rgbdflow_flo3_read(os.fsencode(path), _ptr(flow), flow.size, ctypes.byref(W), ctypes.byref(H), err,
-                                len(err))
-    if rc != OK:
-        raise RgbdFlowError(rc, err.value.decode())
-    return flow
+    return _read_flow_file(load().rgbdflow_flo3_read, path, 3)
+
+
+def write_flo(path, flow):
+    """Write an (H, W, 2) float32 2-D flow as a Middlebury .flo file (rgbdflow_flo_write; writeFlow,
+    src/middleburyFlowIO.cpp:50-65).  Host-only."""
+    _write_flow_file(load().rgbdflow_flo_write, path, flow, 2)
+
+
+def read_flo(path):
+    """Read a Middlebury .flo file into an (H, W, 2) float32 array (rgbdflow_flo_read; readFlow,
+    src/middleburyFlowIO.cpp:22-44).  Host-only."""
+    return _read_flow_file(load().rgbdflow_flo_read, path, 2)
 
 
 def scene_flow_noalloc(pair, params, stream=None):

@@ -1,16 +1,20 @@
 """Command-line equivalent of the reference's demo driver rgbdFlowTest (src/main.cpp).
 
 It reads two RGB-D frames: a colour PNG and an 8- or 16-bit depth PNG in millimetres for each.
-It halves both frames as the demo does "for speed" and solves the forward scene flow on the GPU.
+It halves both frames as the demo does "for speed" and solves the forward flow on the GPU.
 It can also solve the backward flow.  In the output directory it writes:
-  flow0.flo3          the forward flow (u, v in pixels, w in metres, at the halved size);
-  flow0bkwd.flo3      the backward flow, with --run-bkwd 1;
-  fwd-img1.png        frame 1 as solved (halved);
-  fwd-img2sampled.png frame 2 sampled at each pixel of frame 1 moved by its flow.
+  flow0.flo3 / flow0.flo       the forward flow at the halved size: scene flow (u, v in pixels,
+                               w in metres; -t 6) or 2-D flow in the Middlebury format (-t 1);
+  flow0bkwd.flo3 / flow0bkwd.flo   the backward flow, with --run-bkwd 1;
+  fwd-img1.png                 frame 1 as solved (halved);
+  fwd-img2sampled.png          frame 2 sampled at each pixel of frame 1 moved by its flow.
 
 Options, as in main.cpp:53-66:
   -i/--image1, -d/--depth1, -j/--image2, -e/--depth2   the two frames
-  -t/--flow-type                6 = RGB-D scene flow.  The 2-D flow types 1 and 2 are not built.
+  -t/--flow-type                6 = RGB-D scene flow; 1 = Ce Liu's 2-D optical flow on the
+                                colour frames (runFlowTwoFramesCeLiu), which uses only -s.
+                                Type 2 (2-D flow on the depth maps) stops at an assertion in the
+                                reference (im2feature has no 1-channel form) and is rejected.
   -s/--smoothness-weight        default 0.02
   -v/--depth-vs-color-data-weight   default 1
   -z/--regularization-type      0 isotropic, 1 Letouzey, 2 HPB (default, as in the reference).
@@ -23,7 +27,10 @@ KINECT_640_DEFAULT), src/primesensorUtils.cpp:26-34).  The solve rescales it to 
 as runFlowTwoFramesSceneFlowExperiments does.
 
 Image IO, the colour halving (cv::resize) and the debug image's sub-pixel sampling
-(cv::getRectSubPix) go through OpenCV's Python module (cv2), as the demo's do.
+(cv::getRectSubPix) go through OpenCV's Python module (cv2), as the demo's do.  For a 2-D flow the
+debug image samples at (j + u, i + v); the reference reads its 2-D flow there with the stride of
+a 3-channel image (flow.at<cv::Vec3f> on a cv::Vec2f matrix, main.cpp:136), which this does not
+reproduce.
 
 Run: python rgbd-flow_b200/rgbdflow_demo.py -i a.png -d a_depth.png -j b.png -e b_depth.png -t 6 -z 0 -o out
 """
@@ -87,14 +94,21 @@ def downsize_frame(img, depth):
 
 def sample_along_flow(img2, flow):
     """The demo's fwd-img2sampled image (main.cpp:131-139): at every pixel (i, j), frame 2 sampled
-    at (j + u, i + v) with cv::getRectSubPix over a 1x1 patch."""
+    at (j + u, i + v) with cv::getRectSubPix over a 1x1 patch.  getRectSubPix replicates the border
+    outside the image and is undefined for non-finite points (it crashes on some): a pixel whose
+    point is not finite is black, and a point more than 4 pixels outside the image is moved to 4
+    pixels outside, where it samples the same replicated border pixels."""
     cv2 = _cv2()
     H, W = flow.shape[:2]
-    out = np.empty((H, W, img2.shape[2]), np.uint8)
+    h2, w2 = img2.shape[:2]
+    out = np.zeros((H, W, img2.shape[2]), np.uint8)
     for i in range(H):
         for j in range(W):
-            f = flow[i, j]
-            out[i, j] = cv2.getRectSubPix(img2, (1, 1), (float(j + f[0]), float(i + f[1])))[0, 0]
+            x, y = float(j + flow[i, j, 0]), float(i + flow[i, j, 1])
+            if not (math.isfinite(x) and math.isfinite(y)):
+                continue
+            x, y = min(max(x, -4.0), w2 + 3.0), min(max(y, -4.0), h2 + 3.0)
+            out[i, j] = cv2.getRectSubPix(img2, (1, 1), (x, y))[0, 0]
     return out
 
 
@@ -115,7 +129,8 @@ def parse_args(argv=None):
     ap.add_argument("-d", "--depth1", required=True, help="depth image 1 (16-bit png, depth in mm)")
     ap.add_argument("-j", "--image2", required=True, help="color image 2")
     ap.add_argument("-e", "--depth2", required=True, help="depth image 2 (16-bit png, depth in mm)")
-    ap.add_argument("-t", "--flow-type", type=int, required=True, help="6 = RGB-D scene flow")
+    ap.add_argument("-t", "--flow-type", type=int, required=True,
+                    help="6 = RGB-D scene flow; 1 = Ce Liu's 2-D optical flow")
     ap.add_argument("-s", "--smoothness-weight", type=float, default=.02)
     ap.add_argument("-v", "--depth-vs-color-data-weight", type=float, default=1.0)
     ap.add_argument("-z", "--regularization-type", type=int, default=2,
@@ -124,24 +139,35 @@ def parse_args(argv=None):
     ap.add_argument("--run-bkwd", type=int, default=0, help="whether to run backward flow")
     ap.add_argument("-o", "--outdir", required=True)
     a = ap.parse_args(argv)
-    if a.flow_type != 6:
-        ap.error("flow type %d is not built: only 6 (RGB-D scene flow)" % a.flow_type)
+    if a.flow_type == 2:
+        ap.error("flow type 2 (2-D flow on depth maps) stops at an assertion in the reference: "
+                 "im2feature has no 1-channel RGB_WITH_GRADIENT form")
+    if a.flow_type not in (1, 6):
+        ap.error("flow type %d is not built: 1 (2-D optical flow) and 6 (RGB-D scene flow) are" % a.flow_type)
     return a
 
 
 def run(args, solve=None):
     """The demo's main (main.cpp:68-150).  solve(cam, bgr1, depth1, bgr2, depth2, params) -> (H, W, 3)
-    flow; default: a Context's scene_flow_two_frames on device 0."""
+    scene flow (-t 6) or (H, W, 2) 2-D flow (-t 1, params an rgbdflow.Flow2dParams); default: a
+    Context's scene_flow_two_frames or optical_flow_2d on device 0."""
     cv2 = _cv2()
     os.makedirs(args.outdir, exist_ok=True)
     cam = kinect_640_camera()
-    prm = make_params(args.smoothness_weight, args.depth_vs_color_data_weight, args.regularization_type)
+    scene = args.flow_type == 6
+    if scene:
+        prm = make_params(args.smoothness_weight, args.depth_vs_color_data_weight, args.regularization_type)
+    else:
+        prm = rf.flow2d_params(alpha=args.smoothness_weight)  # runFlowTwoFramesCeLiu (runFlowTwoFrames.cpp:30-45)
+    ext, write = (".flo3", rf.write_flo3) if scene else (".flo", rf.write_flo)
     ctx = None
     if solve is None:
         ctx = rf.Context(0)
 
         def solve(c, b1, d1, b2, d2, p):
-            return ctx.scene_flow_two_frames(c, b1, d1, b2, d2, p, stats=False)
+            if scene:
+                return ctx.scene_flow_two_frames(c, b1, d1, b2, d2, p, stats=False)
+            return ctx.optical_flow_2d(b1, b2, p)
     try:
         prev_img, cur_img = read_color_png(args.image1), read_color_png(args.image2)
         prev_depth, cur_depth = read_depth_png(args.depth1), read_depth_png(args.depth2)
@@ -152,8 +178,8 @@ def run(args, solve=None):
             t = time.perf_counter()
             flow = solve(cam, prev_img, prev_depth, cur_img, cur_depth, prm)
             print("time to call runFlowTwoFrames: %gs" % (time.perf_counter() - t))
-            path = os.path.join(args.outdir, "flow0.flo3")
-            rf.write_flo3(path, flow)
+            path = os.path.join(args.outdir, "flow0" + ext)
+            write(path, flow)
             cv2.imwrite(os.path.join(args.outdir, "fwd-img1.png"), prev_img)
             cv2.imwrite(os.path.join(args.outdir, "fwd-img2sampled.png"), sample_along_flow(cur_img, flow))
             written += [path, os.path.join(args.outdir, "fwd-img1.png"), os.path.join(args.outdir, "fwd-img2sampled.png")]
@@ -161,8 +187,8 @@ def run(args, solve=None):
             t = time.perf_counter()
             flow = solve(cam, cur_img, cur_depth, prev_img, prev_depth, prm)
             print("time to call runFlowTwoFrames: %gs" % (time.perf_counter() - t))
-            path = os.path.join(args.outdir, "flow0bkwd.flo3")
-            rf.write_flo3(path, flow)
+            path = os.path.join(args.outdir, "flow0bkwd" + ext)
+            write(path, flow)
             written.append(path)
         return written
     finally:

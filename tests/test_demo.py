@@ -101,9 +101,40 @@ def test_forward_only_by_default_and_flow_types(tmp_path):
     solve = RecordingSolve()
     written = demo.run(a, solve=solve)
     assert len(solve.calls) == 1 and not any(w.endswith("bkwd.flo3") for w in written)
-    for t in ("1", "2", "7"):
+    for t in ("2", "3", "7"):
         with pytest.raises(SystemExit):
             demo.parse_args(["-i", "a", "-d", "b", "-j", "c", "-e", "d", "-t", t, "-o", "x"])
+
+
+class Recording2d(RecordingSolve):
+    """The 2-D flow's stand-in: (H, W, 2) flow."""
+
+    def __call__(self, cam, b1, d1, b2, d2, prm):
+        self.calls.append(types.SimpleNamespace(b1=b1.copy(), b2=b2.copy(), prm=prm))
+        flow = np.empty(d1.shape + (2,), np.float32)
+        flow[...] = self.uvw[:2]
+        return flow
+
+
+def test_cli_2d_flow_type(tmp_path):
+    """-t 1: Ce Liu's 2-D flow on the halved colour frames with alpha = -s, written as Middlebury
+    .flo (flow0.flo, flow0bkwd.flo), and the same debug images."""
+    _, paths = _write_frames(tmp_path, seed=6)
+    out = tmp_path / "o2"
+    solve = Recording2d(u=-0.5, v=2.25)
+    argv = ["-i", paths["image1"], "-d", paths["depth1"], "-j", paths["image2"], "-e", paths["depth2"],
+            "-t", "1", "-s", "0.03", "--run-bkwd", "1", "-o", str(out)]
+    written = demo.run(demo.parse_args(argv), solve=solve)
+    assert sorted(os.path.basename(w) for w in written) == ["flow0.flo", "flow0bkwd.flo", "fwd-img1.png",
+                                                           "fwd-img2sampled.png"]
+    fwd, bkwd = solve.calls
+    assert fwd.prm.alpha == 0.03 and (fwd.prm.n_outer, fwd.prm.n_sor) == (10, 400)
+    np.testing.assert_array_equal(fwd.b1, cv2.resize(cv2.imread(paths["image1"]), (320, 240)))
+    np.testing.assert_array_equal(bkwd.b1, fwd.b2)
+    flow = rf.read_flo(str(out / "flow0.flo"))
+    assert flow.shape == (240, 320, 2) and np.all(flow == np.float32([-0.5, 2.25]))
+    sampled = cv2.imread(str(out / "fwd-img2sampled.png"))
+    np.testing.assert_array_equal(sampled[100, 100], cv2.getRectSubPix(fwd.b2, (1, 1), (99.5, 102.25))[0, 0])
 
 
 def test_depth_png_must_be_single_channel(tmp_path):
@@ -128,3 +159,48 @@ def test_cli_flow_equals_the_library_solve(tmp_path, ctx):
                                        stats=False)
     assert flow.shape == (240, 320, 3) and np.isfinite(flow).all()
     np.testing.assert_array_equal(flow, direct)
+
+
+def _write_textured_shift(tmp_path):
+    """A smooth random texture moved by (3, 1) px, 144x112 (72x56 once halved), with a flat depth:
+    a well-posed 2-D flow (on the synthetic patch scenes the reference's 2-D solver diverges)."""
+    rng = np.random.default_rng(12)
+    t = rng.random((140, 172, 3))
+    for _ in range(3):
+        t = sum(np.roll(np.roll(t, dy, 0), dx, 1) for dy in range(-2, 3) for dx in range(-2, 3)) / 25
+    t = (t - t.min()) / (t.max() - t.min()) * 255
+    paths = {}
+    for k, (dy, dx) in (("1", (0, 0)), ("2", (1, 3))):
+        img = np.rint(np.roll(np.roll(t, dy, 0), dx, 1)[14:126, 14:158]).astype(np.uint8)
+        paths["image" + k] = str(tmp_path / ("t%s.png" % k))
+        paths["depth" + k] = str(tmp_path / ("td%s.png" % k))
+        cv2.imwrite(paths["image" + k], img)
+        cv2.imwrite(paths["depth" + k], np.full(img.shape[:2], 1500, np.uint16))
+    return paths
+
+
+def test_debug_image_survives_non_finite_and_far_points():
+    img = np.arange(4 * 5 * 3, dtype=np.uint8).reshape(4, 5, 3)
+    flow = np.zeros((4, 5, 2), np.float32)
+    flow[0, 0] = (np.nan, 0)
+    flow[1, 1] = (1e30, -1e30)
+    flow[2, 2] = (-3e9, 0.25)
+    out = demo.sample_along_flow(img, flow)
+    assert not out[0, 0].any()
+    np.testing.assert_array_equal(out[1, 1], cv2.getRectSubPix(img, (1, 1), (4 + 3.0, -4.0))[0, 0])
+    np.testing.assert_array_equal(out[2, 2], cv2.getRectSubPix(img, (1, 1), (-4.0, 2.25))[0, 0])
+    np.testing.assert_array_equal(out[3, 4], img[3, 4])
+
+
+@pytest.mark.gpu
+def test_cli_2d_flow_equals_the_library_solve(tmp_path, ctx):
+    paths = _write_textured_shift(tmp_path)
+    out = tmp_path / "o"
+    demo.run(demo.parse_args(["-i", paths["image1"], "-d", paths["depth1"], "-j", paths["image2"], "-e",
+                              paths["depth2"], "-t", "1", "-o", str(out)]))
+    b1, _ = demo.downsize_frame(demo.read_color_png(paths["image1"]), demo.read_depth_png(paths["depth1"]))
+    b2, _ = demo.downsize_frame(demo.read_color_png(paths["image2"]), demo.read_depth_png(paths["depth2"]))
+    flow = rf.read_flo(str(out / "flow0.flo"))
+    assert flow.shape == (56, 72, 2) and np.isfinite(flow).all()
+    assert abs(flow[8:-8, 8:-8, 0].mean() - 1.5) < 0.1 and abs(flow[8:-8, 8:-8, 1].mean() - 0.5) < 0.1
+    np.testing.assert_array_equal(flow, ctx.optical_flow_2d(b1, b2))

@@ -109,3 +109,34 @@ def test_flow2d_defaults_are_the_demos():
     p = rf.flow2d_params()
     assert (p.alpha, p.pyramid_ratio, p.min_width, p.n_outer, p.n_inner, p.n_sor) == (0.02, 0.75, 20, 10, 1, 400)
     assert 2 <= p.sor_ring <= 16
+
+
+def test_middlebury_flo_golden_both_ways(tmp_path):
+    """Middlebury .flo (rgbdflow_flo_read / rgbdflow_flo_write; readFlow / writeFlow,
+    src/middleburyFlowIO.cpp): the golden file reads back bit for bit and is rewritten byte for
+    byte; its tag reads as the float 202021.25 the reference checks."""
+    g = _golden_module()
+    data = open(g.FLO_OUT, "rb").read()
+    assert np.frombuffer(data[:4], "<f4")[0] == np.float32(202021.25)
+    flow = rf.read_flo(g.FLO_OUT)
+    assert flow.shape == (g.H, g.W, 2)
+    np.testing.assert_array_equal(_bits(flow), _bits(g.VALUES[..., :2]))
+    out = tmp_path / "w.flo"
+    rf.write_flo(str(out), g.VALUES[..., :2])
+    assert out.read_bytes() == data == g.encode_flo(g.VALUES)
+
+
+def test_middlebury_flo_errors(tmp_path):
+    g = _golden_module()
+    good = g.encode_flo(g.VALUES)
+    assert _code(rf.read_flo, str(tmp_path / "missing.flo")) == -9
+    p = tmp_path / "short.flo"
+    p.write_bytes(good[:-1])
+    assert _code(rf.read_flo, str(p)) == -9
+    p = tmp_path / "tag.flo"
+    p.write_bytes(b"PIEX" + good[4:])
+    assert _code(rf.read_flo, str(p)) == -10
+    p = tmp_path / "flo3_as_flo.flo"
+    p.write_bytes(g.encode(g.VALUES))
+    assert _code(rf.read_flo, str(p)) == -10
+    assert _code(rf.write_flo, str(tmp_path / "bad.flo"), g.VALUES) == -1
