@@ -794,6 +794,70 @@ void multiscale(const rgbdflow_camera_params& cam, const rgbdflow_params& p, con
 
 using namespace sfo;
 
+/* DepthMapPyramid::ConstructPyramid (src/depthMapPyramid.cpp:15-91), the raw-depth pyramid the
+ * HPB regularisation reads (sceneFlowMultiscale.cpp:82): values <= 0 are invalid and stay -1;
+ * a valid pixel averages, in float, the depths of its 2x2 neighbourhood that lie within
+ * .005 * stereoErrorRatio of its own (or of the diagonally opposite pixel's, when its own group
+ * is alone).  Both sampling factors are the ratio of the heights, as in the reference. */
+void depth_map_pyramid(const Img& image, double ratio, int min_width, std::vector<Img>& lev)
+{
+    if (ratio > 0.98 || ratio < 0.4) ratio = 0.75;
+    double w = image.w * ratio;
+    int nLevels = 1;
+    while (w >= min_width) { nLevels++; w *= ratio; }
+    lev.assign(nLevels, Img());
+    lev[0] = image;
+    for (int m = 1; m < nLevels; m++) {
+        const Img& L = lev[m - 1];
+        const int LW = L.w, LH = L.h;
+        const double levelRatio = std::pow(ratio, m);
+        Img foo;
+        foo.alloc((int)(image.w * levelRatio), (int)(image.h * levelRatio), 1);
+        auto at = [&](int y, int x) { return L.d[(size_t)y * LW + x]; };
+        const float factor = (float)LH / foo.h;
+        const float maxDZ = .005f;
+        for (int i = 0; i < foo.h; i++)
+            for (int j = 0; j < foo.w; j++) {
+                const int x = std::max(0, std::min(LW - 1, (int)std::rint(factor * j)));
+                const int y = std::max(0, std::min(LH - 1, (int)std::rint(factor * i)));
+                double& out = foo.d[(size_t)i * foo.w + j];
+                if (!(at(y, x) > 0)) { out = -1; continue; }
+                const int xs[2] = {std::max(0, std::min(LW - 1, (int)std::floor(factor * j))), 0};
+                const int ys[2] = {std::max(0, std::min(LH - 1, (int)std::floor(factor * i))), 0};
+                const int xs1 = std::min(LW - 1, xs[0] + 1), ys1 = std::min(LH - 1, ys[0] + 1);
+                const int X[2] = {xs[0], xs1}, Y[2] = {ys[0], ys1};
+                const int xi = (x == X[0]) ? 0 : 1, yi = (y == Y[0]) ? 0 : 1;
+                const double z = at(y, x);
+                const double tol = maxDZ * stereo_error_ratio(z);
+                std::vector<float> comp;
+                comp.push_back((float)z);
+                if (std::fabs(at(Y[yi], X[!xi]) - z) < tol) comp.push_back((float)at(Y[yi], X[!xi]));
+                if (std::fabs(at(Y[!yi], X[xi]) - z) < tol) comp.push_back((float)at(Y[!yi], X[xi]));
+                if (std::fabs(at(Y[!yi], X[!xi]) - z) < tol) comp.push_back((float)at(Y[!yi], X[!xi]));
+                if (comp.size() > 1) {
+                    float avg = 0;
+                    for (float v : comp) avg += v;
+                    out = avg / comp.size();
+                } else {
+                    const double zo = at(Y[!yi], X[!xi]);
+                    const double tolo = maxDZ * stereo_error_ratio(zo);
+                    std::vector<float> other;
+                    other.push_back((float)zo);
+                    if (std::fabs(at(Y[yi], X[!xi]) - zo) < tolo) other.push_back((float)at(Y[yi], X[!xi]));
+                    if (std::fabs(at(Y[!yi], X[xi]) - zo) < tolo) other.push_back((float)at(Y[!yi], X[xi]));
+                    if (other.size() > 1) {
+                        float avg = 0;
+                        for (float v : other) avg += v;
+                        out = avg / other.size();
+                    } else {
+                        out = z;
+                    }
+                }
+            }
+        lev[m] = std::move(foo);
+    }
+}
+
 /* ------------------------------------------------------------------------------------------ */
 /* 2-D optical flow: Ce Liu's coarse-to-fine solver, the demo's flow type 1
  * (OpticalFlow::Coarse2FineFlow, src/opticalFlowMultiscale.cpp:4-146, CELIU variant:
@@ -1357,6 +1421,24 @@ int sfo_scene_flow_two_frames(int fp64, const rgbdflow_camera_params* camFull, c
         trace_to_stats(t, stats);
         return 0;
     } catch (const std::exception& e) { g_err = e.what(); return -1; }
+}
+
+/* DepthMapPyramid of a W x H depth map (doubles); out: the levels concatenated (NULL: sizes
+ * only), dims: 2 ints per level.  Returns the level count. */
+int sfo_depth_map_pyramid(const double* depth, int W, int H, double ratio, int min_width, double* out, int* dims)
+{
+    Img d;
+    d.alloc(W, H, 1);
+    std::memcpy(d.data(), depth, sizeof(double) * (size_t)W * H);
+    std::vector<Img> lev;
+    depth_map_pyramid(d, ratio, min_width, lev);
+    size_t off = 0;
+    for (size_t i = 0; i < lev.size(); i++) {
+        if (dims) { dims[2 * i] = lev[i].w; dims[2 * i + 1] = lev[i].h; }
+        if (out) std::memcpy(out + off, lev[i].data(), sizeof(double) * lev[i].n());
+        off += lev[i].n();
+    }
+    return (int)lev.size();
 }
 
 /* 2-D optical flow of two BGR8 images (the demo's flow type 1, runFlowTwoFramesCeLiu,

@@ -17,6 +17,7 @@ ORACLE_SO = os.path.join(ORACLE_DIR, "libsforacle.so")
 REF_CPU_SO = os.path.join(ORACLE_DIR, "_ref", "libref_cpu.so")
 REF_CUDA_SO = os.path.join(ORACLE_DIR, "_ref", "libref_cuda.so")
 REF_FLOW2D_SO = os.path.join(ORACLE_DIR, "_ref", "libref_flow2d.so")
+REF_HPB_SO = os.path.join(ORACLE_DIR, "_ref", "libref_hpb.so")
 
 _P = ctypes.POINTER
 _d = ctypes.c_double
@@ -80,6 +81,7 @@ def oracle():
                                                   ctypes.c_void_p, _pf, _pf, ctypes.c_void_p]
         lib.sfo_optical_flow_2d.argtypes = [_pu8, _pu8, _i, _i, _d, _d, _i, _i, _i, _i, _pd, _pd]
         lib.sfo_optical_flow_2d_ring.argtypes = [_pu8, _pu8, _i, _i, _d, _d, _i, _i, _i, _i, _i, _pd, _pd]
+        lib.sfo_depth_map_pyramid.argtypes = [_pd, _i, _i, _d, _i, _pd, _pi]
         lib.sfo_last_error.restype = ctypes.c_char_p
         lib.sfo_set_threads.argtypes = [_i]
         _oracle = lib
@@ -162,6 +164,38 @@ def optical_flow_2d(bgr1, bgr2, alpha=0.02, ratio=0.75, min_width=20, n_outer=10
         if rc != 0:
             raise RuntimeError("oracle 2-D flow: " + oracle().sfo_last_error().decode())
     return u, v
+
+
+_ref_hpb = None
+
+
+def ref_hpb_available():
+    return os.path.exists(REF_HPB_SO)
+
+
+def depth_map_pyramid(depth, ratio, min_width, impl="oracle"):
+    """DepthMapPyramid::ConstructPyramid (src/depthMapPyramid.cpp:15-91) of a depth map: the list
+    of levels.  impl "oracle" (the restatement) or "ref" (the reference, compiled)."""
+    global _ref_hpb
+    d = _cont(depth, np.float64)
+    H, W = d.shape
+    if impl == "ref":
+        if _ref_hpb is None:
+            _ref_hpb = ctypes.CDLL(REF_HPB_SO)
+            _ref_hpb.ref_depth_map_pyramid.argtypes = [_pd, _i, _i, _d, _i, _pd, _pi]
+        fn = _ref_hpb.ref_depth_map_pyramid
+    else:
+        fn = oracle().sfo_depth_map_pyramid
+    dims = np.zeros(128, np.int32)
+    n = fn(dptr(d), W, H, ratio, min_width, None, iptr(dims))
+    out = np.zeros(sum(int(dims[2 * i]) * int(dims[2 * i + 1]) for i in range(n)))
+    fn(dptr(d), W, H, ratio, min_width, dptr(out), iptr(dims))
+    levels, off = [], 0
+    for i in range(n):
+        w, h = int(dims[2 * i]), int(dims[2 * i + 1])
+        levels.append(out[off:off + w * h].reshape(h, w))
+        off += w * h
+    return levels
 
 
 # ---------------------------------------------------------------------------------------------
