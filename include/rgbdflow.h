@@ -375,8 +375,9 @@ typedef struct rgbdflow_flow2d_params {
 /* The demo's values for flow type 1 (runFlowTwoFramesCeLiu, opticalFlowParams). */
 void rgbdflow_flow2d_params_default(rgbdflow_flow2d_params* p);
 /* Host buffers (BGR8, W*H*3 each), synchronous.  flow_out: W*H*2 floats (u, v in pixels), the
- * reference's cv::Vec2f result (liu2cvFlow2d).  alpha < 0: RGBDFLOW_ERR_INVALID_ARG (the
- * reference asserts alpha >= 0). */
+ * reference's cv::Vec2f result (liu2cvFlow2d).  RGBDFLOW_ERR_INVALID_ARG for alpha < 0 (the
+ * reference asserts alpha >= 0), min_width < 1 (the reference's level count never ends), a
+ * pyramid_ratio that is not a finite number > 0, n_inner or n_sor < 1, sor_ring outside 2..16. */
 int rgbdflow_optical_flow_2d(rgbdflow_ctx* ctx, const uint8_t* bgr1, const uint8_t* bgr2, int W, int H,
                              const rgbdflow_flow2d_params* params, float* flow_out);
 

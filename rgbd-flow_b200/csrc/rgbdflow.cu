@@ -512,6 +512,11 @@ static void run_flow2d(rgbdflow_ctx* c, const uint8_t* bgr1, const uint8_t* bgr2
     if (!(prm.alpha >= 0)) throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "alpha must be >= 0");
     if (prm.n_outer < 0 || prm.n_inner < 1 || prm.n_sor < 1 || prm.sor_ring < 2 || prm.sor_ring > kMaxRing)
         throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "n_inner and n_sor must be >= 1, sor_ring in 2..16");
+    // the level count loop below ends only for min_width >= 1 (the reference's never ends for <= 0),
+    // and the flow is scaled by 1 / pyramid_ratio between levels
+    if (prm.min_width < 1) throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "min_width must be >= 1");
+    if (!(prm.pyramid_ratio > 0) || !std::isfinite(prm.pyramid_ratio))
+        throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "pyramid_ratio must be a finite number > 0");
     // pyramid geometry (GaussianPyramid::ConstructPyramid, GaussianPyramid.cpp:20-63)
     double ratio = prm.pyramid_ratio;
     if (ratio > 0.98 || ratio < 0.4) ratio = 0.75;

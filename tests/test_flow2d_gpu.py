@@ -51,3 +51,11 @@ def test_sweeps_in_flight_do_not_change_the_flow(ctx):
         p = _params("patch")
         p.sor_ring = ring
         np.testing.assert_array_equal(ctx.optical_flow_2d(g["patch_bgr1"], g["patch_bgr2"], p), a)
+
+
+def test_bad_parameters_are_status_codes(ctx):
+    b = np.zeros((24, 32, 3), np.uint8)
+    for over in (dict(min_width=0), dict(pyramid_ratio=0.0), dict(alpha=-1.0), dict(n_sor=0), dict(sor_ring=17)):
+        with pytest.raises(rf.RgbdFlowError) as e:
+            ctx.optical_flow_2d(b, b, rf.flow2d_params(**over))
+        assert e.value.code == -1
