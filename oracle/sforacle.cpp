@@ -859,6 +859,294 @@ void depth_map_pyramid(const Img& image, double ratio, int min_width, std::vecto
 }
 
 /* ------------------------------------------------------------------------------------------ */
+/* HPB: the heuristic boundary probability the reference's default regularisation weights are
+ * made of (computeHeuristicPb, src/heuristicProbBoundary.cpp:21-41 and
+ * src/heuristicBoundaries.cpp:40-358).  Restated with the reference's float / double mix, except
+ * where its arithmetic is fixed by unpinned library versions:
+ *   - normals: the reference takes them from PCL's NormalEstimation (not vendored, version not
+ *     pinned): the eigenvector of the smallest eigenvalue of the neighbourhood's covariance,
+ *     turned towards the camera.  Here: mean and covariance in double, a cyclic Jacobi
+ *     eigen-solve in double, the normal rounded to float.
+ *   - exp of a float: the overload the reference's headers select is not pinned; double here.
+ *   - normalising a zero vector (Eigen version dependent) leaves it zero here; it only happens
+ *     where the normal cue is discarded anyway (fewer than 3 valid normals). */
+
+/* 3x3 symmetric eigen-solve, cyclic Jacobi rotations in double: the eigenvector of the smallest
+ * eigenvalue, unit length. */
+static void smallest_eigvec(double a[3][3], double n[3])
+{
+    double v[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+    for (int sweep = 0; sweep < 64; sweep++) {
+        const double off = a[0][1] * a[0][1] + a[0][2] * a[0][2] + a[1][2] * a[1][2];
+        if (off < 1e-300) break;
+        for (int p = 0; p < 2; p++)
+            for (int q = p + 1; q < 3; q++) {
+                if (a[p][q] == 0) continue;
+                const double theta = (a[q][q] - a[p][p]) / (2 * a[p][q]);
+                const double t = (theta >= 0 ? 1 : -1) / (std::fabs(theta) + std::sqrt(theta * theta + 1));
+                const double c = 1 / std::sqrt(t * t + 1), sn = t * c;
+                for (int k = 0; k < 3; k++) {
+                    const double akp = a[k][p], akq = a[k][q];
+                    a[k][p] = c * akp - sn * akq;
+                    a[k][q] = sn * akp + c * akq;
+                }
+                for (int k = 0; k < 3; k++) {
+                    const double apk = a[p][k], aqk = a[q][k];
+                    a[p][k] = c * apk - sn * aqk;
+                    a[q][k] = sn * apk + c * aqk;
+                }
+                for (int k = 0; k < 3; k++) {
+                    const double vkp = v[k][p], vkq = v[k][q];
+                    v[k][p] = c * vkp - sn * vkq;
+                    v[k][q] = sn * vkp + c * vkq;
+                }
+            }
+    }
+    int m = 0;
+    for (int k = 1; k < 3; k++)
+        if (a[k][k] < a[m][m]) m = k;
+    const double len = std::sqrt(v[0][m] * v[0][m] + v[1][m] * v[1][m] + v[2][m] * v[2][m]);
+    for (int k = 0; k < 3; k++) n[k] = v[k][m] / len;
+}
+
+struct Cloud {
+    int W = 0, H = 0;
+    std::vector<float> x, y, z;       // depth_to_cloud (depth_to_cloud_lib.ipp:13-60)
+    std::vector<float> nx, ny, nz;    // normals; 0 where invalid (markNormalInvalid, cloudNormals.ipp:116-120)
+};
+
+/* depth_to_cloud with every pixel kept (depth_to_cloud_lib.ipp:35-50) and setOrganizedNormals
+ * (cloudNormals.ipp:395-506) with a 9x9 window (k = 4), no downsampling, neighbours whose depth is
+ * within .05 * stereoErrorRatio of the centre's, at least max(6, 81 / 3) of them
+ * (computeOrganizedPointCloudNormalsThreadMain, cloudNormals.ipp:131-205). */
+static void organized_cloud_normals(const float* depth, int W, int H, float cx, float cy, float f, Cloud& cl)
+{
+    const size_t N = (size_t)W * H;
+    cl.W = W; cl.H = H;
+    cl.x.assign(N, 0); cl.y.assign(N, 0); cl.z.assign(N, 0);
+    cl.nx.assign(N, 0); cl.ny.assign(N, 0); cl.nz.assign(N, 0);
+    for (int r = 0; r < H; r++)
+        for (int c = 0; c < W; c++) {
+            const size_t o = (size_t)r * W + c;
+            const float d = depth[o];
+            cl.x[o] = (((float)c - cx) * d / f);
+            cl.y[o] = (((float)r - cy) * d / f);
+            cl.z[o] = d;
+        }
+    const int k = 4;
+    const unsigned minPts = std::max(6u, (unsigned)((2 * k + 1) * (2 * k + 1) / 3));
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < H; i++)
+        for (int j = 0; j < W; j++) {
+            const size_t o = (size_t)i * W + j;
+            if (!(cl.z[o] > 0)) continue;
+            std::vector<size_t> nn;
+            for (int yy = std::max(0, i - k); yy <= std::min(H - 1, i + k); yy++)
+                for (int xx = std::max(0, j - k); xx <= std::min(W - 1, j + k); xx++) {
+                    const size_t o2 = (size_t)yy * W + xx;
+                    // setOrganizedNormals takes the .05 as a float, then passes it on as a double
+                    if (std::fabs(cl.z[o] - cl.z[o2]) < (double).05f * stereo_error_ratio(cl.z[o])) nn.push_back(o2);
+                }
+            if (nn.size() < minPts) continue;
+            double m[3] = {0, 0, 0};
+            for (size_t q : nn) { m[0] += cl.x[q]; m[1] += cl.y[q]; m[2] += cl.z[q]; }
+            for (double& t : m) t /= (double)nn.size();
+            double a[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+            for (size_t q : nn) {
+                const double d[3] = {cl.x[q] - m[0], cl.y[q] - m[1], cl.z[q] - m[2]};
+                for (int r = 0; r < 3; r++)
+                    for (int c = 0; c < 3; c++) a[r][c] += d[r] * d[c];
+            }
+            for (auto& row : a)
+                for (double& t : row) t /= (double)nn.size();
+            double n[3];
+            smallest_eigvec(a, n);
+            if (!(std::isfinite(n[0]) && std::isfinite(n[1]) && std::isfinite(n[2]))) continue;
+            // flipNormalTowardsViewpoint with the viewpoint at the origin
+            const double cosv = -(cl.x[o] * n[0] + cl.y[o] * n[1] + cl.z[o] * n[2]);
+            if (cosv < 0) { n[0] = -n[0]; n[1] = -n[1]; n[2] = -n[2]; }
+            cl.nx[o] = (float)n[0]; cl.ny[o] = (float)n[1]; cl.nz[o] = (float)n[2];
+        }
+}
+
+/* computeIntegralImage (include/image_features/halfDiskFeatures.ipp:102-154): one more row and
+ * column of zeros at index -1 (here 0), float (or uint32) sums in the reference's order. */
+template <typename T>
+static void integral_image(const std::vector<T>& img, int W, int H, int C, std::vector<T>& ii)
+{
+    const int W1 = W + 1;
+    ii.assign((size_t)(H + 1) * W1 * C, 0);
+    for (int j = 0; j < W; j++)
+        for (int l = 0; l < C; l++)
+            ii[((size_t)1 * W1 + j + 1) * C + l] = ii[((size_t)1 * W1 + j) * C + l] + img[((size_t)j) * C + l];
+    for (int i = 1; i < H; i++) {
+        std::vector<T> rowSum(C, 0);
+        for (int j = 0; j < W; j++)
+            for (int l = 0; l < C; l++) {
+                const T v = img[((size_t)i * W + j) * C + l];
+                ii[((size_t)(i + 1) * W1 + j + 1) * C + l] = ii[((size_t)i * W1 + j + 1) * C + l] + rowSum[l] + v;
+                rowSum[l] += v;
+            }
+    }
+}
+
+/* computeHeuristicPb on one pyramid level (heuristicProbBoundary.cpp:21-41 wrapping
+ * heuristicBoundaries.cpp:40-358): img = the level's colour image (3 channels in [0, 1], BGR),
+ * depth = the level of the raw-depth pyramid (<= 0 invalid).  out: W*H*2 floats, (right, down)
+ * boundary probability of each pixel. */
+void heuristic_pb(const double* img, const double* depthd, int W, int H, float* out)
+{
+    const size_t N = (size_t)W * H;
+    // the wrapper's camera: Kinect intrinsics scaled to the level
+    const unsigned xRes = (unsigned)W, yRes = (unsigned)H;
+    const float cx = (float)(xRes / 2), cy = (float)(yRes / 2);
+    const float f = (float)(525.0 * xRes / 640);
+    // the wrapper's 8-bit image: channels reversed, 255 * value truncated; then / 255.0 as float
+    std::vector<float> cols(N * 3);
+    std::vector<float> depth(N);
+    for (size_t l = 0; l < N; l++) {
+        const unsigned char px[3] = {(unsigned char)(255 * img[l * 3 + 2]), (unsigned char)(255 * img[l * 3 + 1]),
+                                     (unsigned char)(255 * img[l * 3 + 0])};
+        for (int k = 0; k < 3; k++) cols[l * 3 + k] = (float)(px[k] / 255.0);
+        depth[l] = (float)depthd[l];
+    }
+    Cloud cl;
+    organized_cloud_normals(depth.data(), W, H, cx, cy, f, cl);
+    std::vector<float> normals(N * 3);
+    std::vector<uint32_t> nvalid(N, 0);
+    for (size_t l = 0; l < N; l++) {
+        const float n0 = cl.nx[l], n1 = cl.ny[l], n2 = cl.nz[l];
+        normals[l * 3] = n0; normals[l * 3 + 1] = n1; normals[l * 3 + 2] = n2;
+        const float sq = n0 * n0 + n1 * n1 + n2 * n2;
+        if (!std::isfinite(n0) || !std::isfinite(n1) || !std::isfinite(n2) || std::fabs(sq - 1) < 1e-4) nvalid[l] = 1;
+    }
+    // half-disk radius per pixel: 2 cm at the pixel's depth, 1..5 pixels (heuristicBoundaries.cpp:101-109)
+    std::vector<int> radii(N);
+    for (size_t l = 0; l < N; l++)
+        radii[l] = depth[l] > 0 ? std::max(1, std::min(5, (int)std::rint(f * .02f / depth[l]))) : 5;
+    std::vector<float> ciI, niI;
+    std::vector<uint32_t> viI;
+    integral_image(cols, W, H, 3, ciI);
+    integral_image(normals, W, H, 3, niI);
+    integral_image(nvalid, W, H, 1, viI);
+    const int W1 = W + 1;
+    auto II = [&](const auto& v, int C, int y, int x, int k) { return v[((size_t)(y + 1) * W1 + (x + 1)) * C + k]; };
+    std::vector<float> colH(N, 0), colV(N, 0), norH(N, 0), norV(N, 0);
+    auto normalize3 = [](float v[3]) {
+        const float n = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        if (n > 0) for (int k = 0; k < 3; k++) v[k] /= n;
+    };
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < H; i++)
+        for (int j = 0; j < W; j++) {
+            const size_t o = (size_t)i * W + j;
+            const int hw = radii[o];
+            const int xmin = std::max(0, j - hw), xmax = std::min(W - 1, j + hw - 1);
+            const int ymin = std::max(0, i - hw), ymax = std::min(H - 1, i + hw - 1);
+            const float hsize0 = (float)((j - xmin) * (ymax - ymin + 1)), hsize1 = (float)((xmax - j + 1) * (ymax - ymin + 1));
+            const float vsize0 = (float)((xmax - xmin + 1) * (i - ymin)), vsize1 = (float)((xmax - xmin + 1) * (ymax - i + 1));
+            auto H1 = [&](const auto& v, int C, int k) { return II(v, C, ymax, xmax, k) - II(v, C, ymax, j - 1, k) - II(v, C, ymin - 1, xmax, k) + II(v, C, ymin - 1, j - 1, k); };
+            auto H0 = [&](const auto& v, int C, int k) { return II(v, C, ymax, j - 1, k) - II(v, C, ymin - 1, j - 1, k) - II(v, C, ymax, xmin - 1, k) + II(v, C, ymin - 1, xmin - 1, k); };
+            auto V1 = [&](const auto& v, int C, int k) { return II(v, C, ymax, xmax, k) - II(v, C, i - 1, xmax, k) - II(v, C, ymax, xmin - 1, k) + II(v, C, i - 1, xmin - 1, k); };
+            auto V0 = [&](const auto& v, int C, int k) { return II(v, C, i - 1, xmax, k) - II(v, C, i - 1, xmin - 1, k) - II(v, C, ymin - 1, xmax, k) + II(v, C, ymin - 1, xmin - 1, k); };
+            auto dot = [](const float a[3], const float b[3]) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; };
+            if (j > 0) {
+                float acc = 0;
+                for (int k = 0; k < 3; k++) { const float d = H1(ciI, 3, k) / hsize1 - H0(ciI, 3, k) / hsize0; acc += d * d; }
+                colH[o] = std::sqrt(acc);
+                float n0[3], n1[3];
+                for (int k = 0; k < 3; k++) { n0[k] = H0(niI, 3, k); n1[k] = H1(niI, 3, k); }
+                normalize3(n0); normalize3(n1);
+                const uint32_t v0 = H0(viI, 1, 0), v1 = H1(viI, 1, 0);
+                norH[o] = (std::min(v0, v1) < 3) ? 0 : (float)(.5 * (1 - dot(n0, n1)));
+                if (std::min(v0, v1) > 3) {
+                    const size_t oa = (size_t)i * W + (j - 1);
+                    float dx[3] = {cl.x[oa] - cl.x[o], cl.y[oa] - cl.y[o], cl.z[oa] - cl.z[o]};
+                    normalize3(dx);
+                    const float mdx[3] = {-dx[0], -dx[1], -dx[2]};
+                    const double convexity = (dot(n0, dx) + dot(n1, mdx)) / 4 + .5;
+                    norH[o] = (float)(norH[o] * (1 - convexity));
+                }
+            }
+            if (i > 0) {
+                float acc = 0;
+                for (int k = 0; k < 3; k++) { const float d = V1(ciI, 3, k) / vsize1 - V0(ciI, 3, k) / vsize0; acc += d * d; }
+                colV[o] = std::sqrt(acc);
+                float n0[3], n1[3];
+                for (int k = 0; k < 3; k++) { n0[k] = V0(niI, 3, k); n1[k] = V1(niI, 3, k); }
+                normalize3(n0); normalize3(n1);
+                const uint32_t v0 = V0(viI, 1, 0), v1 = V1(viI, 1, 0);
+                norV[o] = (std::min(v0, v1) < 3) ? 0 : (float)(.5 * (1 - dot(n0, n1)));
+                if (std::min(v0, v1) > 3) {
+                    const size_t oa = (size_t)(i - 1) * W + j;
+                    float dx[3] = {cl.x[oa] - cl.x[o], cl.y[oa] - cl.y[o], cl.z[oa] - cl.z[o]};
+                    normalize3(dx);
+                    const float mdx[3] = {-dx[0], -dx[1], -dx[2]};
+                    const double convexity = (dot(n0, dx) + dot(n1, mdx)) / 4 + .5;
+                    norV[o] = (float)(norV[o] * (1 - convexity));
+                }
+            }
+        }
+    // the probabilities (heuristicBoundaries.cpp:223-293)
+    const float depthSigma = .02f, colSigma = .7f, normSigma = .4f;
+    std::vector<float> bp(N * 2, 0);
+    auto sqrf = [](float v) { return v * v; };
+    auto calc = [&](int i, int j, int k, float z1, float z2, float dcol, float dnorm) {
+        float colProb, depthProb;
+        if (std::max(z1, z2) <= 0) {
+            depthProb = 0;
+            colProb = (float)(1 - std::exp((double)-sqrf(dcol / colSigma)));
+        } else if (std::min(z1, z2) <= 0) {
+            const int di[4] = {0, -1, 0, 1}, dj[4] = {-1, 0, 1, 0};
+            const int dir = (z1 <= 0) ? (k + 2) % 4 : k;
+            int i0 = (z1 <= 0) ? i : i + di[k], j0 = (z1 <= 0) ? j : j + dj[k];
+            unsigned size = 0;
+            while (j0 >= 0 && j0 < W && i0 >= 0 && i0 < H && depth[(size_t)i0 * W + j0] <= 0) {
+                size++;
+                i0 += di[dir];
+                j0 += dj[dir];
+            }
+            const bool oob = (j0 < 0 || j0 >= W || i0 < 0 || i0 >= H);
+            if (oob) depthProb = 0;
+            else {
+                const double a = std::min(1.0f, (float)size / 30);
+                depthProb = (float)((1 - a) * .2 + a * 1);
+            }
+            colProb = (float)(1 - std::exp((double)-sqrf(dcol / colSigma)));
+        } else {
+            const float dz = (float)(std::fabs(z1 - z2) / stereo_error_ratio(std::min(z1, z2)));
+            depthProb = (float)(1 - std::exp((double)-sqrf(dz / depthSigma)));
+            colProb = 0;
+        }
+        const float normProb = (float)(1 - std::exp((double)-sqrf(dnorm / normSigma)));
+        float v = std::max(depthProb, std::max(colProb, std::max(0.0f, normProb)));
+        if (((i == 0 || i == H - 2) && k == 1) || ((j == 0 || j == W - 2) && k == 0)) v = 0;
+        bp[((size_t)i * W + j) * 2 + k] = v;
+    };
+    for (int i = 0; i < H; i++)
+        for (int j = 0; j < W; j++) {
+            const size_t o = (size_t)i * W + j;
+            if (j < W - 1) calc(i, j, 0, depth[o], depth[o + 1], colH[o + 1], norH[o + 1]);
+            if (i < H - 1) calc(i, j, 1, depth[o], depth[o + W], colV[o + W], norV[o + W]);
+        }
+    // non-maximum suppression along each direction within the pixel's radius (:298-340)
+    std::vector<float> bp2 = bp;
+    for (int i = 0; i < H; i++)
+        for (int j = 0; j < W; j++) {
+            const int hw = radii[(size_t)i * W + j];
+            int mi = -1;
+            for (int k = std::max(0, i - hw); k <= std::min(H - 1, i + hw); k++)
+                if (mi < 0 || bp[((size_t)k * W + j) * 2 + 1] > bp[((size_t)mi * W + j) * 2 + 1]) mi = k;
+            if (mi != i) bp2[((size_t)i * W + j) * 2 + 1] = 0;
+            mi = -1;
+            for (int k = std::max(0, j - hw); k <= std::min(W - 1, j + hw); k++)
+                if (mi < 0 || bp[((size_t)i * W + k) * 2] > bp[((size_t)i * W + mi) * 2]) mi = k;
+            if (mi != j) bp2[((size_t)i * W + j) * 2] = 0;
+        }
+    std::memcpy(out, bp2.data(), sizeof(float) * N * 2);
+}
+
+/* ------------------------------------------------------------------------------------------ */
 /* 2-D optical flow: Ce Liu's coarse-to-fine solver, the demo's flow type 1
  * (OpticalFlow::Coarse2FineFlow, src/opticalFlowMultiscale.cpp:4-146, CELIU variant:
  * OpticalFlow::SmoothFlowSOR, src/SmoothFlowSOR.cpp:8-247).  All FP64, like the reference, with
@@ -1421,6 +1709,13 @@ int sfo_scene_flow_two_frames(int fp64, const rgbdflow_camera_params* camFull, c
         trace_to_stats(t, stats);
         return 0;
     } catch (const std::exception& e) { g_err = e.what(); return -1; }
+}
+
+/* computeHeuristicPb of one level: img W*H*3 doubles in [0, 1] (BGR), depth W*H doubles;
+ * out: W*H*2 floats. */
+void sfo_heuristic_pb(const double* img, const double* depth, int W, int H, float* out)
+{
+    heuristic_pb(img, depth, W, H, out);
 }
 
 /* DepthMapPyramid of a W x H depth map (doubles); out: the levels concatenated (NULL: sizes

@@ -82,6 +82,7 @@ def oracle():
         lib.sfo_optical_flow_2d.argtypes = [_pu8, _pu8, _i, _i, _d, _d, _i, _i, _i, _i, _pd, _pd]
         lib.sfo_optical_flow_2d_ring.argtypes = [_pu8, _pu8, _i, _i, _d, _d, _i, _i, _i, _i, _i, _pd, _pd]
         lib.sfo_depth_map_pyramid.argtypes = [_pd, _i, _i, _d, _i, _pd, _pi]
+        lib.sfo_heuristic_pb.argtypes = [_pd, _pd, _i, _i, _pf]
         lib.sfo_last_error.restype = ctypes.c_char_p
         lib.sfo_set_threads.argtypes = [_i]
         _oracle = lib
@@ -167,6 +168,16 @@ def optical_flow_2d(bgr1, bgr2, alpha=0.02, ratio=0.75, min_width=20, n_outer=10
 
 
 _ref_hpb = None
+
+
+def heuristic_pb(img, depth):
+    """computeHeuristicPb of one pyramid level (oracle): img (H, W, 3) in [0, 1] (BGR), depth
+    (H, W) metres (<= 0 invalid) -> (H, W, 2) float32 boundary probabilities (right, down)."""
+    im, d = _cont(img, np.float64), _cont(depth, np.float64)
+    H, W = d.shape
+    out = np.zeros((H, W, 2), np.float32)
+    oracle().sfo_heuristic_pb(dptr(im), dptr(d), W, H, fptr(out))
+    return out
 
 
 def ref_hpb_available():
