@@ -24,6 +24,7 @@
 #include <cstdint>
 #include <cstring>
 #include <stdexcept>
+#include <set>
 #include <string>
 #include <unordered_set>
 #include <vector>
@@ -701,16 +702,40 @@ void reg_weights(int W, int H, const double* depth, int type, std::vector<double
         }
 }
 
+}  // namespace sfo
+// HPB pieces, defined below
+void heuristic_pb(const double* img, const double* depthd, int W, int H, float* out);
+void depth_map_pyramid(const sfo::Img& image, double ratio, int min_width, std::vector<sfo::Img>& lev);
+void fill_small_regions_color(sfo::Img& depth, const sfo::Img& col, unsigned maxRegion);
+namespace sfo {
+
+/* calculateRegularizationWeights, HPB form (OpticalFlow.cpp:126-131): 1 - .99 hpb for the right and
+ * lower neighbours. */
+static void hpb_reg_weights(const Img& colour, const Img& rawDepth, std::vector<double>& rw)
+{
+    const int W = colour.w, H = colour.h;
+    std::vector<float> hpb((size_t)W * H * 2);
+    heuristic_pb(colour.data(), rawDepth.data(), W, H, hpb.data());
+    rw.assign((size_t)W * H * 2, 0);
+    for (int i = 0, l = 0; i < H; i++)
+        for (int j = 0; j < W; j++, l++) {
+            if (j < W - 1) rw[l * 2 + 0] = (1 - hpb[(size_t)l * 2 + 0] * .99);
+            if (i < H - 1) rw[l * 2 + 1] = (1 - hpb[(size_t)l * 2 + 1] * .99);
+        }
+}
+
 template <bool FP64>
 static void run_level(const rgbdflow_camera_params& camFull, const rgbdflow_params& p, int fixed,
                       const Img& feat1, const Img& d1, const Img& feat2, const Img& d2, Img& wI2, Img& wD2,
-                      const double* ddw, const double* dsw, Img& u, Img& v, Img& w, int allowEarly, LevelTrace* tr)
+                      const double* ddw, const double* dsw, Img& u, Img& v, Img& w, int allowEarly, LevelTrace* tr,
+                      const Img* hpbColour = nullptr, const Img* hpbDepth = nullptr)
 {
     const int W = feat1.w, H = feat1.h;
     const rgbdflow_camera_params ck = resize_cam(camFull, W);
     std::vector<double> mag, rw;
     depth_mag_weights(d1, camFull, mag);
-    reg_weights(W, H, d1.data(), p.regularization, rw);
+    if (p.regularization == RGBDFLOW_REG_HPB) hpb_reg_weights(*hpbColour, *hpbDepth, rw);
+    else reg_weights(W, H, d1.data(), p.regularization, rw);
     SolverIn in;
     in.W = W; in.H = H; in.C = feat1.c; in.f_level = ck.focalLength;
     in.Im1 = feat1.data(); in.dm1 = d1.data(); in.Im2 = feat2.data(); in.dm2 = d2.data();
@@ -750,9 +775,19 @@ void multiscale(const rgbdflow_camera_params& cam, const rgbdflow_params& p, con
         im2feature(Im2, f2);
         warp_cpu(f1, d1, f2, d2, wI2, wD2, u.data(), v.data(), w.data());
         if (trace) { trace->n_levels = 1; trace->w[0] = W; trace->h[0] = H; }
+        // sceneFlowWithInit.cpp:48: HPB of the full-size colour and the raw depth
         run_level<FP64>(cam, p, fixed, f1, d1, f2, d2, wI2, wD2, ddw.data(), dsw.data(), u, v, w, 0,
-                        trace ? &trace->lev[0] : nullptr);
+                        trace ? &trace->lev[0] : nullptr, &Im1, &dm1);
         return;
+    }
+    // the raw-depth pyramid of HPB (sceneFlowMultiscale.cpp:79-83): small invalid regions of the
+    // raw depth filled guided by colour, then DepthMapPyramid
+    std::vector<Img> rawPyr;
+    if (p.regularization == RGBDFLOW_REG_HPB) {
+        Img filtered = dm1;
+        fill_small_regions_color(filtered, Im1, 60);
+        const int mw = p.min_width < 0 ? std::max(1, Im1.w / -p.min_width) : p.min_width;
+        depth_map_pyramid(filtered, p.pyramid_ratio, mw, rawPyr);
     }
     std::vector<Img> pI1, pI2, pD1, pD2, pDDW, pDSW;
     build_pyramid(Im1, p.pyramid_ratio, p.min_width, pI1);
@@ -783,7 +818,7 @@ void multiscale(const rgbdflow_camera_params& cam, const rgbdflow_params& p, con
             warp_cpu(f1, pD1[k], f2, pD2[k], wI2, wD2, u.data(), v.data(), w.data());
         }
         run_level<FP64>(cam, p, fixed, f1, pD1[k], f2, pD2[k], wI2, wD2, pDDW[k].data(), pDSW[k].data(), u, v, w,
-                        k < L - 1, trace ? &trace->lev[k] : nullptr);
+                        k < L - 1, trace ? &trace->lev[k] : nullptr, &pI1[k], rawPyr.empty() ? nullptr : &rawPyr[k]);
     }
 }
 
@@ -855,6 +890,85 @@ void depth_map_pyramid(const Img& image, double ratio, int min_width, std::vecto
                 }
             }
         lev[m] = std::move(foo);
+    }
+}
+
+/* recursiveMedianFilterSmallInvalidRegionsUsingColor (src/recursiveMedianFiltering.cpp:127-222):
+ * each 4-connected region of invalid depth (<= 0) of at most maxRegion pixels is filled, the pixel
+ * with the most valid 3x3 neighbours first, each with the average of its valid neighbours weighted
+ * by exp(-|colour difference|^2 / .6) (float sums, as the reference).  Order: the reference takes
+ * regions in the iteration order of a boost::unordered_map and, among pixels with equally many
+ * valid neighbours, the first of a std::unordered_set, both hashed by boost::hash, whose mixing
+ * depends on the unpinned Boost version.  Here regions go in the raster order of their first
+ * pixel and ties by raster order; values differ from the reference's only where that order
+ * matters (pixels with equal counts, regions that touch diagonally). */
+void fill_small_regions_color(Img& depth, const Img& col, unsigned maxRegion)
+{
+    const int W = depth.w, H = depth.h;
+    const size_t N = (size_t)W * H;
+    auto dz = [&](int i, int j) -> double& { return depth.d[(size_t)i * W + j]; };
+    std::vector<int> comp(N, -1);
+    std::vector<std::vector<int>> comps;
+    for (int i = 0; i < H; i++)
+        for (int j = 0; j < W; j++) {
+            if (!(dz(i, j) <= 0) || comp[(size_t)i * W + j] >= 0) continue;
+            const int id = (int)comps.size();
+            comps.emplace_back();
+            std::vector<int> stack{i * W + j};
+            comp[(size_t)i * W + j] = id;
+            while (!stack.empty()) {
+                const int q = stack.back();
+                stack.pop_back();
+                comps[id].push_back(q);
+                const int qi = q / W, qj = q % W;
+                const int ni[4] = {qi - 1, qi + 1, qi, qi}, nj[4] = {qj, qj, qj - 1, qj + 1};
+                for (int t = 0; t < 4; t++) {
+                    if (ni[t] < 0 || ni[t] >= H || nj[t] < 0 || nj[t] >= W) continue;
+                    const size_t o = (size_t)ni[t] * W + nj[t];
+                    if (comp[o] < 0 && dz(ni[t], nj[t]) <= 0) { comp[o] = id; stack.push_back((int)o); }
+                }
+            }
+        }
+    std::vector<int> count(N, -1);  // valid 3x3 neighbours of the region's unfilled pixels; -1 otherwise
+    for (auto& c : comps) {
+        if (c.size() > maxRegion) continue;
+        std::sort(c.begin(), c.end());
+        std::vector<std::set<int>> bucket(9);
+        for (int q : c) {
+            const int i = q / W, j = q % W;
+            int n = 0;
+            for (int ii = std::max(0, i - 1); ii <= std::min(H - 1, i + 1); ii++)
+                for (int jj = std::max(0, j - 1); jj <= std::min(W - 1, j + 1); jj++)
+                    if (dz(ii, jj) > 0) n++;
+            count[q] = n;
+            bucket[n].insert(q);
+        }
+        for (size_t left = c.size(); left > 0; left--) {
+            int m = 8;
+            while (m >= 0 && bucket[m].empty()) m--;
+            if (m <= 0) throw std::runtime_error("colour-guided fill: a region without valid neighbours");
+            const int q = *bucket[m].begin();
+            bucket[m].erase(bucket[m].begin());
+            count[q] = -1;
+            const int i = q / W, j = q % W;
+            float zSum = 0, weightSum = 0;
+            for (int ii = std::max(0, i - 1); ii <= std::min(H - 1, i + 1); ii++)
+                for (int jj = std::max(0, j - 1); jj <= std::min(W - 1, j + 1); jj++) {
+                    const size_t o2 = (size_t)ii * W + jj;
+                    if (dz(ii, jj) > 0) {
+                        const size_t a = (size_t)q * 3, b = o2 * 3;
+                        const float w = (float)std::exp(-(sqr(col.d[a] - col.d[b]) + sqr(col.d[a + 1] - col.d[b + 1]) +
+                                                          sqr(col.d[a + 2] - col.d[b + 2])) / .6);
+                        zSum = (float)(zSum + dz(ii, jj) * w);  // float += double, as the reference
+                        weightSum += w;
+                    } else if (count[o2] >= 0) {
+                        bucket[count[o2]].erase((int)o2);
+                        count[o2]++;
+                        bucket[count[o2]].insert((int)o2);
+                    }
+                }
+            dz(i, j) = zSum / weightSum;
+        }
     }
 }
 
@@ -1689,7 +1803,6 @@ int sfo_scene_flow_two_frames(int fp64, const rgbdflow_camera_params* camFull, c
                               const float* est_flow, float* flow_out, rgbdflow_stats* stats)
 {
     try {
-        if (prm->regularization == RGBDFLOW_REG_HPB) { g_err = "HPB regularisation is not built"; return RGBDFLOW_ERR_UNSUPPORTED; }
         const rgbdflow_camera_params cam = resize_cam(*camFull, W);
         std::vector<float> s1((size_t)W * H);
         depth_sigma(depth1, W, H, prm->depth_boundary_dist, s1.data());
@@ -1707,6 +1820,22 @@ int sfo_scene_flow_two_frames(int fp64, const rgbdflow_camera_params* camFull, c
             flow_out[l * 3] = (float)u.d[l]; flow_out[l * 3 + 1] = (float)v.d[l]; flow_out[l * 3 + 2] = (float)w.d[l];
         }
         trace_to_stats(t, stats);
+        return 0;
+    } catch (const std::exception& e) { g_err = e.what(); return -1; }
+}
+
+/* recursiveMedianFilterSmallInvalidRegionsUsingColor in place on a W x H depth map, guided by
+ * the W*H*3 colour image (doubles in [0, 1]). */
+int sfo_fill_small_regions_color(double* depth, const double* col, int W, int H, int max_region)
+{
+    try {
+        Img d, c;
+        d.alloc(W, H, 1);
+        c.alloc(W, H, 3);
+        std::memcpy(d.data(), depth, sizeof(double) * (size_t)W * H);
+        std::memcpy(c.data(), col, sizeof(double) * (size_t)W * H * 3);
+        fill_small_regions_color(d, c, (unsigned)max_region);
+        std::memcpy(depth, d.data(), sizeof(double) * (size_t)W * H);
         return 0;
     } catch (const std::exception& e) { g_err = e.what(); return -1; }
 }

@@ -83,6 +83,7 @@ def oracle():
         lib.sfo_optical_flow_2d_ring.argtypes = [_pu8, _pu8, _i, _i, _d, _d, _i, _i, _i, _i, _i, _pd, _pd]
         lib.sfo_depth_map_pyramid.argtypes = [_pd, _i, _i, _d, _i, _pd, _pi]
         lib.sfo_heuristic_pb.argtypes = [_pd, _pd, _i, _i, _pf]
+        lib.sfo_fill_small_regions_color.argtypes = [_pd, _pd, _i, _i, _i]
         lib.sfo_last_error.restype = ctypes.c_char_p
         lib.sfo_set_threads.argtypes = [_i]
         _oracle = lib
@@ -168,6 +169,16 @@ def optical_flow_2d(bgr1, bgr2, alpha=0.02, ratio=0.75, min_width=20, n_outer=10
 
 
 _ref_hpb = None
+
+
+def fill_small_regions_color(depth, col, max_region=60):
+    """recursiveMedianFilterSmallInvalidRegionsUsingColor (oracle, deterministic order): a filled
+    copy of depth (H, W), guided by col (H, W, 3) in [0, 1]."""
+    d, c = _cont(depth, np.float64).copy(), _cont(col, np.float64)
+    H, W = d.shape
+    if oracle().sfo_fill_small_regions_color(dptr(d), dptr(c), W, H, max_region) != 0:
+        raise RuntimeError(oracle().sfo_last_error().decode())
+    return d
 
 
 def heuristic_pb(img, depth):

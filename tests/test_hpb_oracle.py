@@ -90,3 +90,47 @@ def test_hpb_colour_edge_without_depth():
     # the half-disk means come from float integral images, as in the reference; their
     # cancellation error grows with the row (2e-5 at the bottom of this level)
     assert abs(pb[:, 29, 0] - expect).max() < 1e-4
+
+
+def test_colour_guided_fill_known_answers():
+    """recursiveMedianFilterSmallInvalidRegionsUsingColor (recursiveMedianFiltering.cpp:127-222):
+    a hole in constant depth takes that depth; the colour weights pull a hole towards the side of
+    its own colour; a region larger than the limit stays invalid."""
+    col = np.full((20, 30, 3), 0.5)
+    d = np.full((20, 30), 2.0)
+    d[5, 5] = 0
+    d[10:12, 10:13] = 0
+    out = ob.fill_small_regions_color(d, col)
+    np.testing.assert_array_equal(out, np.full((20, 30), 2.0))
+    d = np.full((20, 30), 1.0)
+    d[:, 15:] = 3.0
+    col2 = col.copy()
+    col2[:, 15:] = 0.9
+    d[8, 15] = 0  # a hole on the 3 m side, whose colour it shares
+    out = ob.fill_small_regions_color(d, col2)
+    # 3 neighbours at 1 m of the other colour (weight exp(-3 * .4^2 / .6)), 5 at 3 m of its own (weight 1)
+    w = np.exp(-3 * (0.9 - 0.5) ** 2 / 0.6)
+    assert abs(out[8, 15] - (3 * w * 1.0 + 5 * 3.0) / (3 * w + 5)) < 1e-5
+    d = np.full((20, 30), 2.0)
+    d[2:12, 2:12] = 0  # 100 pixels > 60
+    out = ob.fill_small_regions_color(d, col)
+    assert np.all(out[2:12, 2:12] == 0) and np.all(out[:2] == 2.0)
+
+
+def test_hpb_scene_flow_end_to_end():
+    """The oracle's scene flow with HPB regularisation (per level: colour-guided fill of the raw
+    depth, DepthMapPyramid, computeHeuristicPb, weights 1 - .99 hpb) is finite and no less accurate
+    against ground truth than the isotropic solve on a textured-patch scene."""
+    import rgbdflow as rf
+    p = syn.make_config_pair("320x240", seed=3)
+    cam = rf.CameraParams.make(p["W"], p["H"], p["cam"].f, p["cam"].cx, p["cam"].cy)
+    iso = rf.benchmark_params(320)
+    hpb = rf.benchmark_params(320)
+    hpb.regularization = rf.REG_HPB
+    fi, _ = ob.two_frames(cam, p["bgr1"], p["depth1"], p["bgr2"], p["depth2"], iso)
+    fh, _ = ob.two_frames(cam, p["bgr1"], p["depth1"], p["bgr2"], p["depth2"], hpb)
+    assert np.isfinite(fh).all() and not np.array_equal(fh, fi)
+    valid = p["depth1"] > 0
+    ei = syn.epe3d(fi, p["gt"], p["z1_true"], p["cam"], valid)[0]
+    eh = syn.epe3d(fh, p["gt"], p["z1_true"], p["cam"], valid)[0]
+    assert eh <= ei * 1.05
