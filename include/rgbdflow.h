@@ -270,6 +270,34 @@ int rgbdflow_profile(rgbdflow_ctx* ctx, int enable);
 int rgbdflow_profile_read(rgbdflow_ctx* ctx, rgbdflow_kernel_stat* out, int max);
 
 /* ---------------------------------------------------------------------------------------------
+ * Stage read-back (no reference counterpart; diagnostics and per-stage parity tests).  After a
+ * solve on ctx, any plane of its device state can be read back: the pyramids, the level inputs
+ * the linearisation reads, the flow of each level and the last linear system built at each level.
+ * The reference keeps the same quantities as DImage / device buffers inside sceneFlowMultiscale
+ * (src/sceneFlowMultiscale.cpp:85-177) and sceneFlowSingleScale (.cu:676-870).
+ * ------------------------------------------------------------------------------------------- */
+#define RGBDFLOW_PLANE_PYRAMID     0 /* index 0..9: colour 1 (B, G, R in [0, 1]), colour 2 (B, G, R),
+                                        filled depth 1, filled depth 2 (m), depth-data weight,
+                                        depth-smoothness weight (GaussianPyramid levels) */
+#define RGBDFLOW_PLANE_FEATURES1   1 /* index 0..4: im2feature of colour 1 (gray, dx, dy, G-B, G-R) */
+#define RGBDFLOW_PLANE_FEATURES2   2 /* index 0..4: the same of colour 2 */
+#define RGBDFLOW_PLANE_DEPTH       3 /* index 0, 1: depth 1 / 2 in the storage type */
+#define RGBDFLOW_PLANE_DEPTH_MAG   4 /* index 0: depth-magnitude weight */
+#define RGBDFLOW_PLANE_REG         5 /* index 0, 1: regularisation weight to the right / lower neighbour */
+#define RGBDFLOW_PLANE_FLOW        6 /* index 0..2: u, v (px), w (m) of the level */
+#define RGBDFLOW_PLANE_SYSTEM      7 /* index 0..11: the last linearisation's compact system: 1 / diagonal
+                                        (u, v, w), couplings uv, uw, vw, right-hand sides (u, v, w),
+                                        alpha * phi * right weight, alpha * phi * down weight, depth-
+                                        smoothness weight (fillSystemMtxKernel, .cu:477-575) */
+#define RGBDFLOW_PLANE_FILL_ROUND  8 /* level 0, index 0, 1: the hole-fill round that filled each pixel of
+                                        depth 1 / 2 (0: valid input, 255: never filled) */
+/* Copies plane (kind, index) of pair `pair` (batch order), pyramid level `level` (0 = finest) of
+ * the context's last solve into dst (n doubles, W * H needed, raster order); W and H (either may
+ * be NULL) receive the level's size.  Waits for the solve to finish. */
+int rgbdflow_debug_read_plane(rgbdflow_ctx* ctx, int pair, int level, int kind, int index, double* dst, size_t n,
+                              int* W, int* H);
+
+/* ---------------------------------------------------------------------------------------------
  * Served form (no reference counterpart): continuous batching over camera streams.  A frame
  * submitted on a stream forms a pair with that stream's previous frame; the stream's previous
  * frame pyramid and previous flow stay resident on the device for warm starts.  Requests are
@@ -343,7 +371,13 @@ int rgbdflow_server_counters_read(rgbdflow_server* srv, int reset, rgbdflow_serv
  *   result; est_flow NULL or a warm start).  stream: a cudaStream_t as void*, NULL = the legacy
  *   default stream.  Runs on the current device and returns after enqueue.
  *   Set-up: the first call on each device looks up the workspace address and sets kernel
- *   attributes; make that first call before any stream capture.
+ *   attributes; make that first call before any stream capture.  The set-up is kept for the life
+ *   of the process: after cudaDeviceReset on a device this call is not supported there.
+ *   Host memory: the call's descriptors travel to the workspace as kernel parameters, so nothing
+ *   it enqueues reads host memory after it returns.
+ *   Footprint: the 40 MiB array belongs to the library's device code, so every process that loads
+ *   the library holds it on each device where that code is loaded (at the latest when any of the
+ *   library's kernels first runs there), whether or not it calls this function.
  *   Zeroing: nothing in the workspace has to start at zero; every call clears, on the stream, the
  *   counters it relies on.
  *   Overlap: all calls on a device share the one workspace.  Two calls whose work overlaps on

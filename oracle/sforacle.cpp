@@ -256,6 +256,85 @@ void median_fill(double* data, int width, int height, int hw)
     }
 }
 
+/* The same fill in the device's order (window half-width 1): rounds r = 1, 2, ...  In round r every
+ * hole whose count of known 8-neighbours (valid, or filled in an earlier round) is > 0 and is not
+ * smaller than the count of any unfilled 8-neighbour takes the median of its known neighbours, read
+ * as they were at the start of the round.  Each value still is the median of the 3x3 known values
+ * (recursiveMedianFiltering.cpp:67-94); only the order, among holes that touch, differs from the
+ * reference's hash-set order.  Isolated holes get the reference's value.  This restates the
+ * library's schedule so that the parity tests can separate the fill order (measured on its own)
+ * from the arithmetic of the rest of the solve.  Returns the number of rounds. */
+int median_fill_rounds(double* data, int width, int height)
+{
+    const size_t N = (size_t)width * height;
+    std::vector<int> stamp(N);  // 0 valid, -1 unfilled, r filled in round r
+    size_t left = 0;
+    for (size_t l = 0; l < N; l++) {
+        stamp[l] = data[l] > 0 ? 0 : -1;
+        if (stamp[l] < 0) left++;
+    }
+    int r = 0;
+    std::vector<int> fill_l;
+    std::vector<double> fill_v;
+    while (left > 0) {
+        r++;
+        auto known = [&](int i, int j) {
+            return i >= 0 && j >= 0 && i < height && j < width && stamp[(size_t)i * width + j] >= 0 &&
+                   stamp[(size_t)i * width + j] < r;
+        };
+        auto count = [&](int i, int j) {
+            int k = 0;
+            for (int a = -1; a <= 1; a++)
+                for (int b = -1; b <= 1; b++)
+                    if ((a | b) && known(i + a, j + b)) k++;
+            return k;
+        };
+        fill_l.clear();
+        fill_v.clear();
+        for (int i = 0; i < height; i++)
+            for (int j = 0; j < width; j++) {
+                if (stamp[(size_t)i * width + j] != -1) continue;
+                const int c = count(i, j);
+                bool fill = c > 0;
+                for (int a = -1; a <= 1 && fill; a++)
+                    for (int b = -1; b <= 1 && fill; b++) {
+                        const int ii = i + a, jj = j + b;
+                        if (!(a | b) || ii < 0 || jj < 0 || ii >= height || jj >= width) continue;
+                        if (stamp[(size_t)ii * width + jj] == -1 && count(ii, jj) > c) fill = false;
+                    }
+                if (!fill) continue;
+                float vals[8];
+                int n = 0;
+                for (int a = -1; a <= 1; a++)
+                    for (int b = -1; b <= 1; b++)
+                        if ((a | b) && known(i + a, j + b)) {
+                            const float x = (float)data[(size_t)(i + a) * width + (j + b)];
+                            int k = n++;
+                            while (k > 0 && vals[k - 1] > x) { vals[k] = vals[k - 1]; k--; }
+                            vals[k] = x;
+                        }
+                fill_l.push_back(i * width + j);
+                fill_v.push_back(vals[n / 2]);
+            }
+        if (fill_l.empty()) throw std::runtime_error("median_fill_rounds: a hole region has no valid neighbour");
+        for (size_t q = 0; q < fill_l.size(); q++) {
+            data[fill_l[q]] = fill_v[q];
+            stamp[fill_l[q]] = r;
+        }
+        left -= fill_l.size();
+    }
+    return r;
+}
+
+/* Fill order of the scene-flow solve's hole fill: 0 the reference's (median_fill), 1 the device's
+ * rounds (median_fill_rounds).  Set by sfo_set_fill_order. */
+static int g_fill_order = 0;
+static void fill_depth(double* data, int width, int height)
+{
+    if (g_fill_order == 1) median_fill_rounds(data, width, height);
+    else median_fill(data, width, height, 1);
+}
+
 /* primesensor::stereoError / stereoErrorRatio (src/primesensorUtils.cpp:53-64). */
 double stereo_error(double z) { return sqr(z) / (1 / .00285 + z); }
 double stereo_error_ratio(double z) { return stereo_error(z) / stereo_error(1); }
@@ -724,6 +803,16 @@ static void hpb_reg_weights(const Img& colour, const Img& rawDepth, std::vector<
         }
 }
 
+/* An external per-level solver with the argument list of sceneFlowSingleScale over raw planes
+ * (the reference's own CUDA solver, oracle/ref_cuda_shim.cu): when set, the faithful variant's
+ * levels are solved by it, everything around them by this file (the reference's own split between
+ * host and device).  Set by sfo_set_level_solver; used to time the reference's GPU path. */
+typedef int (*LevelSolverFn)(float f_level, const double* Im1, const double* dm1, const double* Im2, const double* dm2,
+                             double* warpIm2, double* warpDm2, double* u, double* v, double* w, int W, int H, int C,
+                             double colorW, const double* ddw, double alpha, const double* dsw, double gamma,
+                             const double* mag, const double* regw, int nOuter, int nInner, int nSOR, int allowEarly);
+static LevelSolverFn g_level_solver = nullptr;
+
 template <bool FP64>
 static void run_level(const rgbdflow_camera_params& camFull, const rgbdflow_params& p, int fixed,
                       const Img& feat1, const Img& d1, const Img& feat2, const Img& d2, Img& wI2, Img& wD2,
@@ -742,6 +831,13 @@ static void run_level(const rgbdflow_camera_params& camFull, const rgbdflow_para
     in.colorW = p.color_data_weight; in.alpha = p.alpha; in.gamma = p.gamma;
     in.ddw = ddw; in.dsw = dsw; in.mag = mag.data(); in.regw = rw.data();
     in.nOuter = p.n_outer; in.nInner = p.n_inner; in.nSOR = p.n_sor; in.allowEarly = allowEarly;
+    if (g_level_solver && !FP64) {
+        const int rc = g_level_solver(in.f_level, in.Im1, in.dm1, in.Im2, in.dm2, wI2.data(), wD2.data(), u.data(),
+                                      v.data(), w.data(), W, H, in.C, in.colorW, ddw, in.alpha, dsw, in.gamma, in.mag,
+                                      in.regw, in.nOuter, in.nInner, in.nSOR, allowEarly);
+        if (rc != 0) throw std::runtime_error("external level solver failed: " + std::to_string(rc));
+        return;
+    }
     single_scale<FP64>(in, p, fixed, wI2, wD2, u.data(), v.data(), w.data(), tr);
 }
 
@@ -763,8 +859,8 @@ void multiscale(const rgbdflow_camera_params& cam, const rgbdflow_params& p, con
     }
     Img d1 = dm1, d2 = dm2;
     if (p.fill_holes) {
-        median_fill(d1.data(), d1.w, d1.h, 1);
-        median_fill(d2.data(), d2.w, d2.h, 1);
+        fill_depth(d1.data(), d1.w, d1.h);
+        fill_depth(d2.data(), d2.w, d2.h);
     }
     if (est) {
         const int W = Im1.w, H = Im1.h;
@@ -1653,6 +1749,21 @@ void sfo_im2feature(const double* bgr01, int W, int H, double* feat5)
     Img f;
     im2feature(b, f);
     std::memcpy(feat5, f.data(), sizeof(double) * f.n());
+}
+
+void sfo_set_level_solver(void* fn) { g_level_solver = (LevelSolverFn)fn; }
+
+int sfo_set_fill_order(int order)
+{
+    const int old = g_fill_order;
+    g_fill_order = order;
+    return old;
+}
+
+int sfo_median_fill_rounds(double* depth, int W, int H, int* rounds)
+{
+    try { *rounds = median_fill_rounds(depth, W, H); return 0; }
+    catch (const std::exception& e) { g_err = e.what(); return -1; }
 }
 
 int sfo_median_fill(double* depth, int W, int H)

@@ -283,30 +283,69 @@ __global__ void k_sigma(const PrepItem<T>* items, const Tile* tiles)
     it.dsw[l] = it.f2;
 }
 
-// One round of the parallel recursive-median hole fill.  The reference fills holes one at a
-// time, most-known-neighbours first, each from the median of its valid 3x3 neighbours
-// (recursiveMedianFiltering.cpp:35-99).  Here every unfilled pixel whose known-neighbour count is
-// >= that of every unfilled pixel in its 3x3 neighbourhood is filled in the same round, from
-// the pixels valid before the round (round stamps make the rounds deterministic).  Isolated
-// holes get exactly the reference's value; inside larger holes the order (and so the value)
-// can differ from the reference's hash-set order.
-template <class T>
-__global__ void k_fill_round(const PrepItem<T>* items, const Tile* tiles, int n_tiles, int* left, int* tleft, int round)
+// The parallel recursive-median hole fill.  The reference fills holes one at a time,
+// most-known-neighbours first, each from the median of its valid 3x3 neighbours
+// (recursiveMedianFiltering.cpp:35-99).  Here the fill runs in rounds: in round r every unfilled
+// pixel whose known-neighbour count is >= that of every unfilled pixel in its 3x3 neighbourhood is
+// filled, from the pixels valid before the round (round stamps make the rounds deterministic).
+// Isolated holes get exactly the reference's value; inside larger holes the order (and so the
+// value) can differ from the reference's hash-set order.
+
+// Grid-wide barrier of a cooperative launch (every block resident), bounded: a block that waits
+// longer than ~0.3 s sets err and leaves; every later barrier then fails at once.
+struct GridSync {
+    unsigned count;  // blocks arrived at the current barrier
+    unsigned gen;    // barriers completed
+    int err;         // a wait gave up
+    int pad;
+};
+
+__device__ __forceinline__ bool grid_barrier(GridSync* g, unsigned nblocks)
 {
-    // left[r]: hole pixels (all pairs, both frames) still unfilled after round r; tleft[ti]: nonzero
-    // while tile ti holds one.  A block takes the tiles blockIdx.x + k gridDim.x; after round 1 it
-    // gathers, 32 at a time, only those that still hold holes, and once every hole is filled the
-    // remaining rounds end after one load.
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = *(volatile int*)&g->err == 0;
+        const unsigned gen0 = *(volatile unsigned*)&g->gen;  // read before arriving
+        __threadfence();
+        if (atomicAdd(&g->count, 1u) == nblocks - 1) {
+            atomicExch(&g->count, 0u);
+            __threadfence();
+            atomicAdd(&g->gen, 1u);
+        } else {
+            unsigned spins = 0;
+            while (*(volatile unsigned*)&g->gen == gen0) {
+                if (++spins > (1u << 22) || *(volatile int*)&g->err) {
+                    atomicExch(&g->err, 1);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// One round over the tiles of block `blk` of `nblk`.  left[r]: hole pixels (all pairs, both frames)
+// still unfilled after round r; tleft[ti]: nonzero while tile ti holds one.  A block takes the tiles
+// blk + k nblk; after round 1 it gathers, 32 at a time, only those that still hold holes.
+template <class T>
+__device__ __forceinline__ void fill_round(const PrepItem<T>* items, const Tile* tiles, int n_tiles, int* left,
+                                           int* tleft, int round, int blk, int nblk)
+{
     constexpr int FH = LTH + 4, FW = LTW + 4;
     __shared__ int s_list[32];
     __shared__ int s_n;
     __shared__ uint8_t s_st[2][FH][FW];
-    if (round > 1 && left[round - 1] == 0) return;
-    const int per = (n_tiles - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
+    const int per = (n_tiles - blk + nblk - 1) / nblk;
     for (int k0 = 0; k0 < per; k0 += 32) {
         if (threadIdx.x < 32) {
             const int k = k0 + threadIdx.x;
-            const int ti = blockIdx.x + k * gridDim.x;
+            const int ti = blk + k * nblk;
             const bool has = k < per && (round == 1 || tleft[ti] != 0);
             const unsigned m = __ballot_sync(0xffffffffu, has);
             if (has) s_list[__popc(m & ((1u << threadIdx.x) - 1))] = ti;
@@ -364,8 +403,8 @@ __global__ void k_fill_round(const PrepItem<T>* items, const Tile* tiles, int n_
                 it.dep[f][i * W + j] = (T)v[nv / 2];
                 it.stamp[f][i * W + j] = (uint8_t)round;
             }
-            // pixels still unfilled after this round: all pairs (early exit of later rounds) and
-            // per tile (later rounds skip the tile when none is left)
+            // pixels still unfilled after this round: all pairs (end of the rounds) and per tile
+            // (later rounds skip the tile when none is left)
             const int any = __syncthreads_count(nleft > 0);
             const unsigned m = __ballot_sync(0xffffffffu, nleft > 0);
             int tot = nleft;
@@ -374,6 +413,19 @@ __global__ void k_fill_round(const PrepItem<T>* items, const Tile* tiles, int n_
             if (threadIdx.x == 0) tleft[ti] = any;
         }
         __syncthreads();  // s_list is refilled
+    }
+}
+
+// Every round of the fill in one cooperative launch: a grid barrier between rounds, done once no
+// hole is left (or after max_rounds, or when a barrier wait gives up).
+template <class T>
+__global__ void __launch_bounds__(LTW * LTH)
+k_fill(const PrepItem<T>* items, const Tile* tiles, int n_tiles, int* left, int* tleft, GridSync* gs, int max_rounds)
+{
+    for (int round = 1; round <= max_rounds; round++) {
+        if (round > 1 && *(volatile int*)&left[round - 1] == 0) break;  // the same value in every block
+        fill_round<T>(items, tiles, n_tiles, left, tleft, round, blockIdx.x, gridDim.x);
+        if (!grid_barrier(gs, gridDim.x)) break;
     }
 }
 

@@ -272,7 +272,8 @@ struct Plan {
     std::vector<PyrLevelDesc> pyr;
     size_t prep_items_off = 0, prep_tiles_off = 0; int n_prep_tiles = 0;
     size_t out_ptrs_off = 0;
-    size_t unfilled_off = 0;            // int[256]: hole pixels left after each fill round
+    size_t unfilled_off = 0;            // int[256]: hole pixels left after each fill round, then the
+                                        // fill's GridSync (zeroed together)
     size_t tleft_off = 0;               // int[prep tiles]: the tile still holds a hole
     std::vector<std::vector<std::vector<SorLaunch>>> sor_sched;  // [step][inner iteration]
     std::vector<std::vector<int>> n_checks;                     // [step][inner iteration]
@@ -353,7 +354,7 @@ static Plan<T, S> make_plan(const std::vector<PairSpec>& pairs, const HostParams
     Bump A;
     P.ctl_off = A.take(sizeof(PairCtl) * P.n);
     P.ctr_off = A.take(sizeof(int) * 16);
-    P.unfilled_off = A.take(sizeof(int) * 256);
+    P.unfilled_off = A.take(sizeof(int) * 256 + sizeof(GridSync));
     {
         size_t nt = 0;
         for (const auto& p : pairs) nt += (size_t)((p.W + LTW - 1) / LTW) * ((p.H + LTH - 1) / LTH);
@@ -941,7 +942,7 @@ static int enqueue_solve(const Plan<T, S>& P, char* base, cudaStream_t st, Prof*
         RF_PROF_E(pf, st);
         launches++;
     } else {
-        RF_CUDA(cudaMemsetAsync(base + P.unfilled_off, 0, sizeof(int) * 256, st));
+        RF_CUDA(cudaMemsetAsync(base + P.unfilled_off, 0, sizeof(int) * 256 + sizeof(GridSync), st));
         const PrepItem<T>* prep = (const PrepItem<T>*)(db + P.prep_items_off);
         const Tile* pt = (const Tile*)(db + P.prep_tiles_off);
         RF_PROF_B(pf, KC_PREP, st);
@@ -951,14 +952,32 @@ static int enqueue_solve(const Plan<T, S>& P, char* base, cudaStream_t st, Prof*
         k_sigma<T><<<P.n_prep_tiles, LTW * LTH, 0, st>>>(prep, pt);
         RF_PROF_E(pf, st);
         launches += 2;
-        if (P.hp.fill_holes)
-            for (int r = 1; r <= P.hp.fill_rounds; r++) {
-                RF_PROF_B(pf, KC_FILL, st);
-                k_fill_round<T><<<std::min(P.n_prep_tiles, 8 * P.sms), LTW * LTH, 0, st>>>(
-                    prep, pt, P.n_prep_tiles, (int*)(base + P.unfilled_off), (int*)(base + P.tleft_off), r);
-                RF_PROF_E(pf, st);
-                launches++;
-            }
+        if (P.hp.fill_holes) {
+            // one cooperative launch runs every round (grid barriers between rounds)
+            static int per_sm[2] = {0, 0};
+            int& occ = per_sm[sizeof(T) == 8];
+            if (!occ) RF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fill<T>, LTW * LTH, 0));
+            const int grid = std::max(1, std::min(P.n_prep_tiles, std::min(occ, 8) * P.sms));
+            int* left = (int*)(base + P.unfilled_off);
+            GridSync* gs = (GridSync*)(left + 256);
+            int* tleft = (int*)(base + P.tleft_off);
+            const int rounds = P.hp.fill_rounds;
+            const int nt = P.n_prep_tiles;
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(grid);
+            cfg.blockDim = dim3(LTW * LTH);
+            cfg.dynamicSmemBytes = 0;
+            cfg.stream = st;
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeCooperative;
+            at[0].val.cooperative = 1;
+            cfg.attrs = at;
+            cfg.numAttrs = 1;
+            RF_PROF_B(pf, KC_FILL, st);
+            RF_CUDA(cudaLaunchKernelEx(&cfg, k_fill<T>, prep, pt, nt, left, tleft, gs, rounds));
+            RF_PROF_E(pf, st);
+            launches++;
+        }
         for (const auto& lv : P.pyr) {
             const PyrJob<T>* jobs = (const PyrJob<T>*)(db + lv.jobs_off);
             const T* g = (const T*)(db + lv.g_off);

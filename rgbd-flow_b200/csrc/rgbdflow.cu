@@ -12,6 +12,7 @@
 #include <mutex>
 #include <string>
 #include <vector>
+#include <type_traits>
 
 #include "../../include/rgbdflow.h"
 #include "pipeline.cuh"
@@ -29,6 +30,23 @@ struct GraphEntry {
     uint64_t last_use = 0;  // for least-recently-used eviction
 };
 constexpr size_t kGraphCache = 48;  // executable graphs kept per context
+
+// Where the last solve's planes live, per pair and level (rgbdflow_debug_read_plane).
+struct DbgLevel {
+    int W = 0, H = 0, pitch = 0, hwp = 0;
+    const void* pyr[10];
+    const void* I1[5];
+    const void* I2[5];
+    const void* D[2];
+    const void* mag;
+    const void* reg[2];
+    const void* u[3];
+    const void* sys[12];
+};
+struct DbgPair {
+    std::vector<DbgLevel> lev;
+    const void* stamp[2] = {nullptr, nullptr};
+};
 
 struct rgbdflow_ctx {
     int device = 0;
@@ -57,6 +75,10 @@ struct rgbdflow_ctx {
     double prof_ms[KC_TOTAL] = {0};
     int prof_n[KC_TOTAL] = {0};
     double prof_bytes[KC_TOTAL] = {0};
+    // the last solve's layout (stage read-back)
+    std::vector<DbgPair> dbg;
+    int dbg_tsize = 4;  // bytes of the arithmetic type T
+    int dbg_store = 0;  // storage type of the features / depths: 0 FP32, 1 FP16, 2 BF16, 3 FP64
 };
 
 namespace {
@@ -145,7 +167,7 @@ HostParams host_params(const rgbdflow_params& p)
     h.strip_min_px = e ? std::atol(e) : 0;
     e = std::getenv("RGBDFLOW_SOR_LEVEL");
     h.sor_level = e ? std::atoi(e) : 1;
-    h.fill_rounds = 64;
+    h.fill_rounds = 253;  // round stamps are bytes: 0 valid, 1..253 rounds, 254 outside, 255 unfilled
     return h;
 }
 
@@ -227,6 +249,39 @@ void fill_stats(const PairCtl& c, int L, const PyrShape& s, double ms, rgbdflow_
         }
     }
     st->device_ms = ms;
+}
+
+// Records where plan P (bound to the arena) keeps every plane, for rgbdflow_debug_read_plane.
+template <class T, class S>
+void record_layout(rgbdflow_ctx* c, const Plan<T, S>& P)
+{
+    c->dbg.assign(P.n, DbgPair());
+    c->dbg_tsize = (int)sizeof(T);
+    c->dbg_store = sizeof(S) == 8 ? 3 : (sizeof(S) == 4 ? 0 : (std::is_same<S, __half>::value ? 1 : 2));
+    const unsigned char* d = P.desc.data();
+    const PrepItem<T>* prep = (const PrepItem<T>*)(d + P.prep_items_off);
+    for (int p = 0; p < P.n; p++) {
+        c->dbg[p].lev.resize(P.L[p]);
+        c->dbg[p].stamp[0] = prep[p].stamp[0];
+        c->dbg[p].stamp[1] = prep[p].stamp[1];
+    }
+    for (int sidx = 0; sidx < P.Lmax; sidx++) {
+        const int k = P.Lmax - 1 - sidx;
+        const LevelItem<T, S>* it = (const LevelItem<T, S>*)(d + P.steps[sidx].items_off);
+        int q = 0;  // items of a step are its pairs in batch order
+        for (int p = 0; p < P.n; p++) {
+            if (k >= P.L[p]) continue;
+            const LevelItem<T, S>& x = it[q++];
+            DbgLevel& L = c->dbg[p].lev[k];
+            L.W = x.W; L.H = x.H; L.pitch = x.pitch; L.hwp = x.hwp;
+            for (int z = 0; z < 10; z++) L.pyr[z] = x.pyr[z];
+            for (int z = 0; z < 5; z++) { L.I1[z] = x.I1[z]; L.I2[z] = x.I2[z]; }
+            L.D[0] = x.D1; L.D[1] = x.D2;
+            L.mag = x.mag; L.reg[0] = x.rh; L.reg[1] = x.rv;
+            for (int z = 0; z < 3; z++) L.u[z] = x.u[z];
+            for (int z = 0; z < 12; z++) L.sys[z] = x.sys[z];
+        }
+    }
 }
 
 template <class T, class S>
@@ -318,6 +373,7 @@ void run_batch(rgbdflow_ctx* c, const std::vector<PairSpec>& pairs, const HostPa
     P.sms = c->sms;
     ensure_arena(c, P.arena_bytes);
     bind_plan(P, c->arena);
+    record_layout(c, P);
     if (dev) {
         // point the work lists at the caller's device buffers
         unsigned char* d = P.desc.data();
@@ -1047,6 +1103,70 @@ int rgbdflow_optical_flow_2d(rgbdflow_ctx* c, const uint8_t* bgr1, const uint8_t
     API_END(c)
 }
 
+int rgbdflow_debug_read_plane(rgbdflow_ctx* c, int pair, int level, int kind, int index, double* dst, size_t n, int* W,
+                              int* H)
+{
+    if (!c) return RGBDFLOW_ERR_INVALID_ARG;
+    try {
+        if (pair < 0 || pair >= (int)c->dbg.size()) throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "no such pair in the last solve");
+        const DbgPair& dp = c->dbg[pair];
+        if (level < 0 || level >= (int)dp.lev.size()) throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "no such level");
+        if (kind == RGBDFLOW_PLANE_FILL_ROUND && level != 0) throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "fill rounds exist at level 0 only");
+        const DbgLevel& L = dp.lev[level];
+        const int w = L.W, h = L.H;
+        if (W) *W = w;
+        if (H) *H = h;
+        const size_t N = (size_t)w * h;
+        if (!dst) return RGBDFLOW_OK;
+        if (n < N) throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "destination too small");
+        static const int counts[9] = {10, 5, 5, 2, 1, 2, 3, 12, 2};
+        if (kind < 0 || kind > 8 || index < 0 || index >= counts[kind]) throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "bad plane kind or index");
+        const void* src = nullptr;
+        int esize = c->dbg_tsize, etype = c->dbg_tsize == 8 ? 3 : 0;  // 0 FP32, 1 FP16, 2 BF16, 3 FP64, 4 u8
+        int layout = 0;                                                // 0 raster, 1 pitched u, 2 checkerboard
+        switch (kind) {
+        case RGBDFLOW_PLANE_PYRAMID: src = L.pyr[index]; break;
+        case RGBDFLOW_PLANE_FEATURES1: src = L.I1[index]; etype = c->dbg_store; break;
+        case RGBDFLOW_PLANE_FEATURES2: src = L.I2[index]; etype = c->dbg_store; break;
+        case RGBDFLOW_PLANE_DEPTH: src = L.D[index]; etype = c->dbg_store; break;
+        case RGBDFLOW_PLANE_DEPTH_MAG: src = L.mag; break;
+        case RGBDFLOW_PLANE_REG: src = L.reg[index]; break;
+        case RGBDFLOW_PLANE_FLOW: src = L.u[index]; layout = 1; break;
+        case RGBDFLOW_PLANE_SYSTEM: src = L.sys[index]; layout = 2; break;
+        default: src = dp.stamp[index]; etype = 4; break;
+        }
+        if (etype == 1 || etype == 2) esize = 2;
+        if (etype == 4) esize = 1;
+        const size_t elems = layout == 0 ? N : (layout == 1 ? (size_t)L.pitch * h : (size_t)2 * L.hwp * h);
+        wait_idle(c);
+        std::vector<unsigned char> buf(elems * esize);
+        RF_CUDA(cudaMemcpy(buf.data(), src, buf.size(), cudaMemcpyDeviceToHost));
+        auto at = [&](size_t e) -> double {
+            const unsigned char* b = buf.data() + e * esize;
+            switch (etype) {
+            case 0: { float f; std::memcpy(&f, b, 4); return f; }
+            case 1: { __half x; std::memcpy(&x, b, 2); return (double)__half2float(x); }
+            case 2: { __nv_bfloat16 x; std::memcpy(&x, b, 2); return (double)__bfloat162float(x); }
+            case 3: { double f; std::memcpy(&f, b, 8); return f; }
+            default: return (double)b[0];
+            }
+        };
+        for (int i = 0; i < h; i++)
+            for (int j = 0; j < w; j++) {
+                const size_t e = layout == 0 ? (size_t)i * w + j
+                                             : (layout == 1 ? (size_t)i * L.pitch + j : (size_t)cs_idx(i, j, L.hwp));
+                dst[(size_t)i * w + j] = at(e);
+            }
+        return RGBDFLOW_OK;
+    } catch (const ArgError& e) {
+        return fail(c, e.code, e.what());
+    } catch (const CudaError& e) {
+        return fail(c, RGBDFLOW_ERR_CUDA, e.what());
+    } catch (const std::exception& e) {
+        return fail(c, RGBDFLOW_ERR_INTERNAL, e.what());
+    }
+}
+
 int rgbdflow_profile(rgbdflow_ctx* c, int enable)
 {
     if (!c) return RGBDFLOW_ERR_INVALID_ARG;
@@ -1533,6 +1653,17 @@ const NoAllocDevice& noalloc_setup(int dev)
     return d;
 }
 
+// The plan's descriptors reach the workspace as kernel parameters, a chunk per launch: nothing the
+// call enqueues reads host memory after the call returns.
+constexpr int kDescChunk = 3968;  // with the other parameters, under the 4 KB parameter limit
+struct DescChunk {
+    unsigned char b[kDescChunk];
+};
+__global__ void k_put_desc(unsigned char* dst, const DescChunk c, int n)
+{
+    for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = c.b[i];
+}
+
 int noalloc_fail(char* err, size_t err_len, int code, const std::string& m)
 {
     if (err && err_len) {
@@ -1584,8 +1715,13 @@ extern "C" int rgbdflow_scene_flow_noalloc(const rgbdflow_pair* pair, const rgbd
         ((float**)(db + P.out_ptrs_off))[0] = q.flow_out;
         ((EstSrc*)(db + P.est_src_off))[0].f = q.est_flow;
         const cudaStream_t st = (cudaStream_t)stream;
-        // pageable source: the copy is staged before cudaMemcpyAsync returns, so P may go out of scope
-        RF_CUDA(cudaMemcpyAsync(d.scratch + P.desc_off, P.desc.data(), P.desc_bytes, cudaMemcpyHostToDevice, st));
+        for (size_t o = 0; o < P.desc_bytes; o += kDescChunk) {
+            DescChunk ch;
+            const int n = (int)std::min<size_t>(kDescChunk, P.desc_bytes - o);
+            std::memcpy(ch.b, P.desc.data() + o, n);
+            k_put_desc<<<1, 256, 0, st>>>((unsigned char*)d.scratch + P.desc_off + o, ch, n);
+        }
+        RF_CUDA(cudaGetLastError());
         enqueue_solve(P, d.scratch, st);
         return RGBDFLOW_OK;
     } catch (const ArgError& e) {

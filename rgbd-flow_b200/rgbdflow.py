@@ -22,6 +22,9 @@ LIB_PATH = os.path.join(HERE, "librgbdflow.so")
 
 REG_ISOTROPIC, REG_LETOUZEY, REG_HPB = 0, 1, 2
 STORE_FP32, STORE_FP16, STORE_BF16 = 0, 1, 2
+# plane kinds of Context.debug_plane (RGBDFLOW_PLANE_* of include/rgbdflow.h)
+(PLANE_PYRAMID, PLANE_FEATURES1, PLANE_FEATURES2, PLANE_DEPTH, PLANE_DEPTH_MAG, PLANE_REG, PLANE_FLOW, PLANE_SYSTEM,
+ PLANE_FILL_ROUND) = range(9)
 COMPUTE_FP32, COMPUTE_FP64 = 0, 1
 MAX_LEVELS, MAX_OUTER = 16, 64
 
@@ -191,6 +194,7 @@ SIGNATURES = {
     "rgbdflow_ctx_last_launch_count": (_i, [_vp]),
     "rgbdflow_profile": (_i, [_vp, _i]),
     "rgbdflow_profile_read": (_i, [_vp, _P(KernelStat), _i]),
+    "rgbdflow_debug_read_plane": (_i, [_vp, _i, _i, _i, _i, _P(_d), ctypes.c_size_t, _P(_i), _P(_i)]),
     "rgbdflow_server_create": (_i, [_vp, _P(ServerConfig), _P(_vp)]),
     "rgbdflow_server_destroy": (_i, [_vp]),
     "rgbdflow_server_submit": (_i, [_vp, _i, ctypes.c_uint64, _P(CameraParams), _vp, _vp, _i, _i, _vp]),
@@ -449,6 +453,17 @@ class Context:
         buf = (KernelStat * 32)()
         n = self.lib.rgbdflow_profile_read(self.h, buf, 32)
         return {buf[i].name.decode(): (buf[i].launches, buf[i].ms, buf[i].bytes) for i in range(min(n, 32))}
+
+    def debug_plane(self, pair, level, kind, index=0):
+        """Plane (kind, index) of pair `pair`, pyramid level `level` of the last solve, as an (H, W)
+        float64 array (rgbdflow_debug_read_plane; kind is one of the PLANE_* constants)."""
+        w, h = ctypes.c_int(0), ctypes.c_int(0)
+        self._check(self.lib.rgbdflow_debug_read_plane(self.h, pair, level, kind, index, None, 0, ctypes.byref(w),
+                                                       ctypes.byref(h)))
+        out = np.zeros((h.value, w.value), np.float64)
+        self._check(self.lib.rgbdflow_debug_read_plane(self.h, pair, level, kind, index,
+                                                       out.ctypes.data_as(_P(_d)), out.size, None, None))
+        return out
 
     def scene_flow_batch_device(self, pairs, params, stream=None):
         """Device-pointer batch: pairs hold torch CUDA tensors (bgr1/bgr2 uint8 HxWx3, depth1/depth2

@@ -148,6 +148,20 @@ def _holes(rng, H, W, frac):
     return mask
 
 
+def _motion_gt(cam, W, H, patches, z1, sid1, d):
+    """Analytic motion (u px, v px, w m) of the surface points seen in a frame when every patch
+    makes its rigid motion; the background stays."""
+    P1 = d * z1[..., None]
+    P2 = P1.copy()
+    for k, p in enumerate(patches):
+        m = sid1 == k
+        P2[m] = (P1[m] - p.c) @ p.R.T + p.c + p.T
+    x2 = cam.f * P2[..., 0] / P2[..., 2] + cam.cx
+    y2 = cam.f * P2[..., 1] / P2[..., 2] + cam.cy
+    xs, ys = np.meshgrid(np.arange(W, dtype=np.float64), np.arange(H, dtype=np.float64))
+    return np.stack([x2 - xs, y2 - ys, P2[..., 2] - z1], -1).astype(np.float32)
+
+
 def make_pair(W=640, H=480, f=525.0, cx=319.5, cy=239.5, n_patches=6, hole_frac=0.08, seed=0,
               color_noise=2.0, depth_noise=1.45e-3):
     """One frame pair.  Returns a dict with bgr1, bgr2 (H,W,3 uint8), depth1, depth2 (H,W float32
@@ -160,16 +174,7 @@ def make_pair(W=640, H=480, f=525.0, cx=319.5, cy=239.5, n_patches=6, hole_frac=
     moved = [p.moved() for p in patches]
     col1, z1, sid1, d = _render(cam, W, H, patches, bg_tex)
     col2, z2, _, _ = _render(cam, W, H, moved, bg_tex)
-    # analytic motion of frame-1 surface points
-    P1 = d * z1[..., None]
-    P2 = P1.copy()
-    for k, p in enumerate(patches):
-        m = sid1 == k
-        P2[m] = (P1[m] - p.c) @ p.R.T + p.c + p.T
-    x2 = cam.f * P2[..., 0] / P2[..., 2] + cam.cx
-    y2 = cam.f * P2[..., 1] / P2[..., 2] + cam.cy
-    xs, ys = np.meshgrid(np.arange(W, dtype=np.float64), np.arange(H, dtype=np.float64))
-    gt = np.stack([x2 - xs, y2 - ys, P2[..., 2] - z1], -1).astype(np.float32)
+    gt = _motion_gt(cam, W, H, patches, z1, sid1, d)
 
     def sensor(col, z):
         c = np.clip(np.rint(col + rng.normal(0, color_noise, col.shape)), 0, 255).astype(np.uint8)
@@ -199,12 +204,13 @@ def make_sequence(W=640, H=480, f=525.0, cx=319.5, cy=239.5, n_patches=6, hole_f
     frames = []
     cur = patches
     for t in range(n_frames):
-        col, z, _, _ = _render(cam, W, H, cur, bg_tex)
+        col, z, sid, d = _render(cam, W, H, cur, bg_tex)
         c = np.clip(np.rint(col + rng.normal(0, color_noise, col.shape)), 0, 255).astype(np.uint8)
         zn = z + rng.normal(0, 1, z.shape) * depth_noise * z * z
         dep = (np.clip(np.rint(zn * 1000.0), 0, 65535).astype(np.uint16) * 0.001).astype(np.float32)
         dep[_holes(rng, H, W, hole_frac)] = 0
-        frames.append(dict(bgr=c, depth=dep))
+        # gt_next: the analytic motion of this frame's surface points to the next frame
+        frames.append(dict(bgr=c, depth=dep, z_true=z, gt_next=_motion_gt(cam, W, H, cur, z, sid, d)))
         cur = [p.moved() for p in cur]
     return dict(frames=frames, cam=cam, W=W, H=H)
 

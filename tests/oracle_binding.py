@@ -17,6 +17,7 @@ ORACLE_SO = os.path.join(ORACLE_DIR, "libsforacle.so")
 REF_CPU_SO = os.path.join(ORACLE_DIR, "_ref", "libref_cpu.so")
 REF_CUDA_SO = os.path.join(ORACLE_DIR, "_ref", "libref_cuda.so")
 REF_FLOW2D_SO = os.path.join(ORACLE_DIR, "_ref", "libref_flow2d.so")
+REF_RMF_SO = os.path.join(ORACLE_DIR, "_ref", "libref_rmf.so")
 REF_HPB_SO = os.path.join(ORACLE_DIR, "_ref", "libref_hpb.so")
 
 _P = ctypes.POINTER
@@ -69,6 +70,9 @@ def oracle():
         lib.sfo_resize_dims.argtypes = [_pd, _i, _i, _i, _i, _i, _pd]
         lib.sfo_im2feature.argtypes = [_pd, _i, _i, _pd]
         lib.sfo_median_fill.argtypes = [_pd, _i, _i]
+        lib.sfo_median_fill_rounds.argtypes = [_pd, _i, _i, _pi]
+        lib.sfo_set_fill_order.argtypes = [_i]
+        lib.sfo_set_level_solver.argtypes = [ctypes.c_void_p]
         lib.sfo_depth_sigma.argtypes = [_pf, _i, _i, _i, _pf]
         lib.sfo_warp_cpu.argtypes = [_pd, _pd, _pd, _pd, _i, _i, _i, _pd, _pd, _pd, _pd, _pd]
         lib.sfo_depth_mag_weights.argtypes = [_pd, _i, _i, ctypes.c_void_p, _pd]
@@ -286,13 +290,70 @@ def warp(feat1, d1, feat2, d2, u, v, w, impl="oracle"):
     return wI, wD
 
 
-def median_fill(depth):
+_ref_rmf = None
+
+
+def ref_rmf_available():
+    return os.path.exists(REF_RMF_SO)
+
+
+def median_fill(depth, impl="oracle"):
+    """recursiveMedianFilter, the restatement (impl="oracle") or the reference's own code compiled in
+    place (impl="ref", oracle/_ref/libref_rmf.so)."""
+    global _ref_rmf
     d = _cont(depth, np.float64).copy()
     H, W = d.shape
+    if impl == "ref":
+        if _ref_rmf is None:
+            _ref_rmf = ctypes.CDLL(REF_RMF_SO)
+            _ref_rmf.ref_median_fill.argtypes = [_pd, _i, _i]
+            _ref_rmf.ref_median_fill.restype = None
+        _ref_rmf.ref_median_fill(dptr(d), W, H)
+        return d
     rc = oracle().sfo_median_fill(dptr(d), W, H)
     if rc != 0:
         raise RuntimeError(oracle().sfo_last_error().decode())
     return d
+
+
+def median_fill_rounds(depth):
+    """The hole fill in the library's order (parallel rounds); returns (filled depth, rounds)."""
+    d = _cont(depth, np.float64).copy()
+    H, W = d.shape
+    r = ctypes.c_int(0)
+    rc = oracle().sfo_median_fill_rounds(dptr(d), W, H, ctypes.byref(r))
+    if rc != 0:
+        raise RuntimeError(oracle().sfo_last_error().decode())
+    return d, r.value
+
+
+class reference_cuda_levels:
+    """Context manager: the oracle's faithful scene-flow solves hand every pyramid level to the
+    reference's own CUDA solver (oracle/_ref/libref_cuda.so, needs a GPU), as the reference's
+    sceneFlowMultiscale does; pyramids, features, warps and weights stay on the host."""
+
+    def __enter__(self):
+        fn = ctypes.cast(ref_cuda().ref_single_scale, ctypes.c_void_p).value
+        oracle().sfo_set_level_solver(fn)
+        return self
+
+    def __exit__(self, *a):
+        oracle().sfo_set_level_solver(None)
+
+
+class fill_order:
+    """Context manager: the oracle's scene-flow solves fill holes in the given order ("reference":
+    the reference's hash-set order; "rounds": the library's parallel rounds)."""
+
+    def __init__(self, order):
+        self.order = {"reference": 0, "rounds": 1}[order]
+
+    def __enter__(self):
+        self.old = oracle().sfo_set_fill_order(self.order)
+        return self
+
+    def __exit__(self, *a):
+        oracle().sfo_set_fill_order(self.old)
 
 
 def depth_sigma(depth_m, max_dist=4):
@@ -319,6 +380,42 @@ def two_frames(cam, bgr1, depth1, bgr2, depth2, params, fp64=False, est_flow=Non
     if rc != 0:
         raise RuntimeError("oracle: %s" % oracle().sfo_last_error().decode())
     return out, st
+
+
+def depth_mag_weights(depth_k, cam_full):
+    """calculateDepthMagnitudeTermWeights at a level, with the reference's full-resolution indexing."""
+    d = _cont(depth_k, np.float64)
+    H, W = d.shape
+    out = np.zeros((H, W), np.float64)
+    oracle().sfo_depth_mag_weights(dptr(d), W, H, ctypes.byref(cam_full), dptr(out))
+    return out
+
+
+def reg_weights(depth, reg_type):
+    """calculateRegularizationWeights (ISOTROPIC / LETOUZEY): (H, W, 2) right / down weights."""
+    d = _cont(depth, np.float64)
+    H, W = d.shape
+    out = np.zeros((H, W, 2), np.float64)
+    oracle().sfo_reg_weights(dptr(d), W, H, reg_type, dptr(out))
+    return out
+
+
+def linearize(Im1, dm1, Im2, dm2, wI2, wD2, u3, du3, colorW, ddw, alpha, dsw, gamma, mag, regw, params=None,
+              fp64=False):
+    """One linearisation (fillSystemMtxKernel and the kernels before it, .cu:84-575) from the state
+    (u3, du3: (H, W, 3)); returns the reference's 8 system planes as an (8, H, W, 3) array."""
+    Im1, Im2 = _cont(Im1, np.float64), _cont(Im2, np.float64)
+    dm1, dm2, wI2, wD2 = (_cont(x, np.float64) for x in (dm1, dm2, wI2, wD2))
+    u3, du3 = _cont(u3, np.float64), _cont(du3, np.float64)
+    ddw, dsw, mag, regw = (_cont(x, np.float64) for x in (ddw, dsw, mag, regw))
+    H, W, C = Im1.shape
+    A = np.zeros((8, H, W, 3), np.float64)
+    rc = oracle().sfo_linearize(int(fp64), dptr(Im1), dptr(dm1), dptr(Im2), dptr(dm2), dptr(wI2), dptr(wD2),
+                                dptr(u3), dptr(du3), W, H, C, colorW, dptr(ddw), alpha, dptr(dsw), gamma, dptr(mag),
+                                dptr(regw), ctypes.byref(params) if params is not None else None, dptr(A))
+    if rc != 0:
+        raise RuntimeError("oracle: %s" % oracle().sfo_last_error().decode())
+    return A
 
 
 def single_scale(f_level, Im1, dm1, Im2, dm2, wI2, wD2, u, v, w, colorW, ddw, alpha, dsw, gamma, mag, regw,

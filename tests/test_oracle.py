@@ -99,6 +99,44 @@ def test_median_fill_known_answers(oracle_lib):
         ob.median_fill(np.zeros((4, 4)))
 
 
+def test_median_fill_matches_reference_golden(oracle_lib):
+    """The restatement against the reference's own recursiveMedianFilterAux
+    (recursiveMedianFiltering.cpp:35-99, compiled in place; tests/golden/make_rmf_golden.py): the same
+    hash-set fill order, so every filled value equal."""
+    g = np.load(os.path.join(GOLDEN, "ref_rmf_golden.npz"))
+    for tag in ("a", "b", "c"):
+        d = g["in_" + tag]
+        assert (d <= 0).sum() > 0
+        assert np.array_equal(ob.median_fill(d), g["out_" + tag]), tag
+
+
+@pytest.mark.skipif(not ob.ref_rmf_available(), reason="reference median fill not built (oracle/_ref)")
+@pytest.mark.parametrize("seed", [0, 1])
+def test_median_fill_matches_live_reference(oracle_lib, seed):
+    p = syn.make_config_pair("320x240", seed=seed)
+    for k in ("depth1", "depth2"):
+        assert np.array_equal(ob.median_fill(p[k]), ob.median_fill(p[k], impl="ref"))
+
+
+def test_rounds_fill_order(oracle_lib):
+    """The library's fill order (parallel rounds), restated in the oracle: isolated holes get the
+    reference's value; clustered holes are all filled, each with a value taken from the valid
+    depths (a median picks one of its inputs); a hole region with no valid neighbour is an error."""
+    rng = np.random.default_rng(1)
+    d = rng.uniform(1, 3, (30, 40))
+    d[1::3, 2::3] = 0  # no two holes are 8-neighbours
+    out, rounds = ob.median_fill_rounds(d)
+    assert rounds == 1
+    assert np.array_equal(out, ob.median_fill(d))
+    p = syn.make_config_pair("320x240", seed=2)
+    d = p["depth1"].astype(np.float64)
+    out, rounds = ob.median_fill_rounds(d)
+    assert rounds > 1 and (out > 0).all()
+    assert np.isin(out[d <= 0], np.unique(d[d > 0].astype(np.float32))).all()
+    with pytest.raises(RuntimeError):
+        ob.median_fill_rounds(np.zeros((4, 4)))
+
+
 def test_depth_sigma_known_answers(oracle_lib):
     """computeDepthMapStdevsPointwise + increaseStdevsNearDepthBoundaries
     (staticDepthNoiseModeling.cpp:232-258, 85-137)."""

@@ -3,7 +3,8 @@ that takes device pointers (rgbdflow_scene_flow_batch_async).
 
 Both run the same plan and kernels, so the flows are expected to agree bit for bit; the test
 allows 1e-6 (pixels for u and v, metres for w) per component.  Two calls in a row on one stream
-check that the shared static workspace carries nothing from one call into the next.  This file is
+check that the shared static workspace carries nothing from one call into the next; a third pair of
+calls passes a warm start (the first solve's flow as est_flow) to both entry points.  This file is
 collected last and also passes on its own in a fresh process.
 """
 import ctypes
@@ -62,3 +63,27 @@ def test_noalloc_matches_batch_async_two_calls(ctx):
         assert np.isfinite(a).all()
         assert np.abs(a - b).max() <= TOL
         assert np.abs(a).max() > 0  # a real solve, not an untouched buffer
+
+
+@pytest.mark.gpu
+def test_noalloc_warm_start_matches_batch_async(ctx):
+    """A warm start (est_flow, a device pointer) through both entry points."""
+    import torch
+    prm = rf.benchmark_params(320)
+    p = syn.make_config_pair("320x240", seed=43)
+    st = torch.cuda.Stream()
+    with torch.cuda.stream(st):
+        cold = device_pair(p, torch)
+        ctx.scene_flow_batch_device([cold], prm, stream=st)
+        st.synchronize()
+        est = cold["out"].clone()
+        a, b = device_pair(p, torch), device_pair(p, torch)
+        a["est"] = est
+        b["est"] = est
+        ctx.scene_flow_batch_device([b], prm, stream=st)
+        rf.scene_flow_noalloc(a, prm, stream=st)
+        st.synchronize()
+    x, y = a["out"].cpu().numpy(), b["out"].cpu().numpy()
+    assert np.isfinite(x).all()
+    assert np.abs(x - y).max() <= TOL
+    assert np.abs(x - est.cpu().numpy()).max() > 0  # the warm-started solve moved the flow
