@@ -622,7 +622,8 @@ def main():
                 "plain": plain, "batch_equals_solo": same, "served": served, "served_warm": served_warm,
                 "mixed_batch": mixed, "precision": precision,
                 "gpu_launches": launches_per_step * args.steps,
-                "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk}
+                "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
+                "autotune": rf.autotune_describe(local)}
         print(json.dumps(compact(line)), flush=True)
     ctx.close()
     if world > 1:

@@ -266,6 +266,15 @@ typedef struct rgbdflow_kernel_stat {
 } rgbdflow_kernel_stat;
 
 int rgbdflow_profile(rgbdflow_ctx* ctx, int enable);
+
+/* SOR autotuner (no reference counterpart; the reference has one SOR kernel configuration).  The
+ * first time a pyramid level with given pair sizes is solved on a device, each SOR configuration
+ * (tile or strip kernel, sweeps per launch, lane mapping, strip band height) is timed on that
+ * level with CUDA events and the fastest is kept for the life of the process; every configuration
+ * gives the same flow bit for bit.  RGBDFLOW_AUTOTUNE=0 in the environment turns it off.  Writes
+ * the choices made on `device` ("sizes kernel K ... us per SOR iteration; ...") into buf (len bytes,
+ * NUL-terminated; either may be 0) and returns the full length. */
+int rgbdflow_autotune_describe(int device, char* buf, size_t len);
 /* Fills up to max entries; returns the number of kernel classes with launches. */
 int rgbdflow_profile_read(rgbdflow_ctx* ctx, rgbdflow_kernel_stat* out, int max);
 
@@ -291,6 +300,9 @@ int rgbdflow_profile_read(rgbdflow_ctx* ctx, rgbdflow_kernel_stat* out, int max)
                                         smoothness weight (fillSystemMtxKernel, .cu:477-575) */
 #define RGBDFLOW_PLANE_FILL_ROUND  8 /* level 0, index 0, 1: the hole-fill round that filled each pixel of
                                         depth 1 / 2 (0: valid input, 255: never filled) */
+#define RGBDFLOW_PLANE_HPB_DEPTH   9 /* index 0: HPB regularisation only: the level of the raw-depth pyramid
+                                        (DepthMapPyramid of frame 1's raw depth after the colour-guided
+                                        fill of small invalid regions; -1 invalid) */
 /* Copies plane (kind, index) of pair `pair` (batch order), pyramid level `level` (0 = finest) of
  * the context's last solve into dst (n doubles, W * H needed, raster order); W and H (either may
  * be NULL) receive the level's size.  Waits for the solve to finish. */

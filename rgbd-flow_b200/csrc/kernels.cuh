@@ -550,16 +550,18 @@ __global__ void k_level_setup(const LevelItem<T, S>* items, const Tile* tiles, i
         const T q = (z > 0) ? it.f_full / z : it.f_full / 2;
         it.mag[l] = q * q;
     }
-    T rh = 0, rv = 0;
-    if (regtype == 1) {
-        if (j < W - 1) { const T d = (z1 - it.pyr[6][l + 1]) / (T).02; rh = expT(-(d * d)); }
-        if (i < H - 1) { const T d = (z1 - it.pyr[6][l + W]) / (T).02; rv = expT(-(d * d)); }
-    } else {
-        rh = (j < W - 1) ? (T)1 : (T)0;
-        rv = (i < H - 1) ? (T)1 : (T)0;
+    if (regtype != 2) {  // HPB weights are written by the HPB kernels (hpb.cuh)
+        T rh = 0, rv = 0;
+        if (regtype == 1) {
+            if (j < W - 1) { const T d = (z1 - it.pyr[6][l + 1]) / (T).02; rh = expT(-(d * d)); }
+            if (i < H - 1) { const T d = (z1 - it.pyr[6][l + W]) / (T).02; rv = expT(-(d * d)); }
+        } else {
+            rh = (j < W - 1) ? (T)1 : (T)0;
+            rv = (i < H - 1) ? (T)1 : (T)0;
+        }
+        it.rh[l] = rh;
+        it.rv[l] = rv;
     }
-    it.rh[l] = rh;
-    it.rv[l] = rv;
     if (it.est_init) return;  // flow supplied by the caller
     const int lp = i * it.pitch + j;
     if (it.uc[0] == nullptr) {
@@ -1476,16 +1478,19 @@ k_sor_level(const LevelItem<T, S>* items, const int* which, SolveConst<T> k, Sor
     const int PLS = (H + 2) * 2 * RP;
     T* const red = buf + 15 * PLS;
     const int tid = threadIdx.x, NT = blockDim.x;
-    // stage: valid pixels from global, zero everywhere else (padding, positions past a row's count)
-    for (int e = tid; e < 15 * PLS; e += NT) {
-        const int z = e / PLS, rem = e % PLS, rr = rem / (2 * RP) - 1, c = (rem / RP) & 1, p = rem % RP - 1;
-        T v = 0;
-        if (rr >= 0 && rr < H && p >= 0 && p < ((W + 1 - (c ^ (rr & 1))) >> 1)) {
-            const size_t g = (size_t)rr * 2 * hw + c * hw + p;
-            if (z < 12) v = it.sys[z][g];
-            else if (!L.xin_zero) v = it.x[L.xin][z - 12][g];
-        }
-        buf[e] = v;
+    // stage: valid pixels from global, zero everywhere else (padding, positions past a row's count);
+    // a thread's position is decoded once and its 15 planes' loads are all in flight together
+    for (int e = tid; e < PLS; e += NT) {
+        const int rr = e / (2 * RP) - 1, c = (e / RP) & 1, p = e % RP - 1;
+        const bool valid = rr >= 0 && rr < H && p >= 0 && p < ((W + 1 - (c ^ (rr & 1))) >> 1);
+        const size_t g = valid ? (size_t)rr * 2 * hw + c * hw + p : 0;
+        T v[15];
+#pragma unroll
+        for (int z = 0; z < 12; z++) v[z] = valid ? it.sys[z][g] : (T)0;
+#pragma unroll
+        for (int z = 12; z < 15; z++) v[z] = (valid && !L.xin_zero) ? it.x[L.xin][z - 12][g] : (T)0;
+#pragma unroll
+        for (int z = 0; z < 15; z++) buf[z * PLS + e] = v[z];
     }
     if (tid == 0) s_stop = 0;
     __syncthreads();

@@ -8,13 +8,16 @@
 // The enqueue is pure stream work with no host synchronisation, so it is captured once into a
 // CUDA graph per batch shape and replayed.
 #pragma once
+#include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <stdexcept>
 #include <string>
 #include <vector>
 
 #include "kernels.cuh"
+#include "hpb.cuh"
 
 namespace rgbdflow {
 
@@ -171,6 +174,52 @@ static inline SorConfig choose_sor_config(const HostParams& hp, long level_px)
     return c;
 }
 
+// The SOR configuration chosen for one level step by the autotuner (rgbdflow.cu, tune_sor): kernel
+// (tile or strip), sweeps per launch, lane mapping, strip band height.  The choice changes speed
+// only: every configuration gives the same flow bit for bit.
+struct SorChoice {
+    int strip = 0;   // strip kernel for the step's strip-eligible items
+    int K = 5;       // sweeps per launch
+    int ilp = 2;     // tile kernel lane mapping
+    int seg = 0;     // strip band height (0: automatic)
+    double us_per_it = 0;  // measured time per SOR iteration of the step
+};
+struct TuneTable {
+    std::map<std::string, SorChoice> m;  // by step key (sor_step_key)
+};
+
+// A level step's tuning key: the arithmetic type and the sorted sizes of its items.
+template <class T, class X>
+static std::string sor_step_key(const std::vector<X>& items)
+{
+    std::vector<std::pair<int, int>> sz;
+    for (const auto& x : items) sz.push_back({x.W, x.H});
+    std::sort(sz.begin(), sz.end());
+    std::string k = sizeof(T) == 8 ? "d" : "f";
+    for (size_t i = 0; i < sz.size();) {
+        size_t j = i;
+        while (j < sz.size() && sz[j] == sz[i]) j++;
+        k += std::to_string(sz[i].first) + "x" + std::to_string(sz[i].second) + "*" + std::to_string(j - i) + ",";
+        i = j;
+    }
+    return k;
+}
+
+// Whether the SOR configuration may be tuned: no explicit sweeps per launch and no measurement
+// overrides.
+static inline bool sor_tunable(const HostParams& hp)
+{
+    return hp.K == 0 && hp.sor_ilp == 0 && hp.sor_nbuf == 0 && hp.sor_strip == 1 && hp.strip_min_w == 0 &&
+           hp.strip_min_h == 0 && hp.strip_seg == 0 && hp.strip_min_px == 0;
+}
+
+// Items the autotuner may put on the strip kernel (FP32, at least two strips wide and two bands high).
+template <class T>
+static inline bool strip_ok(const HostParams& hp, int W, int H)
+{
+    return sizeof(T) == 4 && hp.sor_strip && W >= 2 * kStripW && H >= 64;
+}
+
 // Whether an item's level may run on the strip SOR: FP32 planes, at most 5 sweeps per launch, and
 // a level large enough that its strips carry many rows (the pipeline fill costs about 6 nit rows).
 // Measured on the 640x480 benchmark: strips beat tiles on the 640-wide level of a 16-pair batch,
@@ -276,9 +325,20 @@ struct Plan {
                                         // fill's GridSync (zeroed together)
     size_t tleft_off = 0;               // int[prep tiles]: the tile still holds a hole
     std::vector<std::vector<std::vector<SorLaunch>>> sor_sched;  // [step][inner iteration]
+    std::vector<std::string> step_keys;                         // autotuner key per step
+    std::vector<int> step_tuned;                                // the step's SOR configuration came from the tuner
+    std::string tune_desc;                                      // the tuned choices in use (part of the graph key)
     std::vector<std::vector<int>> n_checks;                     // [step][inner iteration]
     std::vector<std::vector<size_t>> u_off;         // per pair per level: offset of u[0] (for warm-start upload)
     std::vector<int> est_flag;
+    // HPB regularisation weights (regularization == HPB, kinds 0 and 1)
+    bool hpb = false;
+    size_t hpb_ctr_off = 0;             // int[n] region counts, then the fill's GridSync (zeroed each solve)
+    size_t hpb_fill_off = 0;            // HpbFill[n] (descriptor offset)
+    struct HpbDepthLevel { size_t jobs_off; int n_jobs; size_t tiles_off; int n_tiles; };
+    std::vector<HpbDepthLevel> hpb_dpyr;  // raw-depth pyramid, level index 1..Lmax-1
+    struct HpbStep { size_t items_off; int n_items; size_t row_first_off, col_first_off; int row_threads, col_threads; };
+    std::vector<HpbStep> hpb_step;      // per step (as steps)
 
     template <class X> size_t put(const std::vector<X>& v)
     {
@@ -330,8 +390,9 @@ static inline std::vector<SorLaunch> sor_schedule(int nSOR, int K, int period, i
 }
 
 template <class T, class S>
-static Plan<T, S> make_plan(const std::vector<PairSpec>& pairs, const HostParams& hp)
+static Plan<T, S> make_plan(const std::vector<PairSpec>& pairs, const HostParams& hp, const TuneTable* tune = nullptr)
 {
+    if (!sor_tunable(hp)) tune = nullptr;
     Plan<T, S> P;
     P.hp = hp;
     P.n = (int)pairs.size();
@@ -375,7 +436,7 @@ static Plan<T, S> make_plan(const std::vector<PairSpec>& pairs, const HostParams
     P.out_off = out0; P.out_bytes = A.off - out0;
 
     // per pair per level planes
-    struct LevelMem { size_t pyr[10], I1[5], I2[5], D1, D2, mag, rh, rv, u[3], x[2][3], sys[12], stat; int nsor; };
+    struct LevelMem { size_t pyr[10], I1[5], I2[5], D1, D2, mag, rh, rv, u[3], x[2][3], sys[12], stat, hz; int nsor; };
     std::vector<std::vector<LevelMem>> mem(P.n);
     struct L0Mem { size_t stamp[2], bmask, tmp; };
     std::vector<L0Mem> l0(P.n);
@@ -399,6 +460,36 @@ static Plan<T, S> make_plan(const std::vector<PairSpec>& pairs, const HostParams
             for (int c = 0; c < 12; c++) m.sys[c] = A.take(sizeof(T) * NC);
             m.nsor = ((s.w[k] + kSorTW - 1) / kSorTW) * ((s.h[k] + kSorTH - 1) / kSorTH);
             m.stat = A.take(sizeof(T) * m.nsor);
+            m.hz = 0;
+        }
+    }
+    // HPB: the raw-depth pyramid per level and, per pair, scratch for one level at a time
+    P.hpb = hp.regularization == 2 && P.kind != 2;
+    struct HpbMem { size_t label, done, reps, nrm[3], nval, rad, pre[6], pre_v, ii[6], ii_v, feat[4], bp[2]; };
+    std::vector<HpbMem> hm(P.n);
+    if (P.hpb) {
+        P.hpb_ctr_off = A.take(sizeof(int) * P.n + sizeof(GridSync));
+        for (int p = 0; p < P.n; p++) {
+            const auto& s = P.shapes[p];
+            // DepthMapPyramid's level sizes must be the colour pyramid's: the reference reads one
+            // with the other's size (heuristicProbBoundary.cpp:31-38)
+            for (int k = 1; k < P.L[p]; k++) {
+                const double r = std::pow(s.ratio, k);
+                if ((int)(s.w[0] * r) != s.w[k] || (int)(s.h[0] * r) != s.h[k])
+                    throw ArgError(-2, "HPB: the raw-depth pyramid's level size differs from the colour pyramid's");
+            }
+            for (int k = 0; k < P.L[p]; k++) mem[p][k].hz = A.take(sizeof(T) * (size_t)s.w[k] * s.h[k]);
+            const size_t N0 = (size_t)s.w[0] * s.h[0], NI = (size_t)(s.w[0] + 1) * (s.h[0] + 1);
+            HpbMem& h = hm[p];
+            h.label = A.take(sizeof(int) * N0); h.done = A.take(N0); h.reps = A.take(sizeof(int) * (N0 / 2 + 2));
+            for (int c = 0; c < 3; c++) h.nrm[c] = A.take(sizeof(float) * N0);
+            h.nval = A.take(sizeof(unsigned) * N0); h.rad = A.take(sizeof(int) * N0);
+            for (int c = 0; c < 6; c++) h.pre[c] = A.take(sizeof(float) * N0);
+            h.pre_v = A.take(sizeof(unsigned) * N0);
+            for (int c = 0; c < 6; c++) h.ii[c] = A.take(sizeof(float) * NI);
+            h.ii_v = A.take(sizeof(unsigned) * NI);
+            for (int c = 0; c < 4; c++) h.feat[c] = A.take(sizeof(float) * N0);
+            for (int c = 0; c < 2; c++) h.bp[c] = A.take(sizeof(float) * N0);
         }
     }
     P.arena_bytes = A.off;  // descriptors are appended after planning (desc_off)
@@ -503,6 +594,78 @@ static Plan<T, S> make_plan(const std::vector<PairSpec>& pairs, const HostParams
         P.pyr.push_back(d);
     }
 
+    if (P.hpb) {
+        // the colour-guided fill of frame 1's raw depth (level 0), read through the pair's PrepItem
+        std::vector<HpbFill<T>> fills(P.n);
+        for (int p = 0; p < P.n; p++) {
+            HpbFill<T>& f = fills[p];
+            std::memset(&f, 0, sizeof(f));
+            f.W = P.shapes[p].w[0]; f.H = P.shapes[p].h[0];
+            f.src = (const PrepItem<T>*)(P.prep_items_off + sizeof(PrepItem<T>) * p);  // descriptor-relative
+            f.fill = P.est_flag[p] ? 0 : 1;  // the warm start reads the raw depth (sceneFlowWithInit.cpp:48)
+            f.out = (T*)mem[p][0].hz;
+            f.label = (int*)hm[p].label; f.done = (uint8_t*)hm[p].done; f.reps = (int*)hm[p].reps;
+            f.n_reps = (int*)(P.hpb_ctr_off + sizeof(int) * p);
+        }
+        P.hpb_fill_off = P.put(fills);
+        // DepthMapPyramid levels (depthMapPyramid.cpp:15-91)
+        for (int i = 1; i < P.Lmax; i++) {
+            std::vector<DepthPyrJob<T>> jobs;
+            std::vector<Tile> tl;
+            for (int p = 0; p < P.n; p++) {
+                if (i >= P.L[p]) continue;
+                const auto& s = P.shapes[p];
+                DepthPyrJob<T> jb;
+                jb.sW = s.w[i - 1]; jb.sH = s.h[i - 1]; jb.dW = s.w[i]; jb.dH = s.h[i];
+                jb.src = (const T*)mem[p][i - 1].hz;
+                jb.dst = (T*)mem[p][i].hz;
+                const int jid = (int)jobs.size();
+                for (int y = 0; y < (jb.dH + LTH - 1) / LTH; y++)
+                    for (int x = 0; x < (jb.dW + LTW - 1) / LTW; x++) tl.push_back(Tile{jid, x, y, 0});
+                jobs.push_back(jb);
+            }
+            typename Plan<T, S>::HpbDepthLevel d;
+            d.jobs_off = P.put(jobs); d.n_jobs = (int)jobs.size();
+            d.tiles_off = P.put(tl); d.n_tiles = (int)tl.size();
+            P.hpb_dpyr.push_back(d);
+        }
+        // computeHeuristicPb per level, items in the order of the level step's items
+        for (int sidx = 0; sidx < P.Lmax; sidx++) {
+            const int k = P.Lmax - 1 - sidx;
+            std::vector<HpbItem<T>> its;
+            std::vector<int> rf{0}, cf{0};
+            for (int p = 0; p < P.n; p++) {
+                if (k >= P.L[p]) continue;
+                const int W = P.shapes[p].w[k], H = P.shapes[p].h[k];
+                HpbItem<T> it;
+                std::memset(&it, 0, sizeof(it));
+                it.W = W; it.H = H;
+                // the wrapper's camera (heuristicProbBoundary.cpp:24-29)
+                it.f = (float)(525.0 * (unsigned)W / 640);
+                it.cx = (float)((unsigned)W / 2);
+                it.cy = (float)((unsigned)H / 2);
+                for (int c = 0; c < 3; c++) it.col[c] = (const T*)mem[p][k].pyr[c];
+                it.z = (const T*)mem[p][k].hz;
+                it.rh = (T*)mem[p][k].rh; it.rv = (T*)mem[p][k].rv;
+                const HpbMem& h = hm[p];
+                for (int c = 0; c < 3; c++) it.nrm[c] = (float*)h.nrm[c];
+                it.nval = (unsigned*)h.nval; it.rad = (int*)h.rad;
+                for (int c = 0; c < 6; c++) { it.pre[c] = (float*)h.pre[c]; it.ii[c] = (float*)h.ii[c]; }
+                it.pre_v = (unsigned*)h.pre_v; it.ii_v = (unsigned*)h.ii_v;
+                for (int c = 0; c < 4; c++) it.feat[c] = (float*)h.feat[c];
+                for (int c = 0; c < 2; c++) it.bp[c] = (float*)h.bp[c];
+                its.push_back(it);
+                rf.push_back(rf.back() + 7 * H);
+                cf.push_back(cf.back() + 7 * (W + 1));
+            }
+            typename Plan<T, S>::HpbStep d;
+            d.items_off = P.put(its); d.n_items = (int)its.size();
+            d.row_first_off = P.put(rf); d.col_first_off = P.put(cf);
+            d.row_threads = rf.back(); d.col_threads = cf.back();
+            P.hpb_step.push_back(d);
+        }
+    }
+
     // level steps
     for (int sidx = 0; sidx < P.Lmax; sidx++) {
         const int k = P.Lmax - 1 - sidx;
@@ -555,7 +718,16 @@ static Plan<T, S> make_plan(const std::vector<PairSpec>& pairs, const HostParams
         long strip_px = 0;
         for (const auto& x : items)
             if (use_strip<T>(hp, x.W, x.H)) strip_px += (long)x.W * x.H;
-        const bool strips = strip_px >= (hp.strip_min_px > 0 ? hp.strip_min_px : 2000000L);
+        // the tuned choice for this step's sizes, where the tuner has measured one
+        const std::string skey = sor_step_key<T>(items);
+        const SorChoice* ch = nullptr;
+        if (tune) {
+            const auto f = tune->m.find(skey);
+            if (f != tune->m.end()) ch = &f->second;
+        }
+        P.step_keys.push_back(skey);
+        P.step_tuned.push_back(ch != nullptr);
+        const bool strips = ch ? ch->strip != 0 : strip_px >= (hp.strip_min_px > 0 ? hp.strip_min_px : 2000000L);
         for (auto& x : items) {
             const int sx = (x.W + kSorTW - 1) / kSorTW, sy = (x.H + kSorTH - 1) / kSorTH;
             x.n_sor_tiles = sx * sy;
@@ -565,14 +737,19 @@ static Plan<T, S> make_plan(const std::vector<PairSpec>& pairs, const HostParams
                 level_thr = std::max(level_thr, level_threads(x.H, x.hwp));
                 continue;
             }
-            if (strips && use_strip<T>(hp, x.W, x.H)) {
+            if (strips && (ch ? strip_ok<T>(hp, x.W, x.H) : use_strip<T>(hp, x.W, x.H))) {
                 strip_items.push_back((int)(&x - items.data()));
                 continue;
             }
             for (int y = 0; y < sy; y++)
                 for (int xx = 0; xx < sx; xx++) stt.push_back(Tile{(int)(&x - items.data()), xx, y, y * sx + xx});
         }
-        const std::vector<StripUnit> units = strip_units(items, strip_items, hp, P.sms);
+        HostParams hs = hp;
+        if (ch) hs.strip_seg = ch->seg;
+        const std::vector<StripUnit> units = strip_units(items, strip_items, hs, P.sms);
+        if (ch)
+            P.tune_desc += skey + (ch->strip ? "s" + std::to_string(ch->seg) : "t") + std::to_string(ch->K) +
+                           std::to_string(ch->ilp) + ";";
         typename Plan<T, S>::StepDesc d;
         d.level_px = 0;
         for (const auto& x : items) d.level_px += (long)x.W * x.H;
@@ -611,7 +788,14 @@ static Plan<T, S> make_plan(const std::vector<PairSpec>& pairs, const HostParams
 
     // SOR configuration and launch schedule per step (level) and inner iteration
     for (int sidx = 0; sidx < P.Lmax; sidx++) {
-        const SorConfig c = choose_sor_config<T>(hp, P.steps[sidx].level_px);
+        SorConfig c = choose_sor_config<T>(hp, P.steps[sidx].level_px);
+        if (P.step_tuned[sidx]) {
+            const SorChoice& ch = tune->m.find(P.step_keys[sidx])->second;
+            c.K = ch.K;
+            c.ilp = ch.ilp;
+            c.nbuf = 1;
+            while (c.K > 1 && !sor_cfg_fits<T>(c)) c.K--;
+        }
         P.sor_cfg.push_back(c);
         int cur = 0;
         std::vector<std::vector<SorLaunch>> sch;
@@ -672,6 +856,30 @@ static void bind_plan(Plan<T, S>& P, char* base)
             for (int c = 0; c < 3; c++) rebase_nz(x.uc[c], base);
         }
     }
+    if (P.hpb) {
+        HpbFill<T>* fl = (HpbFill<T>*)(d + P.hpb_fill_off);
+        for (int p = 0; p < P.n; p++) {
+            rebase(fl[p].src, base + P.desc_off);
+            rebase(fl[p].out, base); rebase(fl[p].label, base); rebase(fl[p].done, base);
+            rebase(fl[p].reps, base); rebase(fl[p].n_reps, base);
+        }
+        for (auto& lv : P.hpb_dpyr) {
+            DepthPyrJob<T>* jb = (DepthPyrJob<T>*)(d + lv.jobs_off);
+            for (int j = 0; j < lv.n_jobs; j++) { rebase(jb[j].src, base); rebase(jb[j].dst, base); }
+        }
+        for (auto& st : P.hpb_step) {
+            HpbItem<T>* it = (HpbItem<T>*)(d + st.items_off);
+            for (int i = 0; i < st.n_items; i++) {
+                HpbItem<T>& x = it[i];
+                for (int c = 0; c < 3; c++) { rebase(x.col[c], base); rebase(x.nrm[c], base); }
+                rebase(x.z, base); rebase(x.rh, base); rebase(x.rv, base);
+                rebase(x.nval, base); rebase(x.rad, base); rebase(x.pre_v, base); rebase(x.ii_v, base);
+                for (int c = 0; c < 6; c++) { rebase(x.pre[c], base); rebase(x.ii[c], base); }
+                for (int c = 0; c < 4; c++) rebase(x.feat[c], base);
+                for (int c = 0; c < 2; c++) rebase(x.bp[c], base);
+            }
+        }
+    }
     T** outs = (T**)(d + P.out_ptrs_off);
     for (int p = 0; p < P.n; p++) rebase(outs[p], base);
     EstSrc* est = (EstSrc*)(d + P.est_src_off);
@@ -700,11 +908,11 @@ static SolveConst<T> solve_const(const HostParams& hp)
 // ------------------------------------------------------------------------------------------
 // Optional kernel timing: CUDA events around every launch, aggregated per kernel class.
 
-enum KClass { KC_PREP, KC_SIGMA, KC_FILL, KC_PYR_H, KC_PYR_V, KC_SETUP, KC_LIN, KC_SOR, KC_CTL, KC_OUT, KC_MISC, KC_N };
+enum KClass { KC_PREP, KC_SIGMA, KC_FILL, KC_PYR_H, KC_PYR_V, KC_SETUP, KC_LIN, KC_SOR, KC_CTL, KC_OUT, KC_MISC, KC_HPB, KC_N };
 constexpr int KC_SOR_LEVEL0 = KC_N;           // per-level SOR classes: KC_SOR_LEVEL0 + level
 constexpr int KC_TOTAL = KC_N + 16;
 static const char* const kClassNames[KC_N] = {"prep", "depth_sigma", "hole_fill", "pyr_hfilter", "pyr_vresize",
-                                              "level_setup", "linearize", "sor", "control", "output", "misc"};
+                                              "level_setup", "linearize", "sor", "control", "output", "misc", "hpb"};
 
 struct Prof {
     std::vector<cudaEvent_t> pool;
@@ -920,6 +1128,67 @@ static int enqueue_level(const Plan<T, S>& P, char* base, int sidx, cudaStream_t
     return launches;
 }
 
+// Launches a cooperative kernel (every block resident: its blocks meet at grid barriers).
+template <class K, class... A>
+static void launch_cooperative(K kernel, int grid, int block, cudaStream_t st, A... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    RF_CUDA(cudaLaunchKernelEx(&cfg, kernel, args...));
+}
+
+// The HPB regularisation weights of every level (sceneFlowMultiscale.cpp:79-83, 114-116): the
+// colour-guided fill of frame 1's raw depth, its DepthMapPyramid, then computeHeuristicPb per
+// level into the levels' regularisation weights.
+template <class T, class S>
+static int enqueue_hpb(const Plan<T, S>& P, char* base, cudaStream_t st, Prof* pf)
+{
+    int launches = 0;
+    char* db = base + P.desc_off;
+    const HpbFill<T>* fills = (const HpbFill<T>*)(db + P.hpb_fill_off);
+    RF_PROF_B(pf, KC_HPB, st);
+    k_hpb_label<T><<<P.n_prep_tiles, LTW * LTH, 0, st>>>(fills, (const Tile*)(db + P.prep_tiles_off));
+    launches++;
+    {
+        static int per_sm = 0;
+        if (!per_sm) RF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_hpb_fill<T>, 128, 0));
+        const int grid = std::max(1, std::min(per_sm, 4) * P.sms);
+        GridSync* gs = (GridSync*)(base + P.hpb_ctr_off + sizeof(int) * P.n);
+        launch_cooperative(k_hpb_fill<T>, grid, 128, st, fills, P.n, gs, 4096);
+        launches++;
+    }
+    for (const auto& lv : P.hpb_dpyr) {
+        if (!lv.n_tiles) continue;
+        k_depth_pyr<T><<<lv.n_tiles, LTW * LTH, 0, st>>>((const DepthPyrJob<T>*)(db + lv.jobs_off),
+                                                        (const Tile*)(db + lv.tiles_off));
+        launches++;
+    }
+    for (int sidx = 0; sidx < P.Lmax; sidx++) {
+        const auto& d = P.steps[sidx];
+        const auto& h = P.hpb_step[sidx];
+        if (!h.n_items) continue;
+        const HpbItem<T>* items = (const HpbItem<T>*)(db + h.items_off);
+        const Tile* lt = (const Tile*)(db + d.lin_tiles_off);
+        k_hpb_normals<T><<<d.n_lin, LTW * LTH, 0, st>>>(items, lt);
+        k_hpb_rowsum<T><<<(h.row_threads + 127) / 128, 128, 0, st>>>(items, (const int*)(db + h.row_first_off), h.n_items);
+        k_hpb_colsum<T><<<(h.col_threads + 127) / 128, 128, 0, st>>>(items, (const int*)(db + h.col_first_off), h.n_items);
+        k_hpb_halfdisk<T><<<d.n_lin, LTW * LTH, 0, st>>>(items, lt);
+        k_hpb_prob<T><<<d.n_lin, LTW * LTH, 0, st>>>(items, lt);
+        k_hpb_nms<T><<<d.n_lin, LTW * LTH, 0, st>>>(items, lt);
+        launches += 6;
+    }
+    RF_PROF_E(pf, st);
+    return launches;
+}
+
 // Whole solve after the inputs are resident: preprocessing, hole fill, pyramids, levels, output.
 // outs: the output-pointer array the final kernels write through (device memory).
 template <class T, class S>
@@ -943,6 +1212,7 @@ static int enqueue_solve(const Plan<T, S>& P, char* base, cudaStream_t st, Prof*
         launches++;
     } else {
         RF_CUDA(cudaMemsetAsync(base + P.unfilled_off, 0, sizeof(int) * 256 + sizeof(GridSync), st));
+        if (P.hpb) RF_CUDA(cudaMemsetAsync(base + P.hpb_ctr_off, 0, sizeof(int) * P.n + sizeof(GridSync), st));
         const PrepItem<T>* prep = (const PrepItem<T>*)(db + P.prep_items_off);
         const Tile* pt = (const Tile*)(db + P.prep_tiles_off);
         RF_PROF_B(pf, KC_PREP, st);
@@ -961,20 +1231,8 @@ static int enqueue_solve(const Plan<T, S>& P, char* base, cudaStream_t st, Prof*
             int* left = (int*)(base + P.unfilled_off);
             GridSync* gs = (GridSync*)(left + 256);
             int* tleft = (int*)(base + P.tleft_off);
-            const int rounds = P.hp.fill_rounds;
-            const int nt = P.n_prep_tiles;
-            cudaLaunchConfig_t cfg = {};
-            cfg.gridDim = dim3(grid);
-            cfg.blockDim = dim3(LTW * LTH);
-            cfg.dynamicSmemBytes = 0;
-            cfg.stream = st;
-            cudaLaunchAttribute at[1];
-            at[0].id = cudaLaunchAttributeCooperative;
-            at[0].val.cooperative = 1;
-            cfg.attrs = at;
-            cfg.numAttrs = 1;
             RF_PROF_B(pf, KC_FILL, st);
-            RF_CUDA(cudaLaunchKernelEx(&cfg, k_fill<T>, prep, pt, nt, left, tleft, gs, rounds));
+            launch_cooperative(k_fill<T>, grid, LTW * LTH, st, prep, pt, P.n_prep_tiles, left, tleft, gs, P.hp.fill_rounds);
             RF_PROF_E(pf, st);
             launches++;
         }
@@ -989,6 +1247,7 @@ static int enqueue_solve(const Plan<T, S>& P, char* base, cudaStream_t st, Prof*
             RF_PROF_E(pf, st);
             launches += 2;
         }
+        if (P.hpb) launches += enqueue_hpb(P, base, st, pf);
         if (P.any_warm) {
             RF_PROF_B(pf, KC_MISC, st);
             k_load_est<T, S><<<fin.n_lin, LTW * LTH, 0, st>>>(fin_items, fin_tiles, (const EstSrc*)(db + P.est_src_off));

@@ -42,6 +42,7 @@ struct DbgLevel {
     const void* reg[2];
     const void* u[3];
     const void* sys[12];
+    const void* hz;  // HPB raw-depth pyramid level (null without HPB)
 };
 struct DbgPair {
     std::vector<DbgLevel> lev;
@@ -174,10 +175,8 @@ HostParams host_params(const rgbdflow_params& p)
 void validate(const rgbdflow_params* p)
 {
     if (!p) throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "params is NULL");
-    if (p->regularization == RGBDFLOW_REG_HPB)
-        throw ArgError(RGBDFLOW_ERR_UNSUPPORTED,
-                       "HPB regularisation (heuristic probability of boundary) is not built; use ISOTROPIC or LETOUZEY");
-    if (p->regularization != RGBDFLOW_REG_ISOTROPIC && p->regularization != RGBDFLOW_REG_LETOUZEY)
+    if (p->regularization != RGBDFLOW_REG_ISOTROPIC && p->regularization != RGBDFLOW_REG_LETOUZEY &&
+        p->regularization != RGBDFLOW_REG_HPB)
         throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "unknown regularisation type");
     if (p->n_outer < 0 || p->n_inner < 1 || p->n_sor < 0) throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "bad iteration counts");
     if (p->n_outer > 64) throw ArgError(RGBDFLOW_ERR_UNSUPPORTED, "n_outer > 64");
@@ -280,6 +279,16 @@ void record_layout(rgbdflow_ctx* c, const Plan<T, S>& P)
             L.mag = x.mag; L.reg[0] = x.rh; L.reg[1] = x.rv;
             for (int z = 0; z < 3; z++) L.u[z] = x.u[z];
             for (int z = 0; z < 12; z++) L.sys[z] = x.sys[z];
+            L.hz = nullptr;
+        }
+    }
+    if (P.hpb) {
+        for (int sidx = 0; sidx < P.Lmax; sidx++) {
+            const int k = P.Lmax - 1 - sidx;
+            const HpbItem<T>* hi = (const HpbItem<T>*)(d + P.hpb_step[sidx].items_off);
+            int q = 0;
+            for (int p = 0; p < P.n; p++)
+                if (k < P.L[p]) c->dbg[p].lev[k].hz = hi[q++].z;
         }
     }
 }
@@ -294,9 +303,10 @@ void ensure_attrs(rgbdflow_ctx* c, int slot)
 
 // Key of a batch's executable graph: the exact batch (sizes, kinds, warm starts, parameters), the
 // storage slot and the input form.
-std::string graph_key(const std::vector<PairSpec>& pairs, const HostParams& hp, int slot, bool dev)
+std::string graph_key(const std::vector<PairSpec>& pairs, const HostParams& hp, int slot, bool dev,
+                      const std::string& tune_desc)
 {
-    return plan_key(pairs, hp, slot) + (dev ? "|dev" : "");
+    return plan_key(pairs, hp, slot) + (dev ? "|dev" : "") + "|" + tune_desc;
 }
 
 // The executable graph of plan P (bound to the context's arena) for `pairs`: from the cache, or
@@ -309,7 +319,7 @@ template <class T, class S>
 GraphEntry& graph_for(rgbdflow_ctx* c, const Plan<T, S>& P, const std::vector<PairSpec>& pairs, const HostParams& hp,
                       int slot, bool dev)
 {
-    const std::string exact = graph_key(pairs, hp, slot, dev);
+    const std::string exact = graph_key(pairs, hp, slot, dev, P.tune_desc);
     auto it = c->graphs.find(exact);
     if (it == c->graphs.end()) {
         MaxTimer timer(&c->max_build_ms);
@@ -359,6 +369,132 @@ GraphEntry& graph_for(rgbdflow_ctx* c, const Plan<T, S>& P, const std::vector<Pa
     return it->second;
 }
 
+// ------------------------------------------------------------------------------------------
+// SOR autotuner.  The first time a level step with given item sizes is planned, every candidate
+// SOR configuration of that step (tile kernel with K = 2..6 sweeps per launch and either lane
+// mapping; strip kernel with K = 5 and band heights 64..256 where the items allow strips) runs a
+// few launches on the context's stream over the step's real descriptors, timed with CUDA events,
+// and the fastest per SOR iteration is kept.  Every configuration computes the same flow bit for
+// bit, so the choice changes speed only.  Convergence checks are off during timing and every pair
+// is treated as active, so the work timed is the full schedule's; the planes the timing launches
+// overwrite (the increment ping-pong, control blocks, tickets) are reset by the next solve.  The
+// table is kept per device for the life of the process.  RGBDFLOW_AUTOTUNE=0 turns it off (the
+// measured defaults of choose_sor_config / use_strip are used).
+
+struct TuneState {
+    std::mutex mu;
+    TuneTable table[64];  // per device
+};
+TuneState& tune_state()
+{
+    static TuneState s;
+    return s;
+}
+bool autotune_enabled()
+{
+    static const bool on = [] {
+        const char* e = std::getenv("RGBDFLOW_AUTOTUNE");
+        return !(e && std::atoi(e) == 0);
+    }();
+    return on;
+}
+
+template <class T, class S>
+std::vector<SorChoice> sor_candidates(const Plan<T, S>& P, int sidx)
+{
+    std::vector<SorChoice> v;
+    for (int K = 2; K <= 6; K++)
+        for (int ilp = 1; ilp <= 2; ilp++) {
+            SorConfig c;
+            c.K = K; c.ilp = ilp; c.nbuf = 1;
+            if (!sor_cfg_fits<T>(c)) continue;
+            SorChoice ch;
+            ch.strip = 0; ch.K = K; ch.ilp = ilp;
+            v.push_back(ch);
+        }
+    bool any_strip = false;
+    const LevelItem<T, S>* it = (const LevelItem<T, S>*)(P.desc.data() + P.steps[sidx].items_off);
+    for (int i = 0; i < P.steps[sidx].n_items; i++) any_strip = any_strip || strip_ok<T>(P.hp, it[i].W, it[i].H);
+    if (any_strip && sizeof(T) == 4)
+        for (int seg : {64, 128, 192, 256}) {
+            SorChoice ch;
+            ch.strip = 1; ch.K = kStripMaxNit; ch.ilp = 2; ch.seg = seg;
+            v.push_back(ch);
+        }
+    return v;
+}
+
+// Tunes every untuned step of the batch's plan (synchronous on the context's stream).
+template <class T, class S>
+void tune_sor(rgbdflow_ctx* c, const std::vector<PairSpec>& pairs, const HostParams& hp)
+{
+    if (!autotune_enabled() || !sor_tunable(hp) || !c->use_graphs) return;
+    TuneState& ts = tune_state();
+    std::lock_guard<std::mutex> lk(ts.mu);
+    TuneTable& tt = ts.table[c->device & 63];
+    const Plan<T, S> P0 = make_plan<T, S>(pairs, hp, &tt);
+    std::vector<int> todo;
+    for (int sidx = 0; sidx < P0.Lmax; sidx++)
+        if (!P0.step_tuned[sidx] && (P0.steps[sidx].n_sor || P0.steps[sidx].n_units)) todo.push_back(sidx);
+    if (todo.empty()) return;
+    wait_idle(c);
+    ensure_attrs<T, S>(c, sizeof(T) == 8 ? 1 : (std::is_same<S, __half>::value ? 2 : (std::is_same<S, float>::value ? 0 : 3)));
+    const SolveConst<T> k = solve_const<T>(hp);
+    cudaEvent_t ea, eb;
+    RF_CUDA(cudaEventCreate(&ea));
+    RF_CUDA(cudaEventCreate(&eb));
+    for (int sidx : todo) {
+        SorChoice best;
+        double best_us = 1e30;
+        for (SorChoice cand : sor_candidates(P0, sidx)) {
+            TuneTable one = tt;
+            one.m[P0.step_keys[sidx]] = cand;
+            Plan<T, S> Pc = make_plan<T, S>(pairs, hp, &one);
+            Pc.sms = c->sms;
+            ensure_arena(c, Pc.arena_bytes);
+            bind_plan(Pc, c->arena);
+            RF_CUDA(cudaMemcpy(c->arena + Pc.desc_off, Pc.desc.data(), Pc.desc_bytes, cudaMemcpyHostToDevice));
+            const auto& d = Pc.steps[sidx];
+            char* db = c->arena + Pc.desc_off;
+            const LevelItem<T, S>* items = (const LevelItem<T, S>*)(db + d.items_off);
+            int* ticket = (int*)(c->arena + Pc.ctr_off) + sidx;
+            RF_CUDA(cudaMemsetAsync(c->arena + Pc.ctl_off, 0, Pc.ctr_off + sizeof(int) * 16 - Pc.ctl_off, c->stream));
+            const int reps = 3;
+            for (int r = 0; r <= reps; r++) {
+                if (r == 1) RF_CUDA(cudaEventRecord(ea, c->stream));
+                SorLaunch L{};
+                L.it0 = 0; L.nit = Pc.sor_cfg[sidx].K; L.xin = r & 1; L.final_keep = 1; L.seq = r;
+                if (d.n_sor)
+                    launch_sor<T, S>(Pc.sor_cfg[sidx], items, (const Tile*)(db + d.sor_tiles_off), d.n_sor, Pc.sms, k, L, c->stream);
+                if (d.n_units)
+                    launch_sor_strip<T, S>(items, (const StripUnit*)(db + d.strip_units_off), d.n_units, d.strip_grid, ticket,
+                                           k, L, c->stream);
+            }
+            RF_CUDA(cudaEventRecord(eb, c->stream));
+            RF_CUDA(cudaEventSynchronize(eb));
+            float ms = 0;
+            RF_CUDA(cudaEventElapsedTime(&ms, ea, eb));
+            const double us = 1e3 * ms / (reps * Pc.sor_cfg[sidx].K);
+            if (us < best_us) { best_us = us; best = cand; best.K = Pc.sor_cfg[sidx].K; }
+        }
+        best.us_per_it = best_us;
+        tt.m[P0.step_keys[sidx]] = best;
+    }
+    cudaEventDestroy(ea);
+    cudaEventDestroy(eb);
+    RF_CUDA(cudaGetLastError());
+}
+
+// The plan of a batch with the device's tuned SOR choices (tuning first where a step has none).
+template <class T, class S>
+Plan<T, S> plan_for(rgbdflow_ctx* c, const std::vector<PairSpec>& pairs, const HostParams& hp)
+{
+    tune_sor<T, S>(c, pairs, hp);
+    TuneState& ts = tune_state();
+    std::lock_guard<std::mutex> lk(ts.mu);
+    return make_plan<T, S>(pairs, hp, autotune_enabled() ? &ts.table[c->device & 63] : nullptr);
+}
+
 // Runs a batch through one graph launch.
 //   user_stream == nullptr: host buffers, synchronous (pinned staging, H2D, solve, D2H).
 //   user_stream != nullptr: every PairSpec pointer is device memory; the solve is enqueued on
@@ -369,7 +505,7 @@ void run_batch(rgbdflow_ctx* c, const std::vector<PairSpec>& pairs, const HostPa
 {
     ensure_attrs<T, S>(c, slot);
     const bool dev = user_stream != nullptr;
-    Plan<T, S> P = make_plan<T, S>(pairs, hp);
+    Plan<T, S> P = plan_for<T, S>(c, pairs, hp);
     P.sms = c->sms;
     ensure_arena(c, P.arena_bytes);
     bind_plan(P, c->arena);
@@ -525,9 +661,9 @@ template <class T, class S>
 static bool prepare_batch(rgbdflow_ctx* c, const std::vector<PairSpec>& pairs, const HostParams& hp, int slot)
 {
     if (!c->use_graphs || c->prof) return false;
-    if (c->graphs.count(graph_key(pairs, hp, slot, true))) return true;
     ensure_attrs<T, S>(c, slot);
-    Plan<T, S> P = make_plan<T, S>(pairs, hp);
+    Plan<T, S> P = plan_for<T, S>(c, pairs, hp);
+    if (c->graphs.count(graph_key(pairs, hp, slot, true, P.tune_desc))) return true;
     P.sms = c->sms;
     if (!c->arena || P.arena_bytes > c->arena_cap) return false;
     bind_plan(P, c->arena);
@@ -1103,6 +1239,29 @@ int rgbdflow_optical_flow_2d(rgbdflow_ctx* c, const uint8_t* bgr1, const uint8_t
     API_END(c)
 }
 
+int rgbdflow_autotune_describe(int device, char* buf, size_t len)
+{
+    if (device < 0 || device >= 64) return RGBDFLOW_ERR_INVALID_ARG;
+    std::string out;
+    {
+        TuneState& ts = tune_state();
+        std::lock_guard<std::mutex> lk(ts.mu);
+        for (const auto& kv : ts.table[device].m) {
+            const SorChoice& ch = kv.second;
+            char b[160];
+            if (ch.strip) std::snprintf(b, sizeof b, "%s strip band %d K %d %.2f us/it; ", kv.first.c_str(), ch.seg, ch.K, ch.us_per_it);
+            else std::snprintf(b, sizeof b, "%s tile K %d ilp %d %.2f us/it; ", kv.first.c_str(), ch.K, ch.ilp, ch.us_per_it);
+            out += b;
+        }
+    }
+    if (buf && len) {
+        const size_t n = std::min(out.size(), len - 1);
+        std::memcpy(buf, out.data(), n);
+        buf[n] = 0;
+    }
+    return (int)out.size();
+}
+
 int rgbdflow_debug_read_plane(rgbdflow_ctx* c, int pair, int level, int kind, int index, double* dst, size_t n, int* W,
                               int* H)
 {
@@ -1119,8 +1278,9 @@ int rgbdflow_debug_read_plane(rgbdflow_ctx* c, int pair, int level, int kind, in
         const size_t N = (size_t)w * h;
         if (!dst) return RGBDFLOW_OK;
         if (n < N) throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "destination too small");
-        static const int counts[9] = {10, 5, 5, 2, 1, 2, 3, 12, 2};
-        if (kind < 0 || kind > 8 || index < 0 || index >= counts[kind]) throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "bad plane kind or index");
+        static const int counts[10] = {10, 5, 5, 2, 1, 2, 3, 12, 2, 1};
+        if (kind < 0 || kind > 9 || index < 0 || index >= counts[kind]) throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "bad plane kind or index");
+        if (kind == RGBDFLOW_PLANE_HPB_DEPTH && !L.hz) throw ArgError(RGBDFLOW_ERR_INVALID_ARG, "the last solve did not use HPB");
         const void* src = nullptr;
         int esize = c->dbg_tsize, etype = c->dbg_tsize == 8 ? 3 : 0;  // 0 FP32, 1 FP16, 2 BF16, 3 FP64, 4 u8
         int layout = 0;                                                // 0 raster, 1 pitched u, 2 checkerboard
@@ -1133,6 +1293,7 @@ int rgbdflow_debug_read_plane(rgbdflow_ctx* c, int pair, int level, int kind, in
         case RGBDFLOW_PLANE_REG: src = L.reg[index]; break;
         case RGBDFLOW_PLANE_FLOW: src = L.u[index]; layout = 1; break;
         case RGBDFLOW_PLANE_SYSTEM: src = L.sys[index]; layout = 2; break;
+        case RGBDFLOW_PLANE_HPB_DEPTH: src = L.hz; break;
         default: src = dp.stamp[index]; etype = 4; break;
         }
         if (etype == 1 || etype == 2) esize = 2;

@@ -24,7 +24,7 @@ REG_ISOTROPIC, REG_LETOUZEY, REG_HPB = 0, 1, 2
 STORE_FP32, STORE_FP16, STORE_BF16 = 0, 1, 2
 # plane kinds of Context.debug_plane (RGBDFLOW_PLANE_* of include/rgbdflow.h)
 (PLANE_PYRAMID, PLANE_FEATURES1, PLANE_FEATURES2, PLANE_DEPTH, PLANE_DEPTH_MAG, PLANE_REG, PLANE_FLOW, PLANE_SYSTEM,
- PLANE_FILL_ROUND) = range(9)
+ PLANE_FILL_ROUND, PLANE_HPB_DEPTH) = range(10)
 COMPUTE_FP32, COMPUTE_FP64 = 0, 1
 MAX_LEVELS, MAX_OUTER = 16, 64
 
@@ -195,6 +195,7 @@ SIGNATURES = {
     "rgbdflow_profile": (_i, [_vp, _i]),
     "rgbdflow_profile_read": (_i, [_vp, _P(KernelStat), _i]),
     "rgbdflow_debug_read_plane": (_i, [_vp, _i, _i, _i, _i, _P(_d), ctypes.c_size_t, _P(_i), _P(_i)]),
+    "rgbdflow_autotune_describe": (_i, [_i, ctypes.c_char_p, ctypes.c_size_t]),
     "rgbdflow_server_create": (_i, [_vp, _P(ServerConfig), _P(_vp)]),
     "rgbdflow_server_destroy": (_i, [_vp]),
     "rgbdflow_server_submit": (_i, [_vp, _i, ctypes.c_uint64, _P(CameraParams), _vp, _vp, _i, _i, _vp]),
@@ -316,6 +317,15 @@ def read_flo(path):
     """Read a Middlebury .flo file into an (H, W, 2) float32 array (rgbdflow_flo_read; readFlow,
     src/middleburyFlowIO.cpp:22-44).  Host-only."""
     return _read_flow_file(load().rgbdflow_flo_read, path, 2)
+
+
+def autotune_describe(device=0):
+    """The SOR configurations the autotuner chose on `device` (rgbdflow_autotune_describe)."""
+    lib = load()
+    n = lib.rgbdflow_autotune_describe(device, None, 0)
+    buf = ctypes.create_string_buffer(max(n, 0) + 1)
+    lib.rgbdflow_autotune_describe(device, buf, len(buf))
+    return buf.value.decode()
 
 
 def scene_flow_noalloc(pair, params, stream=None):

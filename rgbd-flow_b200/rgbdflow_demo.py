@@ -18,7 +18,6 @@ Options, as in main.cpp:53-66:
   -s/--smoothness-weight        default 0.02
   -v/--depth-vs-color-data-weight   default 1
   -z/--regularization-type      0 isotropic, 1 Letouzey, 2 HPB (default, as in the reference).
-                                HPB is not built: -z 2 fails with UNSUPPORTED.
   --run-fwd / --run-bkwd        default 1 / 0
   -o/--outdir
 
@@ -134,7 +133,7 @@ def parse_args(argv=None):
     ap.add_argument("-s", "--smoothness-weight", type=float, default=.02)
     ap.add_argument("-v", "--depth-vs-color-data-weight", type=float, default=1.0)
     ap.add_argument("-z", "--regularization-type", type=int, default=2,
-                    help="0 = isotropic; 1 = Letouzey; 2 = anisotropic from icra13 paper (HPB, not built)")
+                    help="0 = isotropic; 1 = Letouzey; 2 = anisotropic from icra13 paper (HPB)")
     ap.add_argument("--run-fwd", type=int, default=1, help="whether to run forward flow")
     ap.add_argument("--run-bkwd", type=int, default=0, help="whether to run backward flow")
     ap.add_argument("-o", "--outdir", required=True)

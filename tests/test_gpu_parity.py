@@ -216,6 +216,42 @@ def test_strip_and_tile_sor_agree_bitwise(ctx, monkeypatch, name, seg):
     np.testing.assert_array_equal(tile, strip)
 
 
+def test_every_tunable_sor_choice_agrees_bitwise(ctx, monkeypatch):
+    """Every configuration the SOR autotuner chooses from (tile kernel with 2..6 sweeps per launch and
+    either lane mapping; strip kernel with band heights 64..256) gives the autotuned solve's flow and
+    executed schedule bit for bit, on a ragged batch."""
+    specs = [("320x240", 31), ("160x120", 32), ("320x240", 33)]
+    pairs = [syn.make_config_pair(n, seed=sd) for n, sd in specs]
+    host = [dict(W=p["W"], H=p["H"], cam=cam_of(p), bgr1=p["bgr1"], depth1=p["depth1"], bgr2=p["bgr2"],
+                 depth2=p["depth2"]) for p in pairs]
+    prm = rf.benchmark_params(320)
+    prm.min_width = -16
+    ref = ctx.scene_flow_batch(host, prm, stats=False)
+    print("autotuned:", rf.autotune_describe(0))
+    assert rf.autotune_describe(0)
+    configs = [dict(K=K, ilp=ilp) for K in (2, 3, 4, 5, 6) for ilp in (1, 2)]
+    configs += [dict(K=5, seg=seg) for seg in (64, 128, 192, 256)]
+    for c in configs:
+        q = rf.benchmark_params(320)
+        q.min_width = -16
+        q.sweeps_per_launch = c["K"]
+        if "seg" in c:
+            monkeypatch.setenv("RGBDFLOW_SOR_STRIP", "1")
+            monkeypatch.setenv("RGBDFLOW_STRIP_MIN_W", "128")
+            monkeypatch.setenv("RGBDFLOW_STRIP_MIN_H", "64")
+            monkeypatch.setenv("RGBDFLOW_STRIP_MIN_PX", "1")
+            monkeypatch.setenv("RGBDFLOW_STRIP_SEG", str(c["seg"]))
+        else:
+            monkeypatch.setenv("RGBDFLOW_SOR_STRIP", "0")
+            monkeypatch.setenv("RGBDFLOW_SOR_ILP", str(c["ilp"]))
+        out = ctx.scene_flow_batch(host, q, stats=False)
+        for a, b in zip(ref, out):
+            np.testing.assert_array_equal(a, b, err_msg=str(c))
+        for k in ("RGBDFLOW_SOR_STRIP", "RGBDFLOW_STRIP_MIN_W", "RGBDFLOW_STRIP_MIN_H", "RGBDFLOW_STRIP_MIN_PX",
+                  "RGBDFLOW_STRIP_SEG", "RGBDFLOW_SOR_ILP"):
+            monkeypatch.delenv(k, raising=False)
+
+
 @pytest.mark.parametrize("name,n_inner", [("640x480", 1), ("160x120", 1), ("320x240", 2)])
 def test_whole_level_sor_agrees_bitwise(ctx, monkeypatch, name, n_inner):
     """The whole-level SOR (one CTA runs all iterations of a level that fits its shared memory)
@@ -313,9 +349,11 @@ def test_reduced_precision_pyramids(ctx, storage):
 def test_errors_are_status_codes(ctx):
     p = syn.make_pair(W=40, H=30, f=33.0, cx=19.5, cy=14.5, n_patches=1, hole_frac=0.0, seed=1)
     cam = cam_of(p)
+    bad = rf.benchmark_params(40)
+    bad.regularization = 7
     with pytest.raises(rf.RgbdFlowError) as e:
-        ctx.scene_flow_two_frames(cam, p["bgr1"], p["depth1"], p["bgr2"], p["depth2"], rf.default_params())
-    assert e.value.code == -2  # HPB regularisation is not built
+        ctx.scene_flow_two_frames(cam, p["bgr1"], p["depth1"], p["bgr2"], p["depth2"], bad)
+    assert e.value.code == -1  # no such regularisation type
     small = rf.Context(0, hbm_budget_bytes=64 << 10)
     with pytest.raises(rf.RgbdFlowError) as e:
         small.scene_flow_two_frames(cam, p["bgr1"], p["depth1"], p["bgr2"], p["depth2"], rf.benchmark_params(40))
