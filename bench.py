@@ -152,11 +152,14 @@ def device_pair(rf, torch, p):
                 out=torch.empty((p["H"], p["W"], 3), dtype=torch.float32, device="cuda"))
 
 
-def run_ncu_case(n_pairs, rf, torch):
-    """One batched solve of n_pairs 640x480 pairs through the device-pointer API, graphs off."""
+def run_ncu_case(n_pairs, rf, torch, storage="fp32"):
+    """One batched solve of n_pairs 640x480 pairs through the device-pointer API, graphs off, with
+    the feature / depth pyramids stored as `storage`."""
     ctx = rf.Context(0)
     dev = [device_pair(rf, torch, p) for p in make_pairs(n_pairs, 0)]
-    ctx.scene_flow_batch_device(dev, rf.benchmark_params(W))
+    prm = rf.benchmark_params(W)
+    prm.storage = {"fp32": rf.STORE_FP32, "fp16": rf.STORE_FP16, "bf16": rf.STORE_BF16}[storage]
+    ctx.scene_flow_batch_device(dev, prm)
     torch.cuda.synchronize()
     ctx.close()
 
@@ -398,6 +401,8 @@ def main():
     ap.add_argument("--ncu-case", type=int, default=0, metavar="NP",
                     help="profiling case: one batched solve of NP 640x480 pairs with graphs off "
                          "(every launch visible to a profiler), then exit; prints no bench line")
+    ap.add_argument("--ncu-storage", default="fp32", choices=["fp32", "fp16", "bf16"],
+                    help="storage type of the feature / depth pyramids in the profiling case")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -415,7 +420,7 @@ def main():
 
     torch.cuda.set_device(local)
     if args.ncu_case:
-        run_ncu_case(args.ncu_case, rf, torch)
+        run_ncu_case(args.ncu_case, rf, torch, args.ncu_storage)
         return
     if world > 1:
         import datetime

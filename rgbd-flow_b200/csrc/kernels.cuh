@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 #include <cuda_fp16.h>
 #include <cuda_bf16.h>
+#include <cooperative_groups.h>
 #include <stdint.h>
 
 namespace rgbdflow {
@@ -1321,6 +1322,15 @@ k_sor_strip(const LevelItem<T, S>* items, const StripUnit* units, int n_units, i
         const T fl = it.f_level;
         const int sx = (W + kSorTW - 1) / kSorTW;
         T md = 0, tot0 = 0, tot1 = 0;
+        // Carried from this thread's previous step (row r - 1 of its stage): the other colour's values
+        // of rows r - 1 and r that the next row reads again (its upper neighbour and one of its left /
+        // right neighbours; neither row changes between the two steps: stage s - 1 finished them and
+        // stage s + 1 reaches them later), and the depth-smoothness weight of that upper neighbour
+        // where it was loaded.  dlt: whether the thread's pixel sits one half-row position further
+        // in rows of parity 0 than in rows of parity 1 (the window's first column is odd).
+        T cu[3], cs[3], csU = 0;
+        bool have = false;
+        const int dlt = cl & 1;
 
         if (lkind) {
             load_next();  // rows t0 - 1, t0, t0 + 1: the first group
@@ -1351,21 +1361,40 @@ k_sor_strip(const LevelItem<T, S>* items, const StripUnit* units, int n_units, i
                     const int own = rs + colour * HRW + p, oth = rs + oc;
                     const int ol = oth - 1 + b, orr = oth + b;
                     const int ou = ((r - 1) & NRM) * RW + oc, od = ((r + 1) & NRM) * RW + oc;
+                    // sel: the carried upper neighbour was the previous row's left one (else its right
+                    // one), and this row's right neighbour is the previous row's lower one (else the left)
+                    const bool sel = ((b ^ 1) ^ dlt) != 0;
                     T c[9], xl[3], xu[3], xr[3], xd[3], xp[3], nv[3];
 #pragma unroll
                     for (int z = 0; z < 9; z++) c[z] = ring[z * PL + own];
 #pragma unroll
                     for (int v = 0; v < 3; v++) {
                         const T* xv = ring + (12 + v) * PL;
-                        xl[v] = xv[ol]; xr[v] = xv[orr]; xu[v] = xv[ou]; xd[v] = xv[od]; xp[v] = xv[own];
+                        if (have) {
+                            xu[v] = cu[v];
+                            if (sel) { xr[v] = cs[v]; xl[v] = xv[ol]; }
+                            else { xl[v] = cs[v]; xr[v] = xv[orr]; }
+                        } else {
+                            xl[v] = xv[ol]; xr[v] = xv[orr]; xu[v] = xv[ou];
+                        }
+                        xd[v] = xv[od]; xp[v] = xv[own];
                     }
+                    const T sL = ring[11 * PL + ol];
+                    const T sUv = (have && sel) ? csU : ring[11 * PL + ou];
                     sor_point<T>(c, ring[9 * PL + ol], ring[10 * PL + ou], ring[9 * PL + own], ring[10 * PL + own],
-                                 ring[11 * PL + ol], ring[11 * PL + ou], ring[11 * PL + own], xl, xu, xr, xd, xp,
-                                 k.omega, k.step, nv);
+                                 sL, sUv, ring[11 * PL + own], xl, xu, xr, xd, xp, k.omega, k.step, nv);
 #pragma unroll
                     for (int v = 0; v < 3; v++) ring[(12 + v) * PL + own] = nv[v];
                     if (chk && r >= ya && r < yb && (b ? in1 : in0))
                         for (int v = 0; v < 3; v++) md = maxT(md, absT(nv[v] - xp[v]));
+                    // for the next row (parity b ^ 1): its selector is b ^ dlt
+                    const bool nsel = (b ^ dlt) != 0;
+#pragma unroll
+                    for (int v = 0; v < 3; v++) { cu[v] = nsel ? xl[v] : xr[v]; cs[v] = xd[v]; }
+                    csU = sL;
+                    have = true;
+                } else {
+                    have = false;
                 }
             } else if (outw) {
                 const int ro = t - 4 * nit + 1;  // the row the last stage finished in the previous step
@@ -1595,6 +1624,172 @@ k_sor_level(const LevelItem<T, S>* items, const int* which, SolveConst<T> k, Sor
     }
 }
 
+
+// ------------------------------------------------------------------------------------------
+// Whole-level SOR over a thread-block cluster, for levels whose 15 planes need up to 8 SMs' shared
+// memory (the 80 x 60 and 160 x 120 levels).  One cluster per pair: CTA r of C holds rows
+// [r B, r B + B) (B = ceil(H / C)) with one halo row above and below, runs every SOR iteration of
+// the inner iteration, and after each half-sweep takes the neighbour CTAs' freshly updated boundary
+// row of that colour from their shared memory (distributed shared memory, one cluster barrier per
+// half-sweep).  The convergence check combines the CTAs' maxima through distributed shared memory,
+// so every CTA takes the same decision.  At the end x goes to global memory and, for the fold, each
+// 32 x 32 tile's u += x and statistic partial is taken by one CTA in the tile kernels' order, so
+// results equal the tile kernel's bit for bit, as the one-CTA whole-level kernel's do.
+// Shared layout: 15 planes of [B + 2 rows][2 colours][hwp + 2 positions], padding zero.
+template <class T> __host__ __device__ constexpr size_t level_cluster_smem_bytes(int B, int hwp)
+{
+    return sizeof(T) * ((size_t)15 * (B + 2) * 2 * (hwp + 2) + 64);
+}
+
+template <class T, class S>
+__global__ void __launch_bounds__(1024)
+k_sor_level_cluster(const LevelItem<T, S>* items, const int* which, SolveConst<T> k, SorLaunch L)
+{
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* const buf = reinterpret_cast<T*>(smem_raw);
+    __shared__ int s_stop;
+    __shared__ float s_max;
+    const int C = (int)cl.num_blocks(), rank = (int)cl.block_rank();
+    const LevelItem<T, S>& it = items[which[blockIdx.x / C]];
+    PairCtl* ctl = it.ctl;
+    if (ctl->level_done) return;  // the same for every CTA of the cluster: none reaches a barrier
+    const int W = it.W, H = it.H, hw = it.hwp, RP = hw + 2;
+    const int B = (H + C - 1) / C, r0 = rank * B, nr = max(0, min(H, r0 + B) - r0);
+    const int PLS = (B + 2) * 2 * RP;
+    T* const red = buf + 15 * PLS;
+    const int tid = threadIdx.x, NT = blockDim.x;
+    // stage rows r0 - 1 .. r0 + nr (local rows 0 .. nr + 1): valid pixels from global, zero elsewhere
+    for (int e = tid; e < PLS; e += NT) {
+        const int lr = e / (2 * RP), c = (e / RP) & 1, p = e % RP - 1;
+        const int rr = r0 - 1 + lr;
+        const bool valid = lr <= nr + 1 && rr >= 0 && rr < H && p >= 0 && p < ((W + 1 - (c ^ (rr & 1))) >> 1);
+        const size_t g = valid ? (size_t)rr * 2 * hw + c * hw + p : 0;
+        T v[15];
+#pragma unroll
+        for (int z = 0; z < 12; z++) v[z] = valid ? it.sys[z][g] : (T)0;
+#pragma unroll
+        for (int z = 12; z < 15; z++) v[z] = (valid && !L.xin_zero) ? it.x[L.xin][z - 12][g] : (T)0;
+#pragma unroll
+        for (int z = 0; z < 15; z++) buf[z * PLS + e] = v[z];
+    }
+    if (tid == 0) s_stop = 0;
+    cl.sync();  // every CTA of the cluster has started and staged (its shared memory may be read)
+    T* const up_buf = rank > 0 ? cl.map_shared_rank(buf, rank - 1) : nullptr;
+    T* const dn_buf = rank < C - 1 ? cl.map_shared_rank(buf, rank + 1) : nullptr;
+    for (int itn = 0; itn < k.n_sor; itn++) {
+        const bool chk = !k.fixed && (itn % k.period == k.period - 1);
+        T md = 0;
+        for (int color = 0; color < 2; color++) {
+            for (int q = tid; q < nr * hw; q += NT) {
+                const int li = q / hw, m = q % hw, i = r0 + li;
+                const int b = color ^ (i & 1);
+                if (m >= ((W + 1 - b) >> 1)) continue;
+                const int own = ((li + 1) * 2 + color) * RP + m + 1;
+                const int oth = ((li + 1) * 2 + (color ^ 1)) * RP + m + 1;
+                const int ol = oth - 1 + b, orr = oth + b, ou = oth - 2 * RP, od = oth + 2 * RP;
+                T c[9], xl[3], xu[3], xr[3], xd[3], xp[3], nv[3];
+#pragma unroll
+                for (int z = 0; z < 9; z++) c[z] = buf[z * PLS + own];
+#pragma unroll
+                for (int v = 0; v < 3; v++) {
+                    const T* xv = buf + (12 + v) * PLS;
+                    xl[v] = xv[ol]; xr[v] = xv[orr]; xu[v] = xv[ou]; xd[v] = xv[od]; xp[v] = xv[own];
+                }
+                sor_point<T>(c, buf[9 * PLS + ol], buf[10 * PLS + ou], buf[9 * PLS + own], buf[10 * PLS + own],
+                             buf[11 * PLS + ol], buf[11 * PLS + ou], buf[11 * PLS + own], xl, xu, xr, xd, xp,
+                             k.omega, k.step, nv);
+#pragma unroll
+                for (int v = 0; v < 3; v++) buf[(12 + v) * PLS + own] = nv[v];
+                if (chk)
+                    for (int v = 0; v < 3; v++) md = maxT(md, absT(nv[v] - xp[v]));
+            }
+            cl.sync();  // this half-sweep is done in every CTA
+            // the neighbours' boundary rows of this colour into the halo rows (x planes); the
+            // neighbours write the other colour meanwhile, and reach this colour again only after
+            // the next cluster barrier
+            for (int e = tid; e < 2 * 3 * RP; e += NT) {
+                const int side = e / (3 * RP), v = (e / RP) % 3, p = e % RP;
+                const T* src = side == 0 ? up_buf : dn_buf;
+                if (!src) continue;
+                const int srow = side == 0 ? B : 1;  // the neighbour's last / first own row
+                const int drow = side == 0 ? 0 : nr + 1;
+                buf[(12 + v) * PLS + (drow * 2 + color) * RP + p] = src[(12 + v) * PLS + (srow * 2 + color) * RP + p];
+            }
+            __syncthreads();
+        }
+        if (chk) {
+            float mm = (float)md;
+            for (int off = 16; off > 0; off >>= 1) mm = fmaxf(mm, __shfl_xor_sync(0xffffffffu, mm, off));
+            if ((tid & 31) == 0) red[tid >> 5] = (T)mm;
+            __syncthreads();
+            if (tid == 0) {
+                float g = 0;
+                for (int w = 0; w < NT / 32; w++) g = fmaxf(g, (float)red[w]);
+                s_max = g;
+            }
+            cl.sync();  // every CTA's maximum is in place
+            if (tid == 0) {
+                float g = 0;
+                for (int r = 0; r < C; r++) g = fmaxf(g, *cl.map_shared_rank(&s_max, r));
+                if (rank == 0) {
+                    const int ci = min(itn / k.period, kMaxChecks - 1);
+                    if (g > 0) ctl->maxdiff[ci] = __float_as_uint(g);
+                }
+                if ((double)g < k.sor_tol || (T)g >= k.step) {
+                    s_stop = 1;
+                    if (rank == 0) { ctl->sor_stop = 1; ctl->sor_stop_iter = itn + 1; }
+                }
+            }
+            cl.sync();  // every CTA has read the maxima (s_max may be rewritten) and decided
+            if (s_stop) break;
+        }
+    }
+    // x of the own rows to global: the next inner iteration's buffer, or (fold) scratch that the CTA
+    // folding each tile reads (the fold's next use of x starts from zero)
+    T* const* xo = it.x[L.final_fold ? 0 : L.xout];
+    for (int q = tid; q < nr * W; q += NT) {
+        const int li = q / W, gj = q % W, gi = r0 + li;
+        const int o = ((li + 1) * 2 + ((gi + gj) & 1)) * RP + (gj >> 1) + 1;
+        const int lc = cs_idx(gi, gj, hw);
+        for (int v = 0; v < 3; v++) xo[v][lc] = buf[(12 + v) * PLS + o];
+    }
+    if (!L.final_fold) return;
+    __threadfence();
+    cl.sync();  // every CTA's x is in global memory
+    const int sx = (W + kSorTW - 1) / kSorTW, sy = (H + kSorTH - 1) / kSorTH;
+    const int pitch = it.pitch;
+    const T fl = it.f_level;
+    const int lane = tid & 31;
+    for (int ti = rank; ti < sx * sy; ti += C) {
+        const int ix0 = (ti % sx) * kSorTW, iy0 = (ti / sx) * kSorTH;
+        // the tile kernels' order: virtual thread vt (0..511) takes pixels vt and vt + 512 of the
+        // tile, a warp tree per virtual warp, then the 16 virtual warps in order
+        for (int vw = tid >> 5; vw < 16; vw += NT >> 5) {
+            T part = 0;
+            for (int q = vw * 32 + lane; q < kSorTW * kSorTH; q += 512) {
+                const int gi = iy0 + q / kSorTW, gj = ix0 + q % kSorTW;
+                if (gi >= H || gj >= W) continue;
+                const int lc = cs_idx(gi, gj, hw);
+                const T a = __ldcg(xo[0] + lc), bq = __ldcg(xo[1] + lc), cz = __ldcg(xo[2] + lc);
+                const size_t lp = (size_t)gi * pitch + gj;
+                it.u[0][lp] = addR(it.u[0][lp], a); it.u[1][lp] = addR(it.u[1][lp], bq);
+                it.u[2][lp] = addR(it.u[2][lp], cz);
+                part = addR(part, stat_px<T>(a, bq, cz, fl, it.pyr[6][(size_t)gi * W + gj]));
+            }
+            for (int off = 16; off > 0; off >>= 1) part += __shfl_down_sync(0xffffffffu, part, off);
+            if (lane == 0) red[vw] = part;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            T tot = 0;
+            for (int w = 0; w < 16; w++) tot += red[w];
+            it.stat_part[ti] = tot;
+        }
+        __syncthreads();
+    }
+}
 
 // After each outer iteration: the early-termination statistic of the pair (mean over 3N of
 // sqr(du) * (1, 1, f / depth1), .cu:943-951), the stop decision and the executed-schedule record.

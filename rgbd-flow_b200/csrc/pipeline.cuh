@@ -276,6 +276,18 @@ static inline bool use_level(const HostParams& hp, int W, int H, int hwp)
     return hp.sor_level && level_smem_bytes<T>(H, hwp) <= kLevelSmemMax;
 }
 
+// The cluster size for the whole-level SOR over a thread-block cluster: the fewest CTAs (up to 8)
+// whose row bands' 15 planes fit shared memory, every band holding at least one row; 0 when 8 do
+// not suffice.
+template <class T>
+static inline int level_cluster_size(const HostParams& hp, int H, int hwp)
+{
+    if (!hp.sor_level) return 0;
+    for (int C = 2; C <= 8; C++)
+        if (level_cluster_smem_bytes<T>((H + C - 1) / C, hwp) <= kLevelSmemMax && (H + C - 1) / C * (C - 1) < H) return C;
+    return 0;
+}
+
 // Bump allocator over a byte range.
 struct Bump {
     size_t off = 0;
@@ -315,6 +327,9 @@ struct Plan {
         size_t level_items_off; int n_level;  // whole-level SOR: items (one CTA each)
         size_t level_smem;
         int level_threads;
+        size_t clus_items_off; int n_clus;    // whole-level SOR over a cluster of clus_c CTAs per item
+        int clus_c, clus_threads;
+        size_t clus_smem;
     };
     std::vector<StepDesc> steps;
     struct PyrLevelDesc { size_t jobs_off; int n_jobs; size_t src_tiles_off; int n_src; size_t dst_tiles_off; int n_dst; size_t g_off; };
@@ -712,9 +727,9 @@ static Plan<T, S> make_plan(const std::vector<PairSpec>& pairs, const HostParams
                 for (int x = 0; x < it.lin_tiles_x; x++) lt.push_back(Tile{iid, x, y, y * it.lin_tiles_x + x});
             items.push_back(it);
         }
-        std::vector<int> strip_items, level_items;
-        size_t level_smem = 0;
-        int level_thr = 64;
+        std::vector<int> strip_items, level_items, clus_items;
+        size_t level_smem = 0, clus_smem = 0;
+        int level_thr = 64, clus_c = 0, clus_thr = 64;
         long strip_px = 0;
         for (const auto& x : items)
             if (use_strip<T>(hp, x.W, x.H)) strip_px += (long)x.W * x.H;
@@ -735,6 +750,11 @@ static Plan<T, S> make_plan(const std::vector<PairSpec>& pairs, const HostParams
                 level_items.push_back((int)(&x - items.data()));
                 level_smem = std::max(level_smem, level_smem_bytes<T>(x.H, x.hwp));
                 level_thr = std::max(level_thr, level_threads(x.H, x.hwp));
+                continue;
+            }
+            if (level_cluster_size<T>(hp, x.H, x.hwp) > 0 && !(ch && ch->strip)) {
+                clus_items.push_back((int)(&x - items.data()));
+                clus_c = std::max(clus_c, level_cluster_size<T>(hp, x.H, x.hwp));
                 continue;
             }
             if (strips && (ch ? strip_ok<T>(hp, x.W, x.H) : use_strip<T>(hp, x.W, x.H))) {
@@ -761,6 +781,13 @@ static Plan<T, S> make_plan(const std::vector<PairSpec>& pairs, const HostParams
         d.level_items_off = P.put(level_items); d.n_level = (int)level_items.size();
         d.level_smem = level_smem;
         d.level_threads = level_thr;
+        for (int i : clus_items) {
+            const int B = (items[i].H + clus_c - 1) / clus_c;
+            clus_smem = std::max(clus_smem, level_cluster_smem_bytes<T>(B, items[i].hwp));
+            clus_thr = std::max(clus_thr, std::min(1024, (B * items[i].hwp + 31) / 32 * 32));
+        }
+        d.clus_items_off = P.put(clus_items); d.n_clus = (int)clus_items.size();
+        d.clus_c = clus_c; d.clus_smem = clus_smem; d.clus_threads = clus_thr;
         P.steps.push_back(d);
     }
     // output pointers (one per pair, in the order of the finest step's items = pair order)
@@ -1041,6 +1068,7 @@ static void set_kernel_attrs()
         RF_CUDA(cudaFuncSetAttribute(k_sor_strip<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)strip_smem_bytes<T>()));
     RF_CUDA(cudaFuncSetAttribute(k_sor_level<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLevelSmemMax));
+    RF_CUDA(cudaFuncSetAttribute(k_sor_level_cluster<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLevelSmemMax));
 }
 
 // Whether configuration c fits shared memory for type T.
@@ -1099,6 +1127,32 @@ static int enqueue_level(const Plan<T, S>& P, char* base, int sidx, cudaStream_t
                 L.xout = L.final_fold ? 0 : P.sor_sched[sidx][hh + 1].front().xin;
                 RF_PROF_B(pf, KC_SOR_LEVEL0 + lvl, st);
                 k_sor_level<T, S><<<d.n_level, d.level_threads, d.level_smem, st>>>(items, level_items, k, L);
+                RF_PROF_E(pf, st);
+                launches++;
+            }
+            if (d.n_clus) {
+                // the same, each item over a cluster of row bands
+                SorLaunch L{};
+                L.it0 = 0; L.nit = P.hp.n_sor; L.outer = outer;
+                L.xin = sched.front().xin;
+                L.xin_zero = (hh == 0);
+                L.final_fold = (hh == P.hp.n_inner - 1);
+                L.xout = L.final_fold ? 0 : P.sor_sched[sidx][hh + 1].front().xin;
+                cudaLaunchConfig_t cfg = {};
+                cfg.gridDim = dim3(d.n_clus * d.clus_c);
+                cfg.blockDim = dim3(d.clus_threads);
+                cfg.dynamicSmemBytes = d.clus_smem;
+                cfg.stream = st;
+                cudaLaunchAttribute at[1];
+                at[0].id = cudaLaunchAttributeClusterDimension;
+                at[0].val.clusterDim.x = d.clus_c;
+                at[0].val.clusterDim.y = 1;
+                at[0].val.clusterDim.z = 1;
+                cfg.attrs = at;
+                cfg.numAttrs = 1;
+                RF_PROF_B(pf, KC_SOR_LEVEL0 + lvl, st);
+                RF_CUDA(cudaLaunchKernelEx(&cfg, k_sor_level_cluster<T, S>, items,
+                                           (const int*)(base + P.desc_off + d.clus_items_off), k, L));
                 RF_PROF_E(pf, st);
                 launches++;
             }
