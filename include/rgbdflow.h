@@ -49,7 +49,8 @@ extern "C" {
 /* regularisation types (OpticalFlow::sceneFlowRegularizationType, OpticalFlow.h:99-104) */
 #define RGBDFLOW_REG_ISOTROPIC 0
 #define RGBDFLOW_REG_LETOUZEY  1
-#define RGBDFLOW_REG_HPB       2 /* heuristic probability of boundary: not built, returns RGBDFLOW_ERR_UNSUPPORTED */
+#define RGBDFLOW_REG_HPB       2 /* heuristic probability of boundary (the reference's default): 1 - .99 hpb,
+                                    hpb from computeHeuristicPb per level (heuristicBoundaries.cpp:40-358) */
 
 /* storage type of the image / depth / gradient pyramids on the device.
  * The flow, the linear system and every Jacobi accumulation stay FP32. */

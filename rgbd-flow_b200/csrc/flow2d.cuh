@@ -17,6 +17,7 @@
 // channels interleaved.
 #pragma once
 #include <cuda_runtime.h>
+#include <cooperative_groups.h>
 
 #include <cmath>
 #include <vector>
@@ -253,10 +254,17 @@ __global__ void k_rhs(LevelBufs b, double alpha)
 
 // One SOR update (SmoothFlowSOR.cpp:166-215) of pixel (i, j): left / upper neighbours new
 // (nu, nv), right / lower neighbours and the pixel itself old (ou, ov); returns the change.
-__device__ __forceinline__ double sor_update(const LevelBufs& b, double alpha, int i, int j, const double* nu,
-                                             const double* nv, const double* ou, const double* ov, double* wu,
+template <bool CG = false>
+__device__ __forceinline__ double sor_update(const LevelBufs& b, double alpha, int i, int j, const double* nu_,
+                                             const double* nv_, const double* ou_, const double* ov_, double* wu,
                                              double* wv)
 {
+    // CG: the ring is written by other CTAs of a cluster; its values are read from L2
+    struct R {
+        const double* p;
+        __device__ __forceinline__ double operator[](size_t o) const { return CG ? __ldcg(p + o) : p[o]; }
+    };
+    const R nu{nu_}, nv{nv_}, ou{ou_}, ov{ov_};
     const int W = b.W, H = b.H;
     const size_t o = (size_t)i * W + j;
     const double omega = 1.8;
@@ -347,6 +355,94 @@ __global__ void __launch_bounds__(kSorThreads) k_sor_wavefront(LevelBufs b, doub
     for (size_t p = threadIdx.x; p < N; p += blockDim.x) {
         b.du[p] = ring_u[(size_t)last * N + p];
         b.dv[p] = ring_v[(size_t)last * N + p];
+    }
+}
+
+// The same SOR over a thread-block cluster of C CTAs, for the larger levels: every CTA keeps the
+// same sweep schedule (start steps, completed sweeps, the stop), decided by each CTA's thread 0
+// from the same inputs; the pixels of each step's diagonals are spread over all the cluster's
+// threads; a sweep's maximum change is the largest of the CTAs' partial maxima, read through
+// distributed shared memory.  Two cluster barriers a step: after the updates (the ring's new values
+// are visible to the next step) and after the completion check (every CTA has read the partial
+// maxima before a slot is reused).  The order of the updates is the single-CTA kernel's, so the
+// flow is the same bit for bit; with more sweeps in flight (D up to kMaxRingC) a step carries more
+// independent work.
+constexpr int kMaxRingC = 64;
+
+__global__ void __launch_bounds__(kSorThreads) k_sor_wavefront_cluster(LevelBufs b, double alpha, int nSOR, int D,
+                                                                       double* ring_u, double* ring_v, int* sweeps,
+                                                                       int* status)
+{
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    const int C = (int)cl.num_blocks(), rank = (int)cl.block_rank();
+    const int W = b.W, H = b.H, ndiag = W + H - 1, lag = 2;
+    const size_t N = (size_t)W * H;
+    const int G = C * blockDim.x, g = rank * blockDim.x + threadIdx.x;
+    __shared__ long long start[kMaxRingC];
+    __shared__ unsigned long long maxd[kMaxRingC];
+    __shared__ int s_done, s_stop, s_next;
+    for (size_t p = g; p < N; p += G) {
+        ring_u[(size_t)(D - 1) * N + p] = 0;
+        ring_v[(size_t)(D - 1) * N + p] = 0;
+    }
+    if (threadIdx.x == 0) { s_done = -1; s_stop = -1; s_next = 0; }
+    __threadfence();
+    cl.sync();
+    const long long t_max = (long long)nSOR * (ndiag + lag) + ndiag + 8;
+    long long t = 0;
+    for (; t < t_max; t++) {
+        if (threadIdx.x == 0) {
+            const int nx = s_next;
+            if (nx < nSOR && (nx == 0 || t >= start[(nx - 1) % D] + lag) && (nx < D || s_done >= nx - D)) {
+                start[nx % D] = t;
+                maxd[nx % D] = 0ull;
+                s_next = nx + 1;
+            }
+        }
+        __syncthreads();
+        const int done = s_done, next = s_next;
+        if (s_stop >= 0 || done >= nSOR - 1) break;  // the same in every CTA
+        for (int s = done + 1; s < next; s++) {
+            const long long d = t - start[s % D];
+            if (d < 0 || d >= ndiag) continue;
+            const int cur = s % D, prv = (s + D - 1) % D;
+            const double* nu = ring_u + (size_t)cur * N;
+            const double* nv = ring_v + (size_t)cur * N;
+            const double* ou = ring_u + (size_t)prv * N;
+            const double* ov = ring_v + (size_t)prv * N;
+            double* wu = ring_u + (size_t)cur * N;
+            double* wv = ring_v + (size_t)cur * N;
+            const int i0 = (int)max(0LL, d - (W - 1)), i1 = (int)min((long long)H - 1, d);
+            for (int i = i0 + g; i <= i1; i += G) {
+                const double m = sor_update<true>(b, alpha, i, (int)(d - i), nu, nv, ou, ov, wu, wv);
+                if (m == m) atomicMax(&maxd[s % D], (unsigned long long)__double_as_longlong(m));  // NaN is skipped, as std::max skips it
+            }
+        }
+        __threadfence();
+        cl.sync();  // this step's updates are done and visible in every CTA
+        if (threadIdx.x == 0) {
+            while (s_done + 1 < s_next && t - start[(s_done + 1) % D] == ndiag - 1) {
+                s_done++;
+                double mx = 0;
+                for (int r = 0; r < C; r++)
+                    mx = cmax(mx, __longlong_as_double((long long)*cl.map_shared_rank(&maxd[s_done % D], r)));
+                if (mx < 1e-5) {
+                    s_stop = s_done;
+                    break;
+                }
+            }
+        }
+        cl.sync();  // every CTA has read the partial maxima and advanced its schedule alike
+    }
+    if (rank == 0 && threadIdx.x == 0) {
+        *sweeps = s_done + 1;
+        if (t >= t_max) *status = 1;
+    }
+    const int last = (s_stop >= 0 ? s_stop : nSOR - 1) % D;
+    for (size_t p = g; p < N; p += G) {
+        b.du[p] = __ldcg(ring_u + (size_t)last * N + p);
+        b.dv[p] = __ldcg(ring_v + (size_t)last * N + p);
     }
 }
 

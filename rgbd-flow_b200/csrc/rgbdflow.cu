@@ -769,8 +769,14 @@ static void run_flow2d(rgbdflow_ctx* c, const uint8_t* bgr1, const uint8_t* bgr2
     const size_t o_warp = reserve(N0 * 5 * sizeof(double));
     size_t o_plane[8];
     for (auto& o : o_plane) o = reserve(N0 * sizeof(double));
-    const size_t o_ring_u = reserve((size_t)prm.sor_ring * N0 * sizeof(double));
-    const size_t o_ring_v = reserve((size_t)prm.sor_ring * N0 * sizeof(double));
+    // levels of at least this many pixels run their SOR over a cluster of CTAs with more sweeps in
+    // flight (the flow does not depend on it)
+    const char* ce = std::getenv("RGBDFLOW_FLOW2D_CLUSTER_MIN_PX");
+    const long clus_min_px = ce ? std::atol(ce) : 30000L;
+    constexpr int kClusterCtas = 8, kClusterRing = 32;
+    const int ring_slots = std::max(prm.sor_ring, (long)N0 >= clus_min_px ? kClusterRing : 0);
+    const size_t o_ring_u = reserve((size_t)ring_slots * N0 * sizeof(double));
+    const size_t o_ring_v = reserve((size_t)ring_slots * N0 * sizeof(double));
     if (c->budget && total > c->budget) throw ArgError(RGBDFLOW_ERR_BUDGET, "2-D flow needs " + std::to_string(total) + " device bytes");
     RF_CUDA(cudaSetDevice(c->device));
     cudaStream_t st = c->stream;
@@ -850,8 +856,24 @@ static void run_flow2d(rgbdflow_ctx* c, const uint8_t* bgr1, const uint8_t* bgr2
             for (int hh = 0; hh < prm.n_inner; hh++) {
                 k_phi_psi<<<grid(n), kThreads, 0, st>>>(b, d5, hh == 0 ? 1 : 0, eps);
                 k_rhs<<<grid(n), kThreads, 0, st>>>(b, prm.alpha);
-                k_sor_wavefront<<<1, kSorThreads, 0, st>>>(b, prm.alpha, nSOR, prm.sor_ring, D(o_ring_u), D(o_ring_v),
-                                                           ctl + 1, ctl);
+                if ((long)n >= clus_min_px) {
+                    cudaLaunchConfig_t cfg = {};
+                    cfg.gridDim = dim3(kClusterCtas);
+                    cfg.blockDim = dim3(kSorThreads);
+                    cfg.stream = st;
+                    cudaLaunchAttribute at[1];
+                    at[0].id = cudaLaunchAttributeClusterDimension;
+                    at[0].val.clusterDim.x = kClusterCtas;
+                    at[0].val.clusterDim.y = 1;
+                    at[0].val.clusterDim.z = 1;
+                    cfg.attrs = at;
+                    cfg.numAttrs = 1;
+                    RF_CUDA(cudaLaunchKernelEx(&cfg, k_sor_wavefront_cluster, b, prm.alpha, nSOR, kClusterRing,
+                                               D(o_ring_u), D(o_ring_v), ctl + 1, ctl));
+                } else {
+                    k_sor_wavefront<<<1, kSorThreads, 0, st>>>(b, prm.alpha, nSOR, prm.sor_ring, D(o_ring_u), D(o_ring_v),
+                                                               ctl + 1, ctl);
+                }
                 launches += 3;
             }
             k_update<<<grid(n), kThreads, 0, st>>>(b);

@@ -59,3 +59,23 @@ def test_bad_parameters_are_status_codes(ctx):
         with pytest.raises(rf.RgbdFlowError) as e:
             ctx.optical_flow_2d(b, b, rf.flow2d_params(**over))
         assert e.value.code == -1
+
+
+@pytest.mark.parametrize("tag", ["shift", "patch"])
+def test_cluster_sor_equals_reference_golden(ctx, monkeypatch, tag):
+    """Every level's SOR over a cluster of CTAs with 32 sweeps in flight (the path of the larger
+    levels): the same flow as the reference's, bit for bit."""
+    monkeypatch.setenv("RGBDFLOW_FLOW2D_CLUSTER_MIN_PX", "1")
+    g = np.load(os.path.join(GOLDEN_DIR, "ref_flow2d_golden.npz"))
+    flow = ctx.optical_flow_2d(g[tag + "_bgr1"], g[tag + "_bgr2"], _params(tag))
+    expect = np.stack([g[tag + "_u"], g[tag + "_v"]], -1).astype(np.float32)
+    np.testing.assert_array_equal(flow, expect)
+
+
+def test_cluster_sor_equals_single_cta_on_a_config_pair(ctx, monkeypatch):
+    p = syn.make_config_pair("320x240", seed=2)
+    monkeypatch.setenv("RGBDFLOW_FLOW2D_CLUSTER_MIN_PX", "1000000000")
+    a = ctx.optical_flow_2d(p["bgr1"], p["bgr2"])
+    monkeypatch.setenv("RGBDFLOW_FLOW2D_CLUSTER_MIN_PX", "1")
+    b = ctx.optical_flow_2d(p["bgr1"], p["bgr2"])
+    np.testing.assert_array_equal(a, b)
