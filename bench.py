@@ -396,6 +396,7 @@ def main():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-precision", action="store_true")
     ap.add_argument("--no-sweep", action="store_true", help="skip the served load sweep")
+    ap.add_argument("--no-flow2d", action="store_true", help="skip the 2-D optical flow timing")
     ap.add_argument("--serve-frames", type=int, default=150)
     ap.add_argument("--serve-unique", type=int, default=8)
     ap.add_argument("--ncu-case", type=int, default=0, metavar="NP",
@@ -608,6 +609,28 @@ def main():
     # against the FP32 and the FP64 device solves of the same pairs
     precision = None if args.no_precision else run_precision(ctx, rf, torch, stream, dev, host, args)
 
+    # ---- the demo's 2-D optical flow (flow type 1): ms per pair through the host-buffer call,
+    # beside the CPU restatement at 320x240 (FP64 lexicographic SOR, one thread)
+    flow2d = None
+    if rank == 0 and not args.no_flow2d:
+        flow2d = {}
+        for name in ("320x240", "640x480"):
+            p = syn.make_config_pair(name, seed=1)
+            ctx.optical_flow_2d(p["bgr1"], p["bgr2"])
+            ts = []
+            for _ in range(2):
+                t = time.perf_counter()
+                f2 = ctx.optical_flow_2d(p["bgr1"], p["bgr2"])
+                ts.append(time.perf_counter() - t)
+            flow2d["gpu_ms_" + name] = 1e3 * min(ts)
+            if name == "320x240" and world == 1 and not args.no_cpu_baseline:
+                sys.path.insert(0, os.path.join(ROOT, "tests"))
+                import oracle_binding as ob
+                t = time.perf_counter()
+                u, v = ob.optical_flow_2d(p["bgr1"], p["bgr2"])
+                flow2d["cpu_ms_320x240"] = 1e3 * (time.perf_counter() - t)
+                flow2d["gpu_equals_cpu_320x240"] = bool(np.array_equal(f2, np.stack([u, v], -1).astype(np.float32)))
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baselines(host, dev, torch)
@@ -625,7 +648,7 @@ def main():
                 "one_batch_in_flight": {"value": value_one, "p50_ms": float(np.percentile(step1_ms, 50)),
                                         "p99_ms": float(np.percentile(step1_ms, 99))},
                 "plain": plain, "batch_equals_solo": same, "served": served, "served_warm": served_warm,
-                "mixed_batch": mixed, "precision": precision,
+                "mixed_batch": mixed, "precision": precision, "flow2d": flow2d,
                 "gpu_launches": launches_per_step * args.steps,
                 "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
                 "autotune": rf.autotune_describe(local)}

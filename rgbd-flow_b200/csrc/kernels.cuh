@@ -107,7 +107,13 @@ struct SorLaunch {
     int outer;         // outer iteration index (stats)
     int seq;           // index of this launch among the level's SOR launches (strip kernel tickets)
     int xout;          // whole-level kernel: ping-pong buffer that receives x (non-final inner iterations)
+    int control;       // whole-level kernels: run the outer iteration's control after the fold (k_control's work)
+    int n_checks;      // its convergence-check count
 };
+
+template <class T, class S>
+__device__ __forceinline__ void control_item(const LevelItem<T, S>& it, const SolveConst<T>& k, int outer, int n_checks,
+                                             int lane);
 
 // ------------------------------------------------------------------------------------------
 // small helpers
@@ -1614,6 +1620,7 @@ k_sor_level(const LevelItem<T, S>* items, const int* which, SolveConst<T> k, Sor
             }
             __syncthreads();
         }
+        if (L.control && tid < 32) control_item(it, k, L.outer, L.n_checks, tid);
     } else {
         for (int q = tid; q < H * W; q += NT) {
             const int gi = q / W, gj = q % W;
@@ -1789,21 +1796,25 @@ k_sor_level_cluster(const LevelItem<T, S>* items, const int* which, SolveConst<T
         }
         __syncthreads();
     }
+    if (L.control) {
+        __threadfence();
+        cl.sync();  // every tile's statistic partial is written
+        if (rank == 0 && tid < 32) control_item(it, k, L.outer, L.n_checks, tid);
+    }
 }
 
 // After each outer iteration: the early-termination statistic of the pair (mean over 3N of
 // sqr(du) * (1, 1, f / depth1), .cu:943-951), the stop decision and the executed-schedule record.
+// One warp per item (lane = the thread's lane); the statistic partials are read from L2 (the
+// whole-level cluster kernel calls this after other CTAs wrote them).
 template <class T, class S>
-__global__ void k_control(const LevelItem<T, S>* items, int n_items, SolveConst<T> k, int outer, int n_checks)
+__device__ __forceinline__ void control_item(const LevelItem<T, S>& it, const SolveConst<T>& k, int outer, int n_checks,
+                                             int lane)
 {
-    const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    const int lane = threadIdx.x & 31;
-    if (w >= n_items) return;
-    const LevelItem<T, S>& it = items[w];
     PairCtl* ctl = it.ctl;
     if (ctl->level_done) return;
     T s = 0;
-    for (int i = lane; i < it.n_sor_tiles; i += 32) s += it.stat_part[i];
+    for (int i = lane; i < it.n_sor_tiles; i += 32) s += __ldcg(it.stat_part + i);
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
     if (lane == 0) {
         const double st = (double)s / ((double)it.W * it.H * 3);
@@ -1821,6 +1832,14 @@ __global__ void k_control(const LevelItem<T, S>* items, int n_items, SolveConst<
         ctl->outer_exec[lv] = outer + 1;
         if (it.allow_early && !k.fixed && st < k.outer_tol) ctl->level_done = 1;
     }
+}
+
+template <class T, class S>
+__global__ void k_control(const LevelItem<T, S>* items, int n_items, SolveConst<T> k, int outer, int n_checks)
+{
+    const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (w >= n_items) return;
+    control_item(items[w], k, outer, n_checks, threadIdx.x & 31);
 }
 
 // Final flow (level 0) to the caller's interleaved (u, v, w) float layout.

@@ -1107,6 +1107,8 @@ static int enqueue_level(const Plan<T, S>& P, char* base, int sidx, cudaStream_t
         RF_PROF_E(pf, st);
         launches++;
     }
+    // a step whose items are all on the whole-level kernels runs the control in those kernels
+    const bool fold_control = !d.n_sor && !d.n_units && (d.n_level || d.n_clus);
     for (int outer = 0; outer < P.hp.n_outer; outer++) {
         for (int hh = 0; hh < P.hp.n_inner; hh++) {
             const auto& sched = P.sor_sched[sidx][hh];
@@ -1125,6 +1127,8 @@ static int enqueue_level(const Plan<T, S>& P, char* base, int sidx, cudaStream_t
                 L.xin_zero = (hh == 0);
                 L.final_fold = (hh == P.hp.n_inner - 1);
                 L.xout = L.final_fold ? 0 : P.sor_sched[sidx][hh + 1].front().xin;
+                L.control = fold_control && L.final_fold;
+                L.n_checks = P.n_checks[sidx].back();
                 RF_PROF_B(pf, KC_SOR_LEVEL0 + lvl, st);
                 k_sor_level<T, S><<<d.n_level, d.level_threads, d.level_smem, st>>>(items, level_items, k, L);
                 RF_PROF_E(pf, st);
@@ -1138,6 +1142,8 @@ static int enqueue_level(const Plan<T, S>& P, char* base, int sidx, cudaStream_t
                 L.xin_zero = (hh == 0);
                 L.final_fold = (hh == P.hp.n_inner - 1);
                 L.xout = L.final_fold ? 0 : P.sor_sched[sidx][hh + 1].front().xin;
+                L.control = fold_control && L.final_fold;
+                L.n_checks = P.n_checks[sidx].back();
                 cudaLaunchConfig_t cfg = {};
                 cfg.gridDim = dim3(d.n_clus * d.clus_c);
                 cfg.blockDim = dim3(d.clus_threads);
@@ -1172,12 +1178,14 @@ static int enqueue_level(const Plan<T, S>& P, char* base, int sidx, cudaStream_t
                 RF_PROF_E(pf, st);
             }
         }
-        const int wpb = 4;
-        RF_PROF_B(pf, KC_CTL, st);
-        k_control<T, S><<<(d.n_items + wpb - 1) / wpb, 32 * wpb, 0, st>>>(items, d.n_items, k, outer,
-                                                                          P.n_checks[sidx].back());
-        RF_PROF_E(pf, st);
-        launches++;
+        if (!fold_control) {
+            const int wpb = 4;
+            RF_PROF_B(pf, KC_CTL, st);
+            k_control<T, S><<<(d.n_items + wpb - 1) / wpb, 32 * wpb, 0, st>>>(items, d.n_items, k, outer,
+                                                                              P.n_checks[sidx].back());
+            RF_PROF_E(pf, st);
+            launches++;
+        }
     }
     return launches;
 }
