@@ -356,10 +356,28 @@ class fill_order:
         oracle().sfo_set_fill_order(self.old)
 
 
-def depth_sigma(depth_m, max_dist=4):
+REF_SIGMA_SO = os.path.join(ORACLE_DIR, "_ref", "libref_sigma.so")
+_ref_sigma = None
+
+
+def ref_sigma_available():
+    return os.path.exists(REF_SIGMA_SO)
+
+
+def depth_sigma(depth_m, max_dist=4, impl="oracle"):
+    """The depth sigma of setUpSceneFlowParams: the restatement (impl="oracle") or the reference's own
+    depth-noise model compiled in place (impl="ref", oracle/_ref/libref_sigma.so)."""
+    global _ref_sigma
     d = _cont(depth_m, np.float32)
     H, W = d.shape
     out = np.zeros_like(d)
+    if impl == "ref":
+        if _ref_sigma is None:
+            _ref_sigma = ctypes.CDLL(REF_SIGMA_SO)
+            _ref_sigma.ref_depth_sigma.argtypes = [_pf, _i, _i, _i, _pf]
+            _ref_sigma.ref_depth_sigma.restype = None
+        _ref_sigma.ref_depth_sigma(fptr(d), W, H, max_dist, fptr(out))
+        return out
     oracle().sfo_depth_sigma(fptr(d), W, H, max_dist, fptr(out))
     return out
 

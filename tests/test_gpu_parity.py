@@ -1,7 +1,12 @@
 """Parity of the sm_100a solve (through the C ABI) with the CPU oracle, on a B200.
 
 Tolerances (3-D endpoint error over frame-1 pixels with valid depth, metres):
-  * against the faithful oracle, default hole fill:      mean <= 5e-5 (0.05 mm; the bar is 1 mm)
+  * against the faithful oracle, default hole fill:      mean <= 5e-5 (0.05 mm; the bar is 1 mm),
+                                                          max <= 1e-2; every pixel off by more
+                                                          than 0.1 mm lies within 12 pixels (L1) of
+                                                          a hole of either frame
+  * against the faithful oracle with the device's hole-fill order (parallel rounds), which leaves
+    the arithmetic alone:                                 mean <= 2e-5, max <= 1e-3
   * against the oracle on inputs whose holes are isolated (where the parallel hole fill is exact):
                                                           mean <= 2e-5
   * FP64 device solve against the FP64 oracle, isolated holes: mean <= 1e-7
@@ -47,10 +52,25 @@ def test_two_frames_matches_oracle(ctx, name, fixed):
     cam = cam_of(p)
     gpu, st = ctx.scene_flow_two_frames(cam, p["bgr1"], p["depth1"], p["bgr2"], p["depth2"], prm)
     ref, rst = ob.two_frames(cam, p["bgr1"], p["depth1"], p["bgr2"], p["depth2"], prm)
+    with ob.fill_order("rounds"):
+        rnd, _ = ob.two_frames(cam, p["bgr1"], p["depth1"], p["bgr2"], p["depth2"], prm)
     mean, mx = epe(gpu, ref, p)
-    print("%s fixed=%d: EPE vs oracle mean %.3g mm max %.3g mm" % (name, fixed, mean * 1e3, mx * 1e3))
+    m2, x2 = epe(gpu, rnd, p)
+    # where the result departs from the reference-order oracle: near holes, where the fill order
+    # gives a hole pixel another median
+    from scipy.ndimage import distance_transform_cdt
+    hole = (p["depth1"] <= 0) | (p["depth2"] <= 0)
+    dist = distance_transform_cdt(~hole, metric="taxicab")
+    err = np.linalg.norm(gpu.astype(np.float64) - ref.astype(np.float64), axis=-1)
+    big = (err > 1e-4) & (p["depth1"] > 0)
+    far = int(dist[big].max()) if big.any() else 0
+    print("%s fixed=%d: EPE vs oracle mean %.3g mm max %.3g mm (pixels off by > 0.1 mm: %d, farthest %d px from a "
+          "hole); vs the oracle with the device's fill order mean %.3g mm max %.3g mm"
+          % (name, fixed, mean * 1e3, mx * 1e3, big.sum(), far, m2 * 1e3, x2 * 1e3))
     assert np.isfinite(gpu).all()
-    assert mean <= 5e-5
+    assert mean <= 5e-5 and mx <= 1e-2
+    assert far <= 12
+    assert m2 <= 2e-5 and x2 <= 1e-3
     assert st.summary() == rst.summary()
 
 

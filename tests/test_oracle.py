@@ -137,6 +137,22 @@ def test_rounds_fill_order(oracle_lib):
         ob.median_fill_rounds(np.zeros((4, 4)))
 
 
+def test_depth_sigma_matches_reference_golden(oracle_lib):
+    """The restatement against the reference's own depth-noise model (staticDepthNoiseModeling.cpp:
+    85-137, 225-258, compiled in place; tests/golden/make_sigma_golden.py): every sigma equal."""
+    g = np.load(os.path.join(GOLDEN, "ref_sigma_golden.npz"))
+    for tag in ("a", "b", "c"):
+        assert np.array_equal(ob.depth_sigma(g["in_" + tag], 4), g["out_" + tag]), tag
+
+
+@pytest.mark.skipif(not ob.ref_sigma_available(), reason="reference depth-noise model not built (oracle/_ref)")
+@pytest.mark.parametrize("name", ["320x240", "640x480"])
+def test_depth_sigma_matches_live_reference(oracle_lib, name):
+    p = syn.make_config_pair(name, seed=8)
+    for k in ("depth1", "depth2"):
+        assert np.array_equal(ob.depth_sigma(p[k], 4), ob.depth_sigma(p[k], 4, impl="ref"))
+
+
 def test_depth_sigma_known_answers(oracle_lib):
     """computeDepthMapStdevsPointwise + increaseStdevsNearDepthBoundaries
     (staticDepthNoiseModeling.cpp:232-258, 85-137)."""

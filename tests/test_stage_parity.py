@@ -11,6 +11,7 @@ Tolerances ("rel" = largest |device - oracle| over a plane, divided by the plane
     pyramid planes:                             rel <= 2e-6 (LETOUZEY's exp: rel <= 1e-5)
   * hole fill: the device's filled depths equal the oracle's restatement of the device's fill
     order (parallel rounds) bit for bit
+  * depth sigma (through the level-0 depth-data weight): within one float rounding
   * one linearisation (the compact 12-coefficient system against the reference's 8 planes):
                                                 rel <= 1e-5 per coefficient plane
 """
@@ -85,6 +86,20 @@ def test_level_inputs_match_oracle(ctx, solved):
         for c in range(2):
             assert np.array_equal(ctx.debug_plane(0, k, rf.PLANE_REG, c), reg[..., c])
     print("level inputs: worst rel %s" % worst)
+
+
+def test_depth_sigma_weights_match_oracle(ctx, solved):
+    """The device's depth sigma (k_sigma: the boundary distance by an exact L1 search) through the
+    level-0 depth-data weight stereoError(1) / sigma, against the oracle's sigma (itself equal to
+    the reference's own depth-noise model): within one float rounding (the boundary increase goes
+    through exp and log, whose last bit CUDA and the C library may round differently)."""
+    p, prm, _, _ = solved
+    sig = ob.depth_sigma(p["depth1"], 4).astype(np.float64)
+    expect = (ob.stereo_error1() / sig * prm.depth_vs_color_data_weight).astype(np.float32).astype(np.float64)
+    dev = ctx.debug_plane(0, 0, rf.PLANE_PYRAMID, 8)
+    r = np.abs(dev - expect) / np.abs(expect)
+    print("depth-data weights: %.5f equal, max rel %.3g" % (np.mean(dev == expect), r.max()))
+    assert r.max() <= 2.4e-7
 
 
 def test_letouzey_weights_match_oracle(ctx):
