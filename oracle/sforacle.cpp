@@ -152,6 +152,7 @@ void resize_dims(const Img& in, Img& out, int DW, int DH)
 int pyramid_levels(int width, double ratio, int min_width)
 {
     if (min_width < 0) min_width = std::max(1, width / -min_width);  // API convention: W / d per pair
+    if (min_width == 0) throw std::runtime_error("min_width 0: the level count never ends");
     if (ratio > 0.98 || ratio < 0.4) ratio = 0.75;
     double w = width * ratio;
     int n = 1;
@@ -932,6 +933,8 @@ using namespace sfo;
  * is alone).  Both sampling factors are the ratio of the heights, as in the reference. */
 void depth_map_pyramid(const Img& image, double ratio, int min_width, std::vector<Img>& lev)
 {
+    if (min_width < 0) min_width = std::max(1, image.w / -min_width);  // API convention: W / d per pair
+    if (min_width == 0) throw std::runtime_error("min_width 0: the level count never ends");
     if (ratio > 0.98 || ratio < 0.4) ratio = 0.75;
     double w = image.w * ratio;
     int nLevels = 1;
@@ -1705,7 +1708,11 @@ int sfo_set_threads(int n)
 #endif
 }
 
-int sfo_pyramid_levels(int width, double ratio, int min_width) { return pyramid_levels(width, ratio, min_width); }
+int sfo_pyramid_levels(int width, double ratio, int min_width)
+{
+    try { return pyramid_levels(width, ratio, min_width); }
+    catch (const std::exception& e) { g_err = e.what(); return -1; }
+}
 
 /* All levels of GaussianPyramid::ConstructPyramid, concatenated (level 0 first).
  * dims (2 * nLevels ints) receives the level sizes; returns the level count. */
@@ -1714,7 +1721,8 @@ int sfo_build_pyramid(const double* img, int W, int H, int C, double ratio, int 
     Img b; b.alloc(W, H, C);
     std::memcpy(b.data(), img, sizeof(double) * b.n());
     std::vector<Img> lev;
-    build_pyramid(b, ratio, min_width, lev);
+    try { build_pyramid(b, ratio, min_width, lev); }
+    catch (const std::exception& e) { g_err = e.what(); return -1; }
     size_t off = 0;
     for (size_t i = 0; i < lev.size(); i++) {
         if (dims) { dims[2 * i] = lev[i].w; dims[2 * i + 1] = lev[i].h; }
@@ -1966,7 +1974,8 @@ int sfo_depth_map_pyramid(const double* depth, int W, int H, double ratio, int m
     d.alloc(W, H, 1);
     std::memcpy(d.data(), depth, sizeof(double) * (size_t)W * H);
     std::vector<Img> lev;
-    depth_map_pyramid(d, ratio, min_width, lev);
+    try { depth_map_pyramid(d, ratio, min_width, lev); }
+    catch (const std::exception& e) { g_err = e.what(); return -1; }
     size_t off = 0;
     for (size_t i = 0; i < lev.size(); i++) {
         if (dims) { dims[2 * i] = lev[i].w; dims[2 * i + 1] = lev[i].h; }

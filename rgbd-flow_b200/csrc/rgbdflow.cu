@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <map>
+#include <set>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -383,7 +384,8 @@ GraphEntry& graph_for(rgbdflow_ctx* c, const Plan<T, S>& P, const std::vector<Pa
 
 struct TuneState {
     std::mutex mu;
-    TuneTable table[64];  // per device
+    TuneTable table[64];                  // per device
+    std::set<std::string> complete[64];   // per device: batches (plan_key) whose every step is tuned
 };
 TuneState& tune_state()
 {
@@ -432,11 +434,16 @@ void tune_sor(rgbdflow_ctx* c, const std::vector<PairSpec>& pairs, const HostPar
     TuneState& ts = tune_state();
     std::lock_guard<std::mutex> lk(ts.mu);
     TuneTable& tt = ts.table[c->device & 63];
+    const std::string bkey = plan_key(pairs, hp, (int)sizeof(T) * 10 + (int)sizeof(S));
+    if (ts.complete[c->device & 63].count(bkey)) return;
     const Plan<T, S> P0 = make_plan<T, S>(pairs, hp, &tt);
     std::vector<int> todo;
     for (int sidx = 0; sidx < P0.Lmax; sidx++)
         if (!P0.step_tuned[sidx] && (P0.steps[sidx].n_sor || P0.steps[sidx].n_units)) todo.push_back(sidx);
-    if (todo.empty()) return;
+    if (todo.empty()) {
+        ts.complete[c->device & 63].insert(bkey);
+        return;
+    }
     wait_idle(c);
     ensure_attrs<T, S>(c, sizeof(T) == 8 ? 1 : (std::is_same<S, __half>::value ? 2 : (std::is_same<S, float>::value ? 0 : 3)));
     const SolveConst<T> k = solve_const<T>(hp);
@@ -480,6 +487,7 @@ void tune_sor(rgbdflow_ctx* c, const std::vector<PairSpec>& pairs, const HostPar
         best.us_per_it = best_us;
         tt.m[P0.step_keys[sidx]] = best;
     }
+    ts.complete[c->device & 63].insert(bkey);
     cudaEventDestroy(ea);
     cudaEventDestroy(eb);
     RF_CUDA(cudaGetLastError());

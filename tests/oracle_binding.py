@@ -214,6 +214,8 @@ def depth_map_pyramid(depth, ratio, min_width, impl="oracle"):
         fn = oracle().sfo_depth_map_pyramid
     dims = np.zeros(128, np.int32)
     n = fn(dptr(d), W, H, ratio, min_width, None, iptr(dims))
+    if n < 0:
+        raise RuntimeError(oracle().sfo_last_error().decode())
     out = np.zeros(sum(int(dims[2 * i]) * int(dims[2 * i + 1]) for i in range(n)))
     fn(dptr(d), W, H, ratio, min_width, dptr(out), iptr(dims))
     levels, off = [], 0
@@ -235,6 +237,8 @@ def build_pyramid(img, ratio, min_width, impl="oracle"):
     fn = lib.sfo_build_pyramid if impl == "oracle" else lib.ref_build_pyramid
     dims = np.zeros(64, np.int32)
     n = fn(dptr(img), W, H, C, ratio, min_width, None, iptr(dims))
+    if n < 0:
+        raise RuntimeError(oracle().sfo_last_error().decode())
     total = sum(int(dims[2 * i]) * int(dims[2 * i + 1]) * C for i in range(n))
     out = np.zeros(total, np.float64)
     fn(dptr(img), W, H, C, ratio, min_width, dptr(out), iptr(dims))

@@ -134,3 +134,16 @@ def test_hpb_scene_flow_end_to_end():
     ei = syn.epe3d(fi, p["gt"], p["z1_true"], p["cam"], valid)[0]
     eh = syn.epe3d(fh, p["gt"], p["z1_true"], p["cam"], valid)[0]
     assert eh <= ei * 1.05
+
+
+def test_depth_map_pyramid_min_width_conventions(oracle_lib):
+    """A negative min_width is the library's W / d convention; 0 never ends the level count and is
+    an error (the reference loops for ever)."""
+    d = np.full((48, 64), 2.0)
+    a = ob.depth_map_pyramid(d, 0.5, -16)
+    b = ob.depth_map_pyramid(d, 0.5, 4)
+    assert [x.shape for x in a] == [x.shape for x in b]
+    with pytest.raises(RuntimeError):
+        ob.depth_map_pyramid(d, 0.5, 0)
+    with pytest.raises(RuntimeError):
+        ob.build_pyramid(d, 0.5, 0)
