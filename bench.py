@@ -152,13 +152,14 @@ def device_pair(rf, torch, p):
                 out=torch.empty((p["H"], p["W"], 3), dtype=torch.float32, device="cuda"))
 
 
-def run_ncu_case(n_pairs, rf, torch, storage="fp32"):
+def run_ncu_case(n_pairs, rf, torch, storage="fp32", reg="isotropic"):
     """One batched solve of n_pairs 640x480 pairs through the device-pointer API, graphs off, with
-    the feature / depth pyramids stored as `storage`."""
+    the feature / depth pyramids stored as `storage` and the given regularisation."""
     ctx = rf.Context(0)
     dev = [device_pair(rf, torch, p) for p in make_pairs(n_pairs, 0)]
     prm = rf.benchmark_params(W)
     prm.storage = {"fp32": rf.STORE_FP32, "fp16": rf.STORE_FP16, "bf16": rf.STORE_BF16}[storage]
+    prm.regularization = {"isotropic": rf.REG_ISOTROPIC, "letouzey": rf.REG_LETOUZEY, "hpb": rf.REG_HPB}[reg]
     ctx.scene_flow_batch_device(dev, prm)
     torch.cuda.synchronize()
     ctx.close()
@@ -404,6 +405,8 @@ def main():
                          "(every launch visible to a profiler), then exit; prints no bench line")
     ap.add_argument("--ncu-storage", default="fp32", choices=["fp32", "fp16", "bf16"],
                     help="storage type of the feature / depth pyramids in the profiling case")
+    ap.add_argument("--ncu-reg", default="isotropic", choices=["isotropic", "letouzey", "hpb"],
+                    help="regularisation of the profiling case")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -421,7 +424,7 @@ def main():
 
     torch.cuda.set_device(local)
     if args.ncu_case:
-        run_ncu_case(args.ncu_case, rf, torch, args.ncu_storage)
+        run_ncu_case(args.ncu_case, rf, torch, args.ncu_storage, args.ncu_reg)
         return
     if world > 1:
         import datetime

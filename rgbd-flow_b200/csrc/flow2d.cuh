@@ -286,6 +286,44 @@ __device__ __forceinline__ double sor_update(const LevelBufs& b, double alpha, i
     return cmax(fabs(dsub(nDU, prevDU)), fabs(dsub(nDV, prevDV)));
 }
 
+// One step of the overlapping sweeps: for every sweep in flight, the pixels of its current
+// diagonal.  The step's updates are flattened into one list spread over the G threads (thread g
+// takes items g, g + G, ...), so the memory latency of the sweeps' updates overlaps across threads
+// instead of adding up sweep after sweep.  Every update reads only values no other update of the
+// step writes (the diagonal structure), so the order within the step is free.
+template <bool CG>
+__device__ __forceinline__ void sor_step(const LevelBufs& b, double alpha, long long t, int done, int next,
+                                         const long long* start, int D, int ndiag, size_t N, double* ring_u,
+                                         double* ring_v, unsigned long long* maxd, int g, int G)
+{
+    const int W = b.W, H = b.H;
+    int total = 0;
+    for (int s = done + 1; s < next; s++) {
+        const long long d = t - start[s % D];
+        if (d < 0 || d >= ndiag) continue;
+        total += (int)(min((long long)H - 1, d) - max(0LL, d - (W - 1)) + 1);
+    }
+    for (int k = g; k < total; k += G) {
+        int s = done + 1, rem = k, i0 = 0;
+        long long d = 0;
+        for (; s < next; s++) {  // the sweep of item k (k < total: always found)
+            d = t - start[s % D];
+            if (d < 0 || d >= ndiag) continue;
+            i0 = (int)max(0LL, d - (W - 1));
+            const int cnt = (int)(min((long long)H - 1, d) - i0 + 1);
+            if (rem < cnt) break;
+            rem -= cnt;
+        }
+        const int i = i0 + rem;
+        const int cur = s % D, prv = (s + D - 1) % D;
+        double* wu = ring_u + (size_t)cur * N;
+        double* wv = ring_v + (size_t)cur * N;
+        const double m = sor_update<CG>(b, alpha, i, (int)(d - i), wu, wv, ring_u + (size_t)prv * N,
+                                        ring_v + (size_t)prv * N, wu, wv);
+        if (m == m) atomicMax(&maxd[s % D], (unsigned long long)__double_as_longlong(m));  // NaN is skipped, as std::max skips it
+    }
+}
+
 // The SOR iterations of one inner iteration (SmoothFlowSOR.cpp:156-226) as overlapping
 // anti-diagonal sweeps, one CTA.  ring: D slots of (u, v) increments, each N doubles.  Leaves the
 // last sweep's increments (the first that converged, max change < 1e-5, or sweep nSOR - 1) in
@@ -319,22 +357,7 @@ __global__ void __launch_bounds__(kSorThreads) k_sor_wavefront(LevelBufs b, doub
         __syncthreads();
         const int done = s_done, next = s_next;
         if (s_stop >= 0 || done >= nSOR - 1) break;
-        for (int s = done + 1; s < next; s++) {
-            const long long d = t - start[s % D];
-            if (d < 0 || d >= ndiag) continue;
-            const int cur = s % D, prv = (s + D - 1) % D;
-            const double* nu = ring_u + (size_t)cur * N;
-            const double* nv = ring_v + (size_t)cur * N;
-            const double* ou = ring_u + (size_t)prv * N;
-            const double* ov = ring_v + (size_t)prv * N;
-            double* wu = ring_u + (size_t)cur * N;
-            double* wv = ring_v + (size_t)cur * N;
-            const int i0 = (int)max(0LL, d - (W - 1)), i1 = (int)min((long long)H - 1, d);
-            for (int i = i0 + threadIdx.x; i <= i1; i += blockDim.x) {
-                const double m = sor_update(b, alpha, i, (int)(d - i), nu, nv, ou, ov, wu, wv);
-                if (m == m) atomicMax(&maxd[s % D], (unsigned long long)__double_as_longlong(m));  // NaN is skipped, as std::max skips it
-            }
-        }
+        sor_step<false>(b, alpha, t, done, next, start, D, ndiag, N, ring_u, ring_v, maxd, threadIdx.x, blockDim.x);
         __syncthreads();
         if (threadIdx.x == 0) {
             while (s_done + 1 < s_next && t - start[(s_done + 1) % D] == ndiag - 1) {
@@ -403,22 +426,7 @@ __global__ void __launch_bounds__(kSorThreads) k_sor_wavefront_cluster(LevelBufs
         __syncthreads();
         const int done = s_done, next = s_next;
         if (s_stop >= 0 || done >= nSOR - 1) break;  // the same in every CTA
-        for (int s = done + 1; s < next; s++) {
-            const long long d = t - start[s % D];
-            if (d < 0 || d >= ndiag) continue;
-            const int cur = s % D, prv = (s + D - 1) % D;
-            const double* nu = ring_u + (size_t)cur * N;
-            const double* nv = ring_v + (size_t)cur * N;
-            const double* ou = ring_u + (size_t)prv * N;
-            const double* ov = ring_v + (size_t)prv * N;
-            double* wu = ring_u + (size_t)cur * N;
-            double* wv = ring_v + (size_t)cur * N;
-            const int i0 = (int)max(0LL, d - (W - 1)), i1 = (int)min((long long)H - 1, d);
-            for (int i = i0 + g; i <= i1; i += G) {
-                const double m = sor_update<true>(b, alpha, i, (int)(d - i), nu, nv, ou, ov, wu, wv);
-                if (m == m) atomicMax(&maxd[s % D], (unsigned long long)__double_as_longlong(m));  // NaN is skipped, as std::max skips it
-            }
-        }
+        sor_step<true>(b, alpha, t, done, next, start, D, ndiag, N, ring_u, ring_v, maxd, g, G);
         __threadfence();
         cl.sync();  // this step's updates are done and visible in every CTA
         if (threadIdx.x == 0) {

@@ -438,12 +438,27 @@ __global__ void k_hpb_rowsum(const HpbItem<T>* items, const int* first, int n_it
     if (rel < 0 || rel >= 7 * it.H) return;
     const int i = rel / 7, c = rel % 7;
     const size_t base = (size_t)i * it.W;
+    // the loads of 8 pixels are issued together; the sums stay in the reference's order
     if (c == 6) {
         unsigned s = 0;
-        for (int j = 0; j < it.W; j++) { it.pre_v[base + j] = s; s += it.nval[base + j]; }
+        for (int j0 = 0; j0 < it.W; j0 += 8) {
+            unsigned v[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) v[u] = j0 + u < it.W ? it.nval[base + j0 + u] : 0u;
+#pragma unroll
+            for (int u = 0; u < 8; u++)
+                if (j0 + u < it.W) { it.pre_v[base + j0 + u] = s; s += v[u]; }
+        }
     } else {
         float s = 0;
-        for (int j = 0; j < it.W; j++) { it.pre[c][base + j] = s; s = fad(s, hpb_chan(it, base + j, c)); }
+        for (int j0 = 0; j0 < it.W; j0 += 8) {
+            float v[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) v[u] = j0 + u < it.W ? hpb_chan(it, base + j0 + u, c) : 0.f;
+#pragma unroll
+            for (int u = 0; u < 8; u++)
+                if (j0 + u < it.W) { it.pre[c][base + j0 + u] = s; s = fad(s, v[u]); }
+        }
     }
 }
 
@@ -459,24 +474,46 @@ __global__ void k_hpb_colsum(const HpbItem<T>* items, const int* first, int n_it
     if (rel < 0 || rel >= 7 * (it.W + 1)) return;
     const int jj = rel / 7, c = rel % 7;  // jj: column of the integral image (0 = the zero column)
     const int W1 = it.W + 1;
+    // the loads of 8 rows are issued together; the sums stay in the reference's order
     if (c == 6) {
         unsigned* ii = it.ii_v;
         ii[jj] = 0;
         unsigned a = 0;
-        for (int i = 0; i < it.H; i++) {
-            if (jj > 0) a = (a + it.pre_v[(size_t)i * it.W + jj - 1]) + it.nval[(size_t)i * it.W + jj - 1];
-            ii[(size_t)(i + 1) * W1 + jj] = a;
+        for (int i0 = 0; i0 < it.H; i0 += 8) {
+            unsigned p[8], v[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                const bool in = jj > 0 && i0 + u < it.H;
+                const size_t l = in ? (size_t)(i0 + u) * it.W + jj - 1 : 0;
+                p[u] = in ? it.pre_v[l] : 0u;
+                v[u] = in ? it.nval[l] : 0u;
+            }
+#pragma unroll
+            for (int u = 0; u < 8; u++)
+                if (i0 + u < it.H) {
+                    if (jj > 0) a = (a + p[u]) + v[u];
+                    ii[(size_t)(i0 + u + 1) * W1 + jj] = a;
+                }
         }
     } else {
         float* ii = it.ii[c];
         ii[jj] = 0;
         float a = 0;
-        for (int i = 0; i < it.H; i++) {
-            if (jj > 0) {
-                const size_t l = (size_t)i * it.W + jj - 1;
-                a = fad(fad(a, it.pre[c][l]), hpb_chan(it, l, c));
+        for (int i0 = 0; i0 < it.H; i0 += 8) {
+            float p[8], v[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                const bool in = jj > 0 && i0 + u < it.H;
+                const size_t l = in ? (size_t)(i0 + u) * it.W + jj - 1 : 0;
+                p[u] = in ? it.pre[c][l] : 0.f;
+                v[u] = in ? hpb_chan(it, l, c) : 0.f;
             }
-            ii[(size_t)(i + 1) * W1 + jj] = a;
+#pragma unroll
+            for (int u = 0; u < 8; u++)
+                if (i0 + u < it.H) {
+                    if (jj > 0) a = fad(fad(a, p[u]), v[u]);
+                    ii[(size_t)(i0 + u + 1) * W1 + jj] = a;
+                }
         }
     }
 }

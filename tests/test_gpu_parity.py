@@ -2,9 +2,11 @@
 
 Tolerances (3-D endpoint error over frame-1 pixels with valid depth, metres):
   * against the faithful oracle, default hole fill:      mean <= 5e-5 (0.05 mm; the bar is 1 mm),
-                                                          max <= 1e-2; every pixel off by more
-                                                          than 0.1 mm lies within 12 pixels (L1) of
-                                                          a hole of either frame
+                                                          max <= 5e-2; the large pointwise
+    differences come from the hole fill's order alone (the reference's hash-set order against the
+    device's rounds gives ~4.5 % of the hole pixels another median), so every pixel whose flow
+    differs by more than 1e-3 lies within 40 pixels (L1) of a hole pixel the two orders fill
+    differently (measured: 17-25)
   * against the faithful oracle with the device's hole-fill order (parallel rounds), which leaves
     the arithmetic alone:                                 mean <= 2e-5, max <= 1e-3
   * against the oracle on inputs whose holes are isolated (where the parallel hole fill is exact):
@@ -56,20 +58,22 @@ def test_two_frames_matches_oracle(ctx, name, fixed):
         rnd, _ = ob.two_frames(cam, p["bgr1"], p["depth1"], p["bgr2"], p["depth2"], prm)
     mean, mx = epe(gpu, ref, p)
     m2, x2 = epe(gpu, rnd, p)
-    # where the result departs from the reference-order oracle: near holes, where the fill order
-    # gives a hole pixel another median
+    # where the result departs from the reference-order oracle: near the hole pixels that the two
+    # fill orders give different medians
     from scipy.ndimage import distance_transform_cdt
-    hole = (p["depth1"] <= 0) | (p["depth2"] <= 0)
-    dist = distance_transform_cdt(~hole, metric="taxicab")
+    differs = np.zeros(p["depth1"].shape, bool)
+    for k in ("depth1", "depth2"):
+        differs |= ob.median_fill(p[k]) != ob.median_fill_rounds(p[k])[0]
+    dist = distance_transform_cdt(~differs, metric="taxicab")
     err = np.linalg.norm(gpu.astype(np.float64) - ref.astype(np.float64), axis=-1)
-    big = (err > 1e-4) & (p["depth1"] > 0)
+    big = (err > 1e-3) & (p["depth1"] > 0)
     far = int(dist[big].max()) if big.any() else 0
-    print("%s fixed=%d: EPE vs oracle mean %.3g mm max %.3g mm (pixels off by > 0.1 mm: %d, farthest %d px from a "
-          "hole); vs the oracle with the device's fill order mean %.3g mm max %.3g mm"
-          % (name, fixed, mean * 1e3, mx * 1e3, big.sum(), far, m2 * 1e3, x2 * 1e3))
+    print("%s fixed=%d: EPE vs oracle mean %.3g mm max %.3g mm (%d hole pixels filled differently; flow off by > 1e-3 "
+          "at %d pixels, at most %d px from one); vs the oracle with the device's fill order mean %.3g mm max %.3g mm"
+          % (name, fixed, mean * 1e3, mx * 1e3, differs.sum(), big.sum(), far, m2 * 1e3, x2 * 1e3))
     assert np.isfinite(gpu).all()
-    assert mean <= 5e-5 and mx <= 1e-2
-    assert far <= 12
+    assert mean <= 5e-5 and mx <= 5e-2
+    assert far <= 40
     assert m2 <= 2e-5 and x2 <= 1e-3
     assert st.summary() == rst.summary()
 

@@ -74,7 +74,8 @@ def test_hpb_weights_match_oracle(ctx, solved):
                   % (k, "right" if c == 0 else "down", close, diff.mean(), diff.max(), d.min(), d.max()))
             assert close >= 0.995
             assert diff.mean() <= 1e-3
-            assert d.min() >= 0.0099 - 1e-6 and d.max() <= 1.0
+            inner = d[:, :W - 1] if c == 0 else d[:H - 1, :]  # the last column / row has no such neighbour (0)
+            assert inner.min() >= 0.0099 and d.max() <= 1.0
 
 
 @pytest.mark.parametrize("name", ["320x240", "640x480"])

@@ -12,8 +12,11 @@ Tolerances ("rel" = largest |device - oracle| over a plane, divided by the plane
   * hole fill: the device's filled depths equal the oracle's restatement of the device's fill
     order (parallel rounds) bit for bit
   * depth sigma (through the level-0 depth-data weight): within one float rounding
-  * one linearisation (the compact 12-coefficient system against the reference's 8 planes):
-                                                rel <= 1e-5 per coefficient plane
+  * one linearisation (the compact 12-coefficient system against the reference's 8 planes): per
+    coefficient plane, rel <= 10 x (the oracle's own change when its inputs are rounded to FP32,
+    as the device stores them) + 1e-5.  The robust depth weight pi = 1 / (2 sqrt(e^2 + 1e-10))
+    makes the data-term coefficients sensitive to the last bit of the inputs (the FP32 rounding
+    alone moves them by up to ~1e-3), while the regularisation coefficients stay within ~3e-7.
 """
 import numpy as np
 import pytest
@@ -185,8 +188,17 @@ def test_linearisation_matches_oracle(ctx):
     sysd = [ctx.debug_plane(0, 0, rf.PLANE_SYSTEM, z) for z in range(12)]
     u3 = np.stack([u0, v0, w0], -1)
     A = ob.linearize(f1, d1, f2, d2, wi, wd, u3, np.zeros_like(u3), 1.0, ddw, 0.02, dsw, 1e-5, mag, regw)
+    # the same linearisation from inputs rounded to FP32: how far the rounding alone moves each plane
+    r = lambda x: np.asarray(x).astype(np.float32).astype(np.float64)
+    wir, wdr = ob.warp(r(f1), r(d1), r(f2), r(d2), r(u0), r(v0), r(w0))
+    Ar = ob.linearize(r(f1), r(d1), r(f2), r(d2), r(wir), r(wdr), r(u3), np.zeros_like(u3), 1.0, r(ddw), 0.02,
+                      r(dsw), 1e-5, r(mag), r(regw))
     # the compact form's 12 planes as the reference's coefficients
     s = sysd[11]
+    planes = {"diag u": (4, 0), "diag v": (5, 1), "diag w": (6, 2), "uv": (5, 0), "vu": (4, 1), "uw": (6, 0),
+              "wu": (4, 2), "vw": (6, 1), "wv": (5, 2), "rhs u": (7, 0), "rhs v": (7, 1), "rhs w": (7, 2),
+              "right u": (2, 0), "right w": (2, 2), "down v": (3, 1), "down w": (3, 2), "left u": (0, 0),
+              "left w": (0, 2), "up v": (1, 1), "up w": (1, 2)}
     pairs = {
         "diag u": (1 / sysd[0], A[4, ..., 0]), "diag v": (1 / sysd[1], A[5, ..., 1]), "diag w": (1 / sysd[2], A[6, ..., 2]),
         "uv": (sysd[3], A[5, ..., 0]), "vu": (sysd[3], A[4, ..., 1]),
@@ -204,9 +216,11 @@ def test_linearisation_matches_oracle(ctx):
     pairs["left w"] = (left * sl, A[0, ..., 2])
     pairs["up v"] = (up, A[1, ..., 1])
     pairs["up w"] = (up * su, A[1, ..., 2])
-    worst = {}
+    worst, bound = {}, {}
     for name, (d, o) in pairs.items():
-        r = rel(d, o)
-        worst[name] = r
-        assert r <= 1e-5, "%s: rel %.3g" % (name, r)
-    print("linearisation: " + ", ".join("%s %.2g" % kv for kv in worst.items()))
+        pl, var = planes[name]
+        worst[name] = rel(d, o)
+        bound[name] = 10 * rel(Ar[pl, ..., var], o) + 1e-5
+    print("linearisation (rel, bound): " + ", ".join("%s %.2g / %.2g" % (k, worst[k], bound[k]) for k in worst))
+    for name in pairs:
+        assert worst[name] <= bound[name], "%s: rel %.3g > %.3g" % (name, worst[name], bound[name])
