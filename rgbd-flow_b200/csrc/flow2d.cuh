@@ -385,9 +385,9 @@ __global__ void __launch_bounds__(kSorThreads) k_sor_wavefront(LevelBufs b, doub
 // same sweep schedule (start steps, completed sweeps, the stop), decided by each CTA's thread 0
 // from the same inputs; the pixels of each step's diagonals are spread over all the cluster's
 // threads; a sweep's maximum change is the largest of the CTAs' partial maxima, read through
-// distributed shared memory.  Two cluster barriers a step: after the updates (the ring's new values
-// are visible to the next step) and after the completion check (every CTA has read the partial
-// maxima before a slot is reused).  The order of the updates is the single-CTA kernel's, so the
+// distributed shared memory.  One cluster barrier a step, after the updates (the ring's new values
+// are visible to the next step); a ring slot, with its partial-maximum slot, is reused only a step
+// after its sweep completed, so no CTA resets a partial maximum another CTA may still be reading.  The order of the updates is the single-CTA kernel's, so the
 // flow is the same bit for bit; with more sweeps in flight (D up to kMaxRingC) a step carries more
 // independent work.
 constexpr int kMaxRingC = 64;
@@ -403,8 +403,10 @@ __global__ void __launch_bounds__(kSorThreads) k_sor_wavefront_cluster(LevelBufs
     const size_t N = (size_t)W * H;
     const int G = C * blockDim.x, g = rank * blockDim.x + threadIdx.x;
     __shared__ long long start[kMaxRingC];
+    __shared__ long long fin[kMaxRingC];  // the step at which the sweep in each slot completed
     __shared__ unsigned long long maxd[kMaxRingC];
     __shared__ int s_done, s_stop, s_next;
+    if (threadIdx.x < kMaxRingC) fin[threadIdx.x] = -1;
     for (size_t p = g; p < N; p += G) {
         ring_u[(size_t)(D - 1) * N + p] = 0;
         ring_v[(size_t)(D - 1) * N + p] = 0;
@@ -416,8 +418,11 @@ __global__ void __launch_bounds__(kSorThreads) k_sor_wavefront_cluster(LevelBufs
     long long t = 0;
     for (; t < t_max; t++) {
         if (threadIdx.x == 0) {
+            // a slot is reused one step after its sweep completed: other CTAs may read its partial
+            // maximum during the completion step, up to their next cluster barrier
             const int nx = s_next;
-            if (nx < nSOR && (nx == 0 || t >= start[(nx - 1) % D] + lag) && (nx < D || s_done >= nx - D)) {
+            if (nx < nSOR && (nx == 0 || t >= start[(nx - 1) % D] + lag) &&
+                (nx < D || (s_done >= nx - D && fin[nx % D] < t - 1))) {
                 start[nx % D] = t;
                 maxd[nx % D] = 0ull;
                 s_next = nx + 1;
@@ -432,6 +437,7 @@ __global__ void __launch_bounds__(kSorThreads) k_sor_wavefront_cluster(LevelBufs
         if (threadIdx.x == 0) {
             while (s_done + 1 < s_next && t - start[(s_done + 1) % D] == ndiag - 1) {
                 s_done++;
+                fin[s_done % D] = t;
                 double mx = 0;
                 for (int r = 0; r < C; r++)
                     mx = cmax(mx, __longlong_as_double((long long)*cl.map_shared_rank(&maxd[s_done % D], r)));
@@ -441,8 +447,8 @@ __global__ void __launch_bounds__(kSorThreads) k_sor_wavefront_cluster(LevelBufs
                 }
             }
         }
-        cl.sync();  // every CTA has read the partial maxima and advanced its schedule alike
     }
+    cl.sync();  // no CTA leaves while another may still read its partial maxima
     if (rank == 0 && threadIdx.x == 0) {
         *sweeps = s_done + 1;
         if (t >= t_max) *status = 1;

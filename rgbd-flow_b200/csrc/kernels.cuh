@@ -1328,15 +1328,6 @@ k_sor_strip(const LevelItem<T, S>* items, const StripUnit* units, int n_units, i
         const T fl = it.f_level;
         const int sx = (W + kSorTW - 1) / kSorTW;
         T md = 0, tot0 = 0, tot1 = 0;
-        // Carried from this thread's previous step (row r - 1 of its stage): the other colour's values
-        // of rows r - 1 and r that the next row reads again (its upper neighbour and one of its left /
-        // right neighbours; neither row changes between the two steps: stage s - 1 finished them and
-        // stage s + 1 reaches them later), and the depth-smoothness weight of that upper neighbour
-        // where it was loaded.  dlt: whether the thread's pixel sits one half-row position further
-        // in rows of parity 0 than in rows of parity 1 (the window's first column is odd).
-        T cu[3], cs[3], csU = 0;
-        bool have = false;
-        const int dlt = cl & 1;
 
         if (lkind) {
             load_next();  // rows t0 - 1, t0, t0 + 1: the first group
@@ -1367,40 +1358,21 @@ k_sor_strip(const LevelItem<T, S>* items, const StripUnit* units, int n_units, i
                     const int own = rs + colour * HRW + p, oth = rs + oc;
                     const int ol = oth - 1 + b, orr = oth + b;
                     const int ou = ((r - 1) & NRM) * RW + oc, od = ((r + 1) & NRM) * RW + oc;
-                    // sel: the carried upper neighbour was the previous row's left one (else its right
-                    // one), and this row's right neighbour is the previous row's lower one (else the left)
-                    const bool sel = ((b ^ 1) ^ dlt) != 0;
                     T c[9], xl[3], xu[3], xr[3], xd[3], xp[3], nv[3];
 #pragma unroll
                     for (int z = 0; z < 9; z++) c[z] = ring[z * PL + own];
 #pragma unroll
                     for (int v = 0; v < 3; v++) {
                         const T* xv = ring + (12 + v) * PL;
-                        if (have) {
-                            xu[v] = cu[v];
-                            if (sel) { xr[v] = cs[v]; xl[v] = xv[ol]; }
-                            else { xl[v] = cs[v]; xr[v] = xv[orr]; }
-                        } else {
-                            xl[v] = xv[ol]; xr[v] = xv[orr]; xu[v] = xv[ou];
-                        }
-                        xd[v] = xv[od]; xp[v] = xv[own];
+                        xl[v] = xv[ol]; xr[v] = xv[orr]; xu[v] = xv[ou]; xd[v] = xv[od]; xp[v] = xv[own];
                     }
-                    const T sL = ring[11 * PL + ol];
-                    const T sUv = (have && sel) ? csU : ring[11 * PL + ou];
                     sor_point<T>(c, ring[9 * PL + ol], ring[10 * PL + ou], ring[9 * PL + own], ring[10 * PL + own],
-                                 sL, sUv, ring[11 * PL + own], xl, xu, xr, xd, xp, k.omega, k.step, nv);
+                                 ring[11 * PL + ol], ring[11 * PL + ou], ring[11 * PL + own], xl, xu, xr, xd, xp,
+                                 k.omega, k.step, nv);
 #pragma unroll
                     for (int v = 0; v < 3; v++) ring[(12 + v) * PL + own] = nv[v];
                     if (chk && r >= ya && r < yb && (b ? in1 : in0))
                         for (int v = 0; v < 3; v++) md = maxT(md, absT(nv[v] - xp[v]));
-                    // for the next row (parity b ^ 1): its selector is b ^ dlt
-                    const bool nsel = (b ^ dlt) != 0;
-#pragma unroll
-                    for (int v = 0; v < 3; v++) { cu[v] = nsel ? xl[v] : xr[v]; cs[v] = xd[v]; }
-                    csU = sL;
-                    have = true;
-                } else {
-                    have = false;
                 }
             } else if (outw) {
                 const int ro = t - 4 * nit + 1;  // the row the last stage finished in the previous step
@@ -1753,6 +1725,9 @@ k_sor_level_cluster(const LevelItem<T, S>* items, const int* which, SolveConst<T
             if (s_stop) break;
         }
     }
+    // no CTA may leave while a neighbour still copies from its shared memory (the last half-sweep's
+    // halo rows)
+    cl.sync();
     // x of the own rows to global: the next inner iteration's buffer, or (fold) scratch that the CTA
     // folding each tile reads (the fold's next use of x starts from zero)
     T* const* xo = it.x[L.final_fold ? 0 : L.xout];

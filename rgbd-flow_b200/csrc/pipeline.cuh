@@ -139,6 +139,7 @@ struct HostParams {
     int strip_min_w, strip_min_h, strip_seg;  // strip eligibility and band height (0: automatic)
     long strip_min_px;                        // strips only for steps with this many eligible pixels
     int sor_level;                            // whole-level SOR for levels that fit one CTA (0: off)
+    int level_cluster;                        // > 1: such levels run on a cluster of this many CTAs instead
 };
 
 // Row pitch of the u planes, and the checkerboard half-row length of the x / sys planes (16-byte
@@ -210,7 +211,7 @@ static std::string sor_step_key(const std::vector<X>& items)
 static inline bool sor_tunable(const HostParams& hp)
 {
     return hp.K == 0 && hp.sor_ilp == 0 && hp.sor_nbuf == 0 && hp.sor_strip == 1 && hp.strip_min_w == 0 &&
-           hp.strip_min_h == 0 && hp.strip_seg == 0 && hp.strip_min_px == 0;
+           hp.strip_min_h == 0 && hp.strip_seg == 0 && hp.strip_min_px == 0 && hp.level_cluster == 0;
 }
 
 // Items the autotuner may put on the strip kernel (FP32, at least two strips wide and two bands high).
@@ -283,7 +284,7 @@ template <class T>
 static inline int level_cluster_size(const HostParams& hp, int H, int hwp)
 {
     if (!hp.sor_level) return 0;
-    for (int C = 2; C <= 8; C++)
+    for (int C = std::max(2, std::min(hp.level_cluster, 8)); C <= 8; C++)
         if (level_cluster_smem_bytes<T>((H + C - 1) / C, hwp) <= kLevelSmemMax && (H + C - 1) / C * (C - 1) < H) return C;
     return 0;
 }
@@ -746,7 +747,7 @@ static Plan<T, S> make_plan(const std::vector<PairSpec>& pairs, const HostParams
         for (auto& x : items) {
             const int sx = (x.W + kSorTW - 1) / kSorTW, sy = (x.H + kSorTH - 1) / kSorTH;
             x.n_sor_tiles = sx * sy;
-            if (use_level<T>(hp, x.W, x.H, x.hwp)) {
+            if (use_level<T>(hp, x.W, x.H, x.hwp) && !(hp.level_cluster > 1 && x.H >= 2 * hp.level_cluster)) {
                 level_items.push_back((int)(&x - items.data()));
                 level_smem = std::max(level_smem, level_smem_bytes<T>(x.H, x.hwp));
                 level_thr = std::max(level_thr, level_threads(x.H, x.hwp));

@@ -169,6 +169,8 @@ HostParams host_params(const rgbdflow_params& p)
     h.strip_min_px = e ? std::atol(e) : 0;
     e = std::getenv("RGBDFLOW_SOR_LEVEL");
     h.sor_level = e ? std::atoi(e) : 1;
+    e = std::getenv("RGBDFLOW_LEVEL_CLUSTER");
+    h.level_cluster = e ? std::atoi(e) : 0;
     h.fill_rounds = 253;  // round stamps are bytes: 0 valid, 1..253 rounds, 254 outside, 255 unfilled
     return h;
 }
@@ -212,8 +214,8 @@ std::string plan_key(const std::vector<PairSpec>& ps, const HostParams& hp, int 
                   hp.n_sor, hp.max_dist, hp.fill_holes, hp.fixed, hp.omega, hp.step, hp.eps_d, hp.eps_z, hp.eps_s,
                   hp.sor_tol, hp.outer_tol, hp.occ_margin, hp.occ_penalty, hp.max_grad, hp.period, hp.K * 100 + hp.sor_ilp * 10 + hp.sor_nbuf, hp.fill_rounds);
     k += buf;
-    std::snprintf(buf, sizeof buf, " strip %d %d %d %d %ld level %d", hp.sor_strip, hp.strip_min_w, hp.strip_min_h,
-                  hp.strip_seg, hp.strip_min_px, hp.sor_level);
+    std::snprintf(buf, sizeof buf, " strip %d %d %d %d %ld level %d %d", hp.sor_strip, hp.strip_min_w, hp.strip_min_h,
+                  hp.strip_seg, hp.strip_min_px, hp.sor_level, hp.level_cluster);
     return k + buf;
 }
 
@@ -373,7 +375,7 @@ GraphEntry& graph_for(rgbdflow_ctx* c, const Plan<T, S>& P, const std::vector<Pa
 // ------------------------------------------------------------------------------------------
 // SOR autotuner.  The first time a level step with given item sizes is planned, every candidate
 // SOR configuration of that step (tile kernel with K = 2..6 sweeps per launch and either lane
-// mapping; strip kernel with K = 5 and band heights 64..256 where the items allow strips) runs a
+// mapping; strip kernel with K = 5 and band heights 96 and 128 where the items allow strips) runs a
 // few launches on the context's stream over the step's real descriptors, timed with CUDA events,
 // and the fastest per SOR iteration is kept.  Every configuration computes the same flow bit for
 // bit, so the choice changes speed only.  Convergence checks are off during timing and every pair
@@ -418,7 +420,10 @@ std::vector<SorChoice> sor_candidates(const Plan<T, S>& P, int sidx)
     const LevelItem<T, S>* it = (const LevelItem<T, S>*)(P.desc.data() + P.steps[sidx].items_off);
     for (int i = 0; i < P.steps[sidx].n_items; i++) any_strip = any_strip || strip_ok<T>(P.hp, it[i].W, it[i].H);
     if (any_strip && sizeof(T) == 4)
-        for (int seg : {64, 128, 192, 256}) {
+        // bands of 96 and 128 rows: larger bands time faster with every pair active but balance the
+        // SMs worse once pairs stop early (measured on 16 x 640x480: 128 rows 14.8 ms of level-0 SOR
+        // a solve, 192 rows 15.2, 64 rows 15.7)
+        for (int seg : {96, 128}) {
             SorChoice ch;
             ch.strip = 1; ch.K = kStripMaxNit; ch.ilp = 2; ch.seg = seg;
             v.push_back(ch);
@@ -780,7 +785,7 @@ static void run_flow2d(rgbdflow_ctx* c, const uint8_t* bgr1, const uint8_t* bgr2
     // levels of at least this many pixels run their SOR over a cluster of CTAs with more sweeps in
     // flight (the flow does not depend on it)
     const char* ce = std::getenv("RGBDFLOW_FLOW2D_CLUSTER_MIN_PX");
-    const long clus_min_px = ce ? std::atol(ce) : 30000L;
+    const long clus_min_px = ce ? std::atol(ce) : 4096L;
     constexpr int kClusterCtas = 8, kClusterRing = 32;
     const int ring_slots = std::max(prm.sor_ring, (long)N0 >= clus_min_px ? kClusterRing : 0);
     const size_t o_ring_u = reserve((size_t)ring_slots * N0 * sizeof(double));

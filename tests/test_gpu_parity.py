@@ -291,6 +291,11 @@ def test_whole_level_sor_agrees_bitwise(ctx, monkeypatch, name, n_inner):
     whole, st_whole = ctx.scene_flow_two_frames(*args)
     assert st_tile.summary() == st_whole.summary()
     np.testing.assert_array_equal(tile, whole)
+    # every whole-level item on a cluster of at least 4 CTAs (the coarsest levels too)
+    monkeypatch.setenv("RGBDFLOW_LEVEL_CLUSTER", "4")
+    clus, st_clus = ctx.scene_flow_two_frames(*args)
+    assert st_tile.summary() == st_clus.summary()
+    np.testing.assert_array_equal(tile, clus)
 
 
 def test_single_scale_seam_matches_oracle(ctx):
