@@ -39,7 +39,8 @@ extern "C" {
 #define RGBDFLOW_ERR_UNSUPPORTED  (-2)
 #define RGBDFLOW_ERR_CUDA         (-3)
 #define RGBDFLOW_ERR_BUDGET       (-4) /* request does not fit the context's HBM budget */
-#define RGBDFLOW_ERR_TIMEOUT      (-5) /* a bounded device or host wait expired */
+#define RGBDFLOW_ERR_TIMEOUT      (-5) /* a bounded device or host wait expired: the solve's results are
+                                         not valid; the context stays usable */
 #define RGBDFLOW_ERR_NO_DEVICE    (-6)
 #define RGBDFLOW_ERR_BUSY         (-7) /* no free slot; retry later */
 #define RGBDFLOW_ERR_INTERNAL     (-8)
@@ -247,7 +248,10 @@ int rgbdflow_scene_flow_batch_async(rgbdflow_ctx* ctx, const rgbdflow_pair* pair
 int rgbdflow_scene_flow_batch_submit(rgbdflow_ctx* ctx, const rgbdflow_pair* pairs, int n,
                                      const rgbdflow_params* params);
 
-/* Wait for every solve this context enqueued (on any stream). */
+/* Wait for every solve this context enqueued (on any stream).  The device's bounded waits (the
+ * grid barriers of the cooperative hole-fill kernels) record a wait that gave up in a status word
+ * of the context: synchronous calls return RGBDFLOW_ERR_TIMEOUT for it, and for submitted or
+ * device-pointer solves this call does (once; the word is then cleared). */
 int rgbdflow_ctx_synchronize(rgbdflow_ctx* ctx);
 
 /* Kernel launches of the last solve enqueued on this context. */
@@ -309,6 +313,12 @@ int rgbdflow_profile_read(rgbdflow_ctx* ctx, rgbdflow_kernel_stat* out, int max)
  * be NULL) receive the level's size.  Waits for the solve to finish. */
 int rgbdflow_debug_read_plane(rgbdflow_ctx* ctx, int pair, int level, int kind, int index, double* dst, size_t n,
                               int* W, int* H);
+
+/* Self-test of the bounded device waits: runs one grid barrier that no other block reaches, which
+ * gives up after its spin limit and records it in the context's status word.  Returns
+ * RGBDFLOW_ERR_TIMEOUT (the expected outcome) and the wait's duration in *seconds (may be NULL);
+ * the context stays usable. */
+int rgbdflow_debug_wait_timeout(rgbdflow_ctx* ctx, double* seconds);
 
 /* ---------------------------------------------------------------------------------------------
  * Served form (no reference counterpart): continuous batching over camera streams.  A frame

@@ -36,140 +36,222 @@ __device__ __forceinline__ double stereo_err_ratio(double z) { return ddv(stereo
 
 // ------------------------------------------------------------------------------------------
 // Colour-guided fill of small invalid regions of frame 1's raw depth (level 0).
+//
+// One cooperative launch does it all: the invalid pixels' 4-connected regions by union-find
+// (parents always point to a smaller raster index, so a region's root is its first pixel), their
+// sizes and pixel lists, then the fill in passes, one warp per region.
 
-// One pair's fill.  label: per pixel -1 valid, -2 in a region of more than 60 pixels, else the
-// raster index of its region's first pixel.  reps: the regions' first pixels (n_reps of them);
-// done: per pixel, set at a region's first pixel once the region is filled.
+// One pair's fill.
 template <class T>
 struct HpbFill {
     int W, H;
     const PrepItem<T>* src;   // the pair's inputs: colour 1 and raw depth 1 (BGR8 + float, or FP64)
     int fill;                 // 0: no colour-guided fill (the warm start reads the raw depth)
     T* out;                   // level 0 of the raw-depth pyramid (the filled raw depth)
-    int* label;
-    uint8_t* done;
-    int* reps;
-    int* n_reps;
+    int* label;               // per pixel: -1 valid, -2 in a region of more than 60 pixels, else the
+                              // raster index of its region's first pixel
+    int* par;                 // union-find parent of an invalid pixel; at a region's first pixel, then
+                              // the cursor of its pixel list
+    int* csz;                 // region size, at its first pixel
+    uint8_t* done;            // set at a region's first pixel once the region is filled
+    int2* regions;            // per region of at most 60 pixels: {first pixel, list start << 6 | size}
+    int* px;                  // the regions' pixels, region by region
+    int* counts;              // [0] regions listed, [1] pixels listed
 };
 
 constexpr int kHpbMaxRegion = 60;  // largest invalid region the fill takes (sceneFlowMultiscale.cpp:81)
 
+// The pair's colour, read as the reference's fill reads it: BGR8 scaled to [0,1], or FP64.
+struct HpbColour {
+    int kind;
+    const uint8_t* bgr;
+    const double* im;
+    __device__ __forceinline__ double operator()(size_t l, int c) const
+    {
+        return kind == 0 ? (double)__ldg(bgr + l * 3 + c) / 255.0 : __ldg(im + l * 3 + c);
+    }
+};
+
 template <class T>
-__device__ __forceinline__ double hpb_col(const HpbFill<T>& f, size_t l, int c)
+__device__ __forceinline__ double hpb_raw(const PrepItem<T>& s, size_t l)
 {
-    const PrepItem<T>& s = *f.src;
-    return s.kind == 0 ? (double)s.bgr[0][l * 3 + c] / 255.0 : s.im_d[0][l * 3 + c];
-}
-template <class T>
-__device__ __forceinline__ double hpb_raw(const HpbFill<T>& f, size_t l)
-{
-    const PrepItem<T>& s = *f.src;
     return s.kind == 0 ? (double)s.depth[0][l] : s.dep_d[0][l];
 }
 
-// The 4-connected invalid region of pixel l, breadth first, at most kHpbMaxRegion + 1 pixels.
-// Returns its size (kHpbMaxRegion + 1: larger) and its smallest raster index.
-template <class T>
-__device__ int hpb_region(const HpbFill<T>& f, int l, int* q, int* first)
+// Root of x: parents strictly decrease, so the walk ends.
+__device__ __forceinline__ int uf_find(const int* par, int x)
 {
-    const int W = f.W, H = f.H;
-    int n = 1, head = 0;
-    q[0] = l;
-    int mn = l;
-    auto invalid = [&](int o) { return !(hpb_raw(f, o) > 0); };
-    while (head < n) {
-        const int p = q[head++];
-        const int pi = p / W, pj = p % W;
-        const int nb[4] = {pi > 0 ? p - W : -1, pi < H - 1 ? p + W : -1, pj > 0 ? p - 1 : -1, pj < W - 1 ? p + 1 : -1};
-        for (int t = 0; t < 4; t++) {
-            const int o = nb[t];
-            if (o < 0 || !invalid(o)) continue;
-            bool seen = false;
-            for (int k = 0; k < n && !seen; k++) seen = q[k] == o;
-            if (seen) continue;
-            if (n > kHpbMaxRegion) { *first = mn; return kHpbMaxRegion + 1; }
-            q[n++] = o;
-            mn = min(mn, o);
-        }
+    int p = __ldcg(par + x);
+    while (p != x) {
+        x = p;
+        p = __ldcg(par + x);
     }
-    *first = mn;
-    return n;
+    return x;
 }
 
-// Per pixel: the raw depth copied to level 0, the pixel's region label, the regions' first pixels.
-template <class T>
-__global__ void k_hpb_label(const HpbFill<T>* items, const Tile* tiles)
+// Joins the regions of a and b: the larger root is hooked under the smaller one.  When another
+// thread moved the root first, the join is retried from the root's new parent (which keeps every
+// earlier link's region connected).  Bounded: gives up, flagging err, after 2^20 retries.
+__device__ __forceinline__ void uf_union(int* par, int a, int b, int* err)
 {
-    const Tile t = tiles[blockIdx.x];
-    const HpbFill<T>& f = items[t.item];
-    const int j = t.tx * LTW + (threadIdx.x % LTW), i = t.ty * LTH + (threadIdx.x / LTW);
-    if (i >= f.H || j >= f.W) return;
-    const int l = i * f.W + j;
-    const double z = hpb_raw(f, l);
-    f.out[l] = (T)z;
-    f.done[l] = 0;
-    if (z > 0 || !f.fill) { f.label[l] = -1; return; }
-    int q[kHpbMaxRegion + 1];
-    int first;
-    const int n = hpb_region(f, l, q, &first);
-    f.label[l] = n > kHpbMaxRegion ? -2 : first;
-    if (n <= kHpbMaxRegion && first == l) f.reps[atomicAdd(f.n_reps, 1)] = l;
+    for (int k = 0; k < (1 << 20); k++) {
+        a = uf_find(par, a);
+        b = uf_find(par, b);
+        if (a == b) return;
+        if (a < b) { const int t = a; a = b; b = t; }
+        const int old = atomicMin(par + a, b);
+        if (old == a) return;
+        a = old;
+    }
+    atomicExch(err, 1);
 }
 
 // Fills one region (recursiveMedianFilterSmallInvalidRegionsUsingColor's loop over its points):
 // repeatedly the pixel with the most valid 3x3 neighbours (ties: smallest raster index) takes the
 // average of its valid neighbours weighted by exp(-|colour difference|^2 / .6), in float sums.
+// One warp: lane k holds the region's pixels k and k + 32 (q0, q1; -1 past the end) with their
+// valid-neighbour counts; lane k < 9 reads the k-th 3x3 neighbour of the pixel being filled, and
+// the sums run over them in the reference's row-major order.
 template <class T>
-__device__ void hpb_fill_region(const HpbFill<T>& f, const int* q, int n)
+__device__ void hpb_fill_region_warp(const HpbFill<T>& f, const HpbColour& col, int q0, int q1, int n)
 {
-    const int W = f.W, H = f.H;
-    int cnt[kHpbMaxRegion + 1];
+    const int W = f.W, H = f.H, lane = threadIdx.x & 31;
     // depths are read past L1: regions filled by other blocks before this one became ready
     auto dz = [&](int o) { return (double)__ldcg(f.out + o); };
-    for (int a = 0; a < n; a++) {
-        const int i = q[a] / W, j = q[a] % W;
+    auto valid_count = [&](int p) {
+        const int i = p / W, j = p % W;
         int c = 0;
         for (int ii = max(0, i - 1); ii <= min(H - 1, i + 1); ii++)
             for (int jj = max(0, j - 1); jj <= min(W - 1, j + 1); jj++)
                 if (dz(ii * W + jj) > 0) c++;
-        cnt[a] = c;
-    }
-    for (int left = n; left > 0; left--) {
-        int best = -1;
-        for (int a = 0; a < n; a++)
-            if (cnt[a] >= 0 && (best < 0 || cnt[a] > cnt[best] || (cnt[a] == cnt[best] && q[a] < q[best]))) best = a;
-        const int p = q[best];
-        cnt[best] = -1;
+        return c;
+    };
+    int c0 = q0 >= 0 ? valid_count(q0) : -1, c1 = q1 >= 0 ? valid_count(q1) : -1;
+    for (int step = 0; step < n; step++) {
+        // the unfilled pixel with the most valid neighbours, ties to the smaller raster index
+        unsigned long long key = 0;
+        if (c0 >= 0) key = max(key, ((unsigned long long)(c0 + 1) << 32) | (unsigned)~q0);
+        if (c1 >= 0) key = max(key, ((unsigned long long)(c1 + 1) << 32) | (unsigned)~q1);
+        for (int o = 16; o; o >>= 1) key = max(key, __shfl_xor_sync(~0u, key, o));
+        const int p = (int)~(unsigned)key;
+        if (q0 == p) c0 = -1;
+        if (q1 == p) c1 = -1;
         const int i = p / W, j = p % W;
-        float zSum = 0, weightSum = 0;
-        for (int ii = max(0, i - 1); ii <= min(H - 1, i + 1); ii++)
-            for (int jj = max(0, j - 1); jj <= min(W - 1, j + 1); jj++) {
-                const int o2 = ii * W + jj;
-                if (dz(o2) > 0) {
-                    double s = 0;
-                    for (int c = 0; c < 3; c++) {
-                        const double d = dsb(hpb_col(f, p, c), hpb_col(f, o2, c));
-                        s = dad(s, dmu(d, d));
-                    }
-                    const float w = (float)exp(ddv(-s, .6));
-                    zSum = (float)dad((double)zSum, dmu(dz(o2), (double)w));
-                    weightSum = fad(weightSum, w);
-                } else {
-                    for (int a = 0; a < n; a++)
-                        if (q[a] == o2 && cnt[a] >= 0) { cnt[a]++; break; }
+        const int i0 = max(0, i - 1), i1 = min(H - 1, i + 1), j0 = max(0, j - 1), j1 = min(W - 1, j + 1);
+        const int cols = j1 - j0 + 1, m = (i1 - i0 + 1) * cols;
+        int o2 = -1;
+        bool v = false;
+        float w = 0;
+        double term = 0;
+        if (lane < m) {
+            o2 = (i0 + lane / cols) * W + j0 + lane % cols;
+            const double z = dz(o2);
+            v = z > 0;
+            if (v) {
+                double s = 0;
+                for (int c = 0; c < 3; c++) {
+                    const double d = dsb(col(p, c), col(o2, c));
+                    s = dad(s, dmu(d, d));
                 }
+                w = (float)exp(ddv(-s, .6));
+                term = dmu(z, (double)w);
             }
-        f.out[p] = (T)fdv(zSum, weightSum);
+        }
+        const unsigned vm = __ballot_sync(~0u, v);
+        float zSum = 0, weightSum = 0;
+        for (int k = 0; k < m; k++) {
+            const double tk = __shfl_sync(~0u, term, k);
+            const float wk = __shfl_sync(~0u, w, k);
+            if (vm >> k & 1) {
+                zSum = (float)dad((double)zSum, tk);
+                weightSum = fad(weightSum, wk);
+            }
+        }
+        // each unfilled pixel of the region among the invalid neighbours gains a valid neighbour
+        unsigned im = __ballot_sync(~0u, lane < m && !v);
+        while (im) {
+            const int k = __ffs(im) - 1;
+            im &= im - 1;
+            const int ok = __shfl_sync(~0u, o2, k);
+            if (q0 == ok && c0 >= 0) c0++;
+            if (q1 == ok && c1 >= 0) c1++;
+        }
+        if (lane == 0) f.out[p] = (T)fdv(zSum, weightSum);
+        __syncwarp();
     }
 }
 
-// Every region in passes: a region is filled once every region with a smaller first pixel that
-// touches it (a pixel within one step, diagonals included) is filled, which is the raster order's
-// result.  One cooperative launch; a grid barrier between passes; bounded.
+// The whole fill in one cooperative launch, phases split by grid barriers:
+//   1. level 0 of the raw-depth pyramid is the raw depth; each invalid pixel its own region;
+//   2. joins with the left and upper invalid neighbours (4-connectivity);
+//   3. every invalid pixel's region (its first pixel) and the regions' sizes;
+//   4. regions of more than 60 pixels are marked and left unfilled; the others get a list slot;
+//   5. the regions' pixel lists;
+//   6. passes, one warp per region: a region is filled once every region with a smaller first
+//      pixel that touches it (a pixel within one step, diagonals included) is filled, which is
+//      the raster order's result.  Bounded by max_passes.
 template <class T>
 __global__ void __launch_bounds__(128)
-k_hpb_fill(const HpbFill<T>* items, int n_items, GridSync* gs, int max_passes)
+k_hpb_fill(const HpbFill<T>* items, int n_items, GridSync* gs, int max_passes, int* status)
 {
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x, gn = gridDim.x * blockDim.x;
+    for (int it = 0; it < n_items; it++) {
+        const HpbFill<T>& f = items[it];
+        const PrepItem<T>& s = *f.src;
+        for (int l = gt; l < f.W * f.H; l += gn) {
+            const double z = hpb_raw(s, l);
+            f.out[l] = (T)z;
+            f.done[l] = 0;
+            f.csz[l] = 0;
+            f.par[l] = (f.fill && !(z > 0)) ? l : -1;
+        }
+    }
+    if (!grid_barrier(gs, gridDim.x)) { report_wait_failure(status); return; }
+    for (int it = 0; it < n_items; it++) {
+        const HpbFill<T>& f = items[it];
+        for (int l = gt; l < f.W * f.H; l += gn) {
+            if (__ldcg(f.par + l) < 0) continue;
+            if (l % f.W > 0 && __ldcg(f.par + l - 1) >= 0) uf_union(f.par, l, l - 1, &gs->err);
+            if (l >= f.W && __ldcg(f.par + l - f.W) >= 0) uf_union(f.par, l, l - f.W, &gs->err);
+        }
+    }
+    if (!grid_barrier(gs, gridDim.x)) { report_wait_failure(status); return; }
+    for (int it = 0; it < n_items; it++) {
+        const HpbFill<T>& f = items[it];
+        for (int l = gt; l < f.W * f.H; l += gn) {
+            if (__ldcg(f.par + l) < 0) { f.label[l] = -1; continue; }
+            const int r = uf_find(f.par, l);
+            f.label[l] = r;
+            atomicAdd(f.csz + r, 1);
+        }
+    }
+    if (!grid_barrier(gs, gridDim.x)) { report_wait_failure(status); return; }
+    for (int it = 0; it < n_items; it++) {
+        const HpbFill<T>& f = items[it];
+        for (int l = gt; l < f.W * f.H; l += gn) {
+            const int r = __ldcg(f.label + l);
+            if (r < 0) continue;
+            const int sz = __ldcg(f.csz + r);
+            if (sz > kHpbMaxRegion) {
+                f.label[l] = -2;
+            } else if (r == l) {
+                const int slot = atomicAdd(f.counts, 1), start = atomicAdd(f.counts + 1, sz);
+                f.regions[slot] = make_int2(l, start << 6 | sz);
+                f.par[l] = start;  // the list cursor from here on
+            }
+        }
+    }
+    if (!grid_barrier(gs, gridDim.x)) { report_wait_failure(status); return; }
+    for (int it = 0; it < n_items; it++) {
+        const HpbFill<T>& f = items[it];
+        for (int l = gt; l < f.W * f.H; l += gn) {
+            const int r = __ldcg(f.label + l);
+            if (r >= 0) f.px[atomicAdd(f.par + r, 1)] = l;
+        }
+    }
+    if (!grid_barrier(gs, gridDim.x)) { report_wait_failure(status); return; }
+
+    const int lane = threadIdx.x & 31, gw = gt >> 5, nw = gn >> 5;
     __shared__ int s_left;
     for (int pass = 0; pass < max_passes; pass++) {
         if (threadIdx.x == 0) s_left = 0;
@@ -177,29 +259,37 @@ k_hpb_fill(const HpbFill<T>* items, int n_items, GridSync* gs, int max_passes)
         int pending = 0;
         for (int it = 0; it < n_items; it++) {
             const HpbFill<T>& f = items[it];
-            const int nr = *f.n_reps;
-            for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nr; r += gridDim.x * blockDim.x) {
-                const int rep = f.reps[r];
-                if (*(volatile uint8_t*)&f.done[rep]) continue;
-                int q[kHpbMaxRegion + 1];
-                int first;
-                const int n = hpb_region(f, rep, q, &first);
-                bool ready = true;
-                for (int a = 0; a < n && ready; a++) {
-                    const int i = q[a] / f.W, j = q[a] % f.W;
-                    for (int ii = max(0, i - 1); ii <= min(f.H - 1, i + 1) && ready; ii++)
+            const PrepItem<T>& s = *f.src;
+            const HpbColour col{s.kind, s.bgr[0], s.im_d[0]};
+            const int nr = __ldcg(f.counts);
+            for (int r = gw; r < nr; r += nw) {
+                const int2 g = __ldcg(f.regions + r);
+                const int rep = g.x, n = g.y & 63, start = g.y >> 6;
+                int dn = lane == 0 ? *(volatile uint8_t*)&f.done[rep] : 0;
+                if (__shfl_sync(~0u, dn, 0)) continue;
+                const int q0 = lane < n ? __ldcg(f.px + start + lane) : -1;
+                const int q1 = lane + 32 < n ? __ldcg(f.px + start + lane + 32) : -1;
+                bool blocked = false;
+                for (int h = 0; h < 2; h++) {
+                    const int q = h ? q1 : q0;
+                    if (q < 0) continue;
+                    const int i = q / f.W, j = q % f.W;
+                    for (int ii = max(0, i - 1); ii <= min(f.H - 1, i + 1); ii++)
                         for (int jj = max(0, j - 1); jj <= min(f.W - 1, j + 1); jj++) {
-                            const int lb = f.label[ii * f.W + jj];
-                            if (lb >= 0 && lb < rep && !*(volatile uint8_t*)&f.done[lb]) { ready = false; break; }
+                            const int lb = __ldcg(f.label + ii * f.W + jj);
+                            if (lb >= 0 && lb < rep && !*(volatile uint8_t*)&f.done[lb]) blocked = true;
                         }
                 }
-                if (!ready) { pending++; continue; }
-                hpb_fill_region(f, q, n);
-                __threadfence();
-                *(volatile uint8_t*)&f.done[rep] = 1;
+                if (__any_sync(~0u, blocked)) { pending++; continue; }
+                __threadfence();  // the touching regions' depths are read after their done flags
+                hpb_fill_region_warp(f, col, q0, q1, n);
+                if (lane == 0) {
+                    __threadfence();
+                    *(volatile uint8_t*)&f.done[rep] = 1;
+                }
             }
         }
-        if (pending) atomicAdd(&s_left, pending);
+        if (lane == 0 && pending) atomicAdd(&s_left, pending);
         __syncthreads();
         const int mine = s_left;
         // the number of pending regions over the grid: accumulated in the barrier's pad word
@@ -207,10 +297,11 @@ k_hpb_fill(const HpbFill<T>* items, int n_items, GridSync* gs, int max_passes)
         if (!grid_barrier(gs, gridDim.x)) break;
         const int total = *(volatile int*)&gs->pad;
         if (!grid_barrier(gs, gridDim.x)) break;  // every block has read the total
-        if (total == 0) break;
+        if (total == 0) return;
         if (blockIdx.x == 0 && threadIdx.x == 0) atomicExch(&gs->pad, 0);
         if (!grid_barrier(gs, gridDim.x)) break;
     }
+    report_wait_failure(status);  // a wait gave up, or regions were left after max_passes
 }
 
 // ------------------------------------------------------------------------------------------

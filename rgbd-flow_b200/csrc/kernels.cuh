@@ -337,6 +337,20 @@ __device__ __forceinline__ bool grid_barrier(GridSync* g, unsigned nblocks)
     return s_ok != 0;
 }
 
+// A bounded wait that gave up leaves the solve's results invalid: recorded in the context's status
+// word, which the host reads once the solve has finished (null: the caller has none).
+__device__ __forceinline__ void report_wait_failure(int* status)
+{
+    if (status && threadIdx.x == 0) atomicOr(status, 1);
+}
+
+// A grid barrier that no other block reaches: gives up after its bounded wait and reports it (the
+// device side of the wait-timeout self-test).
+__global__ void k_wait_probe(GridSync* gs, int* status)
+{
+    if (!grid_barrier(gs, gridDim.x + 1)) report_wait_failure(status);
+}
+
 // One round over the tiles of block `blk` of `nblk`.  left[r]: hole pixels (all pairs, both frames)
 // still unfilled after round r; tleft[ti]: nonzero while tile ti holds one.  A block takes the tiles
 // blk + k nblk; after round 1 it gathers, 32 at a time, only those that still hold holes.
@@ -427,12 +441,16 @@ __device__ __forceinline__ void fill_round(const PrepItem<T>* items, const Tile*
 // hole is left (or after max_rounds, or when a barrier wait gives up).
 template <class T>
 __global__ void __launch_bounds__(LTW * LTH)
-k_fill(const PrepItem<T>* items, const Tile* tiles, int n_tiles, int* left, int* tleft, GridSync* gs, int max_rounds)
+k_fill(const PrepItem<T>* items, const Tile* tiles, int n_tiles, int* left, int* tleft, GridSync* gs, int max_rounds,
+       int* status)
 {
     for (int round = 1; round <= max_rounds; round++) {
         if (round > 1 && *(volatile int*)&left[round - 1] == 0) break;  // the same value in every block
         fill_round<T>(items, tiles, n_tiles, left, tleft, round, blockIdx.x, gridDim.x);
-        if (!grid_barrier(gs, gridDim.x)) break;
+        if (!grid_barrier(gs, gridDim.x)) {
+            report_wait_failure(status);
+            break;
+        }
     }
 }
 

@@ -349,7 +349,8 @@ struct Plan {
     std::vector<int> est_flag;
     // HPB regularisation weights (regularization == HPB, kinds 0 and 1)
     bool hpb = false;
-    size_t hpb_ctr_off = 0;             // int[n] region counts, then the fill's GridSync (zeroed each solve)
+    int* status = nullptr;              // the context's device status word (bounded waits that gave up)
+    size_t hpb_ctr_off = 0;             // int[2n] region / pixel counts, then the fill's GridSync (zeroed each solve)
     size_t hpb_fill_off = 0;            // HpbFill[n] (descriptor offset)
     struct HpbDepthLevel { size_t jobs_off; int n_jobs; size_t tiles_off; int n_tiles; };
     std::vector<HpbDepthLevel> hpb_dpyr;  // raw-depth pyramid, level index 1..Lmax-1
@@ -481,10 +482,10 @@ static Plan<T, S> make_plan(const std::vector<PairSpec>& pairs, const HostParams
     }
     // HPB: the raw-depth pyramid per level and, per pair, scratch for one level at a time
     P.hpb = hp.regularization == 2 && P.kind != 2;
-    struct HpbMem { size_t label, done, reps, nrm[3], nval, rad, pre[6], pre_v, ii[6], ii_v, feat[4], bp[2]; };
+    struct HpbMem { size_t label, par, csz, done, regions, px, nrm[3], nval, rad, pre[6], pre_v, ii[6], ii_v, feat[4], bp[2]; };
     std::vector<HpbMem> hm(P.n);
     if (P.hpb) {
-        P.hpb_ctr_off = A.take(sizeof(int) * P.n + sizeof(GridSync));
+        P.hpb_ctr_off = A.take(sizeof(int) * 2 * P.n + sizeof(GridSync));
         for (int p = 0; p < P.n; p++) {
             const auto& s = P.shapes[p];
             // DepthMapPyramid's level sizes must be the colour pyramid's: the reference reads one
@@ -497,7 +498,10 @@ static Plan<T, S> make_plan(const std::vector<PairSpec>& pairs, const HostParams
             for (int k = 0; k < P.L[p]; k++) mem[p][k].hz = A.take(sizeof(T) * (size_t)s.w[k] * s.h[k]);
             const size_t N0 = (size_t)s.w[0] * s.h[0], NI = (size_t)(s.w[0] + 1) * (s.h[0] + 1);
             HpbMem& h = hm[p];
-            h.label = A.take(sizeof(int) * N0); h.done = A.take(N0); h.reps = A.take(sizeof(int) * (N0 / 2 + 2));
+            h.label = A.take(sizeof(int) * N0); h.par = A.take(sizeof(int) * N0); h.csz = A.take(sizeof(int) * N0);
+            h.done = A.take(N0);
+            // at most ceil(N0 / 2) 4-connected regions (a checkerboard)
+            h.regions = A.take(sizeof(int2) * (N0 / 2 + 2)); h.px = A.take(sizeof(int) * N0);
             for (int c = 0; c < 3; c++) h.nrm[c] = A.take(sizeof(float) * N0);
             h.nval = A.take(sizeof(unsigned) * N0); h.rad = A.take(sizeof(int) * N0);
             for (int c = 0; c < 6; c++) h.pre[c] = A.take(sizeof(float) * N0);
@@ -620,8 +624,9 @@ static Plan<T, S> make_plan(const std::vector<PairSpec>& pairs, const HostParams
             f.src = (const PrepItem<T>*)(P.prep_items_off + sizeof(PrepItem<T>) * p);  // descriptor-relative
             f.fill = P.est_flag[p] ? 0 : 1;  // the warm start reads the raw depth (sceneFlowWithInit.cpp:48)
             f.out = (T*)mem[p][0].hz;
-            f.label = (int*)hm[p].label; f.done = (uint8_t*)hm[p].done; f.reps = (int*)hm[p].reps;
-            f.n_reps = (int*)(P.hpb_ctr_off + sizeof(int) * p);
+            f.label = (int*)hm[p].label; f.par = (int*)hm[p].par; f.csz = (int*)hm[p].csz;
+            f.done = (uint8_t*)hm[p].done; f.regions = (int2*)hm[p].regions; f.px = (int*)hm[p].px;
+            f.counts = (int*)(P.hpb_ctr_off + sizeof(int) * 2 * p);
         }
         P.hpb_fill_off = P.put(fills);
         // DepthMapPyramid levels (depthMapPyramid.cpp:15-91)
@@ -889,7 +894,8 @@ static void bind_plan(Plan<T, S>& P, char* base)
         for (int p = 0; p < P.n; p++) {
             rebase(fl[p].src, base + P.desc_off);
             rebase(fl[p].out, base); rebase(fl[p].label, base); rebase(fl[p].done, base);
-            rebase(fl[p].reps, base); rebase(fl[p].n_reps, base);
+            rebase(fl[p].par, base); rebase(fl[p].csz, base); rebase(fl[p].regions, base);
+            rebase(fl[p].px, base); rebase(fl[p].counts, base);
         }
         for (auto& lv : P.hpb_dpyr) {
             DepthPyrJob<T>* jb = (DepthPyrJob<T>*)(d + lv.jobs_off);
@@ -1218,14 +1224,12 @@ static int enqueue_hpb(const Plan<T, S>& P, char* base, cudaStream_t st, Prof* p
     char* db = base + P.desc_off;
     const HpbFill<T>* fills = (const HpbFill<T>*)(db + P.hpb_fill_off);
     RF_PROF_B(pf, KC_HPB, st);
-    k_hpb_label<T><<<P.n_prep_tiles, LTW * LTH, 0, st>>>(fills, (const Tile*)(db + P.prep_tiles_off));
-    launches++;
     {
         static int per_sm = 0;
         if (!per_sm) RF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_hpb_fill<T>, 128, 0));
         const int grid = std::max(1, std::min(per_sm, 4) * P.sms);
-        GridSync* gs = (GridSync*)(base + P.hpb_ctr_off + sizeof(int) * P.n);
-        launch_cooperative(k_hpb_fill<T>, grid, 128, st, fills, P.n, gs, 4096);
+        GridSync* gs = (GridSync*)(base + P.hpb_ctr_off + sizeof(int) * 2 * P.n);
+        launch_cooperative(k_hpb_fill<T>, grid, 128, st, fills, P.n, gs, 4096, P.status);
         launches++;
     }
     for (const auto& lv : P.hpb_dpyr) {
@@ -1275,7 +1279,7 @@ static int enqueue_solve(const Plan<T, S>& P, char* base, cudaStream_t st, Prof*
         launches++;
     } else {
         RF_CUDA(cudaMemsetAsync(base + P.unfilled_off, 0, sizeof(int) * 256 + sizeof(GridSync), st));
-        if (P.hpb) RF_CUDA(cudaMemsetAsync(base + P.hpb_ctr_off, 0, sizeof(int) * P.n + sizeof(GridSync), st));
+        if (P.hpb) RF_CUDA(cudaMemsetAsync(base + P.hpb_ctr_off, 0, sizeof(int) * 2 * P.n + sizeof(GridSync), st));
         const PrepItem<T>* prep = (const PrepItem<T>*)(db + P.prep_items_off);
         const Tile* pt = (const Tile*)(db + P.prep_tiles_off);
         RF_PROF_B(pf, KC_PREP, st);
@@ -1295,7 +1299,8 @@ static int enqueue_solve(const Plan<T, S>& P, char* base, cudaStream_t st, Prof*
             GridSync* gs = (GridSync*)(left + 256);
             int* tleft = (int*)(base + P.tleft_off);
             RF_PROF_B(pf, KC_FILL, st);
-            launch_cooperative(k_fill<T>, grid, LTW * LTH, st, prep, pt, P.n_prep_tiles, left, tleft, gs, P.hp.fill_rounds);
+            launch_cooperative(k_fill<T>, grid, LTW * LTH, st, prep, pt, P.n_prep_tiles, left, tleft, gs, P.hp.fill_rounds,
+                               P.status);
             RF_PROF_E(pf, st);
             launches++;
         }

@@ -72,6 +72,10 @@ struct rgbdflow_ctx {
     cudaEvent_t done = nullptr;       // end of the last enqueued solve
     cudaEvent_t desc_up = nullptr;    // last upload out of the pinned staging
     bool pending = false;
+    // bounded device waits that gave up: a sticky device word (the kernels OR into it; [4..] is the
+    // wait self-test's barrier) and its page-locked copy, read once a solve has finished
+    int* dev_status = nullptr;
+    int* pin_status = nullptr;
     // kernel profiling
     std::unique_ptr<Prof> prof;
     double prof_ms[KC_TOTAL] = {0};
@@ -107,6 +111,17 @@ void wait_idle(rgbdflow_ctx* c)
     if (c->pending) RF_CUDA(cudaEventSynchronize(c->done));
     RF_CUDA(cudaStreamSynchronize(c->stream));
     c->pending = false;
+}
+
+// The status finished solves left in the page-locked copy: a bounded device wait that gave up
+// makes the call fail with RGBDFLOW_ERR_TIMEOUT, once; the device word is cleared for the next.
+void check_status(rgbdflow_ctx* c)
+{
+    if (!*c->pin_status) return;
+    *c->pin_status = 0;
+    RF_CUDA(cudaMemsetAsync(c->dev_status, 0, sizeof(int), c->stream));
+    RF_CUDA(cudaStreamSynchronize(c->stream));
+    throw ArgError(RGBDFLOW_ERR_TIMEOUT, "a bounded device wait (grid barrier) gave up: the solve's results are not valid");
 }
 
 void ensure_arena(rgbdflow_ctx* c, size_t need)
@@ -520,6 +535,7 @@ void run_batch(rgbdflow_ctx* c, const std::vector<PairSpec>& pairs, const HostPa
     const bool dev = user_stream != nullptr;
     Plan<T, S> P = plan_for<T, S>(c, pairs, hp);
     P.sms = c->sms;
+    P.status = c->dev_status;
     ensure_arena(c, P.arena_bytes);
     bind_plan(P, c->arena);
     record_layout(c, P);
@@ -605,6 +621,8 @@ void run_batch(rgbdflow_ctx* c, const std::vector<PairSpec>& pairs, const HostPa
     }
     const bool want_ctl = stats || c->prof;
     if (want_ctl) RF_CUDA(cudaMemcpyAsync(pin_ctl, c->arena + P.ctl_off, ctl_bytes, cudaMemcpyDeviceToHost, st));
+    // the status word is sticky, so a later copy also carries an earlier solve's failure
+    if (!dev || want_ctl) RF_CUDA(cudaMemcpyAsync(c->pin_status, c->dev_status, sizeof(int), cudaMemcpyDeviceToHost, st));
     RF_CUDA(cudaEventRecord(c->done, st));
     c->pending = true;
     if (host_async) {
@@ -616,6 +634,7 @@ void run_batch(rgbdflow_ctx* c, const std::vector<PairSpec>& pairs, const HostPa
     if (dev && !want_ctl) return;
     RF_CUDA(cudaEventSynchronize(c->done));
     c->pending = false;
+    check_status(c);
     float ms = 0;
     RF_CUDA(cudaEventElapsedTime(&ms, c->e0, c->e1));
     if (c->prof) {
@@ -1020,6 +1039,10 @@ int rgbdflow_ctx_create(int device, size_t hbm_budget_bytes, rgbdflow_ctx** out)
     if (cudaEventCreateWithFlags(&c->done, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&c->desc_up, cudaEventDisableTiming) != cudaSuccess)
         return RGBDFLOW_ERR_CUDA;
+    if (cudaMalloc(&c->dev_status, 64) != cudaSuccess || cudaMemset(c->dev_status, 0, 64) != cudaSuccess ||
+        cudaMallocHost(&c->pin_status, sizeof(int)) != cudaSuccess)
+        return RGBDFLOW_ERR_CUDA;
+    *c->pin_status = 0;
     const char* g = std::getenv("RGBDFLOW_NO_GRAPHS");
     c->use_graphs = !(g && g[0] == '1');
     *out = c.release();
@@ -1038,6 +1061,8 @@ int rgbdflow_ctx_destroy(rgbdflow_ctx* c)
     if (c->desc_up) cudaEventDestroy(c->desc_up);
     if (c->arena) cudaFree(c->arena);
     if (c->pin) cudaFreeHost(c->pin);
+    if (c->dev_status) cudaFree(c->dev_status);
+    if (c->pin_status) cudaFreeHost(c->pin_status);
     if (c->e0) cudaEventDestroy(c->e0);
     if (c->e1) cudaEventDestroy(c->e1);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -1244,6 +1269,29 @@ int rgbdflow_ctx_synchronize(rgbdflow_ctx* c)
     if (!c) return RGBDFLOW_ERR_INVALID_ARG;
     API_BEGIN
     wait_idle(c);
+    // device-pointer solves leave no copy of the status behind: read it here
+    RF_CUDA(cudaMemcpy(c->pin_status, c->dev_status, sizeof(int), cudaMemcpyDeviceToHost));
+    check_status(c);
+    return RGBDFLOW_OK;
+    API_END(c)
+}
+
+int rgbdflow_debug_wait_timeout(rgbdflow_ctx* c, double* seconds)
+{
+    if (!c) return RGBDFLOW_ERR_INVALID_ARG;
+    API_BEGIN
+    RF_CUDA(cudaSetDevice(c->device));
+    wait_idle(c);
+    GridSync* gs = (GridSync*)(c->dev_status + 4);
+    RF_CUDA(cudaMemsetAsync(gs, 0, sizeof(GridSync), c->stream));
+    RF_CUDA(cudaStreamSynchronize(c->stream));
+    const auto t0 = std::chrono::steady_clock::now();
+    k_wait_probe<<<1, 32, 0, c->stream>>>(gs, c->dev_status);
+    RF_CUDA(cudaGetLastError());
+    RF_CUDA(cudaMemcpyAsync(c->pin_status, c->dev_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    RF_CUDA(cudaStreamSynchronize(c->stream));
+    if (seconds) *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    check_status(c);
     return RGBDFLOW_OK;
     API_END(c)
 }
@@ -1529,13 +1577,19 @@ void server_retire(rgbdflow_server* s, ServerSlot& sl)
 {
     MaxTimer timer(&s->counters.max_retire_ms);
     const double now = mono_now();
+    // a bounded device wait that gave up fails every pair of the batch (and is cleared)
+    const bool failed = *sl.ctx->pin_status != 0;
+    if (failed) {
+        *sl.ctx->pin_status = 0;
+        RF_CUDA(cudaMemsetAsync(sl.ctx->dev_status, 0, sizeof(int), sl.st));
+    }
     for (size_t i = 0; i < sl.reqs.size(); i++) {
         ServerReq& r = sl.reqs[i];
         const size_t N = (size_t)r.W * r.H;
         if (r.out_host) std::memcpy(r.out_host, sl.pin_out + sl.out_off[i], N * 12);
         rgbdflow_result res;
         res.stream_id = r.stream; res.request_id = r.id; res.W = r.W; res.H = r.H; res.flow = r.out_host;
-        res.submit_time_s = r.t_submit; res.done_time_s = now; res.status = RGBDFLOW_OK;
+        res.submit_time_s = r.t_submit; res.done_time_s = now; res.status = failed ? RGBDFLOW_ERR_TIMEOUT : RGBDFLOW_OK;
         s->ready.push_back(res);
         StreamState& ss = s->streams[r.stream];
         ss.in_flight = false;
@@ -1738,6 +1792,7 @@ void server_launch(rgbdflow_server* s, ServerSlot& sl)
     for (size_t i = 0; i < sl.reqs.size(); i++)
         RF_CUDA(cudaMemcpyAsync(sl.pin_out + sl.out_off[i], ps[i].out, (size_t)ps[i].W * ps[i].H * 12,
                                 cudaMemcpyDeviceToHost, sl.st));
+    RF_CUDA(cudaMemcpyAsync(sl.ctx->pin_status, sl.ctx->dev_status, sizeof(int), cudaMemcpyDeviceToHost, sl.st));
     RF_CUDA(cudaEventRecord(sl.done, sl.st));
     sl.busy = true;
     s->counters.launches++;

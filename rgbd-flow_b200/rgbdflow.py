@@ -195,6 +195,7 @@ SIGNATURES = {
     "rgbdflow_profile": (_i, [_vp, _i]),
     "rgbdflow_profile_read": (_i, [_vp, _P(KernelStat), _i]),
     "rgbdflow_debug_read_plane": (_i, [_vp, _i, _i, _i, _i, _P(_d), ctypes.c_size_t, _P(_i), _P(_i)]),
+    "rgbdflow_debug_wait_timeout": (_i, [_vp, _P(_d)]),
     "rgbdflow_autotune_describe": (_i, [_i, ctypes.c_char_p, ctypes.c_size_t]),
     "rgbdflow_server_create": (_i, [_vp, _P(ServerConfig), _P(_vp)]),
     "rgbdflow_server_destroy": (_i, [_vp]),
@@ -474,6 +475,13 @@ class Context:
         self._check(self.lib.rgbdflow_debug_read_plane(self.h, pair, level, kind, index,
                                                        out.ctypes.data_as(_P(_d)), out.size, None, None))
         return out
+
+    def debug_wait_timeout(self):
+        """Runs the bounded-wait self-test (rgbdflow_debug_wait_timeout): (status code, seconds the
+        wait took).  RGBDFLOW_ERR_TIMEOUT is the expected code."""
+        sec = ctypes.c_double(0)
+        rc = self.lib.rgbdflow_debug_wait_timeout(self.h, ctypes.byref(sec))
+        return rc, sec.value
 
     def scene_flow_batch_device(self, pairs, params, stream=None):
         """Device-pointer batch: pairs hold torch CUDA tensors (bgr1/bgr2 uint8 HxWx3, depth1/depth2

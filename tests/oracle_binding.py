@@ -7,6 +7,7 @@ baseline of the benchmark.  The product path never imports this module.
 """
 import ctypes
 import os
+import sys
 import subprocess
 
 import numpy as np
@@ -339,9 +340,17 @@ class reference_cuda_levels:
     def __enter__(self):
         fn = ctypes.cast(ref_cuda().ref_single_scale, ctypes.c_void_p).value
         oracle().sfo_set_level_solver(fn)
+        # the reference solver prints its timings on stdout: sent to stderr while it runs, so that
+        # a caller's stdout (bench.py's one JSON line) stays clean
+        sys.stdout.flush()
+        self._stdout = os.dup(1)
+        os.dup2(2, 1)
         return self
 
     def __exit__(self, *a):
+        ctypes.CDLL(None).fflush(None)
+        os.dup2(self._stdout, 1)
+        os.close(self._stdout)
         oracle().sfo_set_level_solver(None)
 
 
