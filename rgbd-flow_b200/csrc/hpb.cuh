@@ -529,25 +529,26 @@ __global__ void k_hpb_rowsum(const HpbItem<T>* items, const int* first, int n_it
     if (rel < 0 || rel >= 7 * it.H) return;
     const int i = rel / 7, c = rel % 7;
     const size_t base = (size_t)i * it.W;
-    // the loads of 8 pixels are issued together; the sums stay in the reference's order
+    // the loads of 32 pixels are issued together; the sums stay in the reference's order
+    constexpr int B = 32;
     if (c == 6) {
         unsigned s = 0;
-        for (int j0 = 0; j0 < it.W; j0 += 8) {
-            unsigned v[8];
+        for (int j0 = 0; j0 < it.W; j0 += B) {
+            unsigned v[B];
 #pragma unroll
-            for (int u = 0; u < 8; u++) v[u] = j0 + u < it.W ? it.nval[base + j0 + u] : 0u;
+            for (int u = 0; u < B; u++) v[u] = j0 + u < it.W ? it.nval[base + j0 + u] : 0u;
 #pragma unroll
-            for (int u = 0; u < 8; u++)
+            for (int u = 0; u < B; u++)
                 if (j0 + u < it.W) { it.pre_v[base + j0 + u] = s; s += v[u]; }
         }
     } else {
         float s = 0;
-        for (int j0 = 0; j0 < it.W; j0 += 8) {
-            float v[8];
+        for (int j0 = 0; j0 < it.W; j0 += B) {
+            float v[B];
 #pragma unroll
-            for (int u = 0; u < 8; u++) v[u] = j0 + u < it.W ? hpb_chan(it, base + j0 + u, c) : 0.f;
+            for (int u = 0; u < B; u++) v[u] = j0 + u < it.W ? hpb_chan(it, base + j0 + u, c) : 0.f;
 #pragma unroll
-            for (int u = 0; u < 8; u++)
+            for (int u = 0; u < B; u++)
                 if (j0 + u < it.W) { it.pre[c][base + j0 + u] = s; s = fad(s, v[u]); }
         }
     }
@@ -563,24 +564,25 @@ __global__ void k_hpb_colsum(const HpbItem<T>* items, const int* first, int n_it
     const HpbItem<T>& it = items[k];
     const int rel = g - first[k];
     if (rel < 0 || rel >= 7 * (it.W + 1)) return;
-    const int jj = rel / 7, c = rel % 7;  // jj: column of the integral image (0 = the zero column)
     const int W1 = it.W + 1;
-    // the loads of 8 rows are issued together; the sums stay in the reference's order
+    const int c = rel / W1, jj = rel % W1;  // a warp: 32 columns of one channel; jj = 0 the zero column
+    // the loads of 16 rows are issued together; the sums stay in the reference's order
+    constexpr int B = 16;
     if (c == 6) {
         unsigned* ii = it.ii_v;
         ii[jj] = 0;
         unsigned a = 0;
-        for (int i0 = 0; i0 < it.H; i0 += 8) {
-            unsigned p[8], v[8];
+        for (int i0 = 0; i0 < it.H; i0 += B) {
+            unsigned p[B], v[B];
 #pragma unroll
-            for (int u = 0; u < 8; u++) {
+            for (int u = 0; u < B; u++) {
                 const bool in = jj > 0 && i0 + u < it.H;
                 const size_t l = in ? (size_t)(i0 + u) * it.W + jj - 1 : 0;
                 p[u] = in ? it.pre_v[l] : 0u;
                 v[u] = in ? it.nval[l] : 0u;
             }
 #pragma unroll
-            for (int u = 0; u < 8; u++)
+            for (int u = 0; u < B; u++)
                 if (i0 + u < it.H) {
                     if (jj > 0) a = (a + p[u]) + v[u];
                     ii[(size_t)(i0 + u + 1) * W1 + jj] = a;
@@ -590,17 +592,17 @@ __global__ void k_hpb_colsum(const HpbItem<T>* items, const int* first, int n_it
         float* ii = it.ii[c];
         ii[jj] = 0;
         float a = 0;
-        for (int i0 = 0; i0 < it.H; i0 += 8) {
-            float p[8], v[8];
+        for (int i0 = 0; i0 < it.H; i0 += B) {
+            float p[B], v[B];
 #pragma unroll
-            for (int u = 0; u < 8; u++) {
+            for (int u = 0; u < B; u++) {
                 const bool in = jj > 0 && i0 + u < it.H;
                 const size_t l = in ? (size_t)(i0 + u) * it.W + jj - 1 : 0;
                 p[u] = in ? it.pre[c][l] : 0.f;
                 v[u] = in ? hpb_chan(it, l, c) : 0.f;
             }
 #pragma unroll
-            for (int u = 0; u < 8; u++)
+            for (int u = 0; u < B; u++)
                 if (i0 + u < it.H) {
                     if (jj > 0) a = fad(fad(a, p[u]), v[u]);
                     ii[(size_t)(i0 + u + 1) * W1 + jj] = a;

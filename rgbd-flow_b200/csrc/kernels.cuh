@@ -1623,6 +1623,171 @@ k_sor_level(const LevelItem<T, S>* items, const int* which, SolveConst<T> k, Sor
 
 
 // ------------------------------------------------------------------------------------------
+// Whole-level SOR with the system held in registers (FP32; levels of at most kLevelRegMax
+// positions of the checkerboard layout, e.g. 40 x 30).  The same launch and results as
+// k_sor_level, but a thread owns one position (row i, half-row index m): one pixel of each
+// colour, whose 12 coefficients and the 4 neighbour coefficients its update needs (the left
+// pixel's horizontal weight and s, the upper pixel's vertical weight and s) stay in registers for
+// the whole launch, as do its own unknowns.  Shared memory holds only the three increment planes,
+// so a pixel update reads its 4 neighbours' unknowns (12 values) and writes 3, instead of reading
+// 31 values.
+constexpr int kLevelRegMax = 768;  // positions (= threads) of a level on this kernel
+template <class T> __host__ __device__ constexpr size_t level_reg_smem_bytes(int H, int hwp)
+{
+    return sizeof(T) * ((size_t)3 * (H + 2) * 2 * (hwp + 2) + 64);
+}
+
+template <class T, class S>
+__global__ void __launch_bounds__(kLevelRegMax, 1)
+k_sor_level_reg(const LevelItem<T, S>* items, const int* which, SolveConst<T> k, SorLaunch L)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* const xb = reinterpret_cast<T*>(smem_raw);
+    __shared__ int s_stop;
+    __shared__ T red[32];
+    const LevelItem<T, S>& it = items[which[blockIdx.x]];
+    PairCtl* ctl = it.ctl;
+    if (ctl->level_done) return;
+    const int W = it.W, H = it.H, hw = it.hwp, RP = hw + 2;
+    const int PLS = (H + 2) * 2 * RP;
+    const int tid = threadIdx.x, NT = blockDim.x;
+    // the unknowns: valid pixels from global, zero everywhere else (padding, positions past a
+    // row's count)
+    for (int e = tid; e < 3 * PLS; e += NT) {
+        const int v = e / PLS, f = e % PLS;
+        const int rr = f / (2 * RP) - 1, c = (f / RP) & 1, p = f % RP - 1;
+        const bool valid = !L.xin_zero && rr >= 0 && rr < H && p >= 0 && p < ((W + 1 - (c ^ (rr & 1))) >> 1);
+        xb[e] = valid ? it.x[L.xin][v][(size_t)rr * 2 * hw + c * hw + p] : (T)0;
+    }
+    // this thread's position and, per colour, its pixel's system in registers
+    const int i = tid / hw, m = tid % hw;
+    const bool inpos = tid < H * hw;
+    T cf[2][9], aL[2], aU[2], aR[2], aD[2], sL[2], sU[2], sw[2], xp[2][3];
+    bool valid[2];
+    int own[2], oth[2];
+#pragma unroll
+    for (int color = 0; color < 2; color++) {
+        const int b = color ^ (i & 1);
+        valid[color] = inpos && m < ((W + 1 - b) >> 1);
+        own[color] = ((i + 1) * 2 + color) * RP + m + 1;
+        oth[color] = ((i + 1) * 2 + (color ^ 1)) * RP + m + 1;
+        const size_t g = (size_t)i * 2 * hw + color * hw + m;
+        // the left neighbour is the other colour's position m - 1 + b of the row, the upper one its
+        // position m of the row above; outside the level they are zero, as in the staged planes
+        const int ml = m - 1 + b;
+        const bool lok = valid[color] && ml >= 0 && ml < ((W + 1 - (b ^ 1)) >> 1);
+        const bool uok = valid[color] && i >= 1;
+        const size_t gl = (size_t)i * 2 * hw + (color ^ 1) * hw + ml;
+        const size_t gu = (size_t)(i - 1) * 2 * hw + (color ^ 1) * hw + m;
+#pragma unroll
+        for (int z = 0; z < 9; z++) cf[color][z] = valid[color] ? it.sys[z][g] : (T)0;
+        aR[color] = valid[color] ? it.sys[9][g] : (T)0;
+        aD[color] = valid[color] ? it.sys[10][g] : (T)0;
+        sw[color] = valid[color] ? it.sys[11][g] : (T)0;
+        aL[color] = lok ? it.sys[9][gl] : (T)0;
+        sL[color] = lok ? it.sys[11][gl] : (T)0;
+        aU[color] = uok ? it.sys[10][gu] : (T)0;
+        sU[color] = uok ? it.sys[11][gu] : (T)0;
+    }
+    if (tid == 0) s_stop = 0;
+    __syncthreads();
+#pragma unroll
+    for (int color = 0; color < 2; color++)
+#pragma unroll
+        for (int v = 0; v < 3; v++) xp[color][v] = xb[v * PLS + own[color]];
+    for (int itn = 0; itn < k.n_sor; itn++) {
+        const bool chk = !k.fixed && (itn % k.period == k.period - 1);
+        T md = 0;
+#pragma unroll
+        for (int color = 0; color < 2; color++) {
+            if (valid[color]) {
+                const int b = color ^ (i & 1);
+                const int ol = oth[color] - 1 + b, orr = oth[color] + b, ou = oth[color] - 2 * RP, od = oth[color] + 2 * RP;
+                T xl[3], xu[3], xr[3], xd[3], nv[3];
+#pragma unroll
+                for (int v = 0; v < 3; v++) {
+                    const T* xv = xb + v * PLS;
+                    xl[v] = xv[ol]; xr[v] = xv[orr]; xu[v] = xv[ou]; xd[v] = xv[od];
+                }
+                sor_point<T>(cf[color], aL[color], aU[color], aR[color], aD[color], sL[color], sU[color], sw[color],
+                             xl, xu, xr, xd, xp[color], k.omega, k.step, nv);
+#pragma unroll
+                for (int v = 0; v < 3; v++) {
+                    xb[v * PLS + own[color]] = nv[v];
+                    if (chk) md = maxT(md, absT(nv[v] - xp[color][v]));
+                    xp[color][v] = nv[v];
+                }
+            }
+            __syncthreads();
+        }
+        if (chk) {
+            // the check: max |dx| of this iteration over the level (float bits, as the tile kernels)
+            float mm = (float)md;
+            for (int off = 16; off > 0; off >>= 1) mm = fmaxf(mm, __shfl_xor_sync(0xffffffffu, mm, off));
+            if ((tid & 31) == 0) red[tid >> 5] = (T)mm;
+            __syncthreads();
+            if (tid == 0) {
+                float g = 0;
+                for (int w = 0; w < NT / 32; w++) g = fmaxf(g, (float)red[w]);
+                const int ci = min(itn / k.period, kMaxChecks - 1);
+                if (g > 0) ctl->maxdiff[ci] = __float_as_uint(g);
+                if ((double)g < k.sor_tol || (T)g >= k.step) {
+                    s_stop = 1;
+                    ctl->sor_stop = 1;
+                    ctl->sor_stop_iter = itn + 1;
+                }
+            }
+            __syncthreads();
+            if (s_stop) break;
+        }
+    }
+    // out: the fold u += x with the statistic partial per 32 x 32 tile (the tile kernels' order),
+    // or x into the ping-pong buffer the next inner iteration reads
+    const int sx = (W + kSorTW - 1) / kSorTW, sy = (H + kSorTH - 1) / kSorTH;
+    if (L.final_fold) {
+        const int pitch = it.pitch;
+        const T fl = it.f_level;
+        // the partials are summed exactly as a 512-thread tile CTA sums them: "virtual thread" vt
+        // (0..511) takes pixels vt and vt + 512 of the tile, a warp tree per virtual warp, then
+        // the 16 virtual warps in order; a real warp takes virtual warps w, w + NT / 32, ...
+        const int lane = tid & 31;
+        for (int ti = 0; ti < sx * sy; ti++) {
+            const int ix0 = (ti % sx) * kSorTW, iy0 = (ti / sx) * kSorTH;
+            for (int vw = tid >> 5; vw < 16; vw += NT >> 5) {
+                T part = 0;
+                for (int q = vw * 32 + lane; q < kSorTW * kSorTH; q += 512) {
+                    const int gi = iy0 + q / kSorTW, gj = ix0 + q % kSorTW;
+                    if (gi >= H || gj >= W) continue;
+                    const int o = ((gi + 1) * 2 + ((gi + gj) & 1)) * RP + (gj >> 1) + 1;
+                    const T a = xb[o], bq = xb[PLS + o], cz = xb[2 * PLS + o];
+                    const size_t lp = (size_t)gi * pitch + gj;
+                    it.u[0][lp] = addR(it.u[0][lp], a); it.u[1][lp] = addR(it.u[1][lp], bq);
+                    it.u[2][lp] = addR(it.u[2][lp], cz);
+                    part = addR(part, stat_px<T>(a, bq, cz, fl, it.pyr[6][(size_t)gi * W + gj]));
+                }
+                for (int off = 16; off > 0; off >>= 1) part += __shfl_down_sync(0xffffffffu, part, off);
+                if (lane == 0) red[vw] = part;
+            }
+            __syncthreads();
+            if (tid == 0) {
+                T tot = 0;
+                for (int w = 0; w < 16; w++) tot += red[w];
+                it.stat_part[ti] = tot;
+            }
+            __syncthreads();
+        }
+        if (L.control && tid < 32) control_item(it, k, L.outer, L.n_checks, tid);
+    } else {
+        for (int q = tid; q < H * W; q += NT) {
+            const int gi = q / W, gj = q % W;
+            const int o = ((gi + 1) * 2 + ((gi + gj) & 1)) * RP + (gj >> 1) + 1;
+            const int lc = cs_idx(gi, gj, hw);
+            for (int v = 0; v < 3; v++) it.x[L.xout][v][lc] = xb[v * PLS + o];
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------
 // Whole-level SOR over a thread-block cluster, for levels whose 15 planes need up to 8 SMs' shared
 // memory (the 80 x 60 and 160 x 120 levels).  One cluster per pair: CTA r of C holds rows
 // [r B, r B + B) (B = ceil(H / C)) with one halo row above and below, runs every SOR iteration of

@@ -140,6 +140,7 @@ struct HostParams {
     long strip_min_px;                        // strips only for steps with this many eligible pixels
     int sor_level;                            // whole-level SOR for levels that fit one CTA (0: off)
     int level_cluster;                        // > 1: such levels run on a cluster of this many CTAs instead
+    int level_reg;                            // FP32 whole-level SOR with the system in registers (0: off)
 };
 
 // Row pitch of the u planes, and the checkerboard half-row length of the x / sys planes (16-byte
@@ -253,17 +254,47 @@ static std::vector<StripUnit> strip_units(const std::vector<X>& items, const std
         seg = std::max(64, std::min(seg, 512));
     }
     seg = std::max(32, seg & ~31);
-    int max_bands = 0;
-    for (int i : which) max_bands = std::max(max_bands, (items[i].H + seg - 1) / seg);
-    int max_strips = 0;
-    for (int i : which) max_strips = std::max(max_strips, (items[i].W + kStripW - 1) / kStripW);
-    for (int b = 0; b < max_bands; b++)
-        for (int sx = 0; sx < max_strips; sx++)
-            for (int i : which) {
-                const int W = items[i].W, H = items[i].H;
-                if (sx * kStripW >= W || b * seg >= H) continue;
-                v.push_back(StripUnit{i, sx * kStripW, b * seg, std::min(H, (b + 1) * seg)});
+    // Bands of seg rows from the top; the rest of the strip (or, when seg divides it, its last
+    // band) in smaller bands, 2^k x 32 rows largest first, the last one reaching the bottom.  The
+    // units are handed out largest first, so the small bands fill the last wave: the SMs finish
+    // closer together than with equal bands.
+    auto bands_of = [&](int H) {
+        std::vector<std::pair<int, int>> bl;
+        int n = H / seg, rem = H - n * seg;
+        if (rem == 0 && n >= 2) { n--; rem = seg; }
+        for (int b = 0; b < n; b++) bl.push_back({b * seg, (b + 1) * seg});
+        int y = n * seg;
+        while (rem > 0) {
+            int piece = rem;
+            if (rem >= 64) {
+                int p2 = 32;
+                while (p2 * 2 <= rem) p2 *= 2;
+                if (rem - p2 >= 32) piece = p2;
             }
+            bl.push_back({y, y + piece});
+            y += piece;
+            rem -= piece;
+        }
+        return bl;
+    };
+    struct Cand { int h, band, sx, ord; StripUnit u; };
+    std::vector<Cand> c;
+    for (size_t o = 0; o < which.size(); o++) {
+        const int i = which[o];
+        const int W = items[i].W, H = items[i].H;
+        const auto bl = bands_of(H);
+        for (size_t b = 0; b < bl.size(); b++)
+            for (int sx = 0; sx * kStripW < W; sx++)
+                c.push_back(Cand{bl[b].second - bl[b].first, (int)b, sx, (int)o,
+                                 StripUnit{i, sx * kStripW, bl[b].first, bl[b].second}});
+    }
+    std::stable_sort(c.begin(), c.end(), [](const Cand& a, const Cand& b) {
+        if (a.h != b.h) return a.h > b.h;
+        if (a.band != b.band) return a.band < b.band;
+        if (a.sx != b.sx) return a.sx < b.sx;
+        return a.ord < b.ord;
+    });
+    for (const auto& x : c) v.push_back(x.u);
     return v;
 }
 
@@ -328,6 +359,7 @@ struct Plan {
         size_t level_items_off; int n_level;  // whole-level SOR: items (one CTA each)
         size_t level_smem;
         int level_threads;
+        int level_reg;  // the whole-level items run on k_sor_level_reg
         size_t clus_items_off; int n_clus;    // whole-level SOR over a cluster of clus_c CTAs per item
         int clus_c, clus_threads;
         size_t clus_smem;
@@ -734,8 +766,9 @@ static Plan<T, S> make_plan(const std::vector<PairSpec>& pairs, const HostParams
             items.push_back(it);
         }
         std::vector<int> strip_items, level_items, clus_items;
-        size_t level_smem = 0, clus_smem = 0;
+        size_t level_smem = 0, clus_smem = 0, level_reg_smem = 0;
         int level_thr = 64, clus_c = 0, clus_thr = 64;
+        bool level_reg = sizeof(T) == 4 && hp.level_reg != 0;
         long strip_px = 0;
         for (const auto& x : items)
             if (use_strip<T>(hp, x.W, x.H)) strip_px += (long)x.W * x.H;
@@ -755,7 +788,9 @@ static Plan<T, S> make_plan(const std::vector<PairSpec>& pairs, const HostParams
             if (use_level<T>(hp, x.W, x.H, x.hwp) && !(hp.level_cluster > 1 && x.H >= 2 * hp.level_cluster)) {
                 level_items.push_back((int)(&x - items.data()));
                 level_smem = std::max(level_smem, level_smem_bytes<T>(x.H, x.hwp));
+                level_reg_smem = std::max(level_reg_smem, level_reg_smem_bytes<T>(x.H, x.hwp));
                 level_thr = std::max(level_thr, level_threads(x.H, x.hwp));
+                level_reg = level_reg && x.H * x.hwp <= kLevelRegMax;
                 continue;
             }
             if (level_cluster_size<T>(hp, x.H, x.hwp) > 0 && !(ch && ch->strip)) {
@@ -785,7 +820,8 @@ static Plan<T, S> make_plan(const std::vector<PairSpec>& pairs, const HostParams
         d.strip_units_off = P.put(units); d.n_units = (int)units.size();
         d.strip_grid = std::min(P.sms, d.n_units);
         d.level_items_off = P.put(level_items); d.n_level = (int)level_items.size();
-        d.level_smem = level_smem;
+        d.level_reg = level_reg && !level_items.empty();
+        d.level_smem = d.level_reg ? level_reg_smem : level_smem;
         d.level_threads = level_thr;
         for (int i : clus_items) {
             const int B = (items[i].H + clus_c - 1) / clus_c;
@@ -1076,6 +1112,8 @@ static void set_kernel_attrs()
                                      (int)strip_smem_bytes<T>()));
     RF_CUDA(cudaFuncSetAttribute(k_sor_level<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLevelSmemMax));
     RF_CUDA(cudaFuncSetAttribute(k_sor_level_cluster<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLevelSmemMax));
+    if constexpr (sizeof(T) == 4)
+        RF_CUDA(cudaFuncSetAttribute(k_sor_level_reg<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
 }
 
 // Whether configuration c fits shared memory for type T.
@@ -1137,7 +1175,14 @@ static int enqueue_level(const Plan<T, S>& P, char* base, int sidx, cudaStream_t
                 L.control = fold_control && L.final_fold;
                 L.n_checks = P.n_checks[sidx].back();
                 RF_PROF_B(pf, KC_SOR_LEVEL0 + lvl, st);
-                k_sor_level<T, S><<<d.n_level, d.level_threads, d.level_smem, st>>>(items, level_items, k, L);
+                if constexpr (sizeof(T) == 4) {
+                    if (d.level_reg)
+                        k_sor_level_reg<T, S><<<d.n_level, d.level_threads, d.level_smem, st>>>(items, level_items, k, L);
+                    else
+                        k_sor_level<T, S><<<d.n_level, d.level_threads, d.level_smem, st>>>(items, level_items, k, L);
+                } else {
+                    k_sor_level<T, S><<<d.n_level, d.level_threads, d.level_smem, st>>>(items, level_items, k, L);
+                }
                 RF_PROF_E(pf, st);
                 launches++;
             }

@@ -186,6 +186,8 @@ HostParams host_params(const rgbdflow_params& p)
     h.sor_level = e ? std::atoi(e) : 1;
     e = std::getenv("RGBDFLOW_LEVEL_CLUSTER");
     h.level_cluster = e ? std::atoi(e) : 0;
+    e = std::getenv("RGBDFLOW_LEVEL_REG");
+    h.level_reg = e ? std::atoi(e) : 1;
     h.fill_rounds = 253;  // round stamps are bytes: 0 valid, 1..253 rounds, 254 outside, 255 unfilled
     return h;
 }
@@ -229,8 +231,8 @@ std::string plan_key(const std::vector<PairSpec>& ps, const HostParams& hp, int 
                   hp.n_sor, hp.max_dist, hp.fill_holes, hp.fixed, hp.omega, hp.step, hp.eps_d, hp.eps_z, hp.eps_s,
                   hp.sor_tol, hp.outer_tol, hp.occ_margin, hp.occ_penalty, hp.max_grad, hp.period, hp.K * 100 + hp.sor_ilp * 10 + hp.sor_nbuf, hp.fill_rounds);
     k += buf;
-    std::snprintf(buf, sizeof buf, " strip %d %d %d %d %ld level %d %d", hp.sor_strip, hp.strip_min_w, hp.strip_min_h,
-                  hp.strip_seg, hp.strip_min_px, hp.sor_level, hp.level_cluster);
+    std::snprintf(buf, sizeof buf, " strip %d %d %d %d %ld level %d %d %d", hp.sor_strip, hp.strip_min_w, hp.strip_min_h,
+                  hp.strip_seg, hp.strip_min_px, hp.sor_level, hp.level_cluster, hp.level_reg);
     return k + buf;
 }
 

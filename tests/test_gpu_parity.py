@@ -278,9 +278,10 @@ def test_every_tunable_sor_choice_agrees_bitwise(ctx, monkeypatch):
 
 @pytest.mark.parametrize("name,n_inner", [("640x480", 1), ("160x120", 1), ("320x240", 2)])
 def test_whole_level_sor_agrees_bitwise(ctx, monkeypatch, name, n_inner):
-    """The whole-level SOR (one CTA runs all iterations of a level that fits its shared memory)
-    and the tile SOR give the same flow and executed schedule, bit for bit, also with two inner
-    iterations (the increment handed on between them)."""
+    """The whole-level SOR (one CTA runs all iterations of a level that fits its shared memory;
+    FP32 levels of at most 768 positions with the system in registers, or with all 15 planes in
+    shared memory) and the tile SOR give the same flow and executed schedule, bit for bit, also
+    with two inner iterations (the increment handed on between them)."""
     p = syn.make_config_pair(name, seed=13)
     prm = rf.benchmark_params(p["W"])
     prm.n_inner = n_inner
@@ -291,6 +292,11 @@ def test_whole_level_sor_agrees_bitwise(ctx, monkeypatch, name, n_inner):
     whole, st_whole = ctx.scene_flow_two_frames(*args)
     assert st_tile.summary() == st_whole.summary()
     np.testing.assert_array_equal(tile, whole)
+    monkeypatch.setenv("RGBDFLOW_LEVEL_REG", "0")
+    smem, st_smem = ctx.scene_flow_two_frames(*args)
+    assert st_tile.summary() == st_smem.summary()
+    np.testing.assert_array_equal(tile, smem)
+    monkeypatch.delenv("RGBDFLOW_LEVEL_REG")
     # every whole-level item on a cluster of at least 4 CTAs (the coarsest levels too)
     monkeypatch.setenv("RGBDFLOW_LEVEL_CLUSTER", "4")
     clus, st_clus = ctx.scene_flow_two_frames(*args)
