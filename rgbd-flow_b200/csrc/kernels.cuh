@@ -1961,6 +1961,217 @@ k_sor_level_cluster(const LevelItem<T, S>* items, const int* which, SolveConst<T
     }
 }
 
+// ------------------------------------------------------------------------------------------
+// Whole-level SOR over a thread-block cluster with the system in registers (FP32): the schedule,
+// halo exchange and results of k_sor_level_cluster, but a thread owns KP positions of its CTA's
+// row band (one pixel of each colour per position) whose coefficients, the 4 neighbour
+// coefficients their updates need and their own unknowns stay in registers for the whole launch.
+// Shared memory holds only the three increment planes of the band plus a halo row above and
+// below, so a pixel update reads 12 values from shared memory instead of 31.
+template <int KP> __host__ __device__ constexpr int clus_reg_threads_max() { return KP == 1 ? 768 : 640; }
+template <class T> __host__ __device__ constexpr size_t level_cluster_reg_smem_bytes(int B, int hwp)
+{
+    return sizeof(T) * ((size_t)3 * (B + 2) * 2 * (hwp + 2) + 64);
+}
+
+template <class T, class S, int KP>
+__global__ void __launch_bounds__(clus_reg_threads_max<KP>(), 1)
+k_sor_level_cluster_reg(const LevelItem<T, S>* items, const int* which, SolveConst<T> k, SorLaunch L)
+{
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* const xb = reinterpret_cast<T*>(smem_raw);
+    __shared__ int s_stop;
+    __shared__ float s_max;
+    __shared__ T red[32];
+    const int C = (int)cl.num_blocks(), rank = (int)cl.block_rank();
+    const LevelItem<T, S>& it = items[which[blockIdx.x / C]];
+    PairCtl* ctl = it.ctl;
+    if (ctl->level_done) return;  // the same for every CTA of the cluster: none reaches a barrier
+    const int W = it.W, H = it.H, hw = it.hwp, RP = hw + 2;
+    const int B = (H + C - 1) / C, r0 = rank * B, nr = max(0, min(H, r0 + B) - r0);
+    const int PLS = (B + 2) * 2 * RP;
+    const int tid = threadIdx.x, NT = blockDim.x;
+    // the unknowns of rows r0 - 1 .. r0 + nr (local rows 0 .. nr + 1): valid pixels from global,
+    // zero elsewhere
+    for (int e = tid; e < 3 * PLS; e += NT) {
+        const int v = e / PLS, f = e % PLS;
+        const int lr = f / (2 * RP), c = (f / RP) & 1, p = f % RP - 1;
+        const int rr = r0 - 1 + lr;
+        const bool valid = !L.xin_zero && lr <= nr + 1 && rr >= 0 && rr < H && p >= 0 &&
+                           p < ((W + 1 - (c ^ (rr & 1))) >> 1);
+        xb[e] = valid ? it.x[L.xin][v][(size_t)rr * 2 * hw + c * hw + p] : (T)0;
+    }
+    // this thread's positions (local row li, half-row index m) and their pixels' systems
+    T cf[KP][2][9], aL[KP][2], aU[KP][2], aR[KP][2], aD[KP][2], sL[KP][2], sU[KP][2], sw[KP][2], xp[KP][2][3];
+    int li[KP], mm[KP];
+    bool valid[KP][2];
+#pragma unroll
+    for (int kp = 0; kp < KP; kp++) {
+        const int q = tid + kp * NT;
+        li[kp] = q / hw;
+        mm[kp] = q % hw;
+        const int i = r0 + li[kp], m = mm[kp];
+        const bool inpos = q < nr * hw;
+#pragma unroll
+        for (int color = 0; color < 2; color++) {
+            const int b = color ^ (i & 1);
+            const bool vd = inpos && m < ((W + 1 - b) >> 1);
+            valid[kp][color] = vd;
+            const size_t g = (size_t)i * 2 * hw + color * hw + m;
+            // the left neighbour is the other colour's position m - 1 + b of the row, the upper one
+            // its position m of the row above; outside the level they are zero
+            const int ml = m - 1 + b;
+            const bool lok = vd && ml >= 0 && ml < ((W + 1 - (b ^ 1)) >> 1);
+            const bool uok = vd && i >= 1;
+            const size_t gl = (size_t)i * 2 * hw + (color ^ 1) * hw + ml;
+            const size_t gu = (size_t)(i - 1) * 2 * hw + (color ^ 1) * hw + m;
+#pragma unroll
+            for (int z = 0; z < 9; z++) cf[kp][color][z] = vd ? it.sys[z][g] : (T)0;
+            aR[kp][color] = vd ? it.sys[9][g] : (T)0;
+            aD[kp][color] = vd ? it.sys[10][g] : (T)0;
+            sw[kp][color] = vd ? it.sys[11][g] : (T)0;
+            aL[kp][color] = lok ? it.sys[9][gl] : (T)0;
+            sL[kp][color] = lok ? it.sys[11][gl] : (T)0;
+            aU[kp][color] = uok ? it.sys[10][gu] : (T)0;
+            sU[kp][color] = uok ? it.sys[11][gu] : (T)0;
+        }
+    }
+    if (tid == 0) s_stop = 0;
+    cl.sync();  // every CTA of the cluster has started and staged (its shared memory may be read)
+#pragma unroll
+    for (int kp = 0; kp < KP; kp++)
+#pragma unroll
+        for (int color = 0; color < 2; color++)
+#pragma unroll
+            for (int v = 0; v < 3; v++)
+                xp[kp][color][v] = xb[v * PLS + ((li[kp] + 1) * 2 + color) * RP + mm[kp] + 1];
+    T* const up_buf = rank > 0 ? cl.map_shared_rank(xb, rank - 1) : nullptr;
+    T* const dn_buf = rank < C - 1 ? cl.map_shared_rank(xb, rank + 1) : nullptr;
+    for (int itn = 0; itn < k.n_sor; itn++) {
+        const bool chk = !k.fixed && (itn % k.period == k.period - 1);
+        T md = 0;
+#pragma unroll
+        for (int color = 0; color < 2; color++) {
+#pragma unroll
+            for (int kp = 0; kp < KP; kp++) {
+                if (valid[kp][color]) {
+                    const int b = color ^ ((r0 + li[kp]) & 1);
+                    const int own = ((li[kp] + 1) * 2 + color) * RP + mm[kp] + 1;
+                    const int oth = ((li[kp] + 1) * 2 + (color ^ 1)) * RP + mm[kp] + 1;
+                    const int ol = oth - 1 + b, orr = oth + b, ou = oth - 2 * RP, od = oth + 2 * RP;
+                    T xl[3], xu[3], xr[3], xd[3], nv[3];
+#pragma unroll
+                    for (int v = 0; v < 3; v++) {
+                        const T* xv = xb + v * PLS;
+                        xl[v] = xv[ol]; xr[v] = xv[orr]; xu[v] = xv[ou]; xd[v] = xv[od];
+                    }
+                    sor_point<T>(cf[kp][color], aL[kp][color], aU[kp][color], aR[kp][color], aD[kp][color],
+                                 sL[kp][color], sU[kp][color], sw[kp][color], xl, xu, xr, xd, xp[kp][color], k.omega,
+                                 k.step, nv);
+#pragma unroll
+                    for (int v = 0; v < 3; v++) {
+                        xb[v * PLS + own] = nv[v];
+                        if (chk) md = maxT(md, absT(nv[v] - xp[kp][color][v]));
+                        xp[kp][color][v] = nv[v];
+                    }
+                }
+            }
+            cl.sync();  // this half-sweep is done in every CTA
+            // the neighbours' boundary rows of this colour into the halo rows; the neighbours write
+            // the other colour meanwhile, and reach this colour again only after the next cluster
+            // barrier
+            for (int e = tid; e < 2 * 3 * RP; e += NT) {
+                const int side = e / (3 * RP), v = (e / RP) % 3, p = e % RP;
+                const T* src = side == 0 ? up_buf : dn_buf;
+                if (!src) continue;
+                const int srow = side == 0 ? B : 1;  // the neighbour's last / first own row
+                const int drow = side == 0 ? 0 : nr + 1;
+                xb[v * PLS + (drow * 2 + color) * RP + p] = src[v * PLS + (srow * 2 + color) * RP + p];
+            }
+            __syncthreads();
+        }
+        if (chk) {
+            float mx = (float)md;
+            for (int off = 16; off > 0; off >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+            if ((tid & 31) == 0) red[tid >> 5] = (T)mx;
+            __syncthreads();
+            if (tid == 0) {
+                float g = 0;
+                for (int w = 0; w < NT / 32; w++) g = fmaxf(g, (float)red[w]);
+                s_max = g;
+            }
+            cl.sync();  // every CTA's maximum is in place
+            if (tid == 0) {
+                float g = 0;
+                for (int r = 0; r < C; r++) g = fmaxf(g, *cl.map_shared_rank(&s_max, r));
+                if (rank == 0) {
+                    const int ci = min(itn / k.period, kMaxChecks - 1);
+                    if (g > 0) ctl->maxdiff[ci] = __float_as_uint(g);
+                }
+                if ((double)g < k.sor_tol || (T)g >= k.step) {
+                    s_stop = 1;
+                    if (rank == 0) { ctl->sor_stop = 1; ctl->sor_stop_iter = itn + 1; }
+                }
+            }
+            cl.sync();  // every CTA has read the maxima (s_max may be rewritten) and decided
+            if (s_stop) break;
+        }
+    }
+    // no CTA may leave while a neighbour still copies from its shared memory (the last half-sweep's
+    // halo rows)
+    cl.sync();
+    // x of the own rows to global: the next inner iteration's buffer, or (fold) scratch that the CTA
+    // folding each tile reads (the fold's next use of x starts from zero)
+    T* const* xo = it.x[L.final_fold ? 0 : L.xout];
+    for (int q = tid; q < nr * W; q += NT) {
+        const int lr = q / W, gj = q % W, gi = r0 + lr;
+        const int o = ((lr + 1) * 2 + ((gi + gj) & 1)) * RP + (gj >> 1) + 1;
+        const int lc = cs_idx(gi, gj, hw);
+        for (int v = 0; v < 3; v++) xo[v][lc] = xb[v * PLS + o];
+    }
+    if (!L.final_fold) return;
+    __threadfence();
+    cl.sync();  // every CTA's x is in global memory
+    const int sx = (W + kSorTW - 1) / kSorTW, sy = (H + kSorTH - 1) / kSorTH;
+    const int pitch = it.pitch;
+    const T fl = it.f_level;
+    const int lane = tid & 31;
+    for (int ti = rank; ti < sx * sy; ti += C) {
+        const int ix0 = (ti % sx) * kSorTW, iy0 = (ti / sx) * kSorTH;
+        // the tile kernels' order: virtual thread vt (0..511) takes pixels vt and vt + 512 of the
+        // tile, a warp tree per virtual warp, then the 16 virtual warps in order
+        for (int vw = tid >> 5; vw < 16; vw += NT >> 5) {
+            T part = 0;
+            for (int q = vw * 32 + lane; q < kSorTW * kSorTH; q += 512) {
+                const int gi = iy0 + q / kSorTW, gj = ix0 + q % kSorTW;
+                if (gi >= H || gj >= W) continue;
+                const int lc = cs_idx(gi, gj, hw);
+                const T a = __ldcg(xo[0] + lc), bq = __ldcg(xo[1] + lc), cz = __ldcg(xo[2] + lc);
+                const size_t lp = (size_t)gi * pitch + gj;
+                it.u[0][lp] = addR(it.u[0][lp], a); it.u[1][lp] = addR(it.u[1][lp], bq);
+                it.u[2][lp] = addR(it.u[2][lp], cz);
+                part = addR(part, stat_px<T>(a, bq, cz, fl, it.pyr[6][(size_t)gi * W + gj]));
+            }
+            for (int off = 16; off > 0; off >>= 1) part += __shfl_down_sync(0xffffffffu, part, off);
+            if (lane == 0) red[vw] = part;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            T tot = 0;
+            for (int w = 0; w < 16; w++) tot += red[w];
+            it.stat_part[ti] = tot;
+        }
+        __syncthreads();
+    }
+    if (L.control) {
+        __threadfence();
+        cl.sync();  // every tile's statistic partial is written
+        if (rank == 0 && tid < 32) control_item(it, k, L.outer, L.n_checks, tid);
+    }
+}
+
 // After each outer iteration: the early-termination statistic of the pair (mean over 3N of
 // sqr(du) * (1, 1, f / depth1), .cu:943-951), the stop decision and the executed-schedule record.
 // One warp per item (lane = the thread's lane); the statistic partials are read from L2 (the

@@ -14,6 +14,7 @@
 #include <map>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "kernels.cuh"
@@ -320,6 +321,21 @@ static inline int level_cluster_size(const HostParams& hp, int H, int hwp)
     return 0;
 }
 
+// The cluster size and positions per thread of the register variant of the cluster whole-level
+// SOR (FP32): the fewest CTAs (2..8) whose row bands hold at most KP x its thread limit positions
+// each, KP = 1 first, then 2, every band holding at least one row; {0, 0} when none fits.
+static inline std::pair<int, int> level_cluster_reg_shape(const HostParams& hp, int H, int hwp)
+{
+    if (!hp.sor_level || !hp.level_reg) return {0, 0};
+    for (int KP = 1; KP <= 2; KP++)
+        for (int C = std::max(2, std::min(hp.level_cluster, 8)); C <= 8; C++) {
+            const int B = (H + C - 1) / C;
+            if (B * (C - 1) < H && B * hwp <= KP * (KP == 1 ? clus_reg_threads_max<1>() : clus_reg_threads_max<2>()))
+                return {C, KP};
+        }
+    return {0, 0};
+}
+
 // Bump allocator over a byte range.
 struct Bump {
     size_t off = 0;
@@ -363,6 +379,7 @@ struct Plan {
         size_t clus_items_off; int n_clus;    // whole-level SOR over a cluster of clus_c CTAs per item
         int clus_c, clus_threads;
         size_t clus_smem;
+        int clus_kp;  // > 0: the cluster items run on k_sor_level_cluster_reg with this many positions a thread
     };
     std::vector<StepDesc> steps;
     struct PyrLevelDesc { size_t jobs_off; int n_jobs; size_t src_tiles_off; int n_src; size_t dst_tiles_off; int n_dst; size_t g_off; };
@@ -823,13 +840,29 @@ static Plan<T, S> make_plan(const std::vector<PairSpec>& pairs, const HostParams
         d.level_reg = level_reg && !level_items.empty();
         d.level_smem = d.level_reg ? level_reg_smem : level_smem;
         d.level_threads = level_thr;
+        // the register variant when every cluster item fits it (FP32)
+        int reg_c = 0, reg_kp = 0;
+        bool clus_reg = sizeof(T) == 4 && !clus_items.empty();
+        for (int i : clus_items) {
+            const auto sh = level_cluster_reg_shape(hp, items[i].H, items[i].hwp);
+            clus_reg = clus_reg && sh.first > 0;
+            reg_c = std::max(reg_c, sh.first);
+            reg_kp = std::max(reg_kp, sh.second);
+        }
+        if (clus_reg) clus_c = reg_c;
         for (int i : clus_items) {
             const int B = (items[i].H + clus_c - 1) / clus_c;
-            clus_smem = std::max(clus_smem, level_cluster_smem_bytes<T>(B, items[i].hwp));
-            clus_thr = std::max(clus_thr, std::min(1024, (B * items[i].hwp + 31) / 32 * 32));
+            if (clus_reg) {
+                clus_smem = std::max(clus_smem, level_cluster_reg_smem_bytes<T>(B, items[i].hwp));
+                clus_thr = std::max(clus_thr, ((B * items[i].hwp + reg_kp - 1) / reg_kp + 31) / 32 * 32);
+            } else {
+                clus_smem = std::max(clus_smem, level_cluster_smem_bytes<T>(B, items[i].hwp));
+                clus_thr = std::max(clus_thr, std::min(1024, (B * items[i].hwp + 31) / 32 * 32));
+            }
         }
         d.clus_items_off = P.put(clus_items); d.n_clus = (int)clus_items.size();
         d.clus_c = clus_c; d.clus_smem = clus_smem; d.clus_threads = clus_thr;
+        d.clus_kp = clus_reg ? reg_kp : 0;
         P.steps.push_back(d);
     }
     // output pointers (one per pair, in the order of the finest step's items = pair order)
@@ -1112,8 +1145,11 @@ static void set_kernel_attrs()
                                      (int)strip_smem_bytes<T>()));
     RF_CUDA(cudaFuncSetAttribute(k_sor_level<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLevelSmemMax));
     RF_CUDA(cudaFuncSetAttribute(k_sor_level_cluster<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLevelSmemMax));
-    if constexpr (sizeof(T) == 4)
+    if constexpr (sizeof(T) == 4) {
         RF_CUDA(cudaFuncSetAttribute(k_sor_level_reg<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
+        RF_CUDA(cudaFuncSetAttribute(k_sor_level_cluster_reg<T, S, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
+        RF_CUDA(cudaFuncSetAttribute(k_sor_level_cluster_reg<T, S, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
+    }
 }
 
 // Whether configuration c fits shared memory for type T.
@@ -1209,8 +1245,17 @@ static int enqueue_level(const Plan<T, S>& P, char* base, int sidx, cudaStream_t
                 cfg.attrs = at;
                 cfg.numAttrs = 1;
                 RF_PROF_B(pf, KC_SOR_LEVEL0 + lvl, st);
-                RF_CUDA(cudaLaunchKernelEx(&cfg, k_sor_level_cluster<T, S>, items,
-                                           (const int*)(base + P.desc_off + d.clus_items_off), k, L));
+                const int* ci = (const int*)(base + P.desc_off + d.clus_items_off);
+                if constexpr (sizeof(T) == 4) {
+                    if (d.clus_kp == 1)
+                        RF_CUDA(cudaLaunchKernelEx(&cfg, k_sor_level_cluster_reg<T, S, 1>, items, ci, k, L));
+                    else if (d.clus_kp == 2)
+                        RF_CUDA(cudaLaunchKernelEx(&cfg, k_sor_level_cluster_reg<T, S, 2>, items, ci, k, L));
+                    else
+                        RF_CUDA(cudaLaunchKernelEx(&cfg, k_sor_level_cluster<T, S>, items, ci, k, L));
+                } else {
+                    RF_CUDA(cudaLaunchKernelEx(&cfg, k_sor_level_cluster<T, S>, items, ci, k, L));
+                }
                 RF_PROF_E(pf, st);
                 launches++;
             }

@@ -247,7 +247,7 @@ std::string topo_key(const Plan<T, S>& P, const HostParams& hp, int tag, bool de
     for (size_t i = 0; i < P.steps.size(); i++)
         k += std::to_string(P.steps[i].n_items > 0) + std::to_string(P.sor_cfg[i].K) + std::to_string(P.sor_cfg[i].nbuf) +
              std::to_string(P.sor_cfg[i].ilp) + (P.steps[i].n_sor > 0 ? "t" : "") + (P.steps[i].n_units > 0 ? "s" : "") +
-             (P.steps[i].n_level > 0 ? "l" : "") + (P.steps[i].n_clus > 0 ? "c" + std::to_string(P.steps[i].clus_c) : "") + ".";
+             (P.steps[i].n_level > 0 ? "l" : "") + (P.steps[i].n_clus > 0 ? "c" + std::to_string(P.steps[i].clus_c) + "r" + std::to_string(P.steps[i].clus_kp) : "") + ".";
     const std::vector<PairSpec> none;
     return k + plan_key(none, hp, tag);
 }
