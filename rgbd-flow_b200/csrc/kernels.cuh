@@ -1691,10 +1691,11 @@ k_sor_level_reg(const LevelItem<T, S>* items, const int* which, SolveConst<T> k,
     }
     if (tid == 0) s_stop = 0;
     __syncthreads();
+    // own unknowns of the valid pixels (a thread past the level's positions reads nothing)
 #pragma unroll
     for (int color = 0; color < 2; color++)
 #pragma unroll
-        for (int v = 0; v < 3; v++) xp[color][v] = xb[v * PLS + own[color]];
+        for (int v = 0; v < 3; v++) xp[color][v] = valid[color] ? xb[v * PLS + own[color]] : (T)0;
     for (int itn = 0; itn < k.n_sor; itn++) {
         const bool chk = !k.fixed && (itn % k.period == k.period - 1);
         T md = 0;
@@ -2040,13 +2041,14 @@ k_sor_level_cluster_reg(const LevelItem<T, S>* items, const int* which, SolveCon
     }
     if (tid == 0) s_stop = 0;
     cl.sync();  // every CTA of the cluster has started and staged (its shared memory may be read)
+    // own unknowns of the valid pixels (a thread past the band's positions reads nothing)
 #pragma unroll
     for (int kp = 0; kp < KP; kp++)
 #pragma unroll
         for (int color = 0; color < 2; color++)
 #pragma unroll
             for (int v = 0; v < 3; v++)
-                xp[kp][color][v] = xb[v * PLS + ((li[kp] + 1) * 2 + color) * RP + mm[kp] + 1];
+                xp[kp][color][v] = valid[kp][color] ? xb[v * PLS + ((li[kp] + 1) * 2 + color) * RP + mm[kp] + 1] : (T)0;
     T* const up_buf = rank > 0 ? cl.map_shared_rank(xb, rank - 1) : nullptr;
     T* const dn_buf = rank < C - 1 ? cl.map_shared_rank(xb, rank + 1) : nullptr;
     for (int itn = 0; itn < k.n_sor; itn++) {
