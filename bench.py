@@ -407,6 +407,9 @@ def main():
                     help="storage type of the feature / depth pyramids in the profiling case")
     ap.add_argument("--ncu-reg", default="isotropic", choices=["isotropic", "letouzey", "hpb"],
                     help="regularisation of the profiling case")
+    ap.add_argument("--ncu-flow2d", default="", choices=["", "320x240", "640x480"],
+                    help="profiling case: one 2-D optical flow (the demo's flow type 1) of the synthetic "
+                         "pair of this size, then exit; prints no bench line")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -425,6 +428,12 @@ def main():
     torch.cuda.set_device(local)
     if args.ncu_case:
         run_ncu_case(args.ncu_case, rf, torch, args.ncu_storage, args.ncu_reg)
+        return
+    if args.ncu_flow2d:
+        p = syn.make_config_pair(args.ncu_flow2d, seed=1)
+        c = rf.Context(local)
+        c.optical_flow_2d(p["bgr1"], p["bgr2"])
+        c.close()
         return
     if world > 1:
         import datetime

@@ -286,41 +286,86 @@ __device__ __forceinline__ double sor_update(const LevelBufs& b, double alpha, i
     return cmax(fabs(dsub(nDU, prevDU)), fabs(dsub(nDV, prevDV)));
 }
 
+// The step's work table, built by warp 0: for each sweep in flight (done + 1 .. next - 1, at most
+// 64), its diagonal and first row, and the prefix count of the step's items up to it (pre[0] = 0,
+// pre[n] = the step's items).  A sweep not on a diagonal of the level this step has no items.
+__device__ __forceinline__ void sor_table(int W, int H, long long t, int done, int next, const long long* start, int D,
+                                          int ndiag, int* pre, int* dd, int* ii0)
+{
+    const int lane = threadIdx.x & 31;
+    const int n = next - (done + 1);
+    int run = 0;
+    for (int h = 0; h < 2; h++) {
+        const int l = lane + 32 * h;
+        int cnt = 0, d = 0, i0 = 0;
+        if (l < n) {
+            const long long dl = t - start[(done + 1 + l) % D];
+            if (dl >= 0 && dl < ndiag) {
+                d = (int)dl;
+                i0 = max(0, d - (W - 1));
+                cnt = min(H - 1, d) - i0 + 1;
+            }
+        }
+        int x = cnt;  // inclusive scan over the warp
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (l < n) {
+            pre[l + 1] = run + x;
+            dd[l] = d;
+            ii0[l] = i0;
+        }
+        run += __shfl_sync(0xffffffffu, x, 31);
+    }
+    if (lane == 0) pre[0] = 0;
+}
+
 // One step of the overlapping sweeps: for every sweep in flight, the pixels of its current
 // diagonal.  The step's updates are flattened into one list spread over the G threads (thread g
 // takes items g, g + G, ...), so the memory latency of the sweeps' updates overlaps across threads
-// instead of adding up sweep after sweep.  Every update reads only values no other update of the
-// step writes (the diagonal structure), so the order within the step is free.
+// instead of adding up sweep after sweep; an item finds its sweep in the step's table by binary
+// search.  Every update reads only values no other update of the step writes (the diagonal
+// structure), so the order within the step is free.
 template <bool CG>
-__device__ __forceinline__ void sor_step(const LevelBufs& b, double alpha, long long t, int done, int next,
-                                         const long long* start, int D, int ndiag, size_t N, double* ring_u,
+__device__ __forceinline__ void sor_step(const LevelBufs& b, double alpha, int done, int next, const int* pre,
+                                         const int* dd, const int* ii0, int D, size_t N, double* ring_u,
                                          double* ring_v, unsigned long long* maxd, int g, int G)
 {
-    const int W = b.W, H = b.H;
-    int total = 0;
-    for (int s = done + 1; s < next; s++) {
-        const long long d = t - start[s % D];
-        if (d < 0 || d >= ndiag) continue;
-        total += (int)(min((long long)H - 1, d) - max(0LL, d - (W - 1)) + 1);
-    }
-    for (int k = g; k < total; k += G) {
-        int s = done + 1, rem = k, i0 = 0;
-        long long d = 0;
-        for (; s < next; s++) {  // the sweep of item k (k < total: always found)
-            d = t - start[s % D];
-            if (d < 0 || d >= ndiag) continue;
-            i0 = (int)max(0LL, d - (W - 1));
-            const int cnt = (int)(min((long long)H - 1, d) - i0 + 1);
-            if (rem < cnt) break;
-            rem -= cnt;
+    const int n = next - (done + 1);
+    const int total = n > 0 ? pre[n] : 0;
+    // whole warps iterate together (item k = kb + lane), so the sweeps' maxima can be combined
+    // per warp before the shared atomics
+    const int lane = threadIdx.x & 31;
+    for (int kb = g - lane; kb < total; kb += G) {
+        const int k = kb + lane;
+        int slot = -1;
+        unsigned long long bits = 0;
+        if (k < total) {
+            int lo = 0, hi = n - 1;  // the sweep l with pre[l] <= k < pre[l + 1]
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (pre[mid + 1] > k) hi = mid;
+                else lo = mid + 1;
+            }
+            const int s = done + 1 + lo;
+            const int i = ii0[lo] + (k - pre[lo]);
+            const int cur = s % D, prv = (s + D - 1) % D;
+            double* wu = ring_u + (size_t)cur * N;
+            double* wv = ring_v + (size_t)cur * N;
+            const double m = sor_update<CG>(b, alpha, i, dd[lo] - i, wu, wv, ring_u + (size_t)prv * N,
+                                            ring_v + (size_t)prv * N, wu, wv);
+            if (m == m) {  // NaN is skipped, as std::max skips it
+                slot = cur;
+                bits = (unsigned long long)__double_as_longlong(m);  // ordered as the value (m >= 0)
+            }
         }
-        const int i = i0 + rem;
-        const int cur = s % D, prv = (s + D - 1) % D;
-        double* wu = ring_u + (size_t)cur * N;
-        double* wv = ring_v + (size_t)cur * N;
-        const double m = sor_update<CG>(b, alpha, i, (int)(d - i), wu, wv, ring_u + (size_t)prv * N,
-                                        ring_v + (size_t)prv * N, wu, wv);
-        if (m == m) atomicMax(&maxd[s % D], (unsigned long long)__double_as_longlong(m));  // NaN is skipped, as std::max skips it
+        // the largest change of each sweep among the warp's items (exact: the maximum of the
+        // 64-bit patterns, high word first), then one shared atomic per sweep and warp
+        const unsigned peers = __match_any_sync(0xffffffffu, slot);
+        const unsigned hi = __reduce_max_sync(peers, (unsigned)(bits >> 32));
+        const unsigned lo = __reduce_max_sync(peers, (unsigned)(bits >> 32) == hi ? (unsigned)bits : 0u);
+        if (slot >= 0 && lane == __ffs(peers) - 1) atomicMax(&maxd[slot], ((unsigned long long)hi << 32) | lo);
     }
 }
 
@@ -336,6 +381,7 @@ __global__ void __launch_bounds__(kSorThreads) k_sor_wavefront(LevelBufs b, doub
     __shared__ long long start[kMaxRing];
     __shared__ unsigned long long maxd[kMaxRing];
     __shared__ int s_done, s_stop, s_next;
+    __shared__ int pre[kMaxRing + 1], dd[kMaxRing], ii0[kMaxRing];
     for (size_t p = threadIdx.x; p < N; p += blockDim.x) {
         ring_u[(size_t)(D - 1) * N + p] = 0;
         ring_v[(size_t)(D - 1) * N + p] = 0;
@@ -357,7 +403,9 @@ __global__ void __launch_bounds__(kSorThreads) k_sor_wavefront(LevelBufs b, doub
         __syncthreads();
         const int done = s_done, next = s_next;
         if (s_stop >= 0 || done >= nSOR - 1) break;
-        sor_step<false>(b, alpha, t, done, next, start, D, ndiag, N, ring_u, ring_v, maxd, threadIdx.x, blockDim.x);
+        if (threadIdx.x < 32) sor_table(W, H, t, done, next, start, D, ndiag, pre, dd, ii0);
+        __syncthreads();
+        sor_step<false>(b, alpha, done, next, pre, dd, ii0, D, N, ring_u, ring_v, maxd, threadIdx.x, blockDim.x);
         __syncthreads();
         if (threadIdx.x == 0) {
             while (s_done + 1 < s_next && t - start[(s_done + 1) % D] == ndiag - 1) {
@@ -406,6 +454,7 @@ __global__ void __launch_bounds__(kSorThreads) k_sor_wavefront_cluster(LevelBufs
     __shared__ long long fin[kMaxRingC];  // the step at which the sweep in each slot completed
     __shared__ unsigned long long maxd[kMaxRingC];
     __shared__ int s_done, s_stop, s_next;
+    __shared__ int pre[kMaxRingC + 1], dd[kMaxRingC], ii0[kMaxRingC];
     if (threadIdx.x < kMaxRingC) fin[threadIdx.x] = -1;
     for (size_t p = g; p < N; p += G) {
         ring_u[(size_t)(D - 1) * N + p] = 0;
@@ -431,9 +480,10 @@ __global__ void __launch_bounds__(kSorThreads) k_sor_wavefront_cluster(LevelBufs
         __syncthreads();
         const int done = s_done, next = s_next;
         if (s_stop >= 0 || done >= nSOR - 1) break;  // the same in every CTA
-        sor_step<true>(b, alpha, t, done, next, start, D, ndiag, N, ring_u, ring_v, maxd, g, G);
-        __threadfence();
-        cl.sync();  // this step's updates are done and visible in every CTA
+        if (threadIdx.x < 32) sor_table(W, H, t, done, next, start, D, ndiag, pre, dd, ii0);
+        __syncthreads();
+        sor_step<true>(b, alpha, done, next, pre, dd, ii0, D, N, ring_u, ring_v, maxd, g, G);
+        cl.sync();  // this step's updates are done and visible in every CTA (release / acquire at cluster scope)
         if (threadIdx.x == 0) {
             while (s_done + 1 < s_next && t - start[(s_done + 1) % D] == ndiag - 1) {
                 s_done++;
