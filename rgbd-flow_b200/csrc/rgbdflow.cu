@@ -807,7 +807,7 @@ static void run_flow2d(rgbdflow_ctx* c, const uint8_t* bgr1, const uint8_t* bgr2
     // flight (the flow does not depend on it)
     const char* ce = std::getenv("RGBDFLOW_FLOW2D_CLUSTER_MIN_PX");
     const long clus_min_px = ce ? std::atol(ce) : 4096L;
-    constexpr int kClusterCtas = 8, kClusterRing = 32;
+    constexpr int kClusterCtas = 8, kClusterRing = 64;
     const int ring_slots = std::max(prm.sor_ring, (long)N0 >= clus_min_px ? kClusterRing : 0);
     const size_t o_ring_u = reserve((size_t)ring_slots * N0 * sizeof(double));
     const size_t o_ring_v = reserve((size_t)ring_slots * N0 * sizeof(double));
