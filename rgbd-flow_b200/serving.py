@@ -32,9 +32,10 @@ def frame_index(t, n_unique):
 
 def simulate(server, rf, streams, n_frames=300, fps=30.0, seed=0, time_scale=1.0, keep_stream=None, keep_n=0):
     """Submit n_frames per stream at `fps` (exponential inter-arrival times, mean 1/fps) and
-    collect every result.  Returns dict(latencies_ms, pairs, wall_s, kept, host) where kept holds
-    up to keep_n (frame index, flow) results of stream keep_stream and host the longest host times
-    (ms) of one loop iteration (its sleep excluded), one submit call and one step call."""
+    collect every result.  Returns dict(latencies_ms, pairs, wall_s, kept, host, span_s) where kept
+    holds up to keep_n (frame index, flow) results of stream keep_stream, host the longest host
+    times (ms) of one loop iteration (its sleep excluded), one submit call and one step call, and
+    span_s the time of the last arrival."""
     rng = np.random.default_rng(seed)
     arrivals = []
     for s, seq in enumerate(streams):
@@ -79,4 +80,5 @@ def simulate(server, rf, streams, n_frames=300, fps=30.0, seed=0, time_scale=1.0
             if nxt > 0:
                 time.sleep(min(nxt, 0.0005))
     wall = time.perf_counter() - t0
-    return dict(latencies_ms=lat, pairs=done, wall_s=wall, kept=kept, host=host)
+    return dict(latencies_ms=lat, pairs=done, wall_s=wall, kept=kept, host=host,
+                span_s=arrivals[-1][0] if arrivals else 0.0)
