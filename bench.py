@@ -229,7 +229,7 @@ def run_served_sweep(ctx, rf, serving, base, prm, warm, points, seconds=2.0, max
         srv.close()
         lat = np.array(r["latencies_ms"])
         pt = {"streams": n_streams, "fps": fps, "arrivals_per_s": r["pairs"] / max(r["span_s"], 1e-9),
-              "pairs_per_s": r["pairs"] / r["wall_s"],
+              "pairs_per_s": r["pairs"] / r["wall_s"], "wall_s": r["wall_s"], "span_s": r["span_s"],
               "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99))}
         pts.append(pt)
         if pt["p99_ms"] < 33.0 and (best is None or pt["arrivals_per_s"] > best["arrivals_per_s"]):

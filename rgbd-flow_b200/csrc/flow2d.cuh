@@ -166,6 +166,8 @@ struct LevelBufs {
     double* warp;           // frame 2 features warped by the flow (5 channels)
     double *u, *v, *du, *dv, *phi;
     double *dxy, *dx2, *dy2, *dtdx, *dtdy;
+    double* coef;  // the SOR's per-pixel coefficients packed, 8 doubles a pixel: dxy, dx2, dy2,
+                   // dtdx, dtdy, phi (written by k_rhs; read-only during the SOR)
     int W, H;
 };
 
@@ -247,42 +249,62 @@ __global__ void k_rhs(LevelBufs b, double alpha)
     const size_t n = (size_t)W * H;
     for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n; p += (size_t)gridDim.x * blockDim.x) {
         const int i = (int)(p / W), j = (int)(p % W);
-        b.dtdx[p] = dsub(-b.dtdx[p], dmul(alpha, laplacian_phi(b.u, b.phi, W, H, i, j)));
-        b.dtdy[p] = dsub(-b.dtdy[p], dmul(alpha, laplacian_phi(b.v, b.phi, W, H, i, j)));
+        const double tx = dsub(-b.dtdx[p], dmul(alpha, laplacian_phi(b.u, b.phi, W, H, i, j)));
+        const double ty = dsub(-b.dtdy[p], dmul(alpha, laplacian_phi(b.v, b.phi, W, H, i, j)));
+        b.dtdx[p] = tx;
+        b.dtdy[p] = ty;
+        double4* c = reinterpret_cast<double4*>(b.coef + p * 8);
+        c[0] = make_double4(b.dxy[p], b.dx2[p], b.dy2[p], tx);
+        c[1] = make_double4(ty, b.phi[p], 0.0, 0.0);
     }
 }
 
-// One SOR update (SmoothFlowSOR.cpp:166-215) of pixel (i, j): left / upper neighbours new
-// (nu, nv), right / lower neighbours and the pixel itself old (ou, ov); returns the change.
+// One SOR update (SmoothFlowSOR.cpp:166-215) of pixel (i, j): left / upper neighbours new (this
+// sweep's ring slot nw), right / lower neighbours and the pixel itself old (the previous sweep's
+// slot ow); a slot holds (du, dv) pairs.  Writes the new pair to nw and returns the change.
 template <bool CG = false>
-__device__ __forceinline__ double sor_update(const LevelBufs& b, double alpha, int i, int j, const double* nu_,
-                                             const double* nv_, const double* ou_, const double* ov_, double* wu,
-                                             double* wv)
+__device__ __forceinline__ double sor_update(const LevelBufs& b, double alpha, int i, int j, double2* nw,
+                                             const double2* ow)
 {
     // CG: the ring is written by other CTAs of a cluster; its values are read from L2
-    struct R {
-        const double* p;
-        __device__ __forceinline__ double operator[](size_t o) const { return CG ? __ldcg(p + o) : p[o]; }
-    };
-    const R nu{nu_}, nv{nv_}, ou{ou_}, ov{ov_};
+    auto R = [](const double2* p) { return CG ? __ldcg(p) : *p; };
     const int W = b.W, H = b.H;
     const size_t o = (size_t)i * W + j;
     const double omega = 1.8;
+    const double4 c0 = *reinterpret_cast<const double4*>(b.coef + o * 8);            // dxy, dx2, dy2, dtdx
+    const double2 c1 = __ldg(reinterpret_cast<const double2*>(b.coef + o * 8 + 4));  // dtdy, phi
+    const double phi = c1.y;
     double sigmaU = 0, sigmaV = 0, weightSum = 0, w;
-    if (j > 0) { w = b.phi[o - 1]; sigmaU = dadd(sigmaU, dmul(w, nu[o - 1])); sigmaV = dadd(sigmaV, dmul(w, nv[o - 1])); weightSum = dadd(weightSum, w); }
-    if (j < W - 1) { w = b.phi[o]; sigmaU = dadd(sigmaU, dmul(w, ou[o + 1])); sigmaV = dadd(sigmaV, dmul(w, ov[o + 1])); weightSum = dadd(weightSum, w); }
-    if (i > 0) { w = b.phi[o - W]; sigmaU = dadd(sigmaU, dmul(w, nu[o - W])); sigmaV = dadd(sigmaV, dmul(w, nv[o - W])); weightSum = dadd(weightSum, w); }
-    if (i < H - 1) { w = b.phi[o]; sigmaU = dadd(sigmaU, dmul(w, ou[o + W])); sigmaV = dadd(sigmaV, dmul(w, ov[o + W])); weightSum = dadd(weightSum, w); }
+    if (j > 0) {
+        w = __ldg(b.coef + (o - 1) * 8 + 5);
+        const double2 x = R(nw + o - 1);
+        sigmaU = dadd(sigmaU, dmul(w, x.x)); sigmaV = dadd(sigmaV, dmul(w, x.y)); weightSum = dadd(weightSum, w);
+    }
+    if (j < W - 1) {
+        w = phi;
+        const double2 x = R(ow + o + 1);
+        sigmaU = dadd(sigmaU, dmul(w, x.x)); sigmaV = dadd(sigmaV, dmul(w, x.y)); weightSum = dadd(weightSum, w);
+    }
+    if (i > 0) {
+        w = __ldg(b.coef + (o - W) * 8 + 5);
+        const double2 x = R(nw + o - W);
+        sigmaU = dadd(sigmaU, dmul(w, x.x)); sigmaV = dadd(sigmaV, dmul(w, x.y)); weightSum = dadd(weightSum, w);
+    }
+    if (i < H - 1) {
+        w = phi;
+        const double2 x = R(ow + o + W);
+        sigmaU = dadd(sigmaU, dmul(w, x.x)); sigmaV = dadd(sigmaV, dmul(w, x.y)); weightSum = dadd(weightSum, w);
+    }
     sigmaU = dmul(sigmaU, -alpha);
     sigmaV = dmul(sigmaV, -alpha);
     weightSum = dmul(weightSum, alpha);
-    const double prevDU = ou[o], prevDV = ov[o];
-    sigmaU = dadd(sigmaU, dmul(b.dxy[o], prevDV));
-    const double nDU = dadd(dmul(1 - omega, prevDU), dmul(ddiv(omega, dadd(b.dx2[o], weightSum)), dsub(b.dtdx[o], sigmaU)));
-    sigmaV = dadd(sigmaV, dmul(b.dxy[o], nDU));
-    const double nDV = dadd(dmul(1 - omega, prevDV), dmul(ddiv(omega, dadd(b.dy2[o], weightSum)), dsub(b.dtdy[o], sigmaV)));
-    wu[o] = nDU;
-    wv[o] = nDV;
+    const double2 prev = R(ow + o);
+    const double prevDU = prev.x, prevDV = prev.y;
+    sigmaU = dadd(sigmaU, dmul(c0.x, prevDV));
+    const double nDU = dadd(dmul(1 - omega, prevDU), dmul(ddiv(omega, dadd(c0.y, weightSum)), dsub(c0.w, sigmaU)));
+    sigmaV = dadd(sigmaV, dmul(c0.x, nDU));
+    const double nDV = dadd(dmul(1 - omega, prevDV), dmul(ddiv(omega, dadd(c0.z, weightSum)), dsub(c1.x, sigmaV)));
+    nw[o] = make_double2(nDU, nDV);
     return cmax(fabs(dsub(nDU, prevDU)), fabs(dsub(nDV, prevDV)));
 }
 
@@ -329,8 +351,8 @@ __device__ __forceinline__ void sor_table(int W, int H, long long t, int done, i
 // structure), so the order within the step is free.
 template <bool CG>
 __device__ __forceinline__ void sor_step(const LevelBufs& b, double alpha, int done, int next, const int* pre,
-                                         const int* dd, const int* ii0, int D, size_t N, double* ring_u,
-                                         double* ring_v, unsigned long long* maxd, int g, int G)
+                                         const int* dd, const int* ii0, int D, size_t N, double2* ring,
+                                         unsigned long long* maxd, int g, int G)
 {
     const int n = next - (done + 1);
     const int total = n > 0 ? pre[n] : 0;
@@ -351,10 +373,7 @@ __device__ __forceinline__ void sor_step(const LevelBufs& b, double alpha, int d
             const int s = done + 1 + lo;
             const int i = ii0[lo] + (k - pre[lo]);
             const int cur = s % D, prv = (s + D - 1) % D;
-            double* wu = ring_u + (size_t)cur * N;
-            double* wv = ring_v + (size_t)cur * N;
-            const double m = sor_update<CG>(b, alpha, i, dd[lo] - i, wu, wv, ring_u + (size_t)prv * N,
-                                            ring_v + (size_t)prv * N, wu, wv);
+            const double m = sor_update<CG>(b, alpha, i, dd[lo] - i, ring + (size_t)cur * N, ring + (size_t)prv * N);
             if (m == m) {  // NaN is skipped, as std::max skips it
                 slot = cur;
                 bits = (unsigned long long)__double_as_longlong(m);  // ordered as the value (m >= 0)
@@ -374,7 +393,7 @@ __device__ __forceinline__ void sor_step(const LevelBufs& b, double alpha, int d
 // last sweep's increments (the first that converged, max change < 1e-5, or sweep nSOR - 1) in
 // (du, dv) and the number of sweeps run in *sweeps.  status: 0, or 1 when the step bound ran out.
 __global__ void __launch_bounds__(kSorThreads) k_sor_wavefront(LevelBufs b, double alpha, int nSOR, int D,
-                                                               double* ring_u, double* ring_v, int* sweeps, int* status)
+                                                               double2* ring, int* sweeps, int* status)
 {
     const int W = b.W, H = b.H, ndiag = W + H - 1, lag = 2;
     const size_t N = (size_t)W * H;
@@ -383,8 +402,7 @@ __global__ void __launch_bounds__(kSorThreads) k_sor_wavefront(LevelBufs b, doub
     __shared__ int s_done, s_stop, s_next;
     __shared__ int pre[kMaxRing + 1], dd[kMaxRing], ii0[kMaxRing];
     for (size_t p = threadIdx.x; p < N; p += blockDim.x) {
-        ring_u[(size_t)(D - 1) * N + p] = 0;
-        ring_v[(size_t)(D - 1) * N + p] = 0;
+        ring[(size_t)(D - 1) * N + p] = make_double2(0.0, 0.0);
     }
     if (threadIdx.x == 0) { s_done = -1; s_stop = -1; s_next = 0; }
     __syncthreads();
@@ -405,7 +423,7 @@ __global__ void __launch_bounds__(kSorThreads) k_sor_wavefront(LevelBufs b, doub
         if (s_stop >= 0 || done >= nSOR - 1) break;
         if (threadIdx.x < 32) sor_table(W, H, t, done, next, start, D, ndiag, pre, dd, ii0);
         __syncthreads();
-        sor_step<false>(b, alpha, done, next, pre, dd, ii0, D, N, ring_u, ring_v, maxd, threadIdx.x, blockDim.x);
+        sor_step<false>(b, alpha, done, next, pre, dd, ii0, D, N, ring, maxd, threadIdx.x, blockDim.x);
         __syncthreads();
         if (threadIdx.x == 0) {
             while (s_done + 1 < s_next && t - start[(s_done + 1) % D] == ndiag - 1) {
@@ -424,8 +442,9 @@ __global__ void __launch_bounds__(kSorThreads) k_sor_wavefront(LevelBufs b, doub
     }
     const int last = (s_stop >= 0 ? s_stop : nSOR - 1) % D;
     for (size_t p = threadIdx.x; p < N; p += blockDim.x) {
-        b.du[p] = ring_u[(size_t)last * N + p];
-        b.dv[p] = ring_v[(size_t)last * N + p];
+        const double2 x = ring[(size_t)last * N + p];
+        b.du[p] = x.x;
+        b.dv[p] = x.y;
     }
 }
 
@@ -441,7 +460,7 @@ __global__ void __launch_bounds__(kSorThreads) k_sor_wavefront(LevelBufs b, doub
 constexpr int kMaxRingC = 64;
 
 __global__ void __launch_bounds__(kSorThreads) k_sor_wavefront_cluster(LevelBufs b, double alpha, int nSOR, int D,
-                                                                       double* ring_u, double* ring_v, int* sweeps,
+                                                                       double2* ring, int* sweeps,
                                                                        int* status)
 {
     namespace cg = cooperative_groups;
@@ -457,8 +476,7 @@ __global__ void __launch_bounds__(kSorThreads) k_sor_wavefront_cluster(LevelBufs
     __shared__ int pre[kMaxRingC + 1], dd[kMaxRingC], ii0[kMaxRingC];
     if (threadIdx.x < kMaxRingC) fin[threadIdx.x] = -1;
     for (size_t p = g; p < N; p += G) {
-        ring_u[(size_t)(D - 1) * N + p] = 0;
-        ring_v[(size_t)(D - 1) * N + p] = 0;
+        ring[(size_t)(D - 1) * N + p] = make_double2(0.0, 0.0);
     }
     if (threadIdx.x == 0) { s_done = -1; s_stop = -1; s_next = 0; }
     __threadfence();
@@ -482,7 +500,7 @@ __global__ void __launch_bounds__(kSorThreads) k_sor_wavefront_cluster(LevelBufs
         if (s_stop >= 0 || done >= nSOR - 1) break;  // the same in every CTA
         if (threadIdx.x < 32) sor_table(W, H, t, done, next, start, D, ndiag, pre, dd, ii0);
         __syncthreads();
-        sor_step<true>(b, alpha, done, next, pre, dd, ii0, D, N, ring_u, ring_v, maxd, g, G);
+        sor_step<true>(b, alpha, done, next, pre, dd, ii0, D, N, ring, maxd, g, G);
         cl.sync();  // this step's updates are done and visible in every CTA (release / acquire at cluster scope)
         if (threadIdx.x == 0) {
             while (s_done + 1 < s_next && t - start[(s_done + 1) % D] == ndiag - 1) {
@@ -505,8 +523,9 @@ __global__ void __launch_bounds__(kSorThreads) k_sor_wavefront_cluster(LevelBufs
     }
     const int last = (s_stop >= 0 ? s_stop : nSOR - 1) % D;
     for (size_t p = g; p < N; p += G) {
-        b.du[p] = __ldcg(ring_u + (size_t)last * N + p);
-        b.dv[p] = __ldcg(ring_v + (size_t)last * N + p);
+        const double2 x = __ldcg(ring + (size_t)last * N + p);
+        b.du[p] = x.x;
+        b.dv[p] = x.y;
     }
 }
 

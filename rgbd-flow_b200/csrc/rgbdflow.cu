@@ -809,8 +809,8 @@ static void run_flow2d(rgbdflow_ctx* c, const uint8_t* bgr1, const uint8_t* bgr2
     const long clus_min_px = ce ? std::atol(ce) : 4096L;
     constexpr int kClusterCtas = 8, kClusterRing = 64;
     const int ring_slots = std::max(prm.sor_ring, (long)N0 >= clus_min_px ? kClusterRing : 0);
-    const size_t o_ring_u = reserve((size_t)ring_slots * N0 * sizeof(double));
-    const size_t o_ring_v = reserve((size_t)ring_slots * N0 * sizeof(double));
+    const size_t o_ring = reserve((size_t)ring_slots * N0 * sizeof(double2));  // (du, dv) pairs per sweep slot
+    const size_t o_coef = reserve(N0 * 8 * sizeof(double));
     if (c->budget && total > c->budget) throw ArgError(RGBDFLOW_ERR_BUDGET, "2-D flow needs " + std::to_string(total) + " device bytes");
     RF_CUDA(cudaSetDevice(c->device));
     cudaStream_t st = c->stream;
@@ -867,6 +867,7 @@ static void run_flow2d(rgbdflow_ctx* c, const uint8_t* bgr1, const uint8_t* bgr2
         b.dy2 = D(o_plane[5]);
         b.dtdx = D(o_plane[6]);
         b.dtdy = D(o_plane[7]);
+        b.coef = D(o_coef);
         b.W = w;
         b.H = h;
         if (k == L - 1) {
@@ -903,9 +904,9 @@ static void run_flow2d(rgbdflow_ctx* c, const uint8_t* bgr1, const uint8_t* bgr2
                     cfg.attrs = at;
                     cfg.numAttrs = 1;
                     RF_CUDA(cudaLaunchKernelEx(&cfg, k_sor_wavefront_cluster, b, prm.alpha, nSOR, kClusterRing,
-                                               D(o_ring_u), D(o_ring_v), ctl + 1, ctl));
+                                               (double2*)(base + o_ring), ctl + 1, ctl));
                 } else {
-                    k_sor_wavefront<<<1, kSorThreads, 0, st>>>(b, prm.alpha, nSOR, prm.sor_ring, D(o_ring_u), D(o_ring_v),
+                    k_sor_wavefront<<<1, kSorThreads, 0, st>>>(b, prm.alpha, nSOR, prm.sor_ring, (double2*)(base + o_ring),
                                                                ctl + 1, ctl);
                 }
                 launches += 3;

@@ -46,11 +46,12 @@ def simulate(server, rf, streams, n_frames=300, fps=30.0, seed=0, time_scale=1.0
     arrivals.sort()
     cams = [rf.CameraParams.make(seq["W"], seq["H"], seq["cam"].f, seq["cam"].cx, seq["cam"].cy) for seq in streams]
     lat, done, kept = [], 0, []
-    expected = len(streams) * (n_frames - 1)
     host = dict(iter_ms=0.0, submit_ms=0.0, step_ms=0.0)
     t0 = time.perf_counter()
     i = 0
-    while done < expected:
+    # until every frame has arrived and every pair it formed has been returned (a stream that the
+    # server already knows pairs its first frame here with its last frame of an earlier run)
+    while i < len(arrivals) or server.pending() > 0:
         t_iter = time.perf_counter()
         now = t_iter - t0
         while i < len(arrivals) and arrivals[i][0] <= now:
