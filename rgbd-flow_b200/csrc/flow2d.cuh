@@ -410,19 +410,22 @@ __global__ void __launch_bounds__(kSorThreads) k_sor_wavefront(LevelBufs b, doub
     const long long t_max = (long long)nSOR * (ndiag + lag) + ndiag + 8;
     long long t = 0;
     for (; t < t_max; t++) {
-        if (threadIdx.x == 0) {
-            const int nx = s_next;
-            if (nx < nSOR && (nx == 0 || t >= start[(nx - 1) % D] + lag) && (nx < D || s_done >= nx - D)) {
-                start[nx % D] = t;
-                maxd[nx % D] = 0ull;
-                s_next = nx + 1;
+        if (threadIdx.x < 32) {
+            // warp 0: the step's new sweep (lane 0), then the step's table
+            if (threadIdx.x == 0) {
+                const int nx = s_next;
+                if (nx < nSOR && (nx == 0 || t >= start[(nx - 1) % D] + lag) && (nx < D || s_done >= nx - D)) {
+                    start[nx % D] = t;
+                    maxd[nx % D] = 0ull;
+                    s_next = nx + 1;
+                }
             }
+            __syncwarp();
+            sor_table(W, H, t, s_done, s_next, start, D, ndiag, pre, dd, ii0);
         }
         __syncthreads();
         const int done = s_done, next = s_next;
         if (s_stop >= 0 || done >= nSOR - 1) break;
-        if (threadIdx.x < 32) sor_table(W, H, t, done, next, start, D, ndiag, pre, dd, ii0);
-        __syncthreads();
         sor_step<false>(b, alpha, done, next, pre, dd, ii0, D, N, ring, maxd, threadIdx.x, blockDim.x);
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -484,22 +487,25 @@ __global__ void __launch_bounds__(kSorThreads) k_sor_wavefront_cluster(LevelBufs
     const long long t_max = (long long)nSOR * (ndiag + lag) + ndiag + 8;
     long long t = 0;
     for (; t < t_max; t++) {
-        if (threadIdx.x == 0) {
-            // a slot is reused one step after its sweep completed: other CTAs may read its partial
-            // maximum during the completion step, up to their next cluster barrier
-            const int nx = s_next;
-            if (nx < nSOR && (nx == 0 || t >= start[(nx - 1) % D] + lag) &&
-                (nx < D || (s_done >= nx - D && fin[nx % D] < t - 1))) {
-                start[nx % D] = t;
-                maxd[nx % D] = 0ull;
-                s_next = nx + 1;
+        if (threadIdx.x < 32) {
+            // warp 0: the step's new sweep (lane 0), then the step's table.  A slot is reused one
+            // step after its sweep completed: other CTAs may read its partial maximum during the
+            // completion step, up to their next cluster barrier
+            if (threadIdx.x == 0) {
+                const int nx = s_next;
+                if (nx < nSOR && (nx == 0 || t >= start[(nx - 1) % D] + lag) &&
+                    (nx < D || (s_done >= nx - D && fin[nx % D] < t - 1))) {
+                    start[nx % D] = t;
+                    maxd[nx % D] = 0ull;
+                    s_next = nx + 1;
+                }
             }
+            __syncwarp();
+            sor_table(W, H, t, s_done, s_next, start, D, ndiag, pre, dd, ii0);
         }
         __syncthreads();
         const int done = s_done, next = s_next;
         if (s_stop >= 0 || done >= nSOR - 1) break;  // the same in every CTA
-        if (threadIdx.x < 32) sor_table(W, H, t, done, next, start, D, ndiag, pre, dd, ii0);
-        __syncthreads();
         sor_step<true>(b, alpha, done, next, pre, dd, ii0, D, N, ring, maxd, g, G);
         cl.sync();  // this step's updates are done and visible in every CTA (release / acquire at cluster scope)
         if (threadIdx.x == 0) {

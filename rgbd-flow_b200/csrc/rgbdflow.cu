@@ -807,7 +807,34 @@ static void run_flow2d(rgbdflow_ctx* c, const uint8_t* bgr1, const uint8_t* bgr2
     // flight (the flow does not depend on it)
     const char* ce = std::getenv("RGBDFLOW_FLOW2D_CLUSTER_MIN_PX");
     const long clus_min_px = ce ? std::atol(ce) : 4096L;
-    constexpr int kClusterCtas = 8, kClusterRing = 64;
+    constexpr int kClusterRing = 64;
+    // the cluster: 16 CTAs where the device can co-schedule them (a non-portable size), else 8
+    static int clus_ctas = 0;
+    if (!clus_ctas) {
+        const char* cc = std::getenv("RGBDFLOW_FLOW2D_CLUSTER_CTAS");
+        int want = cc ? std::atoi(cc) : 16;
+        want = want >= 16 ? 16 : 8;
+        if (want == 16) {
+            RF_CUDA(cudaFuncSetAttribute(k_sor_wavefront_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+            cudaLaunchConfig_t q = {};
+            q.gridDim = dim3(16);
+            q.blockDim = dim3(kSorThreads);
+            cudaLaunchAttribute qa[1];
+            qa[0].id = cudaLaunchAttributeClusterDimension;
+            qa[0].val.clusterDim.x = 16;
+            qa[0].val.clusterDim.y = 1;
+            qa[0].val.clusterDim.z = 1;
+            q.attrs = qa;
+            q.numAttrs = 1;
+            int nc = 0;
+            if (cudaOccupancyMaxActiveClusters(&nc, k_sor_wavefront_cluster, &q) != cudaSuccess || nc < 1) {
+                cudaGetLastError();
+                want = 8;
+            }
+        }
+        clus_ctas = want;
+    }
+    const int kClusterCtas = clus_ctas;
     const int ring_slots = std::max(prm.sor_ring, (long)N0 >= clus_min_px ? kClusterRing : 0);
     const size_t o_ring = reserve((size_t)ring_slots * N0 * sizeof(double2));  // (du, dv) pairs per sweep slot
     const size_t o_coef = reserve(N0 * 8 * sizeof(double));
