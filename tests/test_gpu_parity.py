@@ -254,7 +254,7 @@ def test_every_tunable_sor_choice_agrees_bitwise(ctx, monkeypatch):
     print("autotuned:", rf.autotune_describe(0))
     assert rf.autotune_describe(0)
     configs = [dict(K=K, ilp=ilp) for K in (2, 3, 4, 5, 6) for ilp in (1, 2)]
-    configs += [dict(K=5, seg=seg) for seg in (64, 128, 192, 256)]
+    configs += [dict(K=5, seg=seg) for seg in (32, 64, 128, 192, 256)]
     for c in configs:
         q = rf.benchmark_params(320)
         q.min_width = -16
