@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <stdexcept>
 #include <string>
@@ -139,6 +140,7 @@ struct HostParams {
     int sor_strip;          // strip SOR for large FP32 levels (0: tiles everywhere)
     int strip_min_w, strip_min_h, strip_seg;  // strip eligibility and band height (0: automatic)
     long strip_min_px;                        // strips only for steps with this many eligible pixels
+    int strip_balanced;                       // untuned strip steps take the balancing model's bands
     int sor_level;                            // whole-level SOR for levels that fit one CTA (0: off)
     int level_cluster;                        // > 1: such levels run on a cluster of this many CTAs instead
     int level_reg;                            // FP32 whole-level SOR with the system in registers (0: off)
@@ -180,11 +182,14 @@ static inline SorConfig choose_sor_config(const HostParams& hp, long level_px)
 // The SOR configuration chosen for one level step by the autotuner (rgbdflow.cu, tune_sor): kernel
 // (tile or strip), sweeps per launch, lane mapping, strip band height.  The choice changes speed
 // only: every configuration gives the same flow bit for bit.
+// Strip SOR band layouts by strip height: the band heights of a strip, top to bottom.
+using BandMap = std::vector<std::pair<int, std::vector<int>>>;
 struct SorChoice {
     int strip = 0;   // strip kernel for the step's strip-eligible items
     int K = 5;       // sweeps per launch
     int ilp = 2;     // tile kernel lane mapping
     int seg = 0;     // strip band height (0: automatic)
+    BandMap bands;   // explicit band layouts (strip_balanced_bands); strips of other heights use seg
     double us_per_it = 0;  // measured time per SOR iteration of the step
 };
 struct TuneTable {
@@ -213,7 +218,8 @@ static std::string sor_step_key(const std::vector<X>& items)
 static inline bool sor_tunable(const HostParams& hp)
 {
     return hp.K == 0 && hp.sor_ilp == 0 && hp.sor_nbuf == 0 && hp.sor_strip == 1 && hp.strip_min_w == 0 &&
-           hp.strip_min_h == 0 && hp.strip_seg == 0 && hp.strip_min_px == 0 && hp.level_cluster == 0;
+           hp.strip_min_h == 0 && hp.strip_seg == 0 && hp.strip_min_px == 0 && hp.strip_balanced == 0 &&
+           hp.level_cluster == 0;
 }
 
 // Items the autotuner may put on the strip kernel (FP32, at least two strips wide and two bands high).
@@ -240,9 +246,32 @@ static inline bool use_strip(const HostParams& hp, int W, int H)
 // about four units per SM over the step, so units of pairs that finish early leave no SM idle
 // for long, and at no fewer than 64 rows, so the pipeline fill stays a small share.  Units are
 // ordered band-major, then strip, then item: consecutive tickets spread over the pairs.
+// Bands of seg rows from the top; the rest of the strip (or, when seg divides it, its last band) in
+// smaller bands, 2^k x 32 rows largest first, the last one reaching the bottom.  The units are
+// handed out largest first, so the small bands fill the last wave: the SMs finish closer together
+// than with equal bands.  Returns the band heights, top to bottom.
+static std::vector<int> strip_default_bands(int H, int seg)
+{
+    std::vector<int> bl;
+    int n = H / seg, rem = H - n * seg;
+    if (rem == 0 && n >= 2) { n--; rem = seg; }
+    for (int b = 0; b < n; b++) bl.push_back(seg);
+    while (rem > 0) {
+        int piece = rem;
+        if (rem >= 64) {
+            int p2 = 32;
+            while (p2 * 2 <= rem) p2 *= 2;
+            if (rem - p2 >= 32) piece = p2;
+        }
+        bl.push_back(piece);
+        rem -= piece;
+    }
+    return bl;
+}
+
 template <class X>
 static std::vector<StripUnit> strip_units(const std::vector<X>& items, const std::vector<int>& which,
-                                          const HostParams& hp, int sms)
+                                          const HostParams& hp, int sms, const BandMap* layouts = nullptr)
 {
     std::vector<StripUnit> v;
     if (which.empty()) return v;
@@ -255,27 +284,15 @@ static std::vector<StripUnit> strip_units(const std::vector<X>& items, const std
         seg = std::max(64, std::min(seg, 512));
     }
     seg = std::max(32, seg & ~31);
-    // Bands of seg rows from the top; the rest of the strip (or, when seg divides it, its last
-    // band) in smaller bands, 2^k x 32 rows largest first, the last one reaching the bottom.  The
-    // units are handed out largest first, so the small bands fill the last wave: the SMs finish
-    // closer together than with equal bands.
+    // the explicit layout of the strip height where one is given, else the default bands
     auto bands_of = [&](int H) {
+        std::vector<int> hs = strip_default_bands(H, seg);
+        if (layouts)
+            for (const auto& e : *layouts)
+                if (e.first == H) hs = e.second;
         std::vector<std::pair<int, int>> bl;
-        int n = H / seg, rem = H - n * seg;
-        if (rem == 0 && n >= 2) { n--; rem = seg; }
-        for (int b = 0; b < n; b++) bl.push_back({b * seg, (b + 1) * seg});
-        int y = n * seg;
-        while (rem > 0) {
-            int piece = rem;
-            if (rem >= 64) {
-                int p2 = 32;
-                while (p2 * 2 <= rem) p2 *= 2;
-                if (rem - p2 >= 32) piece = p2;
-            }
-            bl.push_back({y, y + piece});
-            y += piece;
-            rem -= piece;
-        }
+        int y = 0;
+        for (int h : hs) { bl.push_back({y, y + h}); y += h; }
         return bl;
     };
     struct Cand { int h, band, sx, ord; StripUnit u; };
@@ -297,6 +314,90 @@ static std::vector<StripUnit> strip_units(const std::vector<X>& items, const std
     });
     for (const auto& x : c) v.push_back(x.u);
     return v;
+}
+
+// Band layouts for the strip SOR of one step, chosen on a model of the kernel: a unit of R rows
+// takes about R + 20 pipeline steps (the fill and drain of the 2 nit stages two rows apart, and the
+// prefetch, at nit = 5), and the persistent CTAs take the units largest first as they free up.  A
+// layout's cost is the time at which the last CTA finishes, averaged over the step with all its
+// items active and with only the first 3/4, 1/2 and 1/4 of them (pairs that converge early leave
+// the schedule).  Each strip height of the step in turn gets the layout of at most 3 cuts (at rows
+// that are multiples of 32) that minimises the cost with the other heights' layouts held; a height
+// with too many cut choices for the model's budget keeps the default layout of seg rows.  The
+// layout changes speed only: every band layout gives the same flow bit for bit.
+template <class X>
+static BandMap strip_balanced_bands(const std::vector<X>& items, const std::vector<int>& which, int seg, int sms)
+{
+    constexpr int kOver = 20;
+    BandMap lay;
+    if (which.empty()) return lay;
+    auto find = [&](int H) -> std::vector<int>& {
+        for (auto& e : lay)
+            if (e.first == H) return e.second;
+        lay.push_back({H, strip_default_bands(H, seg)});
+        return lay.back().second;
+    };
+    for (int i : which) find(items[i].H);
+    long units_all = 0;
+    for (int i : which) units_all += (long)((items[i].W + kStripW - 1) / kStripW) * (long)find(items[i].H).size();
+    std::vector<long> heap;
+    std::vector<int> costs;
+    auto cost = [&]() {
+        double acc = 0;
+        const int n = (int)which.size();
+        const double fr[4] = {1.0, 0.75, 0.5, 0.25};
+        for (double f : fr) {
+            const int na = std::max(1, (int)std::lround(f * n));
+            costs.clear();
+            for (int a = 0; a < na; a++) {
+                const int i = which[a];
+                const int nsx = (items[i].W + kStripW - 1) / kStripW;
+                for (int h : find(items[i].H))
+                    for (int q = 0; q < nsx; q++) costs.push_back(h + kOver);
+            }
+            std::sort(costs.begin(), costs.end(), std::greater<int>());
+            const int g = std::min(sms, (int)costs.size());
+            heap.assign(g, 0);
+            long mk = 0;
+            for (int c : costs) {  // list scheduling: the next unit to the CTA that frees up first
+                std::pop_heap(heap.begin(), heap.end(), std::greater<long>());
+                heap.back() += c;
+                mk = std::max(mk, heap.back());
+                std::push_heap(heap.begin(), heap.end(), std::greater<long>());
+            }
+            acc += (double)mk;
+        }
+        return acc;
+    };
+    for (auto& e : lay) {
+        const int H = e.first;
+        std::vector<int> pos;
+        for (int y = 32; y < H; y += 32) pos.push_back(y);
+        const long P = (long)pos.size();
+        const long n_lay = 1 + P + P * (P - 1) / 2 + P * (P - 1) * (P - 2) / 6;
+        if (n_lay * std::max(units_all, 1L) > 4000000L) continue;
+        std::vector<int> best = e.second;
+        double best_c = cost();
+        auto trial = [&](const std::vector<int>& cuts) {
+            std::vector<int> hs;
+            int y = 0;
+            for (int c : cuts) { hs.push_back(c - y); y = c; }
+            hs.push_back(H - y);
+            e.second = hs;
+            const double c = cost();
+            if (c < best_c - 1e-9) { best_c = c; best = hs; }
+        };
+        trial({});
+        for (long a = 0; a < P; a++) {
+            trial({pos[a]});
+            for (long b = a + 1; b < P; b++) {
+                trial({pos[a], pos[b]});
+                for (long d = b + 1; d < P; d++) trial({pos[a], pos[b], pos[d]});
+            }
+        }
+        e.second = best;
+    }
+    return lay;
 }
 
 // Whether an item's level runs on the whole-level SOR: the level's 15 planes fit one CTA's shared
@@ -824,10 +925,19 @@ static Plan<T, S> make_plan(const std::vector<PairSpec>& pairs, const HostParams
         }
         HostParams hs = hp;
         if (ch) hs.strip_seg = ch->seg;
-        const std::vector<StripUnit> units = strip_units(items, strip_items, hs, P.sms);
-        if (ch)
+        BandMap bal;
+        if (!ch && hp.strip_balanced && !strip_items.empty())
+            bal = strip_balanced_bands(items, strip_items, hp.strip_seg > 0 ? hp.strip_seg : 128, P.sms > 0 ? P.sms : 148);
+        const std::vector<StripUnit> units = strip_units(items, strip_items, hs, P.sms, ch ? &ch->bands : &bal);
+        if (ch) {
             P.tune_desc += skey + (ch->strip ? "s" + std::to_string(ch->seg) : "t") + std::to_string(ch->K) +
-                           std::to_string(ch->ilp) + ";";
+                           std::to_string(ch->ilp);
+            for (const auto& e : ch->bands) {
+                P.tune_desc += "b" + std::to_string(e.first);
+                for (int h : e.second) P.tune_desc += "." + std::to_string(h);
+            }
+            P.tune_desc += ";";
+        }
         typename Plan<T, S>::StepDesc d;
         d.level_px = 0;
         for (const auto& x : items) d.level_px += (long)x.W * x.H;

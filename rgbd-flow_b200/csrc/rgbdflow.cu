@@ -182,6 +182,8 @@ HostParams host_params(const rgbdflow_params& p)
     h.strip_seg = e ? std::atoi(e) : 0;
     e = std::getenv("RGBDFLOW_STRIP_MIN_PX");
     h.strip_min_px = e ? std::atol(e) : 0;
+    e = std::getenv("RGBDFLOW_STRIP_BALANCED");
+    h.strip_balanced = e ? std::atoi(e) : 0;
     e = std::getenv("RGBDFLOW_SOR_LEVEL");
     h.sor_level = e ? std::atoi(e) : 1;
     e = std::getenv("RGBDFLOW_LEVEL_CLUSTER");
@@ -231,8 +233,8 @@ std::string plan_key(const std::vector<PairSpec>& ps, const HostParams& hp, int 
                   hp.n_sor, hp.max_dist, hp.fill_holes, hp.fixed, hp.omega, hp.step, hp.eps_d, hp.eps_z, hp.eps_s,
                   hp.sor_tol, hp.outer_tol, hp.occ_margin, hp.occ_penalty, hp.max_grad, hp.period, hp.K * 100 + hp.sor_ilp * 10 + hp.sor_nbuf, hp.fill_rounds);
     k += buf;
-    std::snprintf(buf, sizeof buf, " strip %d %d %d %d %ld level %d %d %d", hp.sor_strip, hp.strip_min_w, hp.strip_min_h,
-                  hp.strip_seg, hp.strip_min_px, hp.sor_level, hp.level_cluster, hp.level_reg);
+    std::snprintf(buf, sizeof buf, " strip %d %d %d %d %ld %d level %d %d %d", hp.sor_strip, hp.strip_min_w, hp.strip_min_h,
+                  hp.strip_seg, hp.strip_min_px, hp.strip_balanced, hp.sor_level, hp.level_cluster, hp.level_reg);
     return k + buf;
 }
 
@@ -392,14 +394,16 @@ GraphEntry& graph_for(rgbdflow_ctx* c, const Plan<T, S>& P, const std::vector<Pa
 // ------------------------------------------------------------------------------------------
 // SOR autotuner.  The first time a level step with given item sizes is planned, every candidate
 // SOR configuration of that step (tile kernel with K = 2..6 sweeps per launch and either lane
-// mapping; strip kernel with K = 5 and band heights 96 and 128 where the items allow strips) runs a
-// few launches on the context's stream over the step's real descriptors, timed with CUDA events,
-// and the fastest per SOR iteration is kept.  Every configuration computes the same flow bit for
-// bit, so the choice changes speed only.  Convergence checks are off during timing and every pair
-// is treated as active, so the work timed is the full schedule's; the planes the timing launches
-// overwrite (the increment ping-pong, control blocks, tickets) are reset by the next solve.  The
-// table is kept per device for the life of the process.  RGBDFLOW_AUTOTUNE=0 turns it off (the
-// measured defaults of choose_sor_config / use_strip are used).
+// mapping; strip kernel with K = 5, bands of 64, 96 and 128 rows and the layout of the balancing
+// model strip_balanced_bands, where the items allow strips) runs a few launches on the context's
+// stream over the step's real descriptors, timed with CUDA events, and the fastest per SOR
+// iteration is kept.  Every configuration computes the same flow bit for bit, so the choice
+// changes speed only.  Convergence checks are off during timing; each candidate is timed with
+// every pair active and again with every other pair's SOR stopped (the pairs that converge early
+// in a real solve), and the mean counts.  The planes the timing launches overwrite (the increment
+// ping-pong, control blocks, tickets) are reset by the next solve.  The table is kept per device
+// for the life of the process.  RGBDFLOW_AUTOTUNE=0 turns it off (the measured defaults of
+// choose_sor_config / use_strip are used).
 
 struct TuneState {
     std::mutex mu;
@@ -433,18 +437,27 @@ std::vector<SorChoice> sor_candidates(const Plan<T, S>& P, int sidx)
             ch.strip = 0; ch.K = K; ch.ilp = ilp;
             v.push_back(ch);
         }
-    bool any_strip = false;
     const LevelItem<T, S>* it = (const LevelItem<T, S>*)(P.desc.data() + P.steps[sidx].items_off);
-    for (int i = 0; i < P.steps[sidx].n_items; i++) any_strip = any_strip || strip_ok<T>(P.hp, it[i].W, it[i].H);
-    if (any_strip && sizeof(T) == 4)
-        // bands of 96 and 128 rows: larger bands time faster with every pair active but balance the
-        // SMs worse once pairs stop early (measured on 16 x 640x480: 128 rows 14.8 ms of level-0 SOR
-        // a solve, 192 rows 15.2, 64 rows 15.7)
-        for (int seg : {96, 128}) {
+    std::vector<LevelItem<T, S>> items(it, it + P.steps[sidx].n_items);
+    std::vector<int> which;
+    for (int i = 0; i < (int)items.size(); i++)
+        if (strip_ok<T>(P.hp, items[i].W, items[i].H)) which.push_back(i);
+    if (!which.empty() && sizeof(T) == 4) {
+        // bands of 64, 96 and 128 rows (larger bands time faster with every pair active but balance
+        // the SMs worse once pairs stop early: measured on 16 x 640x480, 128 rows 14.8 ms of level-0
+        // SOR a solve, 192 rows 15.2, 64 rows 15.7), and the layout of the balancing model
+        for (int seg : {64, 96, 128}) {
             SorChoice ch;
             ch.strip = 1; ch.K = kStripMaxNit; ch.ilp = 2; ch.seg = seg;
             v.push_back(ch);
         }
+        SorChoice ch;
+        ch.strip = 1; ch.K = kStripMaxNit; ch.ilp = 2; ch.seg = 128;
+        ch.bands = strip_balanced_bands(items, which, 128, P.sms > 0 ? P.sms : 148);
+        bool differs = false;
+        for (const auto& e : ch.bands) differs = differs || e.second != strip_default_bands(e.first, 128);
+        if (differs) v.push_back(ch);
+    }
     return v;
 }
 
@@ -487,23 +500,35 @@ void tune_sor(rgbdflow_ctx* c, const std::vector<PairSpec>& pairs, const HostPar
             char* db = c->arena + Pc.desc_off;
             const LevelItem<T, S>* items = (const LevelItem<T, S>*)(db + d.items_off);
             int* ticket = (int*)(c->arena + Pc.ctr_off) + sidx;
-            RF_CUDA(cudaMemsetAsync(c->arena + Pc.ctl_off, 0, Pc.ctr_off + sizeof(int) * 16 - Pc.ctl_off, c->stream));
-            const int reps = 3;
-            for (int r = 0; r <= reps; r++) {
-                if (r == 1) RF_CUDA(cudaEventRecord(ea, c->stream));
-                SorLaunch L{};
-                L.it0 = 0; L.nit = Pc.sor_cfg[sidx].K; L.xin = r & 1; L.final_keep = 1; L.seq = r;
-                if (d.n_sor)
-                    launch_sor<T, S>(Pc.sor_cfg[sidx], items, (const Tile*)(db + d.sor_tiles_off), d.n_sor, Pc.sms, k, L, c->stream);
-                if (d.n_units)
-                    launch_sor_strip<T, S>(items, (const StripUnit*)(db + d.strip_units_off), d.n_units, d.strip_grid, ticket,
-                                           k, L, c->stream);
+            // two activity patterns, each timed: every pair active, and (with two or more pairs)
+            // every other pair's SOR stopped, so that it only carries its increment through, as a
+            // converged pair does; the mean of the two is the candidate's time
+            const int reps = 3, pats = Pc.n > 1 ? 2 : 1;
+            double ms_sum = 0;
+            for (int pat = 0; pat < pats; pat++) {
+                RF_CUDA(cudaMemsetAsync(c->arena + Pc.ctl_off, 0, Pc.ctr_off + sizeof(int) * 16 - Pc.ctl_off, c->stream));
+                if (pat == 1)
+                    for (int p = 1; p < Pc.n; p += 2)
+                        RF_CUDA(cudaMemsetAsync(c->arena + Pc.ctl_off + sizeof(PairCtl) * p + offsetof(PairCtl, sor_stop), 1, 1,
+                                                c->stream));
+                for (int r = 0; r <= reps; r++) {
+                    if (r == 1) RF_CUDA(cudaEventRecord(ea, c->stream));
+                    SorLaunch L{};
+                    L.it0 = 0; L.nit = Pc.sor_cfg[sidx].K; L.xin = r & 1; L.final_keep = 1; L.seq = r;
+                    if (d.n_sor)
+                        launch_sor<T, S>(Pc.sor_cfg[sidx], items, (const Tile*)(db + d.sor_tiles_off), d.n_sor, Pc.sms, k, L,
+                                         c->stream);
+                    if (d.n_units)
+                        launch_sor_strip<T, S>(items, (const StripUnit*)(db + d.strip_units_off), d.n_units, d.strip_grid,
+                                               ticket, k, L, c->stream);
+                }
+                RF_CUDA(cudaEventRecord(eb, c->stream));
+                RF_CUDA(cudaEventSynchronize(eb));
+                float ms = 0;
+                RF_CUDA(cudaEventElapsedTime(&ms, ea, eb));
+                ms_sum += ms;
             }
-            RF_CUDA(cudaEventRecord(eb, c->stream));
-            RF_CUDA(cudaEventSynchronize(eb));
-            float ms = 0;
-            RF_CUDA(cudaEventElapsedTime(&ms, ea, eb));
-            const double us = 1e3 * ms / (reps * Pc.sor_cfg[sidx].K);
+            const double us = 1e3 * ms_sum / (pats * reps * Pc.sor_cfg[sidx].K);
             if (us < best_us) { best_us = us; best = cand; best.K = Pc.sor_cfg[sidx].K; }
         }
         best.us_per_it = best_us;
@@ -1361,8 +1386,15 @@ int rgbdflow_autotune_describe(int device, char* buf, size_t len)
         std::lock_guard<std::mutex> lk(ts.mu);
         for (const auto& kv : ts.table[device].m) {
             const SorChoice& ch = kv.second;
-            char b[160];
-            if (ch.strip) std::snprintf(b, sizeof b, "%s strip band %d K %d %.2f us/it; ", kv.first.c_str(), ch.seg, ch.K, ch.us_per_it);
+            char b[512];
+            std::string lay;
+            for (const auto& e : ch.bands) {
+                lay += " H" + std::to_string(e.first) + ":";
+                for (size_t q = 0; q < e.second.size(); q++) lay += (q ? "/" : "") + std::to_string(e.second[q]);
+            }
+            if (ch.strip && !ch.bands.empty())
+                std::snprintf(b, sizeof b, "%s strip bands%s K %d %.2f us/it; ", kv.first.c_str(), lay.c_str(), ch.K, ch.us_per_it);
+            else if (ch.strip) std::snprintf(b, sizeof b, "%s strip band %d K %d %.2f us/it; ", kv.first.c_str(), ch.seg, ch.K, ch.us_per_it);
             else std::snprintf(b, sizeof b, "%s tile K %d ilp %d %.2f us/it; ", kv.first.c_str(), ch.K, ch.ilp, ch.us_per_it);
             out += b;
         }

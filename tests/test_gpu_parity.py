@@ -219,11 +219,12 @@ def test_batch_submit_equals_batch(ctx):
         other.close()
 
 
-@pytest.mark.parametrize("name,seg", [("320x240", 0), ("640x480", 0), ("640x480", 64), ("160x120", 32)])
+@pytest.mark.parametrize("name,seg", [("320x240", 0), ("640x480", 0), ("640x480", 64), ("160x120", 32),
+                                      ("640x480", "balanced")])
 def test_strip_and_tile_sor_agree_bitwise(ctx, monkeypatch, name, seg):
     """The strip SOR (rows streamed through a shared-memory ring) and the tile SOR (32 x 32 tiles
     with a halo) give the same flow and the same executed schedule, bit for bit, whatever the
-    band height of the strip units."""
+    band height of the strip units (or the balancing model's band layout)."""
     p = syn.make_config_pair(name, seed=12)
     prm = rf.benchmark_params(p["W"])
     cam = cam_of(p)
@@ -231,7 +232,8 @@ def test_strip_and_tile_sor_agree_bitwise(ctx, monkeypatch, name, seg):
     monkeypatch.setenv("RGBDFLOW_STRIP_MIN_W", "64")
     monkeypatch.setenv("RGBDFLOW_STRIP_MIN_H", "32")
     monkeypatch.setenv("RGBDFLOW_STRIP_MIN_PX", "1")
-    monkeypatch.setenv("RGBDFLOW_STRIP_SEG", str(seg))
+    monkeypatch.setenv("RGBDFLOW_STRIP_SEG", "0" if seg == "balanced" else str(seg))
+    monkeypatch.setenv("RGBDFLOW_STRIP_BALANCED", "1" if seg == "balanced" else "0")
     monkeypatch.setenv("RGBDFLOW_SOR_STRIP", "0")
     tile, st_tile = ctx.scene_flow_two_frames(*args)
     monkeypatch.setenv("RGBDFLOW_SOR_STRIP", "1")
@@ -242,8 +244,8 @@ def test_strip_and_tile_sor_agree_bitwise(ctx, monkeypatch, name, seg):
 
 def test_every_tunable_sor_choice_agrees_bitwise(ctx, monkeypatch):
     """Every configuration the SOR autotuner chooses from (tile kernel with 2..6 sweeps per launch and
-    either lane mapping; strip kernel with band heights 64..256) gives the autotuned solve's flow and
-    executed schedule bit for bit, on a ragged batch."""
+    either lane mapping; strip kernel with band heights 32..256 or the balancing model's band
+    layout) gives the autotuned solve's flow and executed schedule bit for bit, on a ragged batch."""
     specs = [("320x240", 31), ("160x120", 32), ("320x240", 33)]
     pairs = [syn.make_config_pair(n, seed=sd) for n, sd in specs]
     host = [dict(W=p["W"], H=p["H"], cam=cam_of(p), bgr1=p["bgr1"], depth1=p["depth1"], bgr2=p["bgr2"],
@@ -254,7 +256,7 @@ def test_every_tunable_sor_choice_agrees_bitwise(ctx, monkeypatch):
     print("autotuned:", rf.autotune_describe(0))
     assert rf.autotune_describe(0)
     configs = [dict(K=K, ilp=ilp) for K in (2, 3, 4, 5, 6) for ilp in (1, 2)]
-    configs += [dict(K=5, seg=seg) for seg in (32, 64, 128, 192, 256)]
+    configs += [dict(K=5, seg=seg) for seg in (32, 64, 128, 192, 256)] + [dict(K=5, seg=0, balanced=1)]
     for c in configs:
         q = rf.benchmark_params(320)
         q.min_width = -16
@@ -265,6 +267,7 @@ def test_every_tunable_sor_choice_agrees_bitwise(ctx, monkeypatch):
             monkeypatch.setenv("RGBDFLOW_STRIP_MIN_H", "64")
             monkeypatch.setenv("RGBDFLOW_STRIP_MIN_PX", "1")
             monkeypatch.setenv("RGBDFLOW_STRIP_SEG", str(c["seg"]))
+            monkeypatch.setenv("RGBDFLOW_STRIP_BALANCED", str(c.get("balanced", 0)))
         else:
             monkeypatch.setenv("RGBDFLOW_SOR_STRIP", "0")
             monkeypatch.setenv("RGBDFLOW_SOR_ILP", str(c["ilp"]))
@@ -272,7 +275,7 @@ def test_every_tunable_sor_choice_agrees_bitwise(ctx, monkeypatch):
         for a, b in zip(ref, out):
             np.testing.assert_array_equal(a, b, err_msg=str(c))
         for k in ("RGBDFLOW_SOR_STRIP", "RGBDFLOW_STRIP_MIN_W", "RGBDFLOW_STRIP_MIN_H", "RGBDFLOW_STRIP_MIN_PX",
-                  "RGBDFLOW_STRIP_SEG", "RGBDFLOW_SOR_ILP"):
+                  "RGBDFLOW_STRIP_SEG", "RGBDFLOW_STRIP_BALANCED", "RGBDFLOW_SOR_ILP"):
             monkeypatch.delenv(k, raising=False)
 
 
