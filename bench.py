@@ -614,7 +614,7 @@ def main():
         served = run_served(ctx, rf, serving, streams, prm, args, warm=False)
         served_warm = run_served(ctx, rf, serving, streams, prm, args, warm=True)
         if not args.no_sweep:
-            pts = [(n, 30) for n in (8, 12, 16, 20, 24, 32, 40, 48)]
+            pts = [(n, 30) for n in (8, 10, 12, 14, 16, 18, 20, 24, 32, 40, 48)]
             served["capacity"] = run_served_sweep(ctx, rf, serving, streams, prm, False, pts)
             served_warm["capacity"] = run_served_sweep(ctx, rf, serving, streams, prm, True, pts)
 

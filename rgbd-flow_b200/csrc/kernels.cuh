@@ -471,26 +471,29 @@ struct PyrJob {
     int tiles_x_src, tile0_src;  // tiles over the computed source columns (horizontal pass)
     int tiles_x_dst, tile0_dst;  // tiles over the destination
     int hstep, hoff;             // horizontal pass computes columns hoff + hstep * k only: the ones the
-                                 // resample reads with a nonzero weight (every other one at ratio 0.5)
+                                 // resample reads with a nonzero weight (columns 2k + 1 at rate 1/2,
+                                 // 4k + 3 at rate 1/4)
+    int tW;                      // row length of tmp: the computed columns side by side
 };
 
 constexpr int kMaxTaps = 33;
 
+// One thread per (plane, computed column, row): plane blockIdx.y.
 template <class T>
 __global__ void k_hfilter(const PyrJob<T>* jobs, const Tile* tiles, const T* __restrict__ gall)
 {
     const Tile t = tiles[blockIdx.x];
     const PyrJob<T>& jb = jobs[t.item];
-    const int j = jb.hoff + jb.hstep * (t.tx * LTW + (threadIdx.x % LTW)), i = t.ty * LTH + (threadIdx.x / LTW);
-    if (i >= jb.sH || j >= jb.sW) return;
+    const int p = blockIdx.y;
+    const int kc = t.tx * LTW + (threadIdx.x % LTW), i = t.ty * LTH + (threadIdx.x / LTW);
+    const int j = jb.hoff + jb.hstep * kc;
+    if (p >= jb.nplanes || i >= jb.sH || kc >= jb.tW || j >= jb.sW) return;
     const T* g = gall + t.item * kMaxTaps;
     const int fs = jb.fs, W = jb.sW;
-    for (int p = 0; p < jb.nplanes; p++) {
-        const T* s = jb.src[p] + (size_t)i * W;
-        T acc = 0;
-        for (int l = -fs; l <= fs; l++) acc += s[clampi(j + l, 0, W - 1)] * g[l + fs];
-        jb.tmp[p][(size_t)i * W + j] = acc;
-    }
+    const T* s = jb.src[p] + (size_t)i * W;
+    T acc = 0;
+    for (int l = -fs; l <= fs; l++) acc += s[clampi(j + l, 0, W - 1)] * g[l + fs];
+    jb.tmp[p][(size_t)i * jb.tW + kc] = acc;
 }
 
 template <class T>
@@ -501,6 +504,10 @@ __device__ __forceinline__ T vtap(const T* tp, int W, int H, int x, int y, const
     return acc;
 }
 
+// One thread per (pair of planes, destination pixel): planes 2 blockIdx.y and 2 blockIdx.y + 1.
+// tmp holds the computed columns side by side: source column u is tmp column (u - hoff) / hstep
+// (corners off the progression have weight 0 and are skipped).
+constexpr int kVresizePlanes = 2;
 template <class T>
 __global__ void k_vresize(const PyrJob<T>* jobs, const Tile* tiles, const T* __restrict__ gall)
 {
@@ -519,14 +526,16 @@ __global__ void k_vresize(const PyrJob<T>* jobs, const Tile* tiles, const T* __r
     const T s00 = (T)(fabs(1 - dx) * fabs(1 - dy)), s01 = (T)(fabs(1 - dx) * fabs(dy));
     const T s10 = (T)(fabs(dx) * fabs(1 - dy)), s11 = (T)(fabs(dx) * fabs(dy));
     // a corner of weight 0 adds exactly 0 (every pyramid value is finite): it is skipped, which at
-    // ratio 0.5 (samples on source pixels) leaves one corner of four
-    for (int p = 0; p < jb.nplanes; p++) {
+    // rates 1/2 and 1/4 (samples on source pixels) leaves one corner of four
+    const int c0 = (u0 - jb.hoff) / jb.hstep, c1 = (u1 - jb.hoff) / jb.hstep;
+    const int p1 = min(jb.nplanes, (int)(blockIdx.y + 1) * kVresizePlanes);
+    for (int p = blockIdx.y * kVresizePlanes; p < p1; p++) {
         const T* tp = jb.tmp[p];
         T acc = 0;
-        acc += vtap(tp, jb.sW, jb.sH, u0, v0, g, jb.fs) * s00;
-        if (s01 != (T)0) acc += vtap(tp, jb.sW, jb.sH, u0, v1, g, jb.fs) * s01;
-        if (s10 != (T)0) acc += vtap(tp, jb.sW, jb.sH, u1, v0, g, jb.fs) * s10;
-        if (s11 != (T)0) acc += vtap(tp, jb.sW, jb.sH, u1, v1, g, jb.fs) * s11;
+        acc += vtap(tp, jb.tW, jb.sH, c0, v0, g, jb.fs) * s00;
+        if (s01 != (T)0) acc += vtap(tp, jb.tW, jb.sH, c0, v1, g, jb.fs) * s01;
+        if (s10 != (T)0) acc += vtap(tp, jb.tW, jb.sH, c1, v0, g, jb.fs) * s10;
+        if (s11 != (T)0) acc += vtap(tp, jb.tW, jb.sH, c1, v1, g, jb.fs) * s11;
         jb.dst[p][(size_t)i * jb.dW + j] = acc;
     }
 }

@@ -729,18 +729,24 @@ static Plan<T, S> make_plan(const std::vector<PairSpec>& pairs, const HostParams
                 jb.dst[c] = (T*)mem[p][i].pyr[c];
             }
             const int jid = (int)jobs.size();
-            // columns the resample reads with a nonzero weight: at rate 0.5 the samples fall on
-            // source pixels x = 2j + 1 (weight 1 on column 2j + 1, 0 on its neighbour)
-            bool odd_only = true;
-            for (int jj = 0; jj < jb.dW && odd_only; jj++) {
-                const double x = (double)(jj + 1) / jb.rate - 1;
-                const int xx = (int)x;
-                odd_only = (x == (double)xx) && (xx & 1) && xx < jb.sW;
+            // columns the resample reads with a nonzero weight: when every sample falls on a source
+            // column of one progression hoff + hstep j (rate 1/2: x = 2j + 1; rate 1/4: x = 4j + 3;
+            // weight 1 there, 0 on the next column), only those columns are filtered, stored side by
+            // side (tmp rows of dW values); otherwise every column (tmp rows of sW values)
+            jb.hstep = 1;
+            jb.hoff = 0;
+            {
+                const double x0 = 1.0 / jb.rate - 1, x1 = 2.0 / jb.rate - 1;
+                const int a = (int)x0, d = (int)x1 - (int)x0;
+                bool prog = jb.dW >= 2 && x0 == (double)a && x1 == (double)(int)x1 && d >= 2 && a >= 0;
+                for (int jj = 0; jj < jb.dW && prog; jj++) {
+                    const double x = (double)(jj + 1) / jb.rate - 1;
+                    prog = x == (double)(a + d * jj) && a + d * jj < jb.sW;
+                }
+                if (prog) { jb.hstep = d; jb.hoff = a; }
             }
-            jb.hstep = odd_only ? 2 : 1;
-            jb.hoff = odd_only ? 1 : 0;
-            const int hcols = odd_only ? jb.sW / 2 : jb.sW;
-            jb.tiles_x_src = (hcols + LTW - 1) / LTW;
+            jb.tW = jb.hstep > 1 ? jb.dW : jb.sW;
+            jb.tiles_x_src = (jb.tW + LTW - 1) / LTW;
             jb.tile0_src = (int)st.size();
             for (int y = 0; y < (jb.sH + LTH - 1) / LTH; y++)
                 for (int x = 0; x < jb.tiles_x_src; x++) st.push_back(Tile{jid, x, y, 0});
@@ -1508,10 +1514,10 @@ static int enqueue_solve(const Plan<T, S>& P, char* base, cudaStream_t st, Prof*
             const PyrJob<T>* jobs = (const PyrJob<T>*)(db + lv.jobs_off);
             const T* g = (const T*)(db + lv.g_off);
             RF_PROF_B(pf, KC_PYR_H, st);
-            k_hfilter<T><<<lv.n_src, LTW * LTH, 0, st>>>(jobs, (const Tile*)(db + lv.src_tiles_off), g);
+            k_hfilter<T><<<dim3(lv.n_src, 10), LTW * LTH, 0, st>>>(jobs, (const Tile*)(db + lv.src_tiles_off), g);
             RF_PROF_E(pf, st);
             RF_PROF_B(pf, KC_PYR_V, st);
-            k_vresize<T><<<lv.n_dst, LTW * LTH, 0, st>>>(jobs, (const Tile*)(db + lv.dst_tiles_off), g);
+            k_vresize<T><<<dim3(lv.n_dst, (10 + kVresizePlanes - 1) / kVresizePlanes), LTW * LTH, 0, st>>>(jobs, (const Tile*)(db + lv.dst_tiles_off), g);
             RF_PROF_E(pf, st);
             launches += 2;
         }
