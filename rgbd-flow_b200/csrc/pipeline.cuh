@@ -320,11 +320,13 @@ static std::vector<StripUnit> strip_units(const std::vector<X>& items, const std
 // takes about R + 20 pipeline steps (the fill and drain of the 2 nit stages two rows apart, and the
 // prefetch, at nit = 5), and the persistent CTAs take the units largest first as they free up.  A
 // layout's cost is the time at which the last CTA finishes, averaged over the step with all its
-// items active and with only the first 3/4, 1/2 and 1/4 of them (pairs that converge early leave
-// the schedule).  Each strip height of the step in turn gets the layout of at most 3 cuts (at rows
-// that are multiples of 32) that minimises the cost with the other heights' layouts held; a height
-// with too many cut choices for the model's budget keeps the default layout of seg rows.  The
-// layout changes speed only: every band layout gives the same flow bit for bit.
+// items active and with 3 in 4, 2 in 4 and 1 in 4 of them (items whose index mod 4 is below 3, 2,
+// 1: pairs that converge early leave the schedule, and every size of a mixed step keeps its share).
+// Each strip height of the step in turn gets the layout of at most 3 cuts (at rows that are
+// multiples of 32, bands of at most 256 rows: a tall band left for last keeps one SM busy alone)
+// that minimises the cost with the other heights' layouts held; a height with too many cut choices
+// for the model's budget keeps the default layout of seg rows.  The layout changes speed only:
+// every band layout gives the same flow bit for bit.
 template <class X>
 static BandMap strip_balanced_bands(const std::vector<X>& items, const std::vector<int>& which, int seg, int sms)
 {
@@ -345,15 +347,14 @@ static BandMap strip_balanced_bands(const std::vector<X>& items, const std::vect
     auto cost = [&]() {
         double acc = 0;
         const int n = (int)which.size();
-        const double fr[4] = {1.0, 0.75, 0.5, 0.25};
-        for (double f : fr) {
-            const int na = std::max(1, (int)std::lround(f * n));
+        for (int q = 4; q >= 1; q--) {  // the items a with a mod 4 < q (item 0 always)
             costs.clear();
-            for (int a = 0; a < na; a++) {
+            for (int a = 0; a < n; a++) {
+                if (a % 4 >= q) continue;
                 const int i = which[a];
                 const int nsx = (items[i].W + kStripW - 1) / kStripW;
                 for (int h : find(items[i].H))
-                    for (int q = 0; q < nsx; q++) costs.push_back(h + kOver);
+                    for (int sx = 0; sx < nsx; sx++) costs.push_back(h + kOver);
             }
             std::sort(costs.begin(), costs.end(), std::greater<int>());
             const int g = std::min(sms, (int)costs.size());
@@ -383,6 +384,8 @@ static BandMap strip_balanced_bands(const std::vector<X>& items, const std::vect
             int y = 0;
             for (int c : cuts) { hs.push_back(c - y); y = c; }
             hs.push_back(H - y);
+            for (int h : hs)
+                if (h > 256) return;
             e.second = hs;
             const double c = cost();
             if (c < best_c - 1e-9) { best_c = c; best = hs; }

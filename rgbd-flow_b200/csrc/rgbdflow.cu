@@ -529,7 +529,10 @@ void tune_sor(rgbdflow_ctx* c, const std::vector<PairSpec>& pairs, const HostPar
                 ms_sum += ms;
             }
             const double us = 1e3 * ms_sum / (pats * reps * Pc.sor_cfg[sidx].K);
-            if (us < best_us) { best_us = us; best = cand; best.K = Pc.sor_cfg[sidx].K; }
+            // the balancing model's layout (timed last) has to win by 3 %: on 16 x 640x480 it timed
+            // even with 128-row bands (67.4 against 67.3 us an iteration) but ran the level-0 SOR of
+            // a real solve 3 % slower (14.9 against 14.5 ms)
+            if (us < best_us * (cand.bands.empty() ? 1.0 : 0.97)) { best_us = us; best = cand; best.K = Pc.sor_cfg[sidx].K; }
         }
         best.us_per_it = best_us;
         tt.m[P0.step_keys[sidx]] = best;
