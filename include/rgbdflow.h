@@ -394,8 +394,8 @@ int rgbdflow_server_counters_read(rgbdflow_server* srv, int reset, rgbdflow_serv
  *   result; est_flow NULL or a warm start).  stream: a cudaStream_t as void*, NULL = the legacy
  *   default stream.  Runs on the current device and returns after enqueue.
  *   Set-up: the first call on each device looks up the workspace address and sets kernel
- *   attributes; make that first call before any stream capture.  The set-up is kept for the life
- *   of the process: after cudaDeviceReset on a device this call is not supported there.
+ *   attributes.  The set-up is kept for the life of the process: after cudaDeviceReset on a
+ *   device this call is not supported there.
  *   Host memory: the call's descriptors travel to the workspace as kernel parameters, so nothing
  *   it enqueues reads host memory after it returns.
  *   Footprint: the 40 MiB array belongs to the library's device code, so every process that loads
