@@ -210,7 +210,7 @@ def run_served(ctx, rf, serving, streams, prm, args, warm):
             "host": {"server": counters, "loop_ms": r["host"]}}
 
 
-def run_served_sweep(ctx, rf, serving, base, prm, warm, points, seconds=2.0, max_batch=16):
+def run_served_sweep(ctx, rf, serving, base, prm, warm, points, seconds=2.0, max_batch=8):
     """Served capacity: camera streams (the 8 base streams replayed as more independent streams) at
     30 fps with Poisson arrivals, more streams per point.  Per point: the arrival rate actually
     drawn (pairs / time of the last arrival), the achieved pairs/s (pairs / wall time, which adds

@@ -324,8 +324,9 @@ int rgbdflow_debug_wait_timeout(rgbdflow_ctx* ctx, double* seconds);
  * Served form (no reference counterpart): continuous batching over camera streams.  A frame
  * submitted on a stream forms a pair with that stream's previous frame; the stream's previous
  * frame pyramid and previous flow stay resident on the device for warm starts.  Requests are
- * admitted while the HBM budget and the slot count allow; newly admitted pairs join the next
- * device step while earlier ones are still in flight.
+ * admitted while the HBM budget and the slot count allow (four solve slots, each a batch of up to
+ * max_batch pairs on its own stream); newly admitted pairs join the next device step while
+ * earlier ones are still in flight.
  * ------------------------------------------------------------------------------------------- */
 typedef struct rgbdflow_server rgbdflow_server;
 

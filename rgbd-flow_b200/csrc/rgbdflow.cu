@@ -1527,6 +1527,10 @@ int rgbdflow_server_create(rgbdflow_ctx* c, const rgbdflow_server_config* cfg, r
     s->ctx = c;
     s->cfg = *cfg;
     RF_CUDA(cudaStreamCreateWithFlags(&s->upload, cudaStreamNonBlocking));
+    {
+        const char* e = std::getenv("RGBDFLOW_SERVER_SLOTS");
+        s->slots.resize(e ? std::max(1, std::min(4, std::atoi(e))) : 4);
+    }
     for (auto& sl : s->slots) {
         const int rc = rgbdflow_ctx_create(c->device, 0, &sl.ctx);
         if (rc != RGBDFLOW_OK) throw ArgError(rc, "slot context creation failed");
@@ -1563,6 +1567,14 @@ int rgbdflow_server_destroy(rgbdflow_server* s)
 namespace {
 void server_prepare(rgbdflow_server* s);
 void server_prepare_slot(rgbdflow_server* s, ServerSlot& sl);
+// Device arena bytes the other solve slots hold (for the HBM budget of one slot's growth).
+size_t other_slot_arenas(const rgbdflow_server* s, const ServerSlot& sl)
+{
+    size_t n = 0;
+    for (const auto& o : s->slots)
+        if (&o != &sl) n += o.ctx->arena_cap;
+    return n;
+}
 constexpr int kServerFramesPerStream = 8;  // frame buffer sets stocked per stream (a backlog of ~6 pairs)
 constexpr int kServerPrecapture = 40;      // batch graphs captured ahead per slot (within kGraphCache)
 }
@@ -1724,7 +1736,7 @@ void server_presize_slot(rgbdflow_server* s, ServerSlot& sl)
     const int nb = std::max(1, std::min(s->cfg.max_batch, s->cfg.max_streams));
     std::vector<PairSpec> ps(nb, q);
     const SlotNeed need = slot_need(ps, host_params(s->cfg.params), s->cfg.params.storage);
-    const size_t other = (&sl == &s->slots[0]) ? s->slots[1].ctx->arena_cap : s->slots[0].ctx->arena_cap;
+    const size_t other = other_slot_arenas(s, sl);
     if (sl.ctx->arena_cap < need.arena &&
         !(s->cfg.hbm_budget_bytes && s->resident_bytes + other + need.arena > s->cfg.hbm_budget_bytes))
         ensure_arena(sl.ctx, need.arena);
@@ -1808,7 +1820,7 @@ void server_launch(rgbdflow_server* s, ServerSlot& sl)
     const HostParams hp = host_params(s->cfg.params);
     std::vector<ServerReq> take;
     std::vector<PairSpec> specs;
-    const size_t other = s->slots[0].ctx == sl.ctx ? s->slots[1].ctx->arena_cap : s->slots[0].ctx->arena_cap;
+    const size_t other = other_slot_arenas(s, sl);
     for (auto it = s->queue.begin(); it != s->queue.end() && (int)take.size() < s->cfg.max_batch;) {
         StreamState& ss = s->streams[it->stream];
         bool dup = false;
