@@ -2,6 +2,8 @@
 the same whether its stream is served alone or in a mix with other streams (bit-identical: the
 kernels treat pairs independently and reduce in a fixed per-tile order), and cold-started served
 pairs equal the plain solve."""
+import os
+
 import numpy as np
 import pytest
 
@@ -75,8 +77,12 @@ def test_admission_respects_the_hbm_budget(ctx):
     srv.close()
 
 
+# solve slots of a server (the library's default, or the RGBDFLOW_SERVER_SLOTS override)
+SLOTS = int(os.environ.get("RGBDFLOW_SERVER_SLOTS", "4"))
+
+
 def test_graphs_are_captured_when_a_stream_registers(ctx):
-    """Registering a stream captures, on both solve slots, the graph of every batch the registered
+    """Registering a stream captures, on every solve slot, the graph of every batch the registered
     streams can form; the pairs that follow launch cached graphs only: the counters read no
     capture, no reallocation and no frame allocation, and one device step per pair."""
     seq = _streams()[0]
@@ -84,7 +90,7 @@ def test_graphs_are_captured_when_a_stream_registers(ctx):
     fr = seq["frames"][0]
     srv.submit(0, 0, _cam(seq), fr["bgr"], fr["depth"])  # the stream's first frame registers it
     reg = srv.counters(reset=True)
-    assert reg["graphs_built"] == 2 and reg["launches"] == 0 and reg["max_graph_build_ms"] > 0
+    assert reg["graphs_built"] == SLOTS and reg["launches"] == 0 and reg["max_graph_build_ms"] > 0
     for k in range(1, 6):
         fr = seq["frames"][k % len(seq["frames"])]
         srv.submit(0, k, _cam(seq), fr["bgr"], fr["depth"])
@@ -123,7 +129,7 @@ def test_a_stream_registered_while_a_slot_runs_is_captured_before_its_next_launc
     start = srv.counters(reset=True)
     # per slot: the 160x120 batch when stream 0 registers; then its memory grows for the 320x240
     # stream (which drops its graphs) and it captures the three batches of the two streams
-    assert start["graphs_built"] == 2 * (1 + 3) and start["arena_grows"] == 2 * 2
+    assert start["graphs_built"] == SLOTS * (1 + 3) and start["arena_grows"] == SLOTS * 2
     for k in range(1, 5):
         submit(1, k)
         if k + 1 < 5:
