@@ -8,10 +8,10 @@ convergence breaks and outer early termination on.  Every pair is an independent
 run N replicas (weak scaling, no collective on the data path).
 
   value      pairs/s with inputs resident in HBM (device-pointer API), two batches in flight on two
-             contexts / streams, timed with CUDA events across both streams, max over ranks; the
+             contexts / streams, timed with CUDA events across the streams, max over ranks; the
              batch's working set (~2.5 GB) is far above L2.  `one_batch_in_flight` beside it.
   e2e        pairs/s through the host-buffer C ABI (rgbdflow_scene_flow_batch_submit on two
-             alternating contexts), every step's host->device inputs and device->host flows inside
+             contexts in rotation), every step's host->device inputs and device->host flows inside
              the timed region
   plain      one pair per call (the drop-in solve): pairs/s and p50 / p99 latency
   roofline   the dominant kernel (red-black SOR) from a profiled pass of the same workload
@@ -241,6 +241,9 @@ def run_served_sweep(ctx, rf, serving, base, prm, warm, points, seconds=2.0, max
 
 
 MIX = [(160, 120, 24), (320, 240, 24), (640, 480, 16)]
+# batches in flight (contexts / streams) of the value and e2e measurements: with three the
+# device-resident value read 758 against 743 pairs/s, but e2e fell from 682 to 652
+LANES = 2
 
 
 def run_mixed(ctx, rf, torch, stream, prm, args, rank):
@@ -462,41 +465,45 @@ def main():
     stream = torch.cuda.Stream()  # the stream every solve below is enqueued on and timed on
     torch.cuda.set_stream(stream)
 
-    # ---- value: device-resident batched solves, two batches in flight.  Steps alternate between
-    # two contexts on two streams; before a context takes its next step the host waits for its
-    # previous one, so the two batches run about half a solve apart and one batch's SM-saturating
-    # 640x480-level SOR overlaps the other's latency-bound coarse levels.  Timed on the device:
-    # from an event both streams wait on to the later of the two streams' last events.
-    ctx_b = rf.Context(local)
-    stream_b = torch.cuda.Stream()
-    dev_b = [dict(d, out=torch.empty_like(d["out"])) for d in dev]
-    lanes = [(ctx, stream, dev), (ctx_b, stream_b, dev_b)]
+    # ---- value: device-resident batched solves, LANES batches in flight.  Steps rotate over LANES
+    # contexts on as many streams; before a context takes its next step the host waits for its
+    # previous one, so the batches run a fraction of a solve apart and one batch's SM-saturating
+    # 640x480-level SOR overlaps the others' latency-bound coarse levels (1, 2, 3 and 4 in
+    # flight: 645, 743, 752 and 761 pairs/s).  Timed on the device: from an event every stream
+    # waits on to the latest of the streams' last events.
+    lanes = [(ctx, stream, dev)]
+    for _ in range(LANES - 1):
+        lanes.append((rf.Context(local), torch.cuda.Stream(), [dict(d, out=torch.empty_like(d["out"])) for d in dev]))
 
-    def timed_steps(n_steps, two):
-        done = [None, None]
+    def timed_steps(n_steps, multi):
+        nl = LANES if multi else 1
+        done = [None] * nl
         starts, ends = [], []
         e0 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        stream_b.wait_event(e0)
+        for _, st, _ in lanes[1:]:
+            st.wait_event(e0)
         for s in range(n_steps):
-            c, st, dv = lanes[s % 2] if two else lanes[0]
-            if two and done[s % 2] is not None:
-                done[s % 2].synchronize()
+            c, st, dv = lanes[s % nl]
+            if done[s % nl] is not None:
+                done[s % nl].synchronize()
             a = torch.cuda.Event(enable_timing=True)
             a.record(st)
             c.scene_flow_batch_device(dv, prm, stream=st)
             b = torch.cuda.Event(enable_timing=True)
             b.record(st)
-            done[s % 2] = b
+            done[s % nl] = b
             starts.append(a)
             ends.append(b)
-        stream.wait_event(done[1] if two and n_steps > 1 else done[0])
+        for d in done:
+            if d is not None:
+                stream.wait_event(d)
         e1 = torch.cuda.Event(enable_timing=True)
         e1.record(stream)
         torch.cuda.synchronize()
         return e0.elapsed_time(e1), [a.elapsed_time(b) for a, b in zip(starts, ends)]
 
-    timed_steps(max(args.warmup, 2), True)
+    timed_steps(max(args.warmup, LANES), True)
     launches_per_step = ctx.last_launch_count()
     clocks = ClockSampler(local)
     barrier()
@@ -509,7 +516,8 @@ def main():
     # the same steps one batch at a time (a step's latency without overlap), for comparison
     ms1_raw, step1_ms = timed_steps(args.steps, False)
     value_one = replicas.aggregate_rate(B * args.steps, world, max_over_ranks(ms1_raw) / 1e3)
-    ctx_b.close()
+    for c, _, _ in lanes[1:]:
+        c.close()
 
     # ---- batched result check: pair 0 of the batch equals the same pair solved alone
     solo = torch.empty((H, W, 3), dtype=torch.float32, device="cuda")
@@ -545,19 +553,21 @@ def main():
     pouts = [torch.empty((H, W, 3), dtype=torch.float32).pin_memory().numpy() for _ in host]
     e2e = None
     if not args.no_e2e:
-        # two contexts alternate: step s uploads its inputs, solves and downloads its flows on one
-        # context (rgbdflow_scene_flow_batch_submit returns once enqueued) while the other context's
-        # step runs; a context is synchronised (its flows read) before it takes the step after next
-        ctxs = [ctx, rf.Context(local)]
-        outs2 = [pouts, [torch.empty((H, W, 3), dtype=torch.float32).pin_memory().numpy() for _ in host]]
+        # LANES contexts rotate, as for the device-resident value: step s uploads its inputs,
+        # solves and downloads its flows on one context (rgbdflow_scene_flow_batch_submit returns
+        # once enqueued) while the other contexts' steps run; a context is synchronised (its flows
+        # read) before it takes its next step
+        ctxs = [ctx] + [rf.Context(local) for _ in range(LANES - 1)]
+        outs2 = [pouts] + [[torch.empty((H, W, 3), dtype=torch.float32).pin_memory().numpy() for _ in host]
+                           for _ in range(LANES - 1)]
 
         def e2e_step(s):
-            c = ctxs[s % 2]
-            if s >= 2:
+            c = ctxs[s % LANES]
+            if s >= LANES:
                 c.synchronize()
-            c.scene_flow_batch_submit(hp, prm, outs2[s % 2])
+            c.scene_flow_batch_submit(hp, prm, outs2[s % LANES])
 
-        for s in range(max(args.warmup, 2)):
+        for s in range(max(args.warmup, LANES)):
             e2e_step(s)
         for c in ctxs:
             c.synchronize()
@@ -568,12 +578,13 @@ def main():
         for c in ctxs:
             c.synchronize()
         e2e_s = max_over_ranks(time.perf_counter() - t)
-        ctxs[1].close()
+        for c in ctxs[1:]:
+            c.close()
         e2e = {"value": B * args.steps * world / e2e_s, "unit": "pairs/s",
                "h2d_bytes_per_step": B * W * H * (3 + 3 + 4 + 4), "d2h_bytes_per_step": B * W * H * 12,
-               "how": "rgbdflow_scene_flow_batch_submit on two alternating contexts: each step uploads its inputs "
-                      "from page-locked host memory, solves, and downloads its flows; one step's transfers overlap "
-                      "the other context's solve"}
+               "how": "rgbdflow_scene_flow_batch_submit on %d contexts in rotation: each step uploads its "
+                      "inputs from page-locked host memory, solves, and downloads its flows; one step's transfers "
+                      "overlap the other contexts' solves" % LANES}
 
     # ---- roofline of the dominant kernel from a profiled pass of the same workload: the SOR of
     # the 640x480 level (the strip kernel), algorithmic bytes / live CUDA-event time
@@ -657,8 +668,8 @@ def main():
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded RGB-D patch scenes, 640x480)",
                 "config": {"workload": "batched solve of %d independent 640x480 pairs per step per GPU "
-                                       "(5 levels x 10 outer x 30 SOR, reference convergence breaks); two "
-                                       "batches in flight on two contexts / streams" % B,
+                                       "(5 levels x 10 outer x 30 SOR, reference convergence breaks); %d "
+                                       "batches in flight on as many contexts / streams" % (B, LANES),
                            "global_batch": B * world, "parallelism": "replicas x%d" % world,
                            "l2": "inputs larger than L2 (working set %.2f GB per GPU)" % (ctx.device_bytes() / 1e9)},
                 "p50_ms": float(np.percentile(step_ms, 50)), "p99_ms": float(np.percentile(step_ms, 99)),
