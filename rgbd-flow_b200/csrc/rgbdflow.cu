@@ -399,8 +399,8 @@ GraphEntry& graph_for(rgbdflow_ctx* c, const Plan<T, S>& P, const std::vector<Pa
 // stream over the step's real descriptors, timed with CUDA events, and the fastest per SOR
 // iteration is kept.  Every configuration computes the same flow bit for bit, so the choice
 // changes speed only.  Convergence checks are off during timing; each candidate is timed with
-// every pair active and again with every other pair's SOR stopped (the pairs that converge early
-// in a real solve), and the mean counts.  The planes the timing launches overwrite (the increment
+// every pair active, with every other pair's SOR stopped and with every other pair done with the
+// level (the pairs that converge early in a real solve), and the mean counts.  The planes the timing launches overwrite (the increment
 // ping-pong, control blocks, tickets) are reset by the next solve.  The table is kept per device
 // for the life of the process.  RGBDFLOW_AUTOTUNE=0 turns it off (the measured defaults of
 // choose_sor_config / use_strip are used).
@@ -500,17 +500,19 @@ void tune_sor(rgbdflow_ctx* c, const std::vector<PairSpec>& pairs, const HostPar
             char* db = c->arena + Pc.desc_off;
             const LevelItem<T, S>* items = (const LevelItem<T, S>*)(db + d.items_off);
             int* ticket = (int*)(c->arena + Pc.ctr_off) + sidx;
-            // two activity patterns, each timed: every pair active, and (with two or more pairs)
-            // every other pair's SOR stopped, so that it only carries its increment through, as a
-            // converged pair does; the mean of the two is the candidate's time
-            const int reps = 3, pats = Pc.n > 1 ? 2 : 1;
+            // three activity patterns, each timed: every pair active; (with two or more pairs) every
+            // other pair's SOR stopped, so that it only carries its increment through, as a converged
+            // pair does; and every other pair done with the level (its work units are skipped, as
+            // after an early outer termination).  The mean of the patterns is the candidate's time.
+            const int reps = 3, pats = Pc.n > 1 ? 3 : 1;
             double ms_sum = 0;
             for (int pat = 0; pat < pats; pat++) {
                 RF_CUDA(cudaMemsetAsync(c->arena + Pc.ctl_off, 0, Pc.ctr_off + sizeof(int) * 16 - Pc.ctl_off, c->stream));
-                if (pat == 1)
+                if (pat > 0)
                     for (int p = 1; p < Pc.n; p += 2)
-                        RF_CUDA(cudaMemsetAsync(c->arena + Pc.ctl_off + sizeof(PairCtl) * p + offsetof(PairCtl, sor_stop), 1, 1,
-                                                c->stream));
+                        RF_CUDA(cudaMemsetAsync(c->arena + Pc.ctl_off + sizeof(PairCtl) * p +
+                                                    (pat == 1 ? offsetof(PairCtl, sor_stop) : offsetof(PairCtl, level_done)),
+                                                1, 1, c->stream));
                 for (int r = 0; r <= reps; r++) {
                     if (r == 1) RF_CUDA(cudaEventRecord(ea, c->stream));
                     SorLaunch L{};
@@ -529,10 +531,9 @@ void tune_sor(rgbdflow_ctx* c, const std::vector<PairSpec>& pairs, const HostPar
                 ms_sum += ms;
             }
             const double us = 1e3 * ms_sum / (pats * reps * Pc.sor_cfg[sidx].K);
-            // the balancing model's layout (timed last) has to win by 3 %: on 16 x 640x480 it timed
-            // even with 128-row bands (67.4 against 67.3 us an iteration) but ran the level-0 SOR of
-            // a real solve 3 % slower (14.9 against 14.5 ms)
-            if (us < best_us * (cand.bands.empty() ? 1.0 : 0.97)) { best_us = us; best = cand; best.K = Pc.sor_cfg[sidx].K; }
+            // the balancing model's layout (timed last) has to win by 1 %: on 16 x 640x480 it timed
+            // even with 128-row bands but ran the level-0 SOR of a real solve 3 % slower
+            if (us < best_us * (cand.bands.empty() ? 1.0 : 0.99)) { best_us = us; best = cand; best.K = Pc.sor_cfg[sidx].K; }
         }
         best.us_per_it = best_us;
         tt.m[P0.step_keys[sidx]] = best;
