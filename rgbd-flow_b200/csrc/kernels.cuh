@@ -1641,9 +1641,19 @@ k_sor_level(const LevelItem<T, S>* items, const int* which, SolveConst<T> k, Sor
 // so a pixel update reads its 4 neighbours' unknowns (12 values) and writes 3, instead of reading
 // 31 values.
 constexpr int kLevelRegMax = 768;  // positions (= threads) of a level on this kernel
+// Row pitch (positions) of a half-row in the shared planes of the register whole-level kernels: at
+// least hwp + 2 (a zero position each side) and with 2 RP = hwp (mod 32), so that the 32 threads of
+// a warp, which span consecutive rows of one colour when hwp < 32, touch 32 consecutive banks (with
+// hwp + 2, 20-position rows put 8 threads of a warp on the banks of 8 others).
+__host__ __device__ constexpr int level_reg_rp(int hwp)
+{
+    int rp = hwp + 2;
+    while (((2 * rp - hwp) & 31) != 0) rp++;
+    return rp;
+}
 template <class T> __host__ __device__ constexpr size_t level_reg_smem_bytes(int H, int hwp)
 {
-    return sizeof(T) * ((size_t)3 * (H + 2) * 2 * (hwp + 2) + 64);
+    return sizeof(T) * ((size_t)3 * (H + 2) * 2 * level_reg_rp(hwp) + 64);
 }
 
 template <class T, class S>
@@ -1657,7 +1667,7 @@ k_sor_level_reg(const LevelItem<T, S>* items, const int* which, SolveConst<T> k,
     const LevelItem<T, S>& it = items[which[blockIdx.x]];
     PairCtl* ctl = it.ctl;
     if (ctl->level_done) return;
-    const int W = it.W, H = it.H, hw = it.hwp, RP = hw + 2;
+    const int W = it.W, H = it.H, hw = it.hwp, RP = level_reg_rp(hw);
     const int PLS = (H + 2) * 2 * RP;
     const int tid = threadIdx.x, NT = blockDim.x;
     // the unknowns: valid pixels from global, zero everywhere else (padding, positions past a
@@ -1981,7 +1991,7 @@ k_sor_level_cluster(const LevelItem<T, S>* items, const int* which, SolveConst<T
 template <int KP> __host__ __device__ constexpr int clus_reg_threads_max() { return KP == 1 ? 768 : 640; }
 template <class T> __host__ __device__ constexpr size_t level_cluster_reg_smem_bytes(int B, int hwp)
 {
-    return sizeof(T) * ((size_t)3 * (B + 2) * 2 * (hwp + 2) + 64);
+    return sizeof(T) * ((size_t)3 * (B + 2) * 2 * level_reg_rp(hwp) + 64);
 }
 
 template <class T, class S, int KP>
@@ -1999,7 +2009,7 @@ k_sor_level_cluster_reg(const LevelItem<T, S>* items, const int* which, SolveCon
     const LevelItem<T, S>& it = items[which[blockIdx.x / C]];
     PairCtl* ctl = it.ctl;
     if (ctl->level_done) return;  // the same for every CTA of the cluster: none reaches a barrier
-    const int W = it.W, H = it.H, hw = it.hwp, RP = hw + 2;
+    const int W = it.W, H = it.H, hw = it.hwp, RP = level_reg_rp(hw);
     const int B = (H + C - 1) / C, r0 = rank * B, nr = max(0, min(H, r0 + B) - r0);
     const int PLS = (B + 2) * 2 * RP;
     const int tid = threadIdx.x, NT = blockDim.x;

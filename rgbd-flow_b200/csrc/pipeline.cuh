@@ -434,7 +434,8 @@ static inline std::pair<int, int> level_cluster_reg_shape(const HostParams& hp, 
     for (int KP = 1; KP <= 2; KP++)
         for (int C = std::max(2, std::min(hp.level_cluster, 8)); C <= 8; C++) {
             const int B = (H + C - 1) / C;
-            if (B * (C - 1) < H && B * hwp <= KP * (KP == 1 ? clus_reg_threads_max<1>() : clus_reg_threads_max<2>()))
+            if (B * (C - 1) < H && B * hwp <= KP * (KP == 1 ? clus_reg_threads_max<1>() : clus_reg_threads_max<2>()) &&
+                level_cluster_reg_smem_bytes<float>(B, hwp) <= 64 * 1024)
                 return {C, KP};
         }
     return {0, 0};
@@ -917,7 +918,7 @@ static Plan<T, S> make_plan(const std::vector<PairSpec>& pairs, const HostParams
                 level_smem = std::max(level_smem, level_smem_bytes<T>(x.H, x.hwp));
                 level_reg_smem = std::max(level_reg_smem, level_reg_smem_bytes<T>(x.H, x.hwp));
                 level_thr = std::max(level_thr, level_threads(x.H, x.hwp));
-                level_reg = level_reg && x.H * x.hwp <= kLevelRegMax;
+                level_reg = level_reg && x.H * x.hwp <= kLevelRegMax && level_reg_smem_bytes<T>(x.H, x.hwp) <= 64 * 1024;
                 continue;
             }
             if (level_cluster_size<T>(hp, x.H, x.hwp) > 0 && !(ch && ch->strip)) {
