@@ -400,10 +400,10 @@ GraphEntry& graph_for(rgbdflow_ctx* c, const Plan<T, S>& P, const std::vector<Pa
 // iteration is kept.  Every configuration computes the same flow bit for bit, so the choice
 // changes speed only.  Convergence checks are off during timing; each candidate is timed with
 // every pair active, with every other pair's SOR stopped and with every other pair done with the
-// level (the pairs that converge early in a real solve), and the mean counts.  The planes the timing launches overwrite (the increment
-// ping-pong, control blocks, tickets) are reset by the next solve.  The table is kept per device
-// for the life of the process.  RGBDFLOW_AUTOTUNE=0 turns it off (the measured defaults of
-// choose_sor_config / use_strip are used).
+// level (the pairs that converge early in a real solve), and the mean counts.  The planes the
+// timing launches overwrite (the increment ping-pong, control blocks, tickets) are reset by the
+// next solve.  The table is kept per device for the life of the process.  RGBDFLOW_AUTOTUNE=0
+// turns it off (the measured defaults of choose_sor_config / use_strip are used).
 
 struct TuneState {
     std::mutex mu;
