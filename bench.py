@@ -9,7 +9,7 @@ run N replicas (weak scaling, no collective on the data path).
 
   value      pairs/s with inputs resident in HBM (device-pointer API), two batches in flight on two
              contexts / streams, timed with CUDA events across the streams, max over ranks; the
-             batch's working set (~2.5 GB) is far above L2.  `one_batch_in_flight` beside it.
+             batch's solve memory (~1.5 GB) is far above L2.  `one_batch_in_flight` beside it.
   e2e        pairs/s through the host-buffer C ABI (rgbdflow_scene_flow_batch_submit on two
              contexts in rotation), every step's host->device inputs and device->host flows inside
              the timed region
@@ -371,11 +371,22 @@ def cpu_baselines(host, dev, torch):
     return cpu
 
 
+def bench_config(rf, B, world):
+    """The workload both arms report: B independent 640x480 pairs per step per GPU, with the batch's
+    solve memory (host-computed from the plan) as the working set against the 126 MB L2."""
+    ws = rf.batch_device_bytes([(W, H)] * B, rf.benchmark_params(W))
+    return {"workload": "batched solve of %d independent 640x480 pairs per step per GPU (5 levels x 10 outer "
+                        "x 30 SOR, reference convergence breaks)" % B,
+            "global_batch": B * world, "parallelism": "replicas x%d" % world,
+            "l2": "inputs larger than L2 (working set %.2f GB per GPU)" % (ws / 1e9)}
+
+
 def run_reference(args, rank, world):
     """The reference arm: the reference has no CPU implementation of its 3-D solver, so its
     restatement (oracle/, the same arithmetic and schedule) runs on the host cores."""
     if rank != 0:
         return
+    import rgbdflow as rf
     # the pairs of the device arm's batch (rank 0's seeds), as many as the timed steps visit
     pairs = make_pairs(max(1, min(args.batch, args.steps)), 0)
     if args.warmup:
@@ -385,13 +396,10 @@ def run_reference(args, rank, world):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(ts)),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64 (mixed, as the reference)",
             "data": "synthetic (seeded RGB-D patch scenes, 640x480)",
-            "config": {"workload": "batched solve of %d independent 640x480 pairs per step (5 levels x 10 outer "
-                                   "x 30 SOR, reference convergence breaks) by the CPU restatement of the "
-                                   "reference on the host cores; each timed step a bounded sample of it: one pair "
-                                   "of the batch" % args.batch,
-                       "global_batch": args.batch, "threads": threads},
+            "config": bench_config(rf, args.batch, world),
             "cpu_baseline": {"value": v, "unit": "pairs/s", "cores": threads, "kind": "port",
-                             "sample": "%d pairs of the 640x480 batch, one per step" % args.steps},
+                             "sample": "%d pairs of the device arm's 640x480 batch, one per step (the CPU "
+                                       "restatement of the reference on the host cores)" % args.steps},
             "e2e": {"value": v, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -671,11 +679,8 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded RGB-D patch scenes, 640x480)",
-                "config": {"workload": "batched solve of %d independent 640x480 pairs per step per GPU "
-                                       "(5 levels x 10 outer x 30 SOR, reference convergence breaks); %d "
-                                       "batches in flight on as many contexts / streams" % (B, LANES),
-                           "global_batch": B * world, "parallelism": "replicas x%d" % world,
-                           "l2": "inputs larger than L2 (working set %.2f GB per GPU)" % (ctx.device_bytes() / 1e9)},
+                "config": bench_config(rf, B, world),
+                "batches_in_flight": LANES,
                 "p50_ms": float(np.percentile(step_ms, 50)), "p99_ms": float(np.percentile(step_ms, 99)),
                 "one_batch_in_flight": {"value": value_one, "p50_ms": float(np.percentile(step1_ms, 50)),
                                         "p99_ms": float(np.percentile(step1_ms, 99))},
