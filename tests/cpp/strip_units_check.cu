@@ -1,9 +1,10 @@
-// Host-side check of the strip SOR's work units (rgbd-flow_b200/csrc/pipeline.cuh): for ragged
+// Host-side checks of rgbd-flow_b200/csrc/pipeline.cuh.  The strip SOR's work units: for ragged
 // steps, every band layout (the fixed band heights and the balancing model's layouts) must cut each
 // item's strips into bands that start on a multiple of 32 rows, cover the strip's rows exactly
-// once, and the work list must hold every (item, strip, band) once, largest band first.  Runs on
-// the host only (no kernel is launched).  Prints one line per case and exits non-zero on the first
-// violation.
+// once, and the work list must hold every (item, strip, band) once, largest band first.  The
+// register whole-level SOR kernels' padded half-row pitch and cluster shapes (check_level_pitch).
+// Runs on the host only (no kernel is launched).  Prints one line per case and exits non-zero on
+// the first violation.
 #include <cstdio>
 #include <cstdlib>
 #include <set>
@@ -64,8 +65,35 @@ static int check(const char* name, const std::vector<Item>& items, int seg, bool
     return 0;
 }
 
+// The padded half-row pitch of the register whole-level kernels: at least a zero position each
+// side, 2 x pitch = row length (mod 32), at most 15 positions of padding; and the cluster shapes the
+// plan picks for them fit the 64 KB of shared memory those kernels are given.
+static int check_level_pitch()
+{
+    for (int hwp = 4; hwp <= 512; hwp += 4) {
+        const int rp = level_reg_rp(hwp);
+        if (rp < hwp + 2 || ((2 * rp - hwp) & 31) != 0 || rp - (hwp + 2) > 15) return fail("pitch", hwp, rp);
+    }
+    HostParams hp{};
+    hp.sor_level = 1;
+    hp.level_reg = 1;
+    int shapes = 0;
+    for (int H = 8; H <= 400; H += 7)
+        for (int hwp = 4; hwp <= 200; hwp += 4) {
+            const auto sh = level_cluster_reg_shape(hp, H, hwp);
+            if (sh.first == 0) continue;
+            shapes++;
+            const int B = (H + sh.first - 1) / sh.first;
+            if (level_cluster_reg_smem_bytes<float>(B, hwp) > 64 * 1024) return fail("cluster smem", H, hwp);
+            if (B * (sh.first - 1) >= H) return fail("empty cluster rank", H, sh.first);
+        }
+    std::printf("ok level pitch: %d cluster shapes\n", shapes);
+    return 0;
+}
+
 int main()
 {
+    if (check_level_pitch()) return 1;
     std::vector<std::pair<const char*, std::vector<Item>>> cases;
     cases.push_back({"16 x 640x480", std::vector<Item>(16, Item{640, 480})});
     cases.push_back({"16 x 320x240", std::vector<Item>(16, Item{320, 240})});

@@ -6,7 +6,9 @@ tests/cpp/strip_units_check.cu includes pipeline.cuh, builds the units of severa
 autotuner or an override can ask for and for the balancing model's layouts, and checks that each
 band starts on a multiple of 32 rows, that model layouts keep bands of at most 256 rows and cover
 their strip, and that the units cover every (item, strip, row) exactly once, largest band first.
-No kernel is launched, so the program runs without a GPU.
+It also checks the padded half-row pitch of the register whole-level SOR kernels (level_reg_rp)
+and that every cluster shape the plan picks for them fits their 64 KB of shared memory.  No
+kernel is launched, so the program runs without a GPU.
 """
 import os
 import shutil
@@ -25,6 +27,8 @@ def test_strip_units_cover_every_row_once(tmp_path):
     r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
     lines = r.stdout.splitlines()
+    assert lines[0].startswith("ok level pitch")
+    lines = lines[1:]
     assert len(lines) == 5 * 7 * 2 and all(x.startswith("ok ") for x in lines)
     # the model's layouts of the benchmark's 320x240 step and of the mix's finest step
     assert "ok 16 x 320x240 seg 128 balanced: 320 units H240:32/64/64/80" in lines
